@@ -1,0 +1,222 @@
+"""Seeded synthetic pair sets with the shapes of the benchmark workloads.
+
+No public dataset is used: every workload below is generated from a numpy
+PCG64 stream seeded with ``20261203 + k`` for workload k, with uniform i.i.d.
+ACGT bases and mutations drawn per position.  All mutation work is vectorised
+over the whole batch (flat arrays + pair ids), so a million pairs take seconds.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+from .capi import (Batch, Params, LOCAL, GLOBAL, SEMI_GLOBAL, KSW, TARGET, WITH_START,
+                   WITHOUT_START, WITH_TB, TRUE, FALSE, REVERSE_COMPLEMENT, N_CODE)
+
+ACGT = np.frombuffer(b"ACGT", dtype=np.uint8)
+SEED_BASE = 20261203
+
+
+def _random_bases(rng, n):
+    return ACGT[rng.integers(0, 4, size=n)]
+
+
+def _stage_flat(flat: np.ndarray, lens: np.ndarray):
+    """Lay out sequences (concatenated in ``flat``) at 8-byte aligned offsets,
+    N-padded, as GASAL2's host batch does."""
+    lens = lens.astype(np.int64)
+    padded = (lens + 7) // 8 * 8
+    offs = np.zeros(len(lens), dtype=np.int64)
+    offs[1:] = np.cumsum(padded)[:-1]
+    total = int(padded.sum())
+    if total >= 2 ** 32:
+        raise ValueError("batch exceeds 4 GiB of bases; split it")
+    buf = np.full(total, N_CODE, dtype=np.uint8)
+    starts = np.zeros(len(lens), dtype=np.int64)
+    starts[1:] = np.cumsum(lens)[:-1]
+    pos = np.repeat(offs - starts, lens) + np.arange(int(lens.sum()), dtype=np.int64)
+    buf[pos] = flat
+    return buf, offs.astype(np.uint32), lens.astype(np.uint32)
+
+
+def mutate(rng, flat: np.ndarray, lens: np.ndarray, sub_rate, ins_rate, del_rate, max_indel):
+    """Apply substitutions, insertions and deletions (lengths U{1..max_indel})
+    independently per position.  Rates may be scalars or per-pair arrays."""
+    n = len(lens)
+    lens = lens.astype(np.int64)
+    pid = np.repeat(np.arange(n), lens)
+    def per_pos(r):
+        r = np.asarray(r, dtype=np.float64)
+        return r[pid] if r.ndim else np.full(len(flat), float(r))
+    u = rng.random(len(flat))
+    ps, pi, pd = per_pos(sub_rate), per_pos(ins_rate), per_pos(del_rate)
+    is_sub = u < ps
+    is_ins = (u >= ps) & (u < ps + pi)
+    is_del = (u >= ps + pi) & (u < ps + pi + pd)
+    out = flat.copy()
+    # substitution: a different base
+    codes = np.searchsorted(ACGT, out[is_sub])
+    codes = np.where(codes < 4, codes, 0)
+    out[is_sub] = ACGT[(codes + rng.integers(1, 4, size=int(is_sub.sum()))) % 4]
+    # deletion: this position and up to max_indel-1 following ones in the same pair
+    keep = np.ones(len(flat), dtype=bool)
+    dl = rng.integers(1, max_indel + 1, size=len(flat))
+    starts_idx = np.nonzero(is_del)[0]
+    for k in range(max_indel):
+        idx = starts_idx[dl[starts_idx] > k] + k
+        idx = idx[idx < len(flat)]
+        same = pid[idx] == pid[idx - k] if k else np.ones(len(idx), dtype=bool)
+        keep[idx[same]] = False
+    # insertion: after this position, il random bases
+    il = np.where(is_ins, rng.integers(1, max_indel + 1, size=len(flat)), 0)
+    rep = 1 + il
+    rep = np.where(keep, rep, il)  # a deleted base still carries its insertion
+    newflat = np.repeat(out, rep)
+    first = np.cumsum(rep) - rep
+    is_orig = np.zeros(len(newflat), dtype=bool)
+    is_orig[first[keep]] = True
+    ins_mask = ~is_orig
+    newflat[ins_mask] = _random_bases(rng, int(ins_mask.sum()))
+    newpid = np.repeat(pid, rep)
+    newlens = np.bincount(newpid, minlength=n).astype(np.int64)
+    return newflat, newlens
+
+
+def _per_pair_slices(flat, lens):
+    starts = np.zeros(len(lens), dtype=np.int64)
+    starts[1:] = np.cumsum(lens)[:-1]
+    return starts
+
+
+def _clip(rng, flat, lens, lo, hi):
+    """Truncate sequences longer than hi and extend ones shorter than lo with
+    random bases, keeping everything vectorised."""
+    lens = lens.astype(np.int64)
+    target = np.clip(lens, lo, hi)
+    starts = _per_pair_slices(flat, lens)
+    keep_n = np.minimum(lens, target)
+    pid = np.repeat(np.arange(len(lens)), keep_n)
+    within = np.arange(int(keep_n.sum())) - np.repeat(np.cumsum(keep_n) - keep_n, keep_n)
+    kept = flat[np.repeat(starts, keep_n) + within]
+    extra = target - keep_n
+    if extra.sum() == 0:
+        return kept, target
+    rep = keep_n + extra
+    out = np.empty(int(rep.sum()), dtype=np.uint8)
+    ostart = np.cumsum(rep) - rep
+    okeep = np.repeat(ostart, keep_n) + within
+    out[okeep] = kept
+    mask = np.ones(len(out), dtype=bool)
+    mask[okeep] = False
+    out[mask] = _random_bases(rng, int(mask.sum()))
+    del pid
+    return out, target
+
+
+def _flank(rng, flat, lens, left, right):
+    """Surround each sequence with left[i] / right[i] random bases."""
+    lens = lens.astype(np.int64)
+    tot = left + lens + right
+    out = _random_bases(rng, int(tot.sum()))
+    ostart = np.cumsum(tot) - tot
+    starts = _per_pair_slices(flat, lens)
+    within = np.arange(int(lens.sum())) - np.repeat(starts, lens)
+    out[np.repeat(ostart + left, lens) + within] = flat
+    return out, tot
+
+
+def _to_batch(qflat, qlens, tflat, tlens, q_op=None, seed=None) -> Batch:
+    q, qo, ql = _stage_flat(qflat, qlens)
+    t, to, tl = _stage_flat(tflat, tlens)
+    return Batch(q, t, qo, to, ql, tl,
+                 q_op=None if q_op is None else np.ascontiguousarray(q_op, dtype=np.uint8),
+                 t_op=None if q_op is None else np.zeros(len(ql), dtype=np.uint8),
+                 seed=None if seed is None else np.ascontiguousarray(seed, dtype=np.uint32))
+
+
+def short_read_pairs(n, seed=SEED_BASE, qlo=100, qhi=150, flank_max=20, sub=0.02, indel=0.005,
+                     max_indel=3, n_rate=0.001, tlo=None, thi=None):
+    """Workload 0 shape: query U[qlo,qhi] with n_rate N; target = query with
+    0..flank_max random flanking bases each side, then substitutions and indels."""
+    rng = np.random.default_rng(seed)
+    qlens = rng.integers(qlo, qhi + 1, size=n)
+    qflat = _random_bases(rng, int(qlens.sum()))
+    if n_rate > 0:
+        m = rng.random(len(qflat)) < n_rate
+        qflat[m] = N_CODE
+    left = rng.integers(0, flank_max + 1, size=n)
+    right = rng.integers(0, flank_max + 1, size=n)
+    tflat, tlens = _flank(rng, qflat, qlens, left, right)
+    tflat, tlens = mutate(rng, tflat, tlens, sub, indel / 2, indel / 2, max_indel)
+    if tlo is not None:
+        tflat, tlens = _clip(rng, tflat, tlens, tlo, thi)
+    return qflat, qlens, tflat, tlens, rng
+
+
+def workload0(n=20000, seed=SEED_BASE + 0) -> Batch:
+    qf, ql, tf, tl, _ = short_read_pairs(n, seed)
+    return _to_batch(qf, ql, tf, tl)
+
+
+WORKLOAD1_PARAMS = [
+    Params(algo=LOCAL, start_pos=WITH_START, second_best=TRUE, reverse_complement=1),
+    Params(algo=GLOBAL, start_pos=WITH_START, reverse_complement=1),
+    Params(algo=SEMI_GLOBAL, start_pos=WITH_START, head=TARGET, tail=TARGET, reverse_complement=1),
+]
+
+
+def workload1(n=1_000_000, seed=SEED_BASE + 1):
+    """Workload 1: 150 bp queries, 150-300 bp targets (3% subs, 1% indels),
+    50% of queries flagged REVERSE_COMPLEMENT; split in thirds LOCAL (second
+    best) / GLOBAL / SEMI_GLOBAL (head=tail=TARGET), all WITH_START.
+    Returns [(Params, Batch)] for the three launches."""
+    rng0 = np.random.default_rng(seed)
+    qf, ql, tf, tl, rng = short_read_pairs(n, seed, qlo=150, qhi=150, flank_max=75, sub=0.03,
+                                           indel=0.01, n_rate=0.0, tlo=150, thi=300)
+    q_op = np.where(rng0.random(n) < 0.5, REVERSE_COMPLEMENT, 0).astype(np.uint8)
+    b = _to_batch(qf, ql, tf, tl, q_op=q_op)
+    thirds = np.array_split(np.arange(n), 3)
+    return [(p, _slice_batch(b, idx)) for p, idx in zip(WORKLOAD1_PARAMS, thirds)]
+
+
+def _slice_batch(b: Batch, idx: np.ndarray) -> Batch:
+    """Contiguous index range -> batch with rebased offsets (no copy of pairs
+    outside the range)."""
+    lo, hi = int(idx[0]), int(idx[-1]) + 1
+    def part(buf, off, ln):
+        o0 = int(off[lo])
+        end = int(off[hi - 1]) + int((int(ln[hi - 1]) + 7) // 8 * 8)
+        return np.ascontiguousarray(buf[o0:end]), (off[lo:hi] - np.uint32(o0)).astype(np.uint32)
+    q, qo = part(b.q, b.q_off, b.q_len)
+    t, to = part(b.t, b.t_off, b.t_len)
+    sl = slice(lo, hi)
+    return Batch(q, t, qo, to, np.ascontiguousarray(b.q_len[sl]), np.ascontiguousarray(b.t_len[sl]),
+                 q_op=None if b.q_op is None else np.ascontiguousarray(b.q_op[sl]),
+                 t_op=None if b.t_op is None else np.ascontiguousarray(b.t_op[sl]),
+                 seed=None if b.seed is None else np.ascontiguousarray(b.seed[sl]))
+
+
+def workload2(n=2_000_000, seed=SEED_BASE + 2) -> Batch:
+    """Workload 2: query length log-uniform 50-1000; target = query with per-pair
+    1-8% substitutions and 0.5-3% indels of length 1-10 (GLOBAL, WITH_TB)."""
+    rng = np.random.default_rng(seed)
+    ql = np.exp(rng.uniform(np.log(50), np.log(1000), size=n)).astype(np.int64)
+    qf = _random_bases(rng, int(ql.sum()))
+    sub = rng.uniform(0.01, 0.08, size=n)
+    ind = rng.uniform(0.005, 0.03, size=n)
+    tf, tl = mutate(rng, qf, ql, sub, ind / 2, ind / 2, 10)
+    tf, tl = _clip(rng, tf, tl, 1, 1 << 30)
+    return _to_batch(qf, ql, tf, tl)
+
+
+def workload3(n=4_000_000, seed=SEED_BASE + 3) -> Batch:
+    """Workload 3: ksw extension, query U[250,2000], indel rate per pair from
+    {0.5,2,5,10}% plus 1-5% substitutions, seed score h0 U[20,60]."""
+    rng = np.random.default_rng(seed)
+    ql = rng.integers(250, 2001, size=n)
+    qf = _random_bases(rng, int(ql.sum()))
+    ind = rng.choice(np.array([0.005, 0.02, 0.05, 0.10]), size=n)
+    sub = rng.uniform(0.01, 0.05, size=n)
+    tf, tl = mutate(rng, qf, ql, sub, ind / 2, ind / 2, 3)
+    tf, tl = _clip(rng, tf, tl, 1, 1 << 30)
+    h0 = rng.integers(20, 61, size=n)
+    return _to_batch(qf, ql, tf, tl, seed=h0)
