@@ -1,0 +1,335 @@
+#!/usr/bin/env python
+"""Throughput of GASAL2's batched alignment path on B200 (aligned pairs/s).
+
+Workload (default): 1,000,000 pairs in three launches -- one third each
+LOCAL (second best) / GLOBAL / SEMI_GLOBAL (head = tail = TARGET), all
+WITH_START, 150 bp queries, 150-300 bp targets (3% substitutions, 1% indels),
+half of the queries REVERSE_COMPLEMENT, scores 1/4/6/1.  Seeded synthetic data
+(numpy PCG64, seed 20261203+1); inputs (~384 MB) exceed the 126 MB L2, so no
+flush is needed between steps.
+
+One step = the three launches.  Reported:
+  value   pairs/s with the batch already in HBM: pack -> reverse/complement ->
+          DP (+ start pass) per launch, timed with CUDA events on the launch
+          stream, max over ranks
+  e2e     pairs/s through the GASAL2 storage API (gasal_aln_async +
+          gasal_is_aln_async_done on three streams): host->device copy of the
+          pinned batch, kernels, device->host copy of every result array
+  roofline  DP kernels' algorithmic integer ops / their CUDA-event time,
+          against this GPU's measured integer-add issue rate
+  cpu_baseline  the scalar C oracle with OpenMP on all host cores, on a
+          bounded sample of the same workload
+
+--impl reference times the reference GASAL2 kernels compiled for the host
+(OpenMP over pairs) on a bounded sample per step; the reference has no CPU
+aligner of its own.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+from gasal_b200 import workloads as W  # noqa: E402
+from gasal_b200.capi import LOCAL, GLOBAL, SEMI_GLOBAL, Params  # noqa: E402
+
+METRIC = "aligned pairs/s (1M-pair mixed LOCAL/GLOBAL/SEMI_GLOBAL WITH_START batch, RC on 50%)"
+UNIT = "pairs/s"
+# integer ops per cell, per algorithm (LOCAL 11, GLOBAL 9, SEMI_GLOBAL 10)
+OPS_PER_CELL = {LOCAL: 11, GLOBAL: 9, SEMI_GLOBAL: 10}
+# DRAM bytes per DP launch of the workload from the committed ncu capture
+# (profiles/dp_kernels_w1.md), scaled to a full launch; None until captured.
+DP_TRAFFIC_BYTES = None
+
+
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle sampling during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.rows = []
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except FileNotFoundError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([x.strip() for x in line.split(",")])
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in self.rows for i, v in enumerate(r[5:9]) if v.strip() == "Active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.rows)}
+
+
+def build_workload(n: int, seed: int):
+    t = time.time()
+    parts = W.workload1(n, seed=seed)
+    log(f"workload: {n} pairs generated in {time.time() - t:.1f}s")
+    return parts
+
+
+def cpu_baseline(parts, budget_s: float = 12.0) -> dict:
+    """Scalar C oracle, OpenMP on every host core, on a bounded sample."""
+    from oracle.bindings import oracle_align
+    cores = os.cpu_count() or 1
+    probe = 3000
+    t0 = time.time()
+    for p, b in parts:
+        oracle_align(p, b.subset(np.arange(min(probe, b.n))), threads=cores)
+    per_pair = (time.time() - t0) / (3 * probe)
+    m = int(max(probe, min(parts[0][1].n, budget_s / per_pair / 3)))
+    t0 = time.time()
+    for p, b in parts:
+        oracle_align(p, b.subset(np.arange(min(m, b.n))), threads=cores)
+    dt = time.time() - t0
+    return {"value": 3 * m / dt, "unit": UNIT, "cores": cores, "kind": "port",
+            "sample": f"first {m} pairs of each of the three launches ({3 * m} pairs), {dt:.1f}s"}
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    from oracle.bindings import ref_host_align
+    cores = os.cpu_count() or 1
+    parts = build_workload(args.pairs, W.SEED_BASE + 1)
+    m = args.ref_sample
+    sample = [(p, b.subset(np.arange(min(m, b.n)))) for p, b in parts]
+    for _ in range(args.warmup):
+        for p, b in sample:
+            ref_host_align(p, b, threads=cores)
+    times = []
+    for _ in range(args.steps):
+        t0 = time.time()
+        for p, b in sample:
+            ref_host_align(p, b, threads=cores)
+        times.append(time.time() - t0)
+    npairs = sum(b.n for _, b in sample)
+    v = npairs / float(np.mean(times))
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * float(np.mean(times)),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int32",
+            "data": "synthetic",
+            "config": {"workload": "w1: 1M pairs, thirds LOCAL(second best)/GLOBAL/SEMI_GLOBAL(TARGET,TARGET), "
+                                   "WITH_START, q=150, t=150-300, RC 50%", "pairs_per_step": npairs},
+            "cpu_baseline": {"value": v, "unit": UNIT, "cores": cores, "kind": "reference",
+                             "sample": f"first {m} pairs of each launch per step ({npairs} pairs); reference "
+                                       f"kernel headers compiled for the host, OpenMP over pairs"},
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--pairs", type=int, default=1_000_000)
+    ap.add_argument("--ref-sample", type=int, default=4000)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        run_reference(args)
+        return
+
+    import torch
+    import ctypes as C
+    from gasal_b200 import lib as gl
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local_rank)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120))
+
+    gl.lib()
+    gl.set_reference_reverse(True)
+    peak = gl.probe_int_peak()
+    parts = build_workload(args.pairs, W.SEED_BASE + 1 + 1000 * rank)
+    npairs = sum(b.n for _, b in parts)
+    dev = torch.device("cuda", local_rank)
+
+    # ---------------- kernel level: inputs resident in HBM -----------------
+    def t_(a, dtype=None):
+        return torch.from_numpy(np.ascontiguousarray(a).view(dtype or a.dtype)).to(dev)
+
+    dparts = []
+    for p, b in parts:
+        d = {"q_t": t_(b.q), "t_t": t_(b.t), "qo": t_(b.q_off, np.int32), "to": t_(b.t_off, np.int32),
+             "ql": t_(b.q_len, np.int32), "tl": t_(b.t_len, np.int32), "qop": t_(b.q_op), "top": t_(b.t_op)}
+        d["pq"] = torch.empty(b.q.shape[0] // 8, dtype=torch.int32, device=dev)
+        d["pt"] = torch.empty(b.t.shape[0] // 8, dtype=torch.int32, device=dev)
+        outs = {k: torch.empty(b.n, dtype=torch.int32, device=dev) for k in
+                ("score", "q_end", "t_end", "q_start", "t_start", "score2", "q_end2", "t_end2")}
+        d["outs"] = outs
+        m = {"q_bytes": b.q.shape[0], "t_bytes": b.t.shape[0], "q": d["q_t"].data_ptr(), "t": d["t_t"].data_ptr(),
+             "pq": d["pq"].data_ptr(), "pt": d["pt"].data_ptr(), "q_off": d["qo"].data_ptr(),
+             "t_off": d["to"].data_ptr(), "q_len": d["ql"].data_ptr(), "t_len": d["tl"].data_ptr(),
+             "q_op": d["qop"].data_ptr(), "t_op": d["top"].data_ptr()}
+        for k, v in outs.items():
+            m["out_" + k] = v.data_ptr()
+        if not p.second_best:
+            m["out_score2"] = m["out_q_end2"] = m["out_t_end2"] = None
+        d["map"] = m
+        dparts.append((p, b, d))
+
+    stream = torch.cuda.Stream(device=dev)
+
+    def step():
+        for p, b, d in dparts:
+            gl.align_dev(p, d["map"], b.q_len, b.t_len, stream.cuda_stream)
+
+    with torch.cuda.stream(stream):
+        for _ in range(args.warmup):
+            step()
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    gl.kernel_timing(True)
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local_rank) as clk:
+        ev0.record(stream)
+        for _ in range(args.steps):
+            step()
+        ev1.record(stream)
+        torch.cuda.synchronize()
+    kt = gl.kernel_timing_read()
+    gl.kernel_timing(False)
+    ms = ev0.elapsed_time(ev1)
+    if dist:
+        x = torch.tensor([ms], device=dev)
+        dist.all_reduce(x, op=dist.ReduceOp.MAX)
+        ms = float(x.item())
+        if dist:
+            dist.barrier()
+    ms_step = ms / args.steps
+    value = npairs * world * args.steps / (ms * 1e-3)
+    cells = sum(b.cells() for _, b in parts)
+    dp_ms, dp_n = kt["dp"]
+    alg_ops = sum(b.cells() * OPS_PER_CELL[p.algo] for p, b in parts) * args.steps
+    achieved = alg_ops / (dp_ms * 1e-3) / 1e12
+    launches = sum(n for _, n in kt.values())
+
+    # ---------------- end to end through the storage API ----------------
+    e2e = None
+    streams = []
+    for p, b in parts:
+        s = gl.Streams(1, 152, 304, b.n, p)
+        streams.append((p, b, s))
+    h2d = sum(int(b.q.shape[0] + b.t.shape[0]) + b.n * (4 * 4 + 2) for _, b, _ in streams)
+    d2h = 0
+    for p, b, s in streams:
+        nf = 5 + (3 if p.second_best else 0)
+        if p.algo == GLOBAL:
+            nf = 1
+        d2h += 4 * b.n * nf
+    e2e_times = []
+    ext = [torch.cuda.ExternalStream(s.view(0).stream, device=dev) for _, _, s in streams]
+    for it in range(args.warmup + args.steps):
+        sizes = [s.fill_fast(0, b) for _, b, s in streams]
+        torch.cuda.synchronize()
+        starts = [torch.cuda.Event(enable_timing=True) for _ in streams]
+        ends = [torch.cuda.Event(enable_timing=True) for _ in streams]
+        for k, ((p, b, s), (qi, ti)) in enumerate(zip(streams, sizes)):
+            starts[k].record(ext[k])
+            s.aln_async(0, qi, ti, b.n)
+            ends[k].record(ext[k])
+        for _, _, s in streams:
+            s.wait(0)
+        torch.cuda.synchronize()
+        if it >= args.warmup:
+            span = max(starts[0].elapsed_time(e) for e in ends)
+            e2e_times.append(span)
+    for _, _, s in streams:
+        s.close()
+    e2e_ms = float(np.mean(e2e_times))
+    if dist:
+        x = torch.tensor([e2e_ms], device=dev)
+        dist.all_reduce(x, op=dist.ReduceOp.MAX)
+        e2e_ms = float(x.item())
+    e2e = {"value": npairs * world / (e2e_ms * 1e-3), "unit": UNIT, "h2d_bytes_per_step": h2d,
+           "d2h_bytes_per_step": d2h, "ms_per_step": e2e_ms,
+           "path": "gasal_c_aln_async + gasal_c_is_aln_async_done (3 streams), pinned host batches"}
+
+    if rank == 0:
+        cpu = None if args.no_cpu_baseline else cpu_baseline(parts)
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "int32", "data": "synthetic (seeded numpy PCG64)",
+            "config": {"workload": "w1: 1M pairs/GPU, thirds LOCAL(second best)/GLOBAL/SEMI_GLOBAL(TARGET,TARGET), "
+                                   "WITH_START, q=150, t=150-300 (3% subs, 1% indels), RC 50% of queries, "
+                                   "scores 1/4/6/1",
+                       "pairs_per_step_per_gpu": npairs, "cells_per_step_per_gpu": cells,
+                       "parallelism": f"pair shards x{world}, no collective in the data path",
+                       "l2": "inputs 384 MB > 126 MB L2, no flush"},
+            "gcups": cells * world / (ms_step * 1e-3) / 1e9,
+            "roofline": {"bound": "int32", "achieved": achieved, "peak": peak["iadd_tops"], "unit": "Tops/s",
+                         "frac": achieved / peak["iadd_tops"], "traffic": DP_TRAFFIC_BYTES,
+                         "kernel": "dp_kernel (LOCAL/GLOBAL/SEMI_GLOBAL, one launch each per step)",
+                         "dp_ms_per_step": dp_ms / args.steps,
+                         "ops_per_cell": {"local": 11, "global": 9, "semi_global": 10},
+                         "peak_source": "measured live: 2-input int32 add issue rate (gb_probe_int_peak)",
+                         "imnmx_tops": peak["imnmx_tops"], "dpx_tops": peak["dpx_tops"]},
+            "kernel_ms_per_step": {k: v[0] / args.steps for k, v in kt.items()},
+            "gpu_launches": launches,
+            "cpu_baseline": cpu,
+            "e2e": e2e,
+            "clocks": clk.summary(),
+        }
+        print(json.dumps(line), flush=True)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,910 @@
+/*
+ * api_host.cpp -- GASAL2's C++ API, re-implemented for the B200 engine.
+ *
+ * Same functions, signatures, buffer ownership and observable behaviour as the
+ * reference (src/ctors.cpp, src/res.cpp, src/host_batch.cpp,
+ * src/interfaces.cpp, src/args_parser.cpp, src/gasal_align.cu:29-339):
+ * which result arrays exist, how host pages chain, which warnings print, and
+ * that errors print "[GASAL ...]" and terminate the process.  The device work
+ * of gasal_aln_async is gb::run_batch.  Per-stream engine state that has no
+ * place in gasal_gpu_storage_t (traceback tiles, row-buffer scratch, n_cigar)
+ * lives in a side table keyed by the storage address, so the struct layout is
+ * the reference's.
+ */
+#include "gasal_header.h"
+#include "res.h"
+#include "gasal_b200_capi.h"
+#include "engine.h"
+
+#include <cmath>
+#include <cstring>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <unordered_map>
+
+/* ========================= Parameters =================================== */
+
+Parameters::Parameters(int argc_, char **argv_)
+{
+    sa = 1;
+    sb = 4;
+    gapo = 6;
+    gape = 1;
+    start_pos = WITHOUT_START;
+    print_out = 0;
+    n_threads = 1;
+    k_band = 0;
+    isPacked = false;
+    isReverseComplement = false;
+    secondBest = FALSE;
+    semiglobal_skipping_head = TARGET;
+    semiglobal_skipping_tail = TARGET;
+    algo = UNKNOWN;
+    query_batch_fasta_filename = "";
+    target_batch_fasta_filename = "";
+    argc = argc_;
+    argv = argv_;
+}
+
+Parameters::~Parameters()
+{
+    query_batch_fasta.close();
+    target_batch_fasta.close();
+}
+
+void Parameters::print()
+{
+    std::cerr << "sa=" << sa << " , sb=" << sb << " , gapo=" << gapo << " , gape=" << gape << std::endl;
+    std::cerr << "start_pos=" << start_pos << " , print_out=" << print_out << " , n_threads=" << n_threads << std::endl;
+    std::cerr << "semiglobal_skipping_head=" << semiglobal_skipping_head
+              << " , semiglobal_skipping_tail=" << semiglobal_skipping_tail << " , algo=" << algo << std::endl;
+    std::cerr << std::boolalpha << "isPacked = " << isPacked << " , secondBest = " << secondBest << std::endl;
+    std::cerr << "query_batch_fasta_filename=" << query_batch_fasta_filename
+              << " , target_batch_fasta_filename=" << target_batch_fasta_filename << std::endl;
+}
+
+void Parameters::failure(fail_type f)
+{
+    switch (f) {
+    case NOT_ENOUGH_ARGS:
+        std::cerr << "Not enough Parameters. Required: -y AL_TYPE file1.fasta file2.fasta. See help (--help, -h) for usage. "
+                  << std::endl;
+        break;
+    case WRONG_ARG:
+        std::cerr << "Wrong argument. See help (--help, -h) for usage. " << std::endl;
+        break;
+    case WRONG_FILES:
+        std::cerr << "File error: either a file doesn't exist, or cannot be opened." << std::endl;
+        break;
+    default:
+        break;
+    }
+    exit(1);
+}
+
+void Parameters::help()
+{
+    std::cerr << "Usage: ./test_prog.out [-a] [-b] [-q] [-r] [-s] [-t] [-p] [-n] [-y] <query_batch.fasta> <target_batch.fasta>" << std::endl;
+    std::cerr << "Options: -a INT    match score [" << sa << "]" << std::endl;
+    std::cerr << "         -b INT    mismatch penalty [" << sb << "]" << std::endl;
+    std::cerr << "         -q INT    gap open penalty [" << gapo << "]" << std::endl;
+    std::cerr << "         -r INT    gap extension penalty [" << gape << "]" << std::endl;
+    std::cerr << "         -s        find the start position" << std::endl;
+    std::cerr << "         -t        compute traceback (implies the start position)" << std::endl;
+    std::cerr << "         -p        print the alignment results" << std::endl;
+    std::cerr << "         -n INT    Number of threads [" << n_threads << "]" << std::endl;
+    std::cerr << "         -y AL_TYPE       Alignment type . Must be \"local\", \"semi_global\", \"global\", \"ksw\" " << std::endl;
+    std::cerr << "         -x HEAD TAIL     semi-global: what to skip at heads and tails (NONE, QUERY, TARGET, BOTH)" << std::endl;
+    std::cerr << "         -k INT    Band width in case \"banded\" is selected." << std::endl;
+    std::cerr << "         --help, -h : displays this message." << std::endl;
+    std::cerr << "         --second-best   displays second best score (WITHOUT_START only)." << std::endl;
+}
+
+static data_source parse_src(const std::string &s, bool *ok)
+{
+    *ok = true;
+    if (s == "NONE") return NONE;
+    if (s == "TARGET") return TARGET;
+    if (s == "QUERY") return QUERY;
+    if (s == "BOTH") return BOTH;
+    *ok = false;
+    return NONE;
+}
+
+void Parameters::parse()
+{
+    for (int c = 1; c < argc; c++) {
+        std::string a(argv[c]);
+        if (a == "--help" || a == "-h") {
+            help();
+            exit(0);
+        }
+    }
+    if (argc < 4) failure(NOT_ENOUGH_ARGS);
+    int c;
+    for (c = 1; c < argc - 2; c++) {
+        std::string cur(argv[c]);
+        if (cur.size() >= 2 && cur[0] == '-' && cur[1] == '-') {
+            if (cur == "--second-best") secondBest = TRUE;
+        } else if (!cur.empty() && cur[0] == '-') {
+            if (cur.size() > 2) failure(WRONG_ARG);
+            bool ok = true;
+            switch (cur[1]) {
+            case 'y': {
+                std::string v(argv[++c]);
+                if (v == "local") algo = LOCAL;
+                else if (v == "semi_global") algo = SEMI_GLOBAL;
+                else if (v == "global") algo = GLOBAL;
+                else if (v == "ksw") algo = KSW;
+                break;
+            }
+            case 'a': sa = std::stoi(argv[++c]); break;
+            case 'b': sb = std::stoi(argv[++c]); break;
+            case 'q': gapo = std::stoi(argv[++c]); break;
+            case 'r': gape = std::stoi(argv[++c]); break;
+            case 's': start_pos = WITH_START; break;
+            case 't': start_pos = WITH_TB; break;
+            case 'p': print_out = 1; break;
+            case 'n': n_threads = std::stoi(argv[++c]); break;
+            case 'k': k_band = std::stoi(argv[++c]); break;
+            case 'x':
+                semiglobal_skipping_head = parse_src(argv[++c], &ok);
+                if (!ok) failure(WRONG_ARG);
+                semiglobal_skipping_tail = parse_src(argv[++c], &ok);
+                if (!ok) failure(WRONG_ARG);
+                break;
+            default: break;
+            }
+        } else {
+            failure(WRONG_ARG);
+        }
+    }
+    query_batch_fasta_filename = std::string(argv[c]);
+    target_batch_fasta_filename = std::string(argv[c + 1]);
+    fileopen();
+}
+
+void Parameters::fileopen()
+{
+    query_batch_fasta.open(query_batch_fasta_filename, std::ifstream::in);
+    if (!query_batch_fasta) failure(WRONG_FILES);
+    target_batch_fasta.open(target_batch_fasta_filename);
+    if (!target_batch_fasta) failure(WRONG_FILES);
+}
+
+/* ========================= helpers ====================================== */
+
+#define GB_FATAL_CUDA(call)                                                                              \
+    do {                                                                                                 \
+        cudaError_t err_ = (call);                                                                       \
+        if (cudaSuccess != err_) {                                                                       \
+            fprintf(stderr, "[GASAL CUDA ERROR:] %s(CUDA error no.=%d). Line no. %d in file %s\n",       \
+                    cudaGetErrorString(err_), err_, __LINE__, __FILE__);                                 \
+            exit(EXIT_FAILURE);                                                                          \
+        }                                                                                                \
+    } while (0)
+
+namespace {
+
+struct StreamState {
+    gb::Workspace ws;
+    uint32_t *d_n_cigar = nullptr;
+    size_t n_cigar_cap = 0;
+};
+
+std::mutex g_mu;
+std::unordered_map<const gasal_gpu_storage_t *, std::unique_ptr<StreamState>> g_state;
+
+StreamState &state_of(const gasal_gpu_storage_t *s)
+{
+    std::lock_guard<std::mutex> lk(g_mu);
+    auto &p = g_state[s];
+    if (!p) p.reset(new StreamState());
+    return *p;
+}
+
+void release_state(const gasal_gpu_storage_t *s)
+{
+    std::unique_ptr<StreamState> p;
+    {
+        std::lock_guard<std::mutex> lk(g_mu);
+        auto it = g_state.find(s);
+        if (it == g_state.end()) return;
+        p = std::move(it->second);
+        g_state.erase(it);
+    }
+    gb::Workspace &w = p->ws;
+    if (w.tb) cudaFree(w.tb);
+    if (w.d_tb_off) cudaFree(w.d_tb_off);
+    if (w.h_tb_off) cudaFreeHost(w.h_tb_off);
+    if (w.scratch) cudaFree(w.scratch);
+    if (w.tb_off_free) cudaEventDestroy(w.tb_off_free);
+    if (p->d_n_cigar) cudaFree(p->d_n_cigar);
+}
+
+uint32_t round8(uint32_t x) { return (x + 7u) & ~7u; }
+
+} // namespace
+
+/* ========================= host batches ================================= */
+/* Pinned pages chained into a list; src/host_batch.cpp:11-244. */
+
+host_batch_t *gasal_host_batch_new(uint32_t batch_bytes, uint32_t offset)
+{
+    host_batch_t *res = (host_batch_t *)calloc(1, sizeof(host_batch_t));
+    GB_FATAL_CUDA(cudaHostAlloc(&(res->data), batch_bytes * sizeof(uint8_t), cudaHostAllocDefault));
+    res->page_size = batch_bytes;
+    res->data_size = 0;
+    res->is_locked = 0;
+    res->offset = offset;
+    res->next = NULL;
+    return res;
+}
+
+void gasal_host_batch_destroy(host_batch_t *res)
+{
+    if (res == NULL) {
+        fprintf(stderr, "[GASAL ERROR] Trying to free a NULL pointer\n");
+        exit(1);
+    }
+    while (res != NULL) {
+        host_batch_t *next = res->next;
+        if (res->data != NULL) GB_FATAL_CUDA(cudaFreeHost(res->data));
+        free(res);
+        res = next;
+    }
+}
+
+host_batch_t *gasal_host_batch_getlast(host_batch_t *arg)
+{
+    while (arg->next != NULL) arg = arg->next;
+    return arg;
+}
+
+void gasal_host_batch_reset(gasal_gpu_storage_t *gpu_storage)
+{
+    host_batch_t *heads[2] = {gpu_storage->extensible_host_unpacked_query_batch,
+                              gpu_storage->extensible_host_unpacked_target_batch};
+    for (host_batch_t *p : heads) {
+        for (; p != NULL; p = p->next) {
+            p->data_size = 0;
+            p->offset = 0;
+            p->is_locked = 0;
+        }
+    }
+}
+
+uint32_t gasal_host_batch_fill(gasal_gpu_storage_t *gpu_storage, uint32_t idx, const char *data, uint32_t size,
+                               data_source SRC)
+{
+    host_batch_t *cur = (SRC == QUERY) ? gpu_storage->extensible_host_unpacked_query_batch
+                                       : gpu_storage->extensible_host_unpacked_target_batch;
+    uint32_t *p_batch_bytes = (SRC == QUERY) ? &gpu_storage->host_max_query_batch_bytes
+                                             : &gpu_storage->host_max_target_batch_bytes;
+    const uint32_t pad = (8u - (size & 7u)) & 7u;
+    const uint32_t need = size + pad;
+    while (cur->is_locked) cur = cur->next;
+    if (cur->next == NULL && cur->page_size - cur->data_size < need) {
+        fprintf(stderr,
+                "[GASAL WARNING:] Trying to write %d bytes while only %d remain (%s) (block size %d, filled %d bytes).\n"
+                "                 Allocating a new block of size %d, total size available reaches %d. Doing this repeadtedly slows down the execution.\n",
+                need, cur->page_size - cur->data_size, (SRC == QUERY ? "query" : "target"), cur->page_size,
+                cur->data_size, cur->page_size * 2, *p_batch_bytes + cur->page_size * 2);
+        host_batch_t *res = gasal_host_batch_new(cur->page_size * 2, cur->offset + cur->data_size);
+        cur->next = res;
+        cur->is_locked = 1;
+        *p_batch_bytes = *p_batch_bytes + cur->page_size * 2;
+        cur = cur->next;
+    }
+    if (cur->next != NULL && cur->page_size - cur->data_size < need) {
+        cur->next->offset = cur->offset + cur->data_size;
+        cur->is_locked = 1;
+        cur = cur->next;
+    }
+    if (cur->page_size - cur->data_size >= need) {
+        memcpy(&(cur->data[idx - cur->offset]), data, size);
+        memset(&(cur->data[idx + size - cur->offset]), N_CODE, pad);
+        idx += need;
+        cur->data_size += need;
+    }
+    return idx;
+}
+
+uint32_t gasal_host_batch_addbase(gasal_gpu_storage_t *gpu_storage, uint32_t idx, const char base, data_source SRC)
+{
+    return gasal_host_batch_add(gpu_storage, idx, &base, 1, SRC);
+}
+
+uint32_t gasal_host_batch_add(gasal_gpu_storage_t *gpu_storage, uint32_t idx, const char *data, uint32_t size,
+                              data_source SRC)
+{
+    host_batch_t *cur = (SRC == QUERY) ? gpu_storage->extensible_host_unpacked_query_batch
+                                       : gpu_storage->extensible_host_unpacked_target_batch;
+    uint32_t *p_batch_bytes = (SRC == QUERY) ? &gpu_storage->host_max_query_batch_bytes
+                                             : &gpu_storage->host_max_target_batch_bytes;
+    for (;;) {
+        if (*p_batch_bytes >= idx + size && (cur->next == NULL || cur->next->offset >= idx + size)) {
+            memcpy(&(cur->data[idx - cur->offset]), data, size);
+            return idx + size;
+        }
+        if (*p_batch_bytes >= idx + size && cur->next != NULL && cur->next->offset < idx + size) {
+            cur = cur->next;
+            continue;
+        }
+        fprintf(stderr,
+                "[GASAL WARNING:] Trying to write %d bytes at position %d on host memory (%s) while only  %d bytes are available. Therefore, allocating %d bytes more on CPU. Repeating this many times can provoke a degradation of performance.\n",
+                size, idx, (SRC == QUERY ? "query" : "target"), *p_batch_bytes, *p_batch_bytes * 2);
+        *p_batch_bytes += *p_batch_bytes;
+        while (*p_batch_bytes < size) *p_batch_bytes += *p_batch_bytes;
+        host_batch_t *res = gasal_host_batch_new(*p_batch_bytes, idx);
+        cur->next = res;
+        cur = cur->next;
+    }
+}
+
+void gasal_host_batch_print(host_batch_t *res)
+{
+    fprintf(stderr, "[GASAL PRINT] Page data: offset=%d, next_offset=%d, data size=%d, page size=%d\n", res->offset,
+            (res->next != NULL ? (int)res->next->offset : -1), res->data_size, res->page_size);
+}
+
+void gasal_host_batch_printall(host_batch_t *res)
+{
+    for (; res != NULL; res = res->next) {
+        gasal_host_batch_print(res);
+        if (res->next != NULL) fprintf(stderr, "+--->");
+    }
+}
+
+/* ========================= results ====================================== */
+/* Which arrays exist: src/res.cpp:8-70 and :106-140. */
+
+gasal_res_t *gasal_res_new_host(uint32_t max_n_alns, Parameters *params)
+{
+    gasal_res_t *res = (gasal_res_t *)calloc(1, sizeof(gasal_res_t));
+    if (res == NULL) {
+        fprintf(stderr, "Malloc error on res host ");
+        exit(1);
+    }
+    GB_FATAL_CUDA(cudaHostAlloc(&(res->aln_score), max_n_alns * sizeof(int32_t), cudaHostAllocDefault));
+    if (params->algo != GLOBAL) {
+        if (params->start_pos == WITH_START || params->start_pos == WITH_TB) {
+            GB_FATAL_CUDA(cudaHostAlloc(&(res->query_batch_start), max_n_alns * sizeof(uint32_t), cudaHostAllocDefault));
+            GB_FATAL_CUDA(cudaHostAlloc(&(res->target_batch_start), max_n_alns * sizeof(uint32_t), cudaHostAllocDefault));
+        }
+        GB_FATAL_CUDA(cudaHostAlloc(&(res->query_batch_end), max_n_alns * sizeof(uint32_t), cudaHostAllocDefault));
+        GB_FATAL_CUDA(cudaHostAlloc(&(res->target_batch_end), max_n_alns * sizeof(uint32_t), cudaHostAllocDefault));
+    }
+    if (params->start_pos == WITH_TB)
+        GB_FATAL_CUDA(cudaHostAlloc(&(res->n_cigar_ops), max_n_alns * sizeof(uint32_t), cudaHostAllocDefault));
+    return res;
+}
+
+gasal_res_t *gasal_res_new_device_cpy(uint32_t max_n_alns, Parameters *params)
+{
+    gasal_res_t *res = (gasal_res_t *)calloc(1, sizeof(gasal_res_t));
+    GB_FATAL_CUDA(cudaMalloc(&(res->aln_score), max_n_alns * sizeof(int32_t)));
+    if (params->algo != GLOBAL) {
+        if (params->start_pos == WITH_START || params->start_pos == WITH_TB) {
+            GB_FATAL_CUDA(cudaMalloc(&(res->query_batch_start), max_n_alns * sizeof(uint32_t)));
+            GB_FATAL_CUDA(cudaMalloc(&(res->target_batch_start), max_n_alns * sizeof(uint32_t)));
+        }
+        GB_FATAL_CUDA(cudaMalloc(&(res->query_batch_end), max_n_alns * sizeof(uint32_t)));
+        GB_FATAL_CUDA(cudaMalloc(&(res->target_batch_end), max_n_alns * sizeof(uint32_t)));
+    }
+    return res;
+}
+
+gasal_res_t *gasal_res_new_device(gasal_res_t *device_cpy)
+{
+    gasal_res_t *d_c;
+    GB_FATAL_CUDA(cudaMalloc((void **)&d_c, sizeof(gasal_res_t)));
+    GB_FATAL_CUDA(cudaMemcpy(d_c, device_cpy, sizeof(gasal_res_t), cudaMemcpyHostToDevice));
+    return d_c;
+}
+
+void gasal_res_destroy_host(gasal_res_t *res)
+{
+    if (res == NULL) return;
+    if (res->aln_score) GB_FATAL_CUDA(cudaFreeHost(res->aln_score));
+    if (res->query_batch_start) GB_FATAL_CUDA(cudaFreeHost(res->query_batch_start));
+    if (res->target_batch_start) GB_FATAL_CUDA(cudaFreeHost(res->target_batch_start));
+    if (res->query_batch_end) GB_FATAL_CUDA(cudaFreeHost(res->query_batch_end));
+    if (res->target_batch_end) GB_FATAL_CUDA(cudaFreeHost(res->target_batch_end));
+    if (res->n_cigar_ops) GB_FATAL_CUDA(cudaFreeHost(res->n_cigar_ops));
+    if (res->cigar) GB_FATAL_CUDA(cudaFreeHost(res->cigar));
+    free(res);
+}
+
+void gasal_res_destroy_device(gasal_res_t *device_res, gasal_res_t *device_cpy)
+{
+    if (device_cpy == NULL || device_res == NULL) return;
+    if (device_cpy->aln_score) GB_FATAL_CUDA(cudaFree(device_cpy->aln_score));
+    if (device_cpy->query_batch_start) GB_FATAL_CUDA(cudaFree(device_cpy->query_batch_start));
+    if (device_cpy->target_batch_start) GB_FATAL_CUDA(cudaFree(device_cpy->target_batch_start));
+    if (device_cpy->query_batch_end) GB_FATAL_CUDA(cudaFree(device_cpy->query_batch_end));
+    if (device_cpy->target_batch_end) GB_FATAL_CUDA(cudaFree(device_cpy->target_batch_end));
+    if (device_cpy->cigar) GB_FATAL_CUDA(cudaFree(device_cpy->cigar));
+    GB_FATAL_CUDA(cudaFree(device_res));
+    free(device_cpy);
+}
+
+/* ========================= streams ====================================== */
+
+gasal_gpu_storage_v gasal_init_gpu_storage_v(int n_streams)
+{
+    gasal_gpu_storage_v v;
+    v.a = (gasal_gpu_storage_t *)calloc(n_streams, sizeof(gasal_gpu_storage_t));
+    v.n = n_streams;
+    return v;
+}
+
+void gasal_init_streams(gasal_gpu_storage_v *vec, int max_query_len, int max_target_len, int max_n_alns,
+                        Parameters *params)
+{
+    const uint32_t q8 = round8((uint32_t)max_query_len), t8 = round8((uint32_t)max_target_len);
+    const uint32_t qbytes = (uint32_t)max_n_alns * q8, tbytes = (uint32_t)max_n_alns * t8;
+    for (int i = 0; i < vec->n; i++) {
+        gasal_gpu_storage_t *s = &vec->a[i];
+        s->extensible_host_unpacked_query_batch = gasal_host_batch_new(qbytes, 0);
+        s->extensible_host_unpacked_target_batch = gasal_host_batch_new(tbytes, 0);
+        GB_FATAL_CUDA(cudaMalloc(&s->unpacked_query_batch, qbytes));
+        GB_FATAL_CUDA(cudaMalloc(&s->unpacked_target_batch, tbytes));
+        GB_FATAL_CUDA(cudaHostAlloc(&s->host_query_op, max_n_alns, cudaHostAllocDefault));
+        GB_FATAL_CUDA(cudaHostAlloc(&s->host_target_op, max_n_alns, cudaHostAllocDefault));
+        memset(s->host_query_op, 0, max_n_alns);
+        memset(s->host_target_op, 0, max_n_alns);
+        GB_FATAL_CUDA(cudaMalloc(&s->query_op, max_n_alns));
+        GB_FATAL_CUDA(cudaMalloc(&s->target_op, max_n_alns));
+        if (params->isPacked) {
+            s->packed_query_batch = (uint32_t *)s->unpacked_query_batch;
+            s->packed_target_batch = (uint32_t *)s->unpacked_target_batch;
+        } else {
+            GB_FATAL_CUDA(cudaMalloc(&s->packed_query_batch, (qbytes / 8) * sizeof(uint32_t)));
+            GB_FATAL_CUDA(cudaMalloc(&s->packed_target_batch, (tbytes / 8) * sizeof(uint32_t)));
+        }
+        if (params->algo == KSW) {
+            GB_FATAL_CUDA(cudaHostAlloc(&s->host_seed_scores, max_n_alns * sizeof(uint32_t), cudaHostAllocDefault));
+            GB_FATAL_CUDA(cudaMalloc(&s->seed_scores, max_n_alns * sizeof(uint32_t)));
+        } else {
+            s->host_seed_scores = NULL;
+            s->seed_scores = NULL;
+        }
+        GB_FATAL_CUDA(cudaHostAlloc(&s->host_query_batch_lens, max_n_alns * sizeof(uint32_t), cudaHostAllocDefault));
+        GB_FATAL_CUDA(cudaHostAlloc(&s->host_target_batch_lens, max_n_alns * sizeof(uint32_t), cudaHostAllocDefault));
+        GB_FATAL_CUDA(cudaHostAlloc(&s->host_query_batch_offsets, max_n_alns * sizeof(uint32_t), cudaHostAllocDefault));
+        GB_FATAL_CUDA(cudaHostAlloc(&s->host_target_batch_offsets, max_n_alns * sizeof(uint32_t), cudaHostAllocDefault));
+        GB_FATAL_CUDA(cudaMalloc(&s->query_batch_lens, max_n_alns * sizeof(uint32_t)));
+        GB_FATAL_CUDA(cudaMalloc(&s->target_batch_lens, max_n_alns * sizeof(uint32_t)));
+        GB_FATAL_CUDA(cudaMalloc(&s->query_batch_offsets, max_n_alns * sizeof(uint32_t)));
+        GB_FATAL_CUDA(cudaMalloc(&s->target_batch_offsets, max_n_alns * sizeof(uint32_t)));
+        s->host_res = gasal_res_new_host(max_n_alns, params);
+        if (params->start_pos == WITH_TB)
+            GB_FATAL_CUDA(cudaHostAlloc(&s->host_res->cigar, qbytes, cudaHostAllocDefault));
+        s->device_cpy = gasal_res_new_device_cpy(max_n_alns, params);
+        s->device_res = gasal_res_new_device(s->device_cpy);
+        if (params->secondBest) {
+            s->host_res_second = gasal_res_new_host(max_n_alns, params);
+            s->device_cpy_second = gasal_res_new_device_cpy(max_n_alns, params);
+            s->device_res_second = gasal_res_new_device(s->device_cpy_second);
+        } else {
+            s->host_res_second = NULL;
+            s->device_cpy_second = NULL;
+            s->device_res_second = NULL;
+        }
+        /* traceback tiles are sized per batch by the engine (packed_tb_matrices
+         * stays NULL; the reference's max_q x max_t x n_alns matrix is not used) */
+        s->packed_tb_matrix_size = 0;
+        s->packed_tb_matrices = NULL;
+        GB_FATAL_CUDA(cudaStreamCreate(&s->str));
+        s->is_free = 1;
+        s->host_max_query_batch_bytes = qbytes;
+        s->host_max_target_batch_bytes = tbytes;
+        s->host_max_n_alns = max_n_alns;
+        s->gpu_max_query_batch_bytes = qbytes;
+        s->gpu_max_target_batch_bytes = tbytes;
+        s->gpu_max_n_alns = max_n_alns;
+        s->current_n_alns = 0;
+        StreamState &ss = state_of(s);
+        (void)ss;
+    }
+}
+
+void gasal_destroy_streams(gasal_gpu_storage_v *vec, Parameters *params)
+{
+    (void)params;
+    for (int i = 0; i < vec->n; i++) {
+        gasal_gpu_storage_t *s = &vec->a[i];
+        if (s->str) cudaStreamSynchronize(s->str);
+        release_state(s);
+        if (s->extensible_host_unpacked_query_batch) gasal_host_batch_destroy(s->extensible_host_unpacked_query_batch);
+        if (s->extensible_host_unpacked_target_batch) gasal_host_batch_destroy(s->extensible_host_unpacked_target_batch);
+        gasal_res_destroy_host(s->host_res);
+        gasal_res_destroy_device(s->device_res, s->device_cpy);
+        gasal_res_destroy_host(s->host_res_second);
+        gasal_res_destroy_device(s->device_res_second, s->device_cpy_second);
+        if (s->seed_scores) GB_FATAL_CUDA(cudaFree(s->seed_scores));
+        if (s->host_seed_scores) GB_FATAL_CUDA(cudaFreeHost(s->host_seed_scores));
+        if (s->query_op) GB_FATAL_CUDA(cudaFree(s->query_op));
+        if (s->target_op) GB_FATAL_CUDA(cudaFree(s->target_op));
+        if (s->host_query_op) GB_FATAL_CUDA(cudaFreeHost(s->host_query_op));
+        if (s->host_target_op) GB_FATAL_CUDA(cudaFreeHost(s->host_target_op));
+        if (s->host_query_batch_offsets) GB_FATAL_CUDA(cudaFreeHost(s->host_query_batch_offsets));
+        if (s->host_target_batch_offsets) GB_FATAL_CUDA(cudaFreeHost(s->host_target_batch_offsets));
+        if (s->host_query_batch_lens) GB_FATAL_CUDA(cudaFreeHost(s->host_query_batch_lens));
+        if (s->host_target_batch_lens) GB_FATAL_CUDA(cudaFreeHost(s->host_target_batch_lens));
+        if (s->packed_query_batch && (void *)s->packed_query_batch != (void *)s->unpacked_query_batch)
+            GB_FATAL_CUDA(cudaFree(s->packed_query_batch));
+        if (s->packed_target_batch && (void *)s->packed_target_batch != (void *)s->unpacked_target_batch)
+            GB_FATAL_CUDA(cudaFree(s->packed_target_batch));
+        if (s->unpacked_query_batch) GB_FATAL_CUDA(cudaFree(s->unpacked_query_batch));
+        if (s->unpacked_target_batch) GB_FATAL_CUDA(cudaFree(s->unpacked_target_batch));
+        if (s->query_batch_offsets) GB_FATAL_CUDA(cudaFree(s->query_batch_offsets));
+        if (s->target_batch_offsets) GB_FATAL_CUDA(cudaFree(s->target_batch_offsets));
+        if (s->query_batch_lens) GB_FATAL_CUDA(cudaFree(s->query_batch_lens));
+        if (s->target_batch_lens) GB_FATAL_CUDA(cudaFree(s->target_batch_lens));
+        if (s->packed_tb_matrices) GB_FATAL_CUDA(cudaFree(s->packed_tb_matrices));
+        if (s->str) GB_FATAL_CUDA(cudaStreamDestroy(s->str));
+        memset(s, 0, sizeof(*s));
+    }
+}
+
+void gasal_destroy_gpu_storage_v(gasal_gpu_storage_v *vec)
+{
+    if (vec->a != NULL) free(vec->a);
+    vec->a = NULL;
+}
+
+void gasal_gpu_mem_alloc(gasal_gpu_storage_t *s, int gpu_max_query_batch_bytes, int gpu_max_target_batch_bytes,
+                         int gpu_max_n_alns, Parameters *params)
+{
+    GB_FATAL_CUDA(cudaMalloc(&s->unpacked_query_batch, gpu_max_query_batch_bytes));
+    GB_FATAL_CUDA(cudaMalloc(&s->unpacked_target_batch, gpu_max_target_batch_bytes));
+    GB_FATAL_CUDA(cudaMalloc(&s->packed_query_batch, (gpu_max_query_batch_bytes / 8) * sizeof(uint32_t)));
+    GB_FATAL_CUDA(cudaMalloc(&s->packed_target_batch, (gpu_max_target_batch_bytes / 8) * sizeof(uint32_t)));
+    GB_FATAL_CUDA(cudaMalloc(&s->query_batch_lens, gpu_max_n_alns * sizeof(uint32_t)));
+    GB_FATAL_CUDA(cudaMalloc(&s->target_batch_lens, gpu_max_n_alns * sizeof(uint32_t)));
+    GB_FATAL_CUDA(cudaMalloc(&s->query_batch_offsets, gpu_max_n_alns * sizeof(uint32_t)));
+    GB_FATAL_CUDA(cudaMalloc(&s->target_batch_offsets, gpu_max_n_alns * sizeof(uint32_t)));
+    s->device_cpy = gasal_res_new_device_cpy(gpu_max_n_alns, params);
+    s->device_res = gasal_res_new_device(s->device_cpy);
+    s->gpu_max_query_batch_bytes = gpu_max_query_batch_bytes;
+    s->gpu_max_target_batch_bytes = gpu_max_target_batch_bytes;
+    s->gpu_max_n_alns = gpu_max_n_alns;
+}
+
+void gasal_gpu_mem_free(gasal_gpu_storage_t *s, Parameters *params)
+{
+    if (s->unpacked_query_batch) GB_FATAL_CUDA(cudaFree(s->unpacked_query_batch));
+    if (s->unpacked_target_batch) GB_FATAL_CUDA(cudaFree(s->unpacked_target_batch));
+    if (s->packed_query_batch) GB_FATAL_CUDA(cudaFree(s->packed_query_batch));
+    if (s->packed_target_batch) GB_FATAL_CUDA(cudaFree(s->packed_target_batch));
+    if (s->query_batch_offsets) GB_FATAL_CUDA(cudaFree(s->query_batch_offsets));
+    if (s->target_batch_offsets) GB_FATAL_CUDA(cudaFree(s->target_batch_offsets));
+    if (s->query_batch_lens) GB_FATAL_CUDA(cudaFree(s->query_batch_lens));
+    if (s->target_batch_lens) GB_FATAL_CUDA(cudaFree(s->target_batch_lens));
+    gasal_res_destroy_device(s->device_res, s->device_cpy);
+    if (params->secondBest) gasal_res_destroy_device(s->device_res_second, s->device_cpy_second);
+}
+
+/* ========================= interfaces =================================== */
+
+template <typename T> static T *host_realloc(T *src, int new_n, int old_n)
+{
+    if (new_n < old_n) {
+        fprintf(stderr, "[GASAL ERROR] cudoHostRealloc: invalid sizes. New size < old size (%d < %d)", new_n, old_n);
+        exit(EXIT_FAILURE);
+    }
+    T *dst = NULL;
+    GB_FATAL_CUDA(cudaHostAlloc(&dst, new_n * sizeof(T), cudaHostAllocMapped));
+    if (src) {
+        memcpy(dst, src, old_n * sizeof(T));
+        GB_FATAL_CUDA(cudaFreeHost(src));
+    }
+    return dst;
+}
+
+void gasal_host_alns_resize(gasal_gpu_storage_t *s, int new_max_alns, Parameters *params)
+{
+    fprintf(stderr, "[GASAL WARNING] Resizing gpu_storage from %d sequences to %d sequences... ", s->host_max_n_alns,
+            new_max_alns);
+    const int old = (int)s->host_max_n_alns;
+    s->host_query_op = host_realloc(s->host_query_op, new_max_alns, old);
+    s->host_target_op = host_realloc(s->host_target_op, new_max_alns, old);
+    if (params->algo == KSW) s->host_seed_scores = host_realloc(s->host_seed_scores, new_max_alns, old);
+    s->host_query_batch_lens = host_realloc(s->host_query_batch_lens, new_max_alns, old);
+    s->host_target_batch_lens = host_realloc(s->host_target_batch_lens, new_max_alns, old);
+    s->host_query_batch_offsets = host_realloc(s->host_query_batch_offsets, new_max_alns, old);
+    s->host_target_batch_offsets = host_realloc(s->host_target_batch_offsets, new_max_alns, old);
+    uint8_t *cigar = s->host_res ? s->host_res->cigar : NULL;
+    if (s->host_res) s->host_res->cigar = NULL;
+    gasal_res_destroy_host(s->host_res);
+    s->host_res = gasal_res_new_host(new_max_alns, params);
+    s->host_res->cigar = cigar;
+    gasal_res_destroy_device(s->device_res, s->device_cpy);
+    s->device_cpy = gasal_res_new_device_cpy(new_max_alns, params);
+    s->device_res = gasal_res_new_device(s->device_cpy);
+    if (params->secondBest) {
+        gasal_res_destroy_host(s->host_res_second);
+        gasal_res_destroy_device(s->device_res_second, s->device_cpy_second);
+        s->host_res_second = gasal_res_new_host(new_max_alns, params);
+        s->device_cpy_second = gasal_res_new_device_cpy(new_max_alns, params);
+        s->device_res_second = gasal_res_new_device(s->device_cpy_second);
+    }
+    s->host_max_n_alns = new_max_alns;
+    if (s->gpu_max_n_alns > (uint32_t)new_max_alns) s->gpu_max_n_alns = new_max_alns;
+    fprintf(stderr, " done. This can harm performance.\n");
+}
+
+void gasal_op_fill(gasal_gpu_storage_t *s, uint8_t *data, uint32_t nbr_seqs_in_stream, data_source SRC)
+{
+    uint8_t *dst = (SRC == QUERY) ? s->host_query_op : s->host_target_op;
+    memcpy(dst, data, nbr_seqs_in_stream);
+}
+
+void gasal_set_device(int gpu_select, bool isPrintingProp)
+{
+    if (isPrintingProp) {
+        int num_devices = 0;
+        cudaGetDeviceCount(&num_devices);
+        fprintf(stderr, "Found %d GPUs\n", num_devices);
+        if (gpu_select > num_devices - 1) {
+            fprintf(stderr, "Error: can't select device %d when only %d devices are selected (range from 0 to %d)\n",
+                    gpu_select, num_devices, num_devices - 1);
+            exit(EXIT_FAILURE);
+        }
+        cudaDeviceProp prop;
+        for (int d = 0; d < num_devices; d++) {
+            cudaGetDeviceProperties(&prop, d);
+            fprintf(stderr, "\tGPU %d: %s\n", d, prop.name);
+        }
+        if (num_devices > 0) {
+            cudaGetDeviceProperties(&prop, gpu_select);
+            fprintf(stderr, "Selected device %d : %s\n", gpu_select, prop.name);
+            cudaSetDevice(gpu_select);
+        }
+    } else {
+        cudaSetDevice(gpu_select);
+    }
+}
+
+/* ========================= alignment ==================================== */
+
+void gasal_copy_subst_scores(gasal_subst_scores *subst)
+{
+    gb::Settings &st = gb::settings();
+    st.sc.match = subst->match;
+    st.sc.mismatch = subst->mismatch;
+    st.sc.o = subst->gap_open;
+    st.sc.e = subst->gap_extend;
+    st.sc.oe = subst->gap_open + subst->gap_extend;
+}
+
+namespace gbapi {
+
+/* Error reporting of one call: the C++ API prints and terminates like the
+ * reference; the C ABI returns the status. */
+struct Errs {
+    bool fatal;
+    int fail(int code, const char *msg) const
+    {
+        fprintf(stderr, "%s", msg);
+        if (fatal) exit(EXIT_FAILURE);
+        return code;
+    }
+};
+
+static int grow_dev(void **p, uint32_t old_bytes, uint32_t new_bytes)
+{
+    (void)old_bytes;
+    if (*p) cudaFree(*p);
+    *p = NULL;
+    return cudaMalloc(p, new_bytes) == cudaSuccess ? GB_OK : GB_ERR_ALLOC;
+}
+
+int aln_async(gasal_gpu_storage_t *s, uint32_t qbytes, uint32_t tbytes, uint32_t n, Parameters *params, bool fatal)
+{
+    Errs E{fatal};
+    char msg[512];
+    if (n <= 0) return E.fail(GB_ERR_ARG, "[GASAL ERROR:] actual_n_alns <= 0\n");
+    if (qbytes <= 0) return E.fail(GB_ERR_ARG, "[GASAL ERROR:] actual_query_batch_bytes <= 0\n");
+    if (tbytes <= 0) return E.fail(GB_ERR_ARG, "[GASAL ERROR:] actual_target_batch_bytes <= 0\n");
+    if (qbytes % 8) {
+        snprintf(msg, sizeof msg, "[GASAL ERROR:] actual_query_batch_bytes=%d is not a multiple of 8\n", qbytes);
+        return E.fail(GB_ERR_ARG, msg);
+    }
+    if (tbytes % 8) {
+        snprintf(msg, sizeof msg, "[GASAL ERROR:] actual_target_batch_bytes=%d is not a multiple of 8\n", tbytes);
+        return E.fail(GB_ERR_ARG, msg);
+    }
+    if (qbytes > s->host_max_query_batch_bytes) {
+        snprintf(msg, sizeof msg, "[GASAL ERROR:] actual_query_batch_bytes(%d) > host_max_query_batch_bytes(%d)\n",
+                 qbytes, s->host_max_query_batch_bytes);
+        return E.fail(GB_ERR_ARG, msg);
+    }
+    if (tbytes > s->host_max_target_batch_bytes) {
+        snprintf(msg, sizeof msg, "[GASAL ERROR:] actual_target_batch_bytes(%d) > host_max_target_batch_bytes(%d)\n",
+                 tbytes, s->host_max_target_batch_bytes);
+        return E.fail(GB_ERR_ARG, msg);
+    }
+    if (n > s->host_max_n_alns) {
+        snprintf(msg, sizeof msg, "[GASAL ERROR:] actual_n_alns(%d) > host_max_n_alns(%d)\n", n, s->host_max_n_alns);
+        return E.fail(GB_ERR_ARG, msg);
+    }
+    if (params->algo != LOCAL && params->algo != GLOBAL && params->algo != SEMI_GLOBAL && params->algo != BANDED &&
+        params->algo != KSW)
+        return E.fail(GB_ERR_ARG, "[GASAL ERROR:] unsupported algorithm\n");
+
+    /* grow device buffers as the reference does (src/gasal_align.cu:70-145) */
+    if (s->gpu_max_query_batch_bytes < qbytes) {
+        uint32_t k = 2;
+        while (s->gpu_max_query_batch_bytes * k < qbytes) k++;
+        fprintf(stderr, "[GASAL WARNING:] actual_query_batch_bytes(%d) > Allocated GPU memory (gpu_max_query_batch_bytes=%d). Therefore, allocating %d bytes on GPU (gpu_max_query_batch_bytes=%d). Performance may be lost if this is repeated many times.\n",
+                qbytes, s->gpu_max_query_batch_bytes, s->gpu_max_query_batch_bytes * k, s->gpu_max_query_batch_bytes * k);
+        const uint32_t nb = s->gpu_max_query_batch_bytes * k;
+        const bool aliased = (void *)s->packed_query_batch == (void *)s->unpacked_query_batch;
+        if (grow_dev((void **)&s->unpacked_query_batch, 0, nb) != GB_OK) return E.fail(GB_ERR_ALLOC, "[GASAL ERROR:] allocation failed\n");
+        if (aliased) s->packed_query_batch = (uint32_t *)s->unpacked_query_batch;
+        else if (grow_dev((void **)&s->packed_query_batch, 0, (nb / 8) * 4) != GB_OK) return E.fail(GB_ERR_ALLOC, "[GASAL ERROR:] allocation failed\n");
+        s->gpu_max_query_batch_bytes = nb;
+        if (params->start_pos == WITH_TB) {
+            if (s->host_res->cigar) cudaFreeHost(s->host_res->cigar);
+            if (cudaHostAlloc(&s->host_res->cigar, nb, cudaHostAllocDefault) != cudaSuccess)
+                return E.fail(GB_ERR_ALLOC, "[GASAL ERROR:] allocation failed\n");
+        }
+    }
+    if (s->gpu_max_target_batch_bytes < tbytes) {
+        uint32_t k = 2;
+        while (s->gpu_max_target_batch_bytes * k < tbytes) k++;
+        fprintf(stderr, "[GASAL WARNING:] actual_target_batch_bytes(%d) > Allocated GPU memory (gpu_max_target_batch_bytes=%d). Therefore, allocating %d bytes on GPU (gpu_max_target_batch_bytes=%d). Performance may be lost if this is repeated many times.\n",
+                tbytes, s->gpu_max_target_batch_bytes, s->gpu_max_target_batch_bytes * k, s->gpu_max_target_batch_bytes * k);
+        const uint32_t nb = s->gpu_max_target_batch_bytes * k;
+        const bool aliased = (void *)s->packed_target_batch == (void *)s->unpacked_target_batch;
+        if (grow_dev((void **)&s->unpacked_target_batch, 0, nb) != GB_OK) return E.fail(GB_ERR_ALLOC, "[GASAL ERROR:] allocation failed\n");
+        if (aliased) s->packed_target_batch = (uint32_t *)s->unpacked_target_batch;
+        else if (grow_dev((void **)&s->packed_target_batch, 0, (nb / 8) * 4) != GB_OK) return E.fail(GB_ERR_ALLOC, "[GASAL ERROR:] allocation failed\n");
+        s->gpu_max_target_batch_bytes = nb;
+    }
+    if (s->gpu_max_n_alns < n) {
+        uint32_t k = 2;
+        while (s->gpu_max_n_alns * k < n) k++;
+        fprintf(stderr, "[GASAL WARNING:] actual_n_alns(%d) > gpu_max_n_alns(%d). Therefore, allocating memory for %d alignments on  GPU (gpu_max_n_alns=%d). Performance may be lost if this is repeated many times.\n",
+                n, s->gpu_max_n_alns, s->gpu_max_n_alns * k, s->gpu_max_n_alns * k);
+        const uint32_t nn = s->gpu_max_n_alns * k;
+        void **arrs[] = {(void **)&s->query_batch_offsets, (void **)&s->target_batch_offsets,
+                         (void **)&s->query_batch_lens, (void **)&s->target_batch_lens};
+        for (void **a : arrs)
+            if (grow_dev(a, 0, nn * 4) != GB_OK) return E.fail(GB_ERR_ALLOC, "[GASAL ERROR:] allocation failed\n");
+        if (grow_dev((void **)&s->query_op, 0, nn) != GB_OK || grow_dev((void **)&s->target_op, 0, nn) != GB_OK)
+            return E.fail(GB_ERR_ALLOC, "[GASAL ERROR:] allocation failed\n");
+        if (s->seed_scores && grow_dev((void **)&s->seed_scores, 0, nn * 4) != GB_OK)
+            return E.fail(GB_ERR_ALLOC, "[GASAL ERROR:] allocation failed\n");
+        gasal_res_destroy_device(s->device_res, s->device_cpy);
+        s->device_cpy = gasal_res_new_device_cpy(nn, params);
+        s->device_res = gasal_res_new_device(s->device_cpy);
+        if (params->secondBest) {
+            gasal_res_destroy_device(s->device_res_second, s->device_cpy_second);
+            s->device_cpy_second = gasal_res_new_device_cpy(nn, params);
+            s->device_res_second = gasal_res_new_device(s->device_cpy_second);
+        }
+        s->gpu_max_n_alns = nn;
+    }
+    StreamState &ss = state_of(s);
+    if (params->start_pos == WITH_TB && ss.n_cigar_cap < s->gpu_max_n_alns) {
+        if (ss.d_n_cigar) cudaFree(ss.d_n_cigar);
+        ss.d_n_cigar = NULL;
+        if (cudaMalloc(&ss.d_n_cigar, (size_t)s->gpu_max_n_alns * 4) != cudaSuccess)
+            return E.fail(GB_ERR_ALLOC, "[GASAL ERROR:] allocation failed\n");
+        ss.n_cigar_cap = s->gpu_max_n_alns;
+    }
+
+    cudaStream_t st = s->str;
+    cudaError_t ce = cudaSuccess;
+#define GB_Q(call)                                                                                  \
+    do {                                                                                            \
+        ce = (call);                                                                                \
+        if (ce != cudaSuccess) {                                                                    \
+            snprintf(msg, sizeof msg, "[GASAL CUDA ERROR:] %s(CUDA error no.=%d). Line no. %d in file %s\n", \
+                     cudaGetErrorString(ce), ce, __LINE__, __FILE__);                               \
+            return E.fail(GB_ERR_CUDA, msg);                                                        \
+        }                                                                                           \
+    } while (0)
+
+    /* host pages -> device (src/gasal_align.cu:152-175) */
+    for (host_batch_t *p = s->extensible_host_unpacked_query_batch; p; p = p->next)
+        if (p->data_size) GB_Q(cudaMemcpyAsync(s->unpacked_query_batch + p->offset, p->data, p->data_size, cudaMemcpyHostToDevice, st));
+    for (host_batch_t *p = s->extensible_host_unpacked_target_batch; p; p = p->next)
+        if (p->data_size) GB_Q(cudaMemcpyAsync(s->unpacked_target_batch + p->offset, p->data, p->data_size, cudaMemcpyHostToDevice, st));
+    GB_Q(cudaMemcpyAsync(s->query_batch_lens, s->host_query_batch_lens, n * 4, cudaMemcpyHostToDevice, st));
+    GB_Q(cudaMemcpyAsync(s->target_batch_lens, s->host_target_batch_lens, n * 4, cudaMemcpyHostToDevice, st));
+    GB_Q(cudaMemcpyAsync(s->query_batch_offsets, s->host_query_batch_offsets, n * 4, cudaMemcpyHostToDevice, st));
+    GB_Q(cudaMemcpyAsync(s->target_batch_offsets, s->host_target_batch_offsets, n * 4, cudaMemcpyHostToDevice, st));
+    if (params->algo == KSW) {
+        if (s->seed_scores == NULL || s->host_seed_scores == NULL) {
+            if (s->seed_scores == NULL) fprintf(stderr, "seed_scores == NULL\n");
+            if (s->host_seed_scores == NULL) fprintf(stderr, "host_seed_scores == NULL\n");
+            return E.fail(GB_ERR_ARG, "");
+        }
+        GB_Q(cudaMemcpyAsync(s->seed_scores, s->host_seed_scores, n * 4, cudaMemcpyHostToDevice, st));
+    }
+    if (params->isReverseComplement) {
+        GB_Q(cudaMemcpyAsync(s->query_op, s->host_query_op, n, cudaMemcpyHostToDevice, st));
+        GB_Q(cudaMemcpyAsync(s->target_op, s->host_target_op, n, cudaMemcpyHostToDevice, st));
+    }
+
+    const gb::Settings &set = gb::settings();
+    gb::RunCfg cfg{};
+    cfg.algo = params->algo, cfg.start = params->start_pos, cfg.second = params->secondBest == TRUE;
+    cfg.head = params->semiglobal_skipping_head, cfg.tail = params->semiglobal_skipping_tail;
+    cfg.k_band = params->k_band, cfg.zdrop = 0, cfg.sc = set.sc;
+    cfg.ref_reverse = set.ref_reverse, cfg.mql = set.mql, cfg.is_packed = params->isPacked;
+    cfg.reverse_complement = params->isReverseComplement;
+    gb::DevBatch b{};
+    b.n = (int32_t)n, b.q_bytes = qbytes, b.t_bytes = tbytes;
+    b.q = s->unpacked_query_batch, b.t = s->unpacked_target_batch;
+    b.pq = s->packed_query_batch, b.pt = s->packed_target_batch;
+    b.q_off = s->query_batch_offsets, b.t_off = s->target_batch_offsets;
+    b.q_len = s->query_batch_lens, b.t_len = s->target_batch_lens;
+    b.q_op = s->query_op, b.t_op = s->target_op, b.seed = s->seed_scores;
+    b.h_q_len = s->host_query_batch_lens, b.h_t_len = s->host_target_batch_lens;
+    gb::DevOut o{};
+    o.score = s->device_cpy->aln_score, o.q_end = s->device_cpy->query_batch_end;
+    o.t_end = s->device_cpy->target_batch_end, o.q_start = s->device_cpy->query_batch_start;
+    o.t_start = s->device_cpy->target_batch_start;
+    if (params->secondBest && s->device_cpy_second) {
+        o.score2 = s->device_cpy_second->aln_score, o.q_end2 = s->device_cpy_second->query_batch_end;
+        o.t_end2 = s->device_cpy_second->target_batch_end;
+    }
+    o.cigar = s->unpacked_query_batch, o.n_cigar = ss.d_n_cigar;
+    const int rc = gb::run_batch(cfg, b, o, ss.ws, st);
+    if (rc != GB_OK) return E.fail(rc, "[GASAL ERROR:] alignment launch failed\n");
+
+    /* results -> host (src/gasal_align.cu:266-304) */
+    gasal_res_t *h = s->host_res, *d = s->device_cpy;
+    if (h->aln_score && d->aln_score) GB_Q(cudaMemcpyAsync(h->aln_score, d->aln_score, n * 4, cudaMemcpyDeviceToHost, st));
+    if (h->query_batch_start && d->query_batch_start) GB_Q(cudaMemcpyAsync(h->query_batch_start, d->query_batch_start, n * 4, cudaMemcpyDeviceToHost, st));
+    if (h->target_batch_start && d->target_batch_start) GB_Q(cudaMemcpyAsync(h->target_batch_start, d->target_batch_start, n * 4, cudaMemcpyDeviceToHost, st));
+    if (h->query_batch_end && d->query_batch_end) GB_Q(cudaMemcpyAsync(h->query_batch_end, d->query_batch_end, n * 4, cudaMemcpyDeviceToHost, st));
+    if (h->target_batch_end && d->target_batch_end) GB_Q(cudaMemcpyAsync(h->target_batch_end, d->target_batch_end, n * 4, cudaMemcpyDeviceToHost, st));
+    if (params->start_pos == WITH_TB) {
+        if (h->cigar) GB_Q(cudaMemcpyAsync(h->cigar, s->unpacked_query_batch, qbytes, cudaMemcpyDeviceToHost, st));
+        if (h->n_cigar_ops) GB_Q(cudaMemcpyAsync(h->n_cigar_ops, ss.d_n_cigar, n * 4, cudaMemcpyDeviceToHost, st));
+    }
+    if (params->secondBest && s->host_res_second && s->device_cpy_second) {
+        gasal_res_t *h2 = s->host_res_second, *d2 = s->device_cpy_second;
+        if (h2->aln_score && d2->aln_score) GB_Q(cudaMemcpyAsync(h2->aln_score, d2->aln_score, n * 4, cudaMemcpyDeviceToHost, st));
+        if (h2->query_batch_end && d2->query_batch_end) GB_Q(cudaMemcpyAsync(h2->query_batch_end, d2->query_batch_end, n * 4, cudaMemcpyDeviceToHost, st));
+        if (h2->target_batch_end && d2->target_batch_end) GB_Q(cudaMemcpyAsync(h2->target_batch_end, d2->target_batch_end, n * 4, cudaMemcpyDeviceToHost, st));
+    }
+#undef GB_Q
+    s->is_free = 0;
+    return GB_OK;
+}
+
+int is_done(gasal_gpu_storage_t *s, bool fatal)
+{
+    if (s->is_free == 1) return -2;
+    const cudaError_t err = cudaStreamQuery(s->str);
+    if (err != cudaSuccess) {
+        if (err == cudaErrorNotReady) return -1;
+        fprintf(stderr, "[GASAL CUDA ERROR:] %s(CUDA error no.=%d). Line no. %d in file %s\n", cudaGetErrorString(err),
+                err, __LINE__, __FILE__);
+        if (fatal) exit(EXIT_FAILURE);
+        return GB_ERR_CUDA;
+    }
+    gasal_host_batch_reset(s);
+    s->is_free = 1;
+    s->current_n_alns = 0;
+    return 0;
+}
+
+} // namespace gbapi
+
+void gasal_aln_async(gasal_gpu_storage_t *gpu_storage, const uint32_t actual_query_batch_bytes,
+                     const uint32_t actual_target_batch_bytes, const uint32_t actual_n_alns, Parameters *params)
+{
+    gbapi::aln_async(gpu_storage, actual_query_batch_bytes, actual_target_batch_bytes, actual_n_alns, params, true);
+}
+
+int gasal_is_aln_async_done(gasal_gpu_storage_t *gpu_storage) { return gbapi::is_done(gpu_storage, true); }

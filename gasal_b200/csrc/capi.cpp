@@ -1,0 +1,334 @@
+/*
+ * capi.cpp -- extern "C" face of the library (declared in
+ * include/gasal_b200_capi.h).  Thin: every gasal_c_* call forwards to the C++
+ * API implementation with errors returned instead of terminating.
+ */
+#include "gasal_header.h"
+#include "res.h"
+#include "gasal_b200_capi.h"
+#include "engine.h"
+
+#include <cstring>
+#include <mutex>
+#include <unordered_map>
+#include <vector>
+
+namespace gbapi {
+int aln_async(gasal_gpu_storage_t *s, uint32_t qbytes, uint32_t tbytes, uint32_t n, Parameters *params, bool fatal);
+int is_done(gasal_gpu_storage_t *s, bool fatal);
+}
+
+static Parameters *P(void *p) { return static_cast<Parameters *>(p); }
+static gasal_gpu_storage_t *S(void *s) { return static_cast<gasal_gpu_storage_t *>(s); }
+
+extern "C" {
+
+void *gasal_c_params_new(void) { return new Parameters(0, nullptr); }
+
+int gasal_c_params_set(void *params, const gb_params_t *p)
+{
+    if (!params || !p) return GB_ERR_ARG;
+    Parameters *q = P(params);
+    q->algo = (algo_type)p->algo;
+    q->start_pos = (comp_start)p->start_pos;
+    q->secondBest = p->second_best ? TRUE : FALSE;
+    q->semiglobal_skipping_head = (data_source)p->head;
+    q->semiglobal_skipping_tail = (data_source)p->tail;
+    q->k_band = p->k_band;
+    q->isReverseComplement = p->reverse_complement != 0;
+    q->sa = p->match, q->sb = p->mismatch, q->gapo = p->gap_open, q->gape = p->gap_extend;
+    return GB_OK;
+}
+
+void gasal_c_params_free(void *params) { delete P(params); }
+
+int gasal_c_copy_subst_scores(int32_t match, int32_t mismatch, int32_t gap_open, int32_t gap_extend)
+{
+    gasal_subst_scores s = {match, mismatch, gap_open, gap_extend};
+    gasal_copy_subst_scores(&s);
+    return GB_OK;
+}
+
+void *gasal_c_init_gpu_storage_v(int n_streams)
+{
+    if (n_streams <= 0) return nullptr;
+    gasal_gpu_storage_v *v = new gasal_gpu_storage_v;
+    *v = gasal_init_gpu_storage_v(n_streams);
+    return v;
+}
+
+int gasal_c_init_streams(void *storage_v, int max_query_len, int max_target_len, int max_n_alns, void *params)
+{
+    if (!storage_v || !params || max_query_len <= 0 || max_target_len <= 0 || max_n_alns <= 0) return GB_ERR_ARG;
+    int dev_count = 0;
+    if (cudaGetDeviceCount(&dev_count) != cudaSuccess || dev_count == 0) {
+        cudaGetLastError();
+        return GB_ERR_CUDA;
+    }
+    gasal_init_streams(static_cast<gasal_gpu_storage_v *>(storage_v), max_query_len, max_target_len, max_n_alns,
+                       P(params));
+    return GB_OK;
+}
+
+int gasal_c_destroy_streams(void *storage_v, void *params)
+{
+    if (!storage_v) return GB_ERR_ARG;
+    gasal_destroy_streams(static_cast<gasal_gpu_storage_v *>(storage_v), P(params));
+    return GB_OK;
+}
+
+int gasal_c_destroy_gpu_storage_v(void *storage_v)
+{
+    if (!storage_v) return GB_ERR_ARG;
+    gasal_gpu_storage_v *v = static_cast<gasal_gpu_storage_v *>(storage_v);
+    gasal_destroy_gpu_storage_v(v);
+    delete v;
+    return GB_OK;
+}
+
+void *gasal_c_storage(void *storage_v, int i)
+{
+    gasal_gpu_storage_v *v = static_cast<gasal_gpu_storage_v *>(storage_v);
+    if (!v || i < 0 || i >= v->n) return nullptr;
+    return &v->a[i];
+}
+
+int gasal_c_storage_view(void *storage, gb_storage_view_t *w)
+{
+    if (!storage || !w) return GB_ERR_ARG;
+    gasal_gpu_storage_t *s = S(storage);
+    memset(w, 0, sizeof(*w));
+    w->host_query_batch_offsets = s->host_query_batch_offsets;
+    w->host_target_batch_offsets = s->host_target_batch_offsets;
+    w->host_query_batch_lens = s->host_query_batch_lens;
+    w->host_target_batch_lens = s->host_target_batch_lens;
+    w->host_query_op = s->host_query_op;
+    w->host_target_op = s->host_target_op;
+    w->host_seed_scores = s->host_seed_scores;
+    if (s->host_res) {
+        w->aln_score = s->host_res->aln_score;
+        w->query_batch_end = s->host_res->query_batch_end;
+        w->target_batch_end = s->host_res->target_batch_end;
+        w->query_batch_start = s->host_res->query_batch_start;
+        w->target_batch_start = s->host_res->target_batch_start;
+        w->cigar = s->host_res->cigar;
+        w->n_cigar_ops = s->host_res->n_cigar_ops;
+    }
+    if (s->host_res_second) {
+        w->aln_score2 = s->host_res_second->aln_score;
+        w->query_batch_end2 = s->host_res_second->query_batch_end;
+        w->target_batch_end2 = s->host_res_second->target_batch_end;
+    }
+    w->stream = (void *)s->str;
+    w->host_max_n_alns = s->host_max_n_alns;
+    w->host_max_query_batch_bytes = s->host_max_query_batch_bytes;
+    w->host_max_target_batch_bytes = s->host_max_target_batch_bytes;
+    return GB_OK;
+}
+
+uint32_t gasal_c_host_batch_fill(void *storage, uint32_t idx, const char *data, uint32_t size, int src)
+{
+    return gasal_host_batch_fill(S(storage), idx, data, size, (data_source)src);
+}
+
+uint32_t gasal_c_host_batch_add(void *storage, uint32_t idx, const char *data, uint32_t size, int src)
+{
+    return gasal_host_batch_add(S(storage), idx, data, size, (data_source)src);
+}
+
+int gasal_c_host_batch_reset(void *storage)
+{
+    if (!storage) return GB_ERR_ARG;
+    gasal_host_batch_reset(S(storage));
+    return GB_OK;
+}
+
+int gasal_c_op_fill(void *storage, const uint8_t *ops, uint32_t n, int src)
+{
+    if (!storage || !ops || (src != QUERY && src != TARGET) || n > S(storage)->host_max_n_alns) return GB_ERR_ARG;
+    gasal_op_fill(S(storage), const_cast<uint8_t *>(ops), n, (data_source)src);
+    return GB_OK;
+}
+
+int gasal_c_host_alns_resize(void *storage, int new_max_alns, void *params)
+{
+    if (!storage || !params || new_max_alns < (int)S(storage)->host_max_n_alns) return GB_ERR_ARG;
+    gasal_host_alns_resize(S(storage), new_max_alns, P(params));
+    return GB_OK;
+}
+
+int gasal_c_set_device(int gpu)
+{
+    return cudaSetDevice(gpu) == cudaSuccess ? GB_OK : GB_ERR_CUDA;
+}
+
+int gasal_c_aln_async(void *storage, uint32_t qb, uint32_t tb, uint32_t n, void *params)
+{
+    if (!storage || !params) return GB_ERR_ARG;
+    return gbapi::aln_async(S(storage), qb, tb, n, P(params), false);
+}
+
+int gasal_c_is_aln_async_done(void *storage)
+{
+    if (!storage) return GB_ERR_ARG;
+    return gbapi::is_done(S(storage), false);
+}
+
+int gb_align(const gb_params_t *p, const gb_batch_t *b, gb_out_t *o)
+{
+    if (!p || !b || !o || b->n <= 0 || (b->q_bytes & 7) || (b->t_bytes & 7)) return GB_ERR_ARG;
+    int dev_count = 0;
+    if (cudaGetDeviceCount(&dev_count) != cudaSuccess || dev_count == 0) {
+        cudaGetLastError();
+        return GB_ERR_CUDA;
+    }
+    const int n = b->n;
+    uint32_t max_q = 8, max_t = 8;
+    for (int i = 0; i < n; i++) {
+        if (b->q_len[i] > max_q) max_q = b->q_len[i];
+        if (b->t_len[i] > max_t) max_t = b->t_len[i];
+        if ((b->q_off[i] & 7) || (b->t_off[i] & 7) || b->q_off[i] + b->q_len[i] > b->q_bytes ||
+            b->t_off[i] + b->t_len[i] > b->t_bytes)
+            return GB_ERR_ARG;
+    }
+    gb::Settings &set = gb::settings();
+    const gb::Scores saved = set.sc;
+    gasal_c_copy_subst_scores(p->match, p->mismatch, p->gap_open, p->gap_extend);
+    Parameters params(0, nullptr);
+    gasal_c_params_set(&params, p);
+    gasal_gpu_storage_v v = gasal_init_gpu_storage_v(1);
+    /* size the host staging for the batch as laid out by the caller */
+    const uint32_t per_q = (b->q_bytes + n - 1) / n, per_t = (b->t_bytes + n - 1) / n;
+    gasal_init_streams(&v, (int)std::max(per_q, max_q), (int)std::max(per_t, max_t), n, &params);
+    gasal_gpu_storage_t *s = &v.a[0];
+    /* stage exactly the caller's bytes and offsets */
+    uint32_t qi = gasal_host_batch_add(s, 0, (const char *)b->q, b->q_bytes, QUERY);
+    uint32_t ti = gasal_host_batch_add(s, 0, (const char *)b->t, b->t_bytes, TARGET);
+    s->extensible_host_unpacked_query_batch->data_size = qi;
+    s->extensible_host_unpacked_target_batch->data_size = ti;
+    memcpy(s->host_query_batch_offsets, b->q_off, n * 4);
+    memcpy(s->host_target_batch_offsets, b->t_off, n * 4);
+    memcpy(s->host_query_batch_lens, b->q_len, n * 4);
+    memcpy(s->host_target_batch_lens, b->t_len, n * 4);
+    if (b->q_op) memcpy(s->host_query_op, b->q_op, n);
+    if (b->t_op) memcpy(s->host_target_op, b->t_op, n);
+    if (p->algo == KSW) {
+        for (int i = 0; i < n; i++) s->host_seed_scores[i] = b->seed ? b->seed[i] : 0u;
+    }
+    s->current_n_alns = n;
+    int rc = gbapi::aln_async(s, b->q_bytes, b->t_bytes, n, &params, false);
+    if (rc == GB_OK) {
+        cudaError_t e = cudaStreamSynchronize(s->str);
+        rc = e == cudaSuccess ? GB_OK : GB_ERR_CUDA;
+    }
+    if (rc == GB_OK) {
+        gasal_res_t *r = s->host_res;
+        if (o->score && r->aln_score) memcpy(o->score, r->aln_score, n * 4);
+        if (o->q_end && r->query_batch_end) memcpy(o->q_end, r->query_batch_end, n * 4);
+        if (o->t_end && r->target_batch_end) memcpy(o->t_end, r->target_batch_end, n * 4);
+        const bool has_start = p->start_pos == WITH_START || (p->start_pos == WITH_TB && p->algo == LOCAL);
+        if (has_start && p->algo != GLOBAL && p->algo != KSW && p->algo != BANDED) {
+            if (o->q_start && r->query_batch_start) memcpy(o->q_start, r->query_batch_start, n * 4);
+            if (o->t_start && r->target_batch_start) memcpy(o->t_start, r->target_batch_start, n * 4);
+        }
+        if (p->start_pos == WITH_TB) {
+            if (o->cigar && r->cigar) memcpy(o->cigar, r->cigar, b->q_bytes);
+            if (o->n_cigar && r->n_cigar_ops) memcpy(o->n_cigar, r->n_cigar_ops, n * 4);
+        }
+        if (p->second_best && s->host_res_second) {
+            gasal_res_t *r2 = s->host_res_second;
+            if (o->score2 && r2->aln_score) memcpy(o->score2, r2->aln_score, n * 4);
+            if (o->q_end2 && r2->query_batch_end) memcpy(o->q_end2, r2->query_batch_end, n * 4);
+            if (o->t_end2 && r2->target_batch_end) memcpy(o->t_end2, r2->target_batch_end, n * 4);
+        }
+        if (o->packed_q) cudaMemcpy(o->packed_q, s->packed_query_batch, (b->q_bytes / 8) * 4, cudaMemcpyDeviceToHost);
+        if (o->packed_t) cudaMemcpy(o->packed_t, s->packed_target_batch, (b->t_bytes / 8) * 4, cudaMemcpyDeviceToHost);
+    }
+    gasal_host_batch_reset(s);
+    gasal_destroy_streams(&v, &params);
+    gasal_destroy_gpu_storage_v(&v);
+    set.sc = saved;
+    return rc;
+}
+
+} // extern "C"
+
+namespace {
+struct DevWs {
+    gb::Workspace ws;
+};
+std::mutex g_dev_mu;
+std::unordered_map<int, DevWs *> g_dev_ws;
+} // namespace
+
+extern "C" int gb_align_dev(const gb_params_t *p, const gb_dev_batch_t *b, const gb_dev_out_t *o, void *stream)
+{
+    if (!p || !b || !o || b->n <= 0 || !b->h_q_len || !b->h_t_len) return GB_ERR_ARG;
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return GB_ERR_CUDA;
+    DevWs *w;
+    {
+        std::lock_guard<std::mutex> lk(g_dev_mu);
+        DevWs *&slot = g_dev_ws[dev];
+        if (!slot) slot = new DevWs();
+        w = slot;
+    }
+    const gb::Settings &set = gb::settings();
+    gb::RunCfg cfg{};
+    cfg.algo = p->algo, cfg.start = p->start_pos, cfg.second = p->second_best != 0;
+    cfg.head = p->head, cfg.tail = p->tail, cfg.k_band = p->k_band, cfg.zdrop = p->zdrop;
+    cfg.sc = {p->match, p->mismatch, p->gap_open, p->gap_extend, p->gap_open + p->gap_extend};
+    cfg.ref_reverse = set.ref_reverse, cfg.mql = set.mql, cfg.is_packed = 0;
+    cfg.reverse_complement = p->reverse_complement;
+    gb::DevBatch db{};
+    db.n = b->n, db.q_bytes = b->q_bytes, db.t_bytes = b->t_bytes, db.q = b->q, db.t = b->t;
+    db.pq = b->pq, db.pt = b->pt, db.q_off = b->q_off, db.t_off = b->t_off, db.q_len = b->q_len;
+    db.t_len = b->t_len, db.q_op = b->q_op, db.t_op = b->t_op, db.seed = b->seed;
+    db.h_q_len = b->h_q_len, db.h_t_len = b->h_t_len;
+    gb::DevOut dout{};
+    dout.score = o->score, dout.q_end = o->q_end, dout.t_end = o->t_end, dout.q_start = o->q_start;
+    dout.t_start = o->t_start, dout.score2 = o->score2, dout.q_end2 = o->q_end2, dout.t_end2 = o->t_end2;
+    dout.cigar = o->cigar, dout.n_cigar = o->n_cigar;
+    std::lock_guard<std::mutex> lk(g_dev_mu);
+    return gb::run_batch(cfg, db, dout, w->ws, (cudaStream_t)stream);
+}
+
+extern "C" int gb_set_reference_reverse(int on)
+{
+    gb::settings().ref_reverse = on ? 1 : 0;
+    return GB_OK;
+}
+
+extern "C" int gb_set_reference_max_query_len(int mql)
+{
+    if (mql <= 0) return GB_ERR_ARG;
+    gb::settings().mql = mql;
+    return GB_OK;
+}
+
+extern "C" int gb_set_tb_budget_mb(int64_t mb)
+{
+    if (mb <= 0) return GB_ERR_ARG;
+    gb::settings().tb_budget_bytes = (size_t)mb << 20;
+    return GB_OK;
+}
+
+extern "C" const char *gb_version(void) { return "gasal-b200 0.1 (sm_100a)"; }
+
+extern "C" int gb_kernel_timing(int on)
+{
+    gb::timing_enable(on != 0);
+    return GB_OK;
+}
+
+extern "C" int gb_kernel_timing_read(double *ms, int64_t *launches)
+{
+    if (!ms || !launches) return GB_ERR_ARG;
+    return gb::timing_read(ms, launches);
+}
+
+extern "C" int gb_probe_int_peak(double *iadd_tops, double *imnmx_tops, double *dpx_tops)
+{
+    if (!iadd_tops || !imnmx_tops || !dpx_tops) return GB_ERR_ARG;
+    return gb::probe_int_peak(iadd_tops, imnmx_tops, dpx_tops) == 0 ? GB_OK : GB_ERR_CUDA;
+}

@@ -1,0 +1,260 @@
+/*
+ * engine.cu -- stream-ordered batch execution (device half of
+ * reference src/gasal_align.cu:180-264).
+ *
+ * Planning is host-side and O(n): the longest query decides where the row
+ * buffers live (shared memory when a block's buffers fit, else a global
+ * scratch sized for the resident grid), and WITH_TB batches are split into
+ * chunks whose traceback tiles fit the tile budget -- the reference sizes one
+ * max_q x max_t matrix per pair, which does not fit HBM for long uneven
+ * batches.  Every chunk runs the DP kernel and then the traceback kernel on
+ * the same stream, reusing one tile buffer.
+ */
+#include "engine.h"
+
+#include <algorithm>
+#include <cstdio>
+#include <cstdlib>
+#include <mutex>
+#include <vector>
+
+namespace gb {
+
+Settings &settings()
+{
+    static Settings s = [] {
+        Settings v;
+        if (const char *e = getenv("GASAL_B200_TB_BUDGET_MB")) v.tb_budget_bytes = (size_t)atoll(e) << 20;
+        if (const char *e = getenv("GASAL_B200_BLOCK")) v.block = atoi(e);
+        return v;
+    }();
+    return s;
+}
+
+/* ---- optional per-kernel timing ---- */
+namespace {
+struct Mark {
+    int kind;
+    cudaEvent_t a, b;
+};
+struct Timing {
+    std::mutex mu;
+    bool on = false;
+    std::vector<Mark> pending;
+    std::vector<cudaEvent_t> pool;
+    cudaEvent_t open[K_KINDS] = {};
+    double ms[K_KINDS] = {};
+    int64_t n[K_KINDS] = {};
+};
+Timing &timing()
+{
+    static Timing t;
+    return t;
+}
+cudaEvent_t take_event(Timing &t)
+{
+    if (!t.pool.empty()) {
+        cudaEvent_t e = t.pool.back();
+        t.pool.pop_back();
+        return e;
+    }
+    cudaEvent_t e = nullptr;
+    cudaEventCreate(&e);
+    return e;
+}
+} // namespace
+
+void timing_enable(bool on)
+{
+    Timing &t = timing();
+    std::lock_guard<std::mutex> lk(t.mu);
+    t.on = on;
+    for (int k = 0; k < K_KINDS; k++) t.ms[k] = 0, t.n[k] = 0;
+}
+
+void timing_mark(int kind, bool start, cudaStream_t s)
+{
+    Timing &t = timing();
+    std::lock_guard<std::mutex> lk(t.mu);
+    if (!t.on) return;
+    cudaEvent_t e = take_event(t);
+    cudaEventRecord(e, s);
+    if (start) {
+        t.open[kind] = e;
+    } else {
+        t.pending.push_back({kind, t.open[kind], e});
+        t.open[kind] = nullptr;
+    }
+}
+
+int timing_read(double ms[K_KINDS], int64_t launches[K_KINDS])
+{
+    Timing &t = timing();
+    std::lock_guard<std::mutex> lk(t.mu);
+    for (Mark &m : t.pending) {
+        if (cudaEventSynchronize(m.b) != cudaSuccess) return GB_ERR_CUDA;
+        float x = 0;
+        cudaEventElapsedTime(&x, m.a, m.b);
+        t.ms[m.kind] += x;
+        t.n[m.kind] += 1;
+        t.pool.push_back(m.a);
+        t.pool.push_back(m.b);
+    }
+    t.pending.clear();
+    for (int k = 0; k < K_KINDS; k++) ms[k] = t.ms[k], launches[k] = t.n[k];
+    return GB_OK;
+}
+
+Workspace::~Workspace()
+{
+    /* device memory is released by the owner (release_workspace) while its
+     * context is current; nothing to do at static destruction time */
+}
+
+static int grow(void **p, size_t *cap, size_t need, size_t elem)
+{
+    if (*cap >= need) return GB_OK;
+    if (*p) cudaFree(*p);
+    *p = nullptr;
+    *cap = 0;
+    size_t want = need + need / 4 + 1024;
+    if (cudaMalloc(p, want * elem) != cudaSuccess) {
+        cudaGetLastError();
+        if (cudaMalloc(p, need * elem) != cudaSuccess) {
+            cudaGetLastError();
+            *p = nullptr;
+            return GB_ERR_ALLOC;
+        }
+        want = need;
+    }
+    *cap = want;
+    return GB_OK;
+}
+
+#define GB_CUDA(call)                                                                                  \
+    do {                                                                                               \
+        cudaError_t e_ = (call);                                                                       \
+        if (e_ != cudaSuccess) {                                                                       \
+            fprintf(stderr, "[GASAL-B200 CUDA ERROR] %s at %s:%d\n", cudaGetErrorString(e_), __FILE__, \
+                    __LINE__);                                                                         \
+            return GB_ERR_CUDA;                                                                        \
+        }                                                                                              \
+    } while (0)
+
+int run_batch(const RunCfg &cfg, const DevBatch &b, const DevOut &o, Workspace &ws, cudaStream_t s)
+{
+    if (b.n <= 0) return GB_ERR_ARG;
+    const Settings &st = settings();
+    const int block = st.block;
+
+    /* ---- pack and reverse/complement ---- */
+    if (!cfg.is_packed) {
+        timing_mark(K_PACK, true, s);
+        GB_CUDA(launch_pack(b.q, b.q_bytes, b.pq, s));
+        timing_mark(K_PACK, false, s);
+        timing_mark(K_PACK, true, s);
+        GB_CUDA(launch_pack(b.t, b.t_bytes, b.pt, s));
+        timing_mark(K_PACK, false, s);
+    }
+    if (cfg.reverse_complement) {
+        timing_mark(K_RC, true, s);
+        GB_CUDA(launch_revcomp(b.pq, b.pt, b.q_off, b.t_off, b.q_len, b.t_len, b.q_op, b.t_op, b.n,
+                               cfg.ref_reverse, s));
+        timing_mark(K_RC, false, s);
+    }
+
+    /* ---- row buffer placement ---- */
+    uint32_t max_q = 0;
+    for (int i = 0; i < b.n; i++) max_q = std::max(max_q, b.h_q_len[i]);
+    const int cols = cfg.algo == KSW_ ? 2 * ((int)max_q + 2) : (int)((max_q + 7) & ~7u);
+    const size_t smem_limit = 160u << 10;
+
+    DpArgs a{};
+    a.pq = b.pq, a.pt = b.pt, a.q_off = b.q_off, a.t_off = b.t_off, a.q_len = b.q_len, a.t_len = b.t_len;
+    a.seed = b.seed, a.order = nullptr, a.n = b.n;
+    a.score = o.score, a.q_end = o.q_end, a.t_end = o.t_end, a.q_start = o.q_start, a.t_start = o.t_start;
+    a.score2 = o.score2, a.q_end2 = o.q_end2, a.t_end2 = o.t_end2;
+    a.sc = cfg.sc, a.head = cfg.head, a.tail = cfg.tail, a.k_band = cfg.k_band, a.zdrop = cfg.zdrop, a.mql = cfg.mql;
+    if ((size_t)cols * block * 4 <= smem_limit) {
+        a.smem_cols = cols;
+    } else {
+        a.smem_cols = 0;
+        const size_t threads = (size_t)dp_scratch_blocks(b.n, block) * block;
+        if (grow((void **)&ws.scratch, &ws.scratch_cap, threads * cols, 4) != GB_OK) return GB_ERR_ALLOC;
+        a.scratch = ws.scratch;
+        a.scratch_cols = (uint32_t)cols;
+    }
+
+    const bool tb = cfg.start == WITH_TB_ && (cfg.algo == LOCAL_ || cfg.algo == GLOBAL_);
+    const int start = (cfg.algo == SEMI_GLOBAL_ && cfg.start == WITH_TB_) ? WITHOUT_START_ : cfg.start;
+    const bool second = cfg.second && (cfg.algo == LOCAL_ || cfg.algo == SEMI_GLOBAL_);
+    if (!tb) {
+        timing_mark(K_DP, true, s);
+        GB_CUDA(launch_dp(cfg.algo, start, second, a, block, cols, s));
+        timing_mark(K_DP, false, s);
+        return GB_OK;
+    }
+
+    /* ---- traceback: chunk pairs so the tiles fit the budget ---- */
+    if (ws.tb_off_free) GB_CUDA(cudaEventSynchronize(ws.tb_off_free));
+    if (ws.tb_off_cap < (size_t)b.n) {
+        if (ws.h_tb_off) cudaFreeHost(ws.h_tb_off);
+        if (ws.d_tb_off) cudaFree(ws.d_tb_off);
+        ws.h_tb_off = nullptr, ws.d_tb_off = nullptr, ws.tb_off_cap = 0;
+        const size_t want = (size_t)b.n + b.n / 4 + 1024;
+        if (cudaMallocHost((void **)&ws.h_tb_off, want * 8) != cudaSuccess ||
+            cudaMalloc((void **)&ws.d_tb_off, want * 8) != cudaSuccess) {
+            cudaGetLastError();
+            return GB_ERR_ALLOC;
+        }
+        ws.tb_off_cap = want;
+    }
+    const uint64_t budget = std::max<uint64_t>(st.tb_budget_bytes / 16, 1);
+    std::vector<int> cut{0};
+    uint64_t run = 0, chunk_max = 0;
+    for (int i = 0; i < b.n; i++) {
+        const uint64_t t = tb_tiles(b.h_q_len[i], b.h_t_len[i]);
+        if (run > 0 && run + t > budget) {
+            chunk_max = std::max(chunk_max, run);
+            cut.push_back(i);
+            run = 0;
+        }
+        ws.h_tb_off[i] = run;
+        run += t;
+    }
+    chunk_max = std::max(chunk_max, run);
+    cut.push_back(b.n);
+    if (grow((void **)&ws.tb, &ws.tb_cap, chunk_max, sizeof(uint4)) != GB_OK) return GB_ERR_ALLOC;
+    GB_CUDA(cudaMemcpyAsync(ws.d_tb_off, ws.h_tb_off, (size_t)b.n * 8, cudaMemcpyHostToDevice, s));
+    if (!ws.tb_off_free) GB_CUDA(cudaEventCreateWithFlags(&ws.tb_off_free, cudaEventDisableTiming));
+    GB_CUDA(cudaEventRecord(ws.tb_off_free, s));
+
+    for (size_t c = 0; c + 1 < cut.size(); c++) {
+        const int p0 = cut[c], p1 = cut[c + 1];
+        DpArgs ca = a;
+        ca.n = p1 - p0;
+        ca.q_off = b.q_off + p0, ca.t_off = b.t_off + p0, ca.q_len = b.q_len + p0, ca.t_len = b.t_len + p0;
+        auto sh = [p0](int32_t *p) { return p ? p + p0 : p; };
+        ca.score = sh(o.score), ca.q_end = sh(o.q_end), ca.t_end = sh(o.t_end);
+        ca.q_start = sh(o.q_start), ca.t_start = sh(o.t_start);
+        ca.score2 = sh(o.score2), ca.q_end2 = sh(o.q_end2), ca.t_end2 = sh(o.t_end2);
+        ca.tb = ws.tb, ca.tb_off = ws.d_tb_off + p0;
+        timing_mark(K_DP, true, s);
+        GB_CUDA(launch_dp(cfg.algo, start, second, ca, block, cols, s));
+        timing_mark(K_DP, false, s);
+        TbArgs t{};
+        t.tb = ws.tb, t.tb_off = ws.d_tb_off + p0;
+        t.q_off = ca.q_off, t.q_len = ca.q_len, t.t_len = ca.t_len;
+        t.score = ca.score, t.q_end = ca.q_end, t.t_end = ca.t_end;
+        t.q_start = ca.q_start, t.t_start = ca.t_start;
+        t.cigar = o.cigar, t.cigar_bytes = b.q_bytes;
+        t.n_cigar = o.n_cigar ? o.n_cigar + p0 : nullptr;
+        t.n = ca.n, t.algo = cfg.algo, t.sc = cfg.sc;
+        timing_mark(K_TB, true, s);
+        GB_CUDA(launch_traceback(t, s));
+        timing_mark(K_TB, false, s);
+    }
+    return GB_OK;
+}
+
+} // namespace gb

@@ -1,0 +1,90 @@
+/*
+ * engine.h -- the batch engine behind both the GASAL2 C++ API and the C ABI.
+ *
+ * One call of run_batch() is the device half of reference
+ * gasal_aln_async (src/gasal_align.cu:180-264): pack -> reverse/complement ->
+ * alignment kernel -> traceback, all stream-ordered on one CUDA stream,
+ * reading inputs already in device memory.  Planning (row-buffer placement,
+ * traceback chunking) uses the host copy of the lengths.
+ */
+#ifndef GB_ENGINE_H
+#define GB_ENGINE_H
+
+#include <cstddef>
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "gb_internal.h"
+#include "gasal_b200_capi.h"
+
+namespace gb {
+
+struct RunCfg {
+    int algo, start, second, head, tail, k_band, zdrop;
+    Scores sc;
+    int ref_reverse; /* reference-identical reversal (default 1) */
+    int mql;         /* reference MAX_QUERY_LEN for the semi-global last-row scan */
+    int is_packed;   /* inputs are already 4-bit words */
+    int reverse_complement;
+};
+
+struct DevBatch {
+    int32_t n;
+    uint32_t q_bytes, t_bytes;
+    const uint8_t *q, *t;       /* ASCII (or packed words when is_packed) */
+    uint32_t *pq, *pt;          /* packed word outputs (may equal q/t when is_packed) */
+    const uint32_t *q_off, *t_off, *q_len, *t_len;
+    const uint8_t *q_op, *t_op;
+    const uint32_t *seed;
+    const uint32_t *h_q_len, *h_t_len; /* host copies, for planning */
+};
+
+struct DevOut {
+    int32_t *score, *q_end, *t_end, *q_start, *t_start, *score2, *q_end2, *t_end2;
+    uint8_t *cigar;             /* device buffer of q_bytes (the query batch) */
+    uint32_t *n_cigar;
+};
+
+/* Device scratch owned by one stream (grown on demand, never shrunk). */
+struct Workspace {
+    int device = -1;
+    uint4 *tb = nullptr;
+    size_t tb_cap = 0;          /* uint4 units */
+    uint64_t *d_tb_off = nullptr, *h_tb_off = nullptr;
+    size_t tb_off_cap = 0;
+    uint32_t *scratch = nullptr;
+    size_t scratch_cap = 0;     /* uint32 units */
+    cudaEvent_t tb_off_free = nullptr;
+    ~Workspace();
+};
+
+/* status codes of gasal_b200_capi.h */
+int run_batch(const RunCfg &cfg, const DevBatch &b, const DevOut &o, Workspace &ws, cudaStream_t s);
+
+/* Traceback tiles of one pair, in uint4 units (two spare tile rows). */
+inline uint64_t tb_tiles(uint32_t qlen, uint32_t tlen)
+{
+    const uint64_t qr = (qlen + 7) >> 3, tr = (tlen + 7) >> 3;
+    return (tr + 2) * 2 * qr;
+}
+
+/* Process-wide settings (set through the C ABI). */
+struct Settings {
+    Scores sc = {1, 4, 6, 1, 7};
+    int ref_reverse = 1;
+    int mql = 2048;
+    size_t tb_budget_bytes = (size_t)16 << 30;
+    int block = 64;
+};
+Settings &settings();
+
+/* Optional per-kernel CUDA-event timing (off by default).  Kinds: */
+enum KernelKind { K_PACK = 0, K_RC = 1, K_DP = 2, K_TB = 3, K_KINDS = 4 };
+void timing_enable(bool on);
+void timing_mark(int kind, bool start, cudaStream_t s);
+int timing_read(double ms[K_KINDS], int64_t launches[K_KINDS]);
+int probe_int_peak(double *iadd, double *imnmx, double *dpx);
+
+} // namespace gb
+
+#endif

@@ -1,0 +1,80 @@
+/*
+ * gb_internal.h -- kernel-side interface of the B200 GASAL2-compatible engine.
+ *
+ * Device data layout (one batch, all in HBM):
+ *   packed query / target words  uint32, 8 bases per word, 4-bit codes, first
+ *                                base in bits 31..28; word offset of pair i is
+ *                                byte_offset[i] >> 3 (GASAL2's layout)
+ *   per-pair lengths, offsets    uint32 [n]
+ *   row-buffer scratch           one uint32 per query column per active
+ *                                thread: H in the low, E in the high 16 bits
+ *                                (int16 each, as the reference's short2)
+ *   traceback tiles              uint4 per 8 target rows x 4 query columns,
+ *                                a 4-bit direction code per cell; pair i owns
+ *                                (tregs+2) x 2*qregs tiles from tb_off[i]
+ */
+#ifndef GB_INTERNAL_H
+#define GB_INTERNAL_H
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace gb {
+
+enum Algo { GLOBAL_ = 1, SEMI_GLOBAL_ = 2, LOCAL_ = 3, BANDED_ = 5, KSW_ = 6 };
+enum Start { WITHOUT_START_ = 0, WITH_START_ = 1, WITH_TB_ = 2 };
+enum Src { NONE_ = 0, QUERY_ = 1, TARGET_ = 2, BOTH_ = 3 };
+
+struct Scores {
+    int32_t match, mismatch, o, e, oe;
+};
+
+/* Everything a DP launch reads and writes.  Passed by value (kernel
+ * parameter space). */
+struct DpArgs {
+    const uint32_t *pq, *pt;            /* packed words */
+    const uint32_t *q_off, *t_off;      /* byte offsets */
+    const uint32_t *q_len, *t_len;
+    const uint32_t *seed;               /* ksw h0 */
+    const uint32_t *order;              /* pair visiting order, or null */
+    int32_t n;
+    int32_t *score, *q_end, *t_end, *q_start, *t_start;
+    int32_t *score2, *q_end2, *t_end2;
+    uint4 *tb;                          /* traceback tiles */
+    const uint64_t *tb_off;             /* per pair, in uint4 units */
+    uint32_t *scratch;                  /* global row buffers (when not in shared memory) */
+    uint32_t scratch_cols;              /* columns per thread in scratch */
+    Scores sc;
+    int32_t head, tail, k_band, zdrop, mql;
+    int32_t smem_cols;                  /* columns per thread held in shared memory (0 = use scratch) */
+};
+
+struct TbArgs {
+    const uint4 *tb;
+    const uint64_t *tb_off;
+    const uint32_t *q_off, *q_len, *t_len;
+    const int32_t *score, *q_end, *t_end;
+    int32_t *q_start, *t_start;
+    uint8_t *cigar;                     /* = the device query batch, as in GASAL2 */
+    uint32_t cigar_bytes;
+    uint32_t *n_cigar;
+    int32_t n;
+    int32_t algo;
+    Scores sc;
+};
+
+/* ---- launchers (stream-ordered, no allocation) ---- */
+cudaError_t launch_pack(const uint8_t *ascii, uint32_t nbytes, uint32_t *words, cudaStream_t s);
+cudaError_t launch_revcomp(uint32_t *pq, uint32_t *pt, const uint32_t *q_off, const uint32_t *t_off,
+                           const uint32_t *q_len, const uint32_t *t_len, const uint8_t *q_op,
+                           const uint8_t *t_op, int32_t n, int ref_reverse, cudaStream_t s);
+cudaError_t launch_dp(int algo, int start, bool second, const DpArgs &a, int block, int max_q8,
+                      cudaStream_t s);
+cudaError_t launch_traceback(const TbArgs &a, cudaStream_t s);
+
+int dp_block_size();
+int dp_scratch_blocks(int n, int block);
+
+} // namespace gb
+
+#endif

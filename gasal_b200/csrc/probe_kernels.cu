@@ -1,0 +1,76 @@
+/*
+ * probe_kernels.cu -- measures the integer throughput the DP kernels are
+ * bounded by, on the GPU the library runs on, so roofline fractions are taken
+ * against this box's own numbers.
+ *
+ *   iadd    2-input 32-bit add (issues at the full 128 lanes/clk/SM)
+ *   imnmx   32-bit max (the ALU class that max, select, compare and the DPX
+ *           max / add-max instructions share)
+ *   dpx     __viaddmax_s32, the fused add-then-max the cell update uses
+ * Each thread runs 8 interleaved dependency chains so the pipes stay full;
+ * the grid is 8 blocks of 256 threads per SM.
+ */
+#include "gb_internal.h"
+
+namespace gb {
+
+template <int OP>
+__global__ void __launch_bounds__(256) probe_kernel(uint32_t *out, uint32_t s0, uint32_t s1, int iters)
+{
+    uint32_t acc[8];
+#pragma unroll
+    for (int k = 0; k < 8; k++) acc[k] = s0 * (threadIdx.x + k) + s1 * k;
+    for (int it = 0; it < iters; it++) {
+#pragma unroll
+        for (int k = 0; k < 8; k++) {
+            const uint32_t a = acc[k], b = acc[(k + 1) & 7], c = acc[(k + 3) & 7];
+            if (OP == 0) acc[k] = a + b;
+            if (OP == 1) acc[k] = (uint32_t)max((int)a, (int)b);
+            if (OP == 2) acc[k] = (uint32_t)__viaddmax_s32((int)a, (int)b, (int)c);
+        }
+    }
+    uint32_t r = 0;
+#pragma unroll
+    for (int k = 0; k < 8; k++) r ^= acc[k];
+    if (r == 0x9E3779B9u) out[0] = r; /* keeps the chains live */
+}
+
+template <int OP>
+static double run_probe(uint32_t *d, cudaStream_t s)
+{
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const int blocks = sms * 8, threads = 256, iters = 4096, reps = 5;
+    cudaEvent_t a, b;
+    cudaEventCreate(&a);
+    cudaEventCreate(&b);
+    probe_kernel<OP><<<blocks, threads, 0, s>>>(d, 3, 5, iters);
+    cudaEventRecord(a, s);
+    for (int r = 0; r < reps; r++) probe_kernel<OP><<<blocks, threads, 0, s>>>(d, 3, 5, iters);
+    cudaEventRecord(b, s);
+    cudaEventSynchronize(b);
+    float ms = 0;
+    cudaEventElapsedTime(&ms, a, b);
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    const double ops = (double)blocks * threads * iters * 8 * reps;
+    return ops / (ms * 1e-3) / 1e12;
+}
+
+int probe_int_peak(double *iadd, double *imnmx, double *dpx)
+{
+    uint32_t *d = nullptr;
+    if (cudaMalloc(&d, 256) != cudaSuccess) return -2;
+    cudaStream_t s;
+    cudaStreamCreate(&s);
+    *iadd = run_probe<0>(d, s);
+    *imnmx = run_probe<1>(d, s);
+    *dpx = run_probe<2>(d, s);
+    const cudaError_t e = cudaStreamSynchronize(s);
+    cudaStreamDestroy(s);
+    cudaFree(d);
+    return e == cudaSuccess ? 0 : -2;
+}
+
+} // namespace gb

@@ -1,0 +1,296 @@
+"""Python binding of libgasal_b200.so (the C ABI of include/gasal_b200_capi.h).
+
+This module is the host-side mirror of GASAL2's interface for Python callers:
+``Streams`` wraps the storage API (gasal_init_streams, gasal_host_batch_fill,
+gasal_op_fill, gasal_aln_async, gasal_is_aln_async_done -- reference
+src/ctors.h, src/host_batch.h, src/interfaces.h, src/gasal_align.h) and
+``align`` is the one-shot batch call.  The library is compiled CUDA for
+sm_100a; there is no CPU path, and every call raises if the shared library is
+missing or returns an error.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from typing import Optional
+
+import numpy as np
+
+from .capi import (Batch, GbBatch, GbOut, GbParams, Outputs, Params, GB_STATUS, KSW, WITH_TB, QUERY,
+                   TARGET, _ptr)
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libgasal_b200.so")
+_lib = None
+
+
+class GasalError(RuntimeError):
+    pass
+
+
+def build(quiet: bool = True) -> str:
+    """Compile the CUDA library in place (nvcc, sm_100a)."""
+    import subprocess
+    subprocess.run(["make", "-C", os.path.join(HERE, "csrc"), "-j8"], check=True,
+                   stdout=subprocess.DEVNULL if quiet else None)
+    return LIB_PATH
+
+
+class GbDevBatch(C.Structure):
+    _fields_ = [("n", C.c_int32), ("q_bytes", C.c_uint32), ("t_bytes", C.c_uint32)] + \
+               [(k, C.c_void_p) for k in ("q", "t", "pq", "pt", "q_off", "t_off", "q_len", "t_len", "q_op",
+                                           "t_op", "seed", "h_q_len", "h_t_len")]
+
+
+class GbDevOut(C.Structure):
+    _fields_ = [(k, C.c_void_p) for k in ("score", "q_end", "t_end", "q_start", "t_start", "score2", "q_end2",
+                                           "t_end2", "cigar", "n_cigar")]
+
+
+class GbStorageView(C.Structure):
+    _fields_ = [(k, C.c_void_p) for k in (
+        "host_query_batch_offsets", "host_target_batch_offsets", "host_query_batch_lens",
+        "host_target_batch_lens", "host_query_op", "host_target_op", "host_seed_scores", "aln_score",
+        "query_batch_end", "target_batch_end", "query_batch_start", "target_batch_start", "cigar",
+        "n_cigar_ops", "aln_score2", "query_batch_end2", "target_batch_end2", "stream")] + \
+        [("host_max_n_alns", C.c_uint32), ("host_max_query_batch_bytes", C.c_uint32),
+         ("host_max_target_batch_bytes", C.c_uint32)]
+
+
+# name -> (restype, argtypes)
+SIGNATURES = {
+    "gasal_c_params_new": (C.c_void_p, []),
+    "gasal_c_params_set": (C.c_int, [C.c_void_p, C.POINTER(GbParams)]),
+    "gasal_c_params_free": (None, [C.c_void_p]),
+    "gasal_c_copy_subst_scores": (C.c_int, [C.c_int32] * 4),
+    "gasal_c_init_gpu_storage_v": (C.c_void_p, [C.c_int]),
+    "gasal_c_init_streams": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_void_p]),
+    "gasal_c_destroy_streams": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "gasal_c_destroy_gpu_storage_v": (C.c_int, [C.c_void_p]),
+    "gasal_c_storage": (C.c_void_p, [C.c_void_p, C.c_int]),
+    "gasal_c_storage_view": (C.c_int, [C.c_void_p, C.POINTER(GbStorageView)]),
+    "gasal_c_host_batch_fill": (C.c_uint32, [C.c_void_p, C.c_uint32, C.c_char_p, C.c_uint32, C.c_int]),
+    "gasal_c_host_batch_add": (C.c_uint32, [C.c_void_p, C.c_uint32, C.c_void_p, C.c_uint32, C.c_int]),
+    "gasal_c_host_batch_reset": (C.c_int, [C.c_void_p]),
+    "gasal_c_op_fill": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_int]),
+    "gasal_c_host_alns_resize": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p]),
+    "gasal_c_set_device": (C.c_int, [C.c_int]),
+    "gasal_c_aln_async": (C.c_int, [C.c_void_p, C.c_uint32, C.c_uint32, C.c_uint32, C.c_void_p]),
+    "gasal_c_is_aln_async_done": (C.c_int, [C.c_void_p]),
+    "gb_align": (C.c_int, [C.POINTER(GbParams), C.POINTER(GbBatch), C.POINTER(GbOut)]),
+    "gb_align_dev": (C.c_int, [C.POINTER(GbParams), C.POINTER(GbDevBatch), C.POINTER(GbDevOut), C.c_void_p]),
+    "gb_set_reference_reverse": (C.c_int, [C.c_int]),
+    "gb_set_reference_max_query_len": (C.c_int, [C.c_int]),
+    "gb_set_tb_budget_mb": (C.c_int, [C.c_int64]),
+    "gb_version": (C.c_char_p, []),
+    "gb_kernel_timing": (C.c_int, [C.c_int]),
+    "gb_kernel_timing_read": (C.c_int, [C.POINTER(C.c_double), C.POINTER(C.c_int64)]),
+    "gb_probe_int_peak": (C.c_int, [C.POINTER(C.c_double)] * 3),
+}
+
+
+def lib() -> C.CDLL:
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise GasalError(f"{LIB_PATH} is not built; run gasal_b200.lib.build() (nvcc, sm_100a)")
+        L = C.CDLL(LIB_PATH)
+        for name, (res, args) in SIGNATURES.items():
+            f = getattr(L, name)
+            f.restype = res
+            f.argtypes = args
+        _lib = L
+    return _lib
+
+
+def _check(rc: int, what: str):
+    if rc != 0:
+        raise GasalError(f"{what} failed: {GB_STATUS.get(rc, rc)}")
+
+
+def align(p: Params, b: Batch, want_packed: bool = False) -> Outputs:
+    """Align one batch on the GPU (host buffers in, host buffers out)."""
+    out = Outputs(b, want_packed)
+    cp, cb, co = p.to_c(), b.to_c(), out.to_c()
+    _check(lib().gb_align(C.byref(cp), C.byref(cb), C.byref(co)), "gb_align")
+    return out
+
+
+def set_reference_max_query_len(mql: int):
+    _check(lib().gb_set_reference_max_query_len(int(mql)), "gb_set_reference_max_query_len")
+
+
+def set_reference_reverse(on: bool):
+    _check(lib().gb_set_reference_reverse(1 if on else 0), "gb_set_reference_reverse")
+
+
+def set_tb_budget_mb(mb: int):
+    _check(lib().gb_set_tb_budget_mb(int(mb)), "gb_set_tb_budget_mb")
+
+
+KERNEL_KINDS = ("pack", "revcomp", "dp", "traceback")
+
+
+def kernel_timing(on: bool):
+    _check(lib().gb_kernel_timing(1 if on else 0), "gb_kernel_timing")
+
+
+def kernel_timing_read() -> dict:
+    ms = (C.c_double * 4)()
+    n = (C.c_int64 * 4)()
+    _check(lib().gb_kernel_timing_read(ms, n), "gb_kernel_timing_read")
+    return {k: (ms[i], n[i]) for i, k in enumerate(KERNEL_KINDS)}
+
+
+def probe_int_peak() -> dict:
+    a, b, c = C.c_double(), C.c_double(), C.c_double()
+    _check(lib().gb_probe_int_peak(C.byref(a), C.byref(b), C.byref(c)), "gb_probe_int_peak")
+    return {"iadd_tops": a.value, "imnmx_tops": b.value, "dpx_tops": c.value}
+
+
+def align_dev(p: Params, dev: dict, h_q_len: np.ndarray, h_t_len: np.ndarray, stream_handle: int = 0):
+    """Kernel-level call on device-resident buffers.  ``dev`` maps the
+    gb_dev_batch_t / gb_dev_out_t field names to device addresses (ints)."""
+    b = GbDevBatch()
+    b.n = int(h_q_len.shape[0])
+    b.q_bytes, b.t_bytes = int(dev["q_bytes"]), int(dev["t_bytes"])
+    for k in ("q", "t", "pq", "pt", "q_off", "t_off", "q_len", "t_len", "q_op", "t_op", "seed"):
+        setattr(b, k, dev.get(k))
+    b.h_q_len, b.h_t_len = _ptr(h_q_len), _ptr(h_t_len)
+    o = GbDevOut()
+    for k, _ in GbDevOut._fields_:
+        setattr(o, k, dev.get("out_" + k))
+    cp = p.to_c()
+    _check(lib().gb_align_dev(C.byref(cp), C.byref(b), C.byref(o), C.c_void_p(stream_handle)), "gb_align_dev")
+
+
+class Streams:
+    """GASAL2's stream storage vector: gasal_init_gpu_storage_v +
+    gasal_init_streams (reference src/ctors.cpp:17-128)."""
+
+    def __init__(self, n_streams: int, max_query_len: int, max_target_len: int, max_n_alns: int, params: Params):
+        L = lib()
+        self.params = params
+        self._p = L.gasal_c_params_new()
+        cp = params.to_c()
+        _check(L.gasal_c_params_set(self._p, C.byref(cp)), "gasal_c_params_set")
+        _check(L.gasal_c_copy_subst_scores(params.match, params.mismatch, params.gap_open, params.gap_extend),
+               "gasal_copy_subst_scores")
+        self._v = L.gasal_c_init_gpu_storage_v(n_streams)
+        _check(L.gasal_c_init_streams(self._v, max_query_len, max_target_len, max_n_alns, self._p),
+               "gasal_init_streams")
+        self.n = n_streams
+        self._views = []
+        for i in range(n_streams):
+            v = GbStorageView()
+            _check(L.gasal_c_storage_view(L.gasal_c_storage(self._v, i), C.byref(v)), "gasal_c_storage_view")
+            self._views.append(v)
+
+    def storage(self, i: int):
+        return lib().gasal_c_storage(self._v, i)
+
+    def view(self, i: int) -> GbStorageView:
+        v = GbStorageView()
+        _check(lib().gasal_c_storage_view(self.storage(i), C.byref(v)), "gasal_c_storage_view")
+        return v
+
+    @staticmethod
+    def _arr(ptr, ctype, n):
+        return np.ctypeslib.as_array(C.cast(ptr, C.POINTER(ctype)), shape=(n,))
+
+    def fill(self, i: int, b: Batch):
+        """Stage a batch exactly as GASAL2 callers do: one
+        gasal_host_batch_fill per sequence, then offsets / lengths / ops /
+        seed scores written into the storage's pinned host arrays."""
+        L = lib()
+        s = self.storage(i)
+        v = self.view(i)
+        n = b.n
+        if n > v.host_max_n_alns:
+            raise GasalError("batch larger than max_n_alns")
+        qoff = self._arr(v.host_query_batch_offsets, C.c_uint32, n)
+        toff = self._arr(v.host_target_batch_offsets, C.c_uint32, n)
+        qi = ti = 0
+        qbuf, tbuf = b.q.ctypes.data, b.t.ctypes.data
+        for k in range(n):
+            qoff[k] = qi
+            toff[k] = ti
+            qi = L.gasal_c_host_batch_fill(s, qi, C.c_char_p(qbuf + int(b.q_off[k])), int(b.q_len[k]), QUERY)
+            ti = L.gasal_c_host_batch_fill(s, ti, C.c_char_p(tbuf + int(b.t_off[k])), int(b.t_len[k]), TARGET)
+        self._arr(v.host_query_batch_lens, C.c_uint32, n)[:] = b.q_len
+        self._arr(v.host_target_batch_lens, C.c_uint32, n)[:] = b.t_len
+        zeros = np.zeros(n, dtype=np.uint8)
+        _check(L.gasal_c_op_fill(s, _ptr(b.q_op if b.q_op is not None else zeros), n, QUERY), "gasal_op_fill")
+        _check(L.gasal_c_op_fill(s, _ptr(b.t_op if b.t_op is not None else zeros), n, TARGET), "gasal_op_fill")
+        if self.params.algo == KSW:
+            self._arr(v.host_seed_scores, C.c_uint32, n)[:] = b.seed if b.seed is not None else 0
+        return qi, ti
+
+    def fill_fast(self, i: int, b: Batch):
+        """Stage a batch whose layout already is GASAL2's (padded, offsets
+        ascending) with two bulk copies instead of one call per sequence."""
+        L = lib()
+        s = self.storage(i)
+        v = self.view(i)
+        n = b.n
+        qi = L.gasal_c_host_batch_add(s, 0, b.q.ctypes.data, int(b.q.shape[0]), QUERY)
+        ti = L.gasal_c_host_batch_add(s, 0, b.t.ctypes.data, int(b.t.shape[0]), TARGET)
+        self._arr(v.host_query_batch_offsets, C.c_uint32, n)[:] = b.q_off
+        self._arr(v.host_target_batch_offsets, C.c_uint32, n)[:] = b.t_off
+        self._arr(v.host_query_batch_lens, C.c_uint32, n)[:] = b.q_len
+        self._arr(v.host_target_batch_lens, C.c_uint32, n)[:] = b.t_len
+        zeros = np.zeros(n, dtype=np.uint8)
+        _check(L.gasal_c_op_fill(s, _ptr(b.q_op if b.q_op is not None else zeros), n, QUERY), "gasal_op_fill")
+        _check(L.gasal_c_op_fill(s, _ptr(b.t_op if b.t_op is not None else zeros), n, TARGET), "gasal_op_fill")
+        if self.params.algo == KSW:
+            self._arr(v.host_seed_scores, C.c_uint32, n)[:] = b.seed if b.seed is not None else 0
+        return qi, ti
+
+    def aln_async(self, i: int, qbytes: int, tbytes: int, n: int):
+        _check(lib().gasal_c_aln_async(self.storage(i), qbytes, tbytes, n, self._p), "gasal_aln_async")
+
+    def is_done(self, i: int) -> int:
+        rc = lib().gasal_c_is_aln_async_done(self.storage(i))
+        if rc not in (0, -1, -2):
+            raise GasalError(f"gasal_is_aln_async_done: {GB_STATUS.get(rc, rc)}")
+        return rc
+
+    def wait(self, i: int):
+        while self.is_done(i) == -1:
+            pass
+
+    def results(self, i: int, n: int, b: Optional[Batch] = None) -> dict:
+        v = self.view(i)
+        p = self.params
+        d = {}
+        def get(name, ptr, ct=C.c_int32):
+            if ptr:
+                d[name] = self._arr(ptr, ct, n).copy()
+        get("score", v.aln_score)
+        get("q_end", v.query_batch_end)
+        get("t_end", v.target_batch_end)
+        get("q_start", v.query_batch_start)
+        get("t_start", v.target_batch_start)
+        if p.second_best:
+            get("score2", v.aln_score2)
+            get("q_end2", v.query_batch_end2)
+            get("t_end2", v.target_batch_end2)
+        if p.start_pos == WITH_TB:
+            get("n_cigar", v.n_cigar_ops, C.c_uint32)
+            if b is not None and v.cigar:
+                d["cigar"] = self._arr(v.cigar, C.c_uint8, int(b.q.shape[0])).copy()
+        return d
+
+    def close(self):
+        if self._v:
+            L = lib()
+            L.gasal_c_destroy_streams(self._v, self._p)
+            L.gasal_c_destroy_gpu_storage_v(self._v)
+            L.gasal_c_params_free(self._p)
+            self._v = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()

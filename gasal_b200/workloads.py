@@ -17,7 +17,7 @@ SEED_BASE = 20261203
 
 
 def _random_bases(rng, n):
-    return ACGT[rng.integers(0, 4, size=n)]
+    return ACGT[rng.integers(0, 4, size=n, dtype=np.uint8)]
 
 
 def _stage_flat(flat: np.ndarray, lens: np.ndarray):
@@ -43,42 +43,46 @@ def mutate(rng, flat: np.ndarray, lens: np.ndarray, sub_rate, ins_rate, del_rate
     independently per position.  Rates may be scalars or per-pair arrays."""
     n = len(lens)
     lens = lens.astype(np.int64)
-    pid = np.repeat(np.arange(n), lens)
-    def per_pos(r):
-        r = np.asarray(r, dtype=np.float64)
-        return r[pid] if r.ndim else np.full(len(flat), float(r))
-    u = rng.random(len(flat))
-    ps, pi, pd = per_pos(sub_rate), per_pos(ins_rate), per_pos(del_rate)
+    N = len(flat)
+    scalar = all(np.ndim(r) == 0 for r in (sub_rate, ins_rate, del_rate))
+    pid = None if scalar else np.repeat(np.arange(n, dtype=np.int32), lens)
+    u = rng.random(N, dtype=np.float32)
+    if scalar:
+        ps, pi, pd = np.float32(sub_rate), np.float32(ins_rate), np.float32(del_rate)
+    else:
+        ps = np.asarray(sub_rate, dtype=np.float32)[pid]
+        pi = np.asarray(ins_rate, dtype=np.float32)[pid]
+        pd = np.asarray(del_rate, dtype=np.float32)[pid]
     is_sub = u < ps
-    is_ins = (u >= ps) & (u < ps + pi)
-    is_del = (u >= ps + pi) & (u < ps + pi + pd)
+    ins_at = np.nonzero((u >= ps) & (u < ps + pi))[0]
+    del_at = np.nonzero((u >= ps + pi) & (u < ps + pi + pd))[0]
+    del u
     out = flat.copy()
-    # substitution: a different base
-    codes = np.searchsorted(ACGT, out[is_sub])
+    sub_idx = np.nonzero(is_sub)[0]
+    codes = np.searchsorted(ACGT, out[sub_idx])
     codes = np.where(codes < 4, codes, 0)
-    out[is_sub] = ACGT[(codes + rng.integers(1, 4, size=int(is_sub.sum()))) % 4]
-    # deletion: this position and up to max_indel-1 following ones in the same pair
-    keep = np.ones(len(flat), dtype=bool)
-    dl = rng.integers(1, max_indel + 1, size=len(flat))
-    starts_idx = np.nonzero(is_del)[0]
+    out[sub_idx] = ACGT[(codes + rng.integers(1, 4, size=len(sub_idx))) % 4]
+    # pair boundaries: a deletion never crosses into the next pair
+    ends = np.cumsum(lens)
+    keep = np.ones(N, dtype=bool)
+    dl = rng.integers(1, max_indel + 1, size=len(del_at))
+    del_end = np.minimum(del_at + dl, ends[np.searchsorted(ends, del_at, side="right")])
     for k in range(max_indel):
-        idx = starts_idx[dl[starts_idx] > k] + k
-        idx = idx[idx < len(flat)]
-        same = pid[idx] == pid[idx - k] if k else np.ones(len(idx), dtype=bool)
-        keep[idx[same]] = False
+        idx = del_at + k
+        keep[idx[idx < del_end]] = False
     # insertion: after this position, il random bases
-    il = np.where(is_ins, rng.integers(1, max_indel + 1, size=len(flat)), 0)
-    rep = 1 + il
-    rep = np.where(keep, rep, il)  # a deleted base still carries its insertion
+    rep = keep.astype(np.int64)
+    il = rng.integers(1, max_indel + 1, size=len(ins_at))
+    rep[ins_at] += il
     newflat = np.repeat(out, rep)
     first = np.cumsum(rep) - rep
-    is_orig = np.zeros(len(newflat), dtype=bool)
-    is_orig[first[keep]] = True
-    ins_mask = ~is_orig
+    ins_mask = np.ones(len(newflat), dtype=bool)
+    ins_mask[first[keep]] = False
     newflat[ins_mask] = _random_bases(rng, int(ins_mask.sum()))
-    newpid = np.repeat(pid, rep)
-    newlens = np.bincount(newpid, minlength=n).astype(np.int64)
-    return newflat, newlens
+    starts = ends - lens
+    newlens = np.add.reduceat(rep, starts) if N else np.zeros(n, np.int64)
+    newlens = np.where(lens > 0, newlens, 0)
+    return newflat, newlens.astype(np.int64)
 
 
 def _per_pair_slices(flat, lens):

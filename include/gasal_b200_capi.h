@@ -85,6 +85,117 @@ typedef struct {
     uint32_t *packed_t; /* [t_bytes/8] */
 } gb_out_t;
 
+/* ---- device-resident batch (kernel-level entry point) ------------------- */
+typedef struct {
+    int32_t n;
+    uint32_t q_bytes, t_bytes;
+    const uint8_t *q, *t;          /* device: ASCII batches */
+    uint32_t *pq, *pt;             /* device: packed words out [q_bytes/8], [t_bytes/8] */
+    const uint32_t *q_off, *t_off; /* device */
+    const uint32_t *q_len, *t_len; /* device */
+    const uint8_t *q_op, *t_op;    /* device or NULL */
+    const uint32_t *seed;          /* device or NULL */
+    const uint32_t *h_q_len, *h_t_len; /* host copies of the lengths (launch planning) */
+} gb_dev_batch_t;
+
+typedef struct {
+    int32_t *score, *q_end, *t_end, *q_start, *t_start, *score2, *q_end2, *t_end2; /* device or NULL */
+    uint8_t *cigar;     /* device [q_bytes] (may be the ASCII query batch, as GASAL2 does) */
+    uint32_t *n_cigar;  /* device [n] */
+} gb_dev_out_t;
+
+/* ---- host-side arrays of one stream storage, for callers that cannot read
+ *      gasal_gpu_storage_t directly (the C++ API exposes them as members) --- */
+typedef struct {
+    uint32_t *host_query_batch_offsets, *host_target_batch_offsets;
+    uint32_t *host_query_batch_lens, *host_target_batch_lens;
+    uint8_t *host_query_op, *host_target_op;
+    uint32_t *host_seed_scores;
+    int32_t *aln_score, *query_batch_end, *target_batch_end, *query_batch_start, *target_batch_start;
+    uint8_t *cigar;
+    uint32_t *n_cigar_ops;
+    int32_t *aln_score2, *query_batch_end2, *target_batch_end2;
+    void *stream;                  /* cudaStream_t of the storage */
+    uint32_t host_max_n_alns, host_max_query_batch_bytes, host_max_target_batch_bytes;
+} gb_storage_view_t;
+
+/* ==== entry points ======================================================== */
+/* Each gasal_c_* function is the C-linkage twin of the GASAL2 C++ function
+ * named in its comment, with the same meaning; where the reference prints and
+ * exits, these return a gb_status instead. */
+
+/* Parameters object (reference src/args_parser.h:24-68): opaque handle. */
+void *gasal_c_params_new(void);
+int gasal_c_params_set(void *params, const gb_params_t *p);
+void gasal_c_params_free(void *params);
+
+/* gasal_copy_subst_scores, reference src/gasal_align.cu:329 (scores are
+ * process-wide).  Takes match, mismatch, gap_open, gap_extend. */
+int gasal_c_copy_subst_scores(int32_t match, int32_t mismatch, int32_t gap_open, int32_t gap_extend);
+
+/* gasal_init_gpu_storage_v / gasal_init_streams / gasal_destroy_streams /
+ * gasal_destroy_gpu_storage_v, reference src/ctors.h:5-15.  The storage
+ * vector is returned as an opaque handle; gasal_c_storage() gives element i. */
+void *gasal_c_init_gpu_storage_v(int n_streams);
+int gasal_c_init_streams(void *storage_v, int max_query_len, int max_target_len, int max_n_alns, void *params);
+int gasal_c_destroy_streams(void *storage_v, void *params);
+int gasal_c_destroy_gpu_storage_v(void *storage_v);
+void *gasal_c_storage(void *storage_v, int i);
+int gasal_c_storage_view(void *storage, gb_storage_view_t *view);
+
+/* gasal_host_batch_fill / _add / _reset, reference src/host_batch.h:9-17.
+ * src: 1 = QUERY, 2 = TARGET.  Returns the next free byte index. */
+uint32_t gasal_c_host_batch_fill(void *storage, uint32_t idx, const char *data, uint32_t size, int src);
+uint32_t gasal_c_host_batch_add(void *storage, uint32_t idx, const char *data, uint32_t size, int src);
+int gasal_c_host_batch_reset(void *storage);
+
+/* gasal_op_fill / gasal_host_alns_resize / gasal_set_device, reference
+ * src/interfaces.h:9-14. */
+int gasal_c_op_fill(void *storage, const uint8_t *ops, uint32_t n, int src);
+int gasal_c_host_alns_resize(void *storage, int new_max_alns, void *params);
+int gasal_c_set_device(int gpu);
+
+/* gasal_aln_async / gasal_is_aln_async_done, reference
+ * src/gasal_align.h:116-120.  aln_async returns a gb_status; is_done returns
+ * 0 (done), -1 (running), -2 (nothing launched) or GB_ERR_CUDA. */
+int gasal_c_aln_async(void *storage, uint32_t query_batch_bytes, uint32_t target_batch_bytes, uint32_t n_alns,
+                      void *params);
+int gasal_c_is_aln_async_done(void *storage);
+
+/* One-shot convenience over the calls above: copies the batch from host
+ * memory, aligns, and fills every non-NULL output array (synchronous).  No
+ * reference counterpart; it is the sequence test_prog.cpp:264-437 performs. */
+int gb_align(const gb_params_t *p, const gb_batch_t *b, gb_out_t *o);
+
+/* Kernel-level entry point: pack -> reverse/complement -> alignment ->
+ * traceback on inputs already in device memory, queued on `stream`
+ * (a cudaStream_t, NULL = legacy default stream).  Uses a per-device
+ * workspace the library grows on demand.  The device half of
+ * gasal_aln_async (src/gasal_align.cu:180-264). */
+int gb_align_dev(const gb_params_t *p, const gb_dev_batch_t *b, const gb_dev_out_t *o, void *stream);
+
+/* Library settings.
+ * reference_reverse: 1 (default) reverses sequences exactly as the
+ *   reference's sm_100a build does; 0 reverses the real bases only.
+ * reference_max_query_len: the reference build's MAX_QUERY_LEN, which bounds
+ *   the semi-global last-row scan (default 2048).
+ * tb_budget_mb: device memory for traceback tiles per stream (default 16384);
+ *   larger WITH_TB batches run in chunks. */
+int gb_set_reference_reverse(int on);
+int gb_set_reference_max_query_len(int mql);
+int gb_set_tb_budget_mb(int64_t mb);
+const char *gb_version(void);
+
+/* Instrumentation (no reference counterpart).  gb_kernel_timing(1) resets
+ * and starts recording a CUDA event pair around every kernel the library
+ * launches; gb_kernel_timing_read() waits for them and returns, per kind
+ * (0 pack, 1 reverse/complement, 2 alignment DP, 3 traceback), the summed
+ * milliseconds and the number of launches.  gb_probe_int_peak() times the
+ * integer instructions the DP is bound by on the current GPU (tera-ops/s). */
+int gb_kernel_timing(int on);
+int gb_kernel_timing_read(double *ms, int64_t *launches);
+int gb_probe_int_peak(double *iadd_tops, double *imnmx_tops, double *dpx_tops);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1,0 +1,155 @@
+"""CUDA path against the reference's own outputs (golden fixtures) and
+against the oracle on larger seeded workloads.  Everything goes through the C
+ABI (gb_align / the gasal_c_* storage API).  Bit-exact equality is required:
+this is integer and index work."""
+import numpy as np
+import pytest
+
+from gasal_b200 import lib as gl
+from gasal_b200 import workloads as W
+from gasal_b200.capi import (Params, LOCAL, GLOBAL, SEMI_GLOBAL, BANDED, KSW, WITHOUT_START, WITH_START,
+                             WITH_TB, NONE, QUERY, TARGET, BOTH)
+from golden_cases import cases, case_ids
+from oracle.bindings import oracle_align, ORC_ALL
+
+pytestmark = pytest.mark.gpu
+
+ALL = list(cases())
+
+
+@pytest.fixture(scope="module", autouse=True)
+def _settings():
+    gl.set_reference_max_query_len(2048)  # the golden reference build's MAX_QUERY_LEN
+    gl.set_reference_reverse(True)
+    yield
+
+
+def assert_same(got: dict, exp: dict, what: str):
+    for k, v in exp.items():
+        assert k in got, f"{what}: missing {k}"
+        g = got[k]
+        if not np.array_equal(g, v):
+            bad = np.nonzero(g != v)[0]
+            raise AssertionError(f"{what} {k}: {len(bad)} differ, first {bad[:5]}: got {g[bad[:5]]} want {v[bad[:5]]}")
+
+
+@pytest.mark.parametrize("case", ALL, ids=case_ids())
+def test_cuda_matches_reference_golden(case):
+    name, p, b, exp = case
+    o = gl.align(p, b, want_packed=True)
+    got = o.as_dict(p)
+    if name == "rc":
+        got["packed_q"], got["packed_t"] = o.packed_q, o.packed_t
+    assert_same(got, exp, f"{name} {p.key()}")
+
+
+def _vs_oracle(p, b, **kw):
+    o = gl.align(p, b)
+    r = oracle_align(p, b, **kw)
+    assert_same(o.as_dict(p), r.as_dict(p), p.key())
+
+
+def test_workload0_full_size():
+    """Workload 0 at its full size (20,000 pairs, LOCAL WITHOUT_START)."""
+    _vs_oracle(Params(algo=LOCAL), W.workload0())
+
+
+@pytest.mark.parametrize("p", W.WORKLOAD1_PARAMS, ids=lambda p: p.key())
+def test_workload1_shape(p):
+    """Workload 1's three launches on 6,000 pairs each (RC on half)."""
+    parts = W.workload1(18000, seed=99)
+    for pp, bb in parts:
+        if pp.key() == p.key():
+            _vs_oracle(pp, bb)
+
+
+def test_workload2_traceback_chunked():
+    """GLOBAL WITH_TB on uneven 50-1000 bp pairs, with a tiny tile budget so
+    the batch runs in many chunks."""
+    b = W.workload2(1500, seed=7)
+    gl.set_tb_budget_mb(8)
+    try:
+        _vs_oracle(Params(algo=GLOBAL, start_pos=WITH_TB), b)
+    finally:
+        gl.set_tb_budget_mb(16384)
+
+
+def test_local_traceback_and_second_best():
+    b = W.workload0(3000, seed=5)
+    _vs_oracle(Params(algo=LOCAL, start_pos=WITH_TB, second_best=1), b)
+    _vs_oracle(Params(algo=LOCAL, start_pos=WITH_START, second_best=1, match=2, mismatch=3, gap_open=5,
+                      gap_extend=2), b)
+
+
+def test_ksw_long():
+    b = W.workload3(400, seed=8)
+    _vs_oracle(Params(algo=KSW), b)
+
+
+@pytest.mark.parametrize("head", [NONE, QUERY, TARGET, BOTH])
+@pytest.mark.parametrize("tail", [NONE, QUERY, TARGET, BOTH])
+def test_semi_global_variants(head, tail):
+    b = W.workload0(800, seed=head * 4 + tail)
+    _vs_oracle(Params(algo=SEMI_GLOBAL, head=head, tail=tail, second_best=1), b)
+    if tail in (TARGET, NONE):
+        _vs_oracle(Params(algo=SEMI_GLOBAL, head=head, tail=tail, start_pos=WITH_START), b)
+
+
+def test_long_queries_use_global_row_buffer():
+    """Queries long enough that the row buffers leave shared memory."""
+    b = W.workload3(64, seed=9)
+    _vs_oracle(Params(algo=LOCAL, start_pos=WITH_START, second_best=1), b)
+    _vs_oracle(Params(algo=GLOBAL), b)
+
+
+def test_banded():
+    b = W.workload0(1000, seed=10)
+    for k in (8, 24, 64):
+        _vs_oracle(Params(algo=BANDED, k_band=k), b)
+
+
+def test_correct_reverse_mode():
+    """With the reference-compatible reversal off, sequences are truly
+    reverse-complemented; checked against the oracle's same mode."""
+    b = W.workload1(3000, seed=11)[0][1]
+    gl.set_reference_reverse(False)
+    try:
+        p = Params(algo=LOCAL, start_pos=WITH_START, reverse_complement=1)
+        o = gl.align(p, b, want_packed=True)
+        r = oracle_align(p, b, want_packed=True, compat=ORC_ALL & ~1)
+        assert np.array_equal(o.packed_q, r.packed_q)
+        assert_same(o.as_dict(p), r.as_dict(p), "rc-correct")
+    finally:
+        gl.set_reference_reverse(True)
+
+
+def test_streams_api_per_sequence_fill():
+    """The GASAL2 call sequence: init streams, gasal_host_batch_fill per
+    sequence, gasal_op_fill, gasal_aln_async, poll gasal_is_aln_async_done,
+    read host_res -- on two streams in flight at once."""
+    p = Params(algo=LOCAL, start_pos=WITH_START, second_best=1, reverse_complement=1)
+    parts = [W.workload1(2000, seed=12)[0][1], W.workload1(2000, seed=13)[0][1]]
+    with gl.Streams(2, 160, 310, 1000, p) as st:
+        sizes = [st.fill(i, b) for i, b in enumerate(parts)]
+        for i, b in enumerate(parts):
+            st.aln_async(i, sizes[i][0], sizes[i][1], b.n)
+        for i, b in enumerate(parts):
+            st.wait(i)
+            got = st.results(i, b.n, b)
+            exp = oracle_align(p, b).as_dict(p)
+            assert_same(got, exp, f"stream {i}")
+            assert st.is_done(i) == -2  # nothing in flight after completion
+
+
+def test_streams_api_grows_buffers():
+    """A batch larger than the storage was created for is accepted after the
+    host pages chain and device buffers regrow (reference behaviour)."""
+    p = Params(algo=GLOBAL, start_pos=WITH_TB)
+    b = W.workload2(300, seed=14)
+    with gl.Streams(1, 64, 64, 300, p) as st:
+        qi, ti = st.fill(0, b)
+        st.aln_async(0, qi, ti, b.n)
+        st.wait(0)
+        got = st.results(0, b.n, b)
+    exp = oracle_align(p, b).as_dict(p)
+    assert_same(got, exp, "grown")
