@@ -87,6 +87,74 @@ struct Band {
     }
 };
 
+/* PRMT-based substitution lookup.  Base codes fall into classes A C G T N
+ * and "0" (the code the reference's reversal writes); a per-block table in
+ * shared memory holds, for every query code, the 8 signed score bytes against
+ * the classes.  Per band each row gets a byte selector whose upper three
+ * nibbles replicate the selected byte's sign, so one prmt yields the
+ * sign-extended score of a cell.  Pairs holding any other code (IUPAC letters
+ * etc.) use the compare-based Band instead. */
+__device__ __forceinline__ uint32_t prmt(uint32_t a, uint32_t b, uint32_t c)
+{
+    uint32_t d;
+    asm("prmt.b32 %0, %1, %2, %3;" : "=r"(d) : "r"(a), "r"(b), "r"(c));
+    return d;
+}
+
+/* code -> class: 1(A)->0 3(C)->1 7(G)->2 4(T)->3 14(N)->4 0->5, others 6 */
+constexpr uint64_t CLASS_LUT = (5ull << 0) | (0ull << 4) | (6ull << 8) | (1ull << 12) | (3ull << 16) |
+                               (6ull << 20) | (6ull << 24) | (2ull << 28) | (6ull << 32) | (6ull << 36) |
+                               (6ull << 40) | (6ull << 44) | (6ull << 48) | (6ull << 52) | (4ull << 56) |
+                               (6ull << 60);
+constexpr uint32_t PLAIN_CODES = (1u << 0) | (1u << 1) | (1u << 3) | (1u << 4) | (1u << 7) | (1u << 14);
+
+__device__ __forceinline__ uint32_t class_of(uint32_t code) { return (uint32_t)(CLASS_LUT >> (4 * code)) & 15u; }
+
+/* 1 when every code of the words is in PLAIN_CODES */
+__device__ __forceinline__ bool plain_words(const uint32_t *w, int n)
+{
+    uint32_t bad = 0;
+    for (int i = 0; i < n; i++) {
+        const uint32_t x = w[i];
+#pragma unroll
+        for (int k = 0; k < 8; k++) bad |= ~(PLAIN_CODES >> ((x >> (4 * k)) & 15u)) & 1u;
+    }
+    return bad == 0;
+}
+
+/* score table: entry r = 8 score bytes of query code r against the classes */
+__device__ void build_score_table(uint2 *tab, const Scores &sc, bool local)
+{
+    const int rep[8] = {1, 3, 7, 4, 14, 0, 2, 2};
+    for (int r = threadIdx.x; r < 16; r += blockDim.x) {
+        uint32_t lo = 0, hi = 0;
+        for (int j = 0; j < 8; j++) {
+            const int g = rep[j];
+            int v;
+            if (local && (r == 14 || g == 14)) v = 0;
+            else v = (r == g) ? sc.match : -sc.mismatch;
+            if (j >= 6) v = 0;
+            const uint32_t byte = (uint32_t)(v & 0xFF);
+            if (j < 4) lo |= byte << (8 * j);
+            else hi |= byte << (8 * (j - 4));
+        }
+        tab[r] = make_uint2(lo, hi);
+    }
+}
+
+struct FastBand {
+    uint32_t sel[8];
+    __device__ __forceinline__ void load(uint32_t gw)
+    {
+#pragma unroll
+        for (int k = 0; k < 8; k++) {
+            const uint32_t c = class_of((gw >> (28 - 4 * k)) & 15u);
+            sel[k] = c | ((c | 8u) * 0x1110u);
+        }
+    }
+    __device__ __forceinline__ int s(int k, uint2 t) const { return (int)prmt(t.x, t.y, sel[k]); }
+};
+
 struct Res {
     int score, q_end, t_end, q_start, t_start, score2, q_end2, t_end2;
 };
@@ -101,18 +169,53 @@ __device__ __forceinline__ uint32_t dir_nib(int M, int diag, int H, int F, int E
     return d;
 }
 
+/* Scorer policies: Fast = prmt table lookup, Cmp = compares (any code). */
+struct ScFast {
+    FastBand b;
+    const uint2 *tab;
+    uint2 col;
+    __device__ __forceinline__ void band(uint32_t gw, const Scores &, bool) { b.load(gw); }
+    __device__ __forceinline__ void column(int rbase) { col = tab[rbase]; }
+    __device__ __forceinline__ int s(int k) const { return b.s(k, col); }
+};
+struct ScCmp {
+    Band b;
+    bool local;
+    int r;
+    bool rz;
+    __device__ __forceinline__ void band(uint32_t gw, const Scores &sc, bool loc)
+    {
+        local = loc;
+        b.load(gw, sc, loc);
+    }
+    __device__ __forceinline__ void column(int rbase)
+    {
+        r = rbase;
+        rz = local && rbase == N_CODE4;
+    }
+    __device__ __forceinline__ int s(int k) const { return b.s(k, r, rz); }
+};
+
+/* first maximum of a column in sweep order: key = 8*H + (7-k) */
+__device__ __forceinline__ int col_key(const int *key)
+{
+    int m = __vimax3_s32(key[0], key[1], key[2]);
+    m = __vimax3_s32(m, key[3], key[4]);
+    m = __vimax3_s32(m, key[5], key[6]);
+    return max(m, key[7]);
+}
+
 /* =========================== LOCAL ====================================== */
-template <bool SECOND, bool TB>
+template <bool SECOND, bool TB, class SC>
 __device__ void local_fwd(const uint32_t *q, int qregs, const uint32_t *t, int tregs, const Scores &sc,
-                          RowBuf rb, uint4 *tb, Res &r)
+                          RowBuf rb, uint4 *tb, SC scr, Res &r)
 {
     const int q8 = qregs << 3;
     for (int c = 0; c < q8; c++) rb.st(c, 0u);
     int best = 0, brow = 0, bcol = 0;
     int sec = 0, srow = 0, scol = 0, sprev = 0;
     for (int T = 0; T < tregs; T++) {
-        Band bd;
-        bd.load(t[T], sc, true);
+        scr.band(t[T], sc, true);
         int F[8], D[8];
 #pragma unroll
         for (int k = 0; k < 8; k++) F[k] = 0, D[k] = 0;
@@ -122,34 +225,40 @@ __device__ void local_fwd(const uint32_t *q, int qregs, const uint32_t *t, int t
 #pragma unroll
             for (int b = 0; b < 8; b++) {
                 const int c = (j << 3) + b;
-                const int rbase = code(qw, b);
-                const bool rN = rbase == N_CODE4;
+                scr.column(code(qw, b));
                 const uint32_t v = rb.ld(c);
                 const int up0 = sext16(v);
                 int e = hi16(v);
                 const int prev = best;
-                int Hn[8];
+                int Hn[8], key[8];
                 uint32_t dw = 0;
 #pragma unroll
                 for (int k = 0; k < 8; k++) {
-                    const int M = D[k] + bd.s(k, rbase, rN);
+                    const int M = D[k] + scr.s(k);
                     const int H = __vimax3_s32_relu(M, F[k], e);
                     if (TB) dw |= dir_nib(M, D[k], H, F[k], e, sc) << (28 - 4 * k);
                     const int t0 = M - sc.oe;
                     F[k] = __viaddmax_s32(F[k], -sc.e, t0);
                     e = __viaddmax_s32(e, -sc.e, t0);
-                    if (best < H) best = H, brow = (T << 3) + k;
-                    if (SECOND && sec < H && best > H) sec = H, srow = (T << 3) + k;
+                    if (SECOND) {
+                        if (best < H) best = H, brow = (T << 3) + k;
+                        if (sec < H && best > H) sec = H, srow = (T << 3) + k;
+                    } else {
+                        key[k] = (H << 3) + (7 - k);
+                    }
                     Hn[k] = H;
                 }
                 rb.st(c, pack_he(Hn[7], e));
                 D[0] = up0;
 #pragma unroll
                 for (int k = 1; k < 8; k++) D[k] = Hn[k - 1];
-                if (prev < best) bcol = c;
                 if (SECOND) {
+                    if (prev < best) bcol = c;
                     if (sprev < best) scol = c;
                     sprev = max(sec, sprev);
+                } else {
+                    const int ck = col_key(key);
+                    if ((ck >> 3) > best) best = ck >> 3, brow = (T << 3) + 7 - (ck & 7), bcol = c;
                 }
                 if (TB) dir[b] = dw;
             }
@@ -169,8 +278,9 @@ __device__ void local_fwd(const uint32_t *q, int qregs, const uint32_t *t, int t
  * (reference src/kernels/local_kernel_template.h:441-509).  The target row is
  * recorded as the reference does, gidx + k with gidx the original row of the
  * band's first reversed row. */
+template <class SC>
 __device__ void local_start(const uint32_t *q, int qregs, const uint32_t *t, int tregs, const Scores &sc,
-                            RowBuf rb, Res &r)
+                            RowBuf rb, SC scr, Res &r)
 {
     const int rend_reg = min((r.q_end >> 3) + 1, qregs);
     const int gend_reg = min((r.t_end >> 3) + 1, tregs);
@@ -180,8 +290,7 @@ __device__ void local_start(const uint32_t *q, int qregs, const uint32_t *t, int
     for (int c = 0; c < qn; c++) rb.st(c, 0u);
     for (int T = 0; T < gend_reg && best < fwd; T++) {
         const int gidx = (gend_reg << 3) - 1 - (T << 3);
-        Band bd;
-        bd.load(nib_rev(t[gend_reg - 1 - T]), sc, true);
+        scr.band(nib_rev(t[gend_reg - 1 - T]), sc, true);
         int F[8], D[8];
 #pragma unroll
         for (int k = 0; k < 8; k++) F[k] = 0, D[k] = 0;
@@ -191,28 +300,27 @@ __device__ void local_start(const uint32_t *q, int qregs, const uint32_t *t, int
             for (int b = 0; b < 8; b++) {
                 if (best >= fwd) break;
                 const int c = (j << 3) + b;
-                const int rbase = code(qw, b);
-                const bool rN = rbase == N_CODE4;
+                scr.column(code(qw, b));
                 const uint32_t v = rb.ld(c);
                 const int up0 = sext16(v);
                 int e = hi16(v);
-                const int prev = best;
-                int Hn[8];
+                int Hn[8], key[8];
 #pragma unroll
                 for (int k = 0; k < 8; k++) {
-                    const int M = D[k] + bd.s(k, rbase, rN);
+                    const int M = D[k] + scr.s(k);
                     const int H = __vimax3_s32_relu(M, F[k], e);
                     const int t0 = M - sc.oe;
                     F[k] = __viaddmax_s32(F[k], -sc.e, t0);
                     e = __viaddmax_s32(e, -sc.e, t0);
-                    if (best < H) best = H, ys = gidx + k;
+                    key[k] = (H << 3) + (7 - k);
                     Hn[k] = H;
                 }
                 rb.st(c, pack_he(Hn[7], e));
                 D[0] = up0;
 #pragma unroll
                 for (int k = 1; k < 8; k++) D[k] = Hn[k - 1];
-                if (prev < best) xs = qn - 1 - c;
+                const int ck = col_key(key);
+                if ((ck >> 3) > best) best = ck >> 3, ys = gidx + 7 - (ck & 7), xs = qn - 1 - c;
             }
         }
     }
@@ -224,9 +332,9 @@ __device__ void local_start(const uint32_t *q, int qregs, const uint32_t *t, int
  * row buffer starts H(-1,c) = 0, -(o+e*c) with E = MINUS_INF; column 0 of row
  * R has diagonal 0 (R = 0) else -(o+e*R) and F = MINUS_INF; score = H at the
  * last real cell. */
-template <bool TB>
+template <bool TB, class SC>
 __device__ void global_fwd(const uint32_t *q, int qregs, int qlen, const uint32_t *t, int tregs, int tlen,
-                           const Scores &sc, RowBuf rb, uint4 *tb, Res &r)
+                           const Scores &sc, RowBuf rb, uint4 *tb, SC scr, Res &r)
 {
     const int q8 = qregs << 3;
     rb.st(0, pack_he(0, NEG16));
@@ -234,8 +342,7 @@ __device__ void global_fwd(const uint32_t *q, int qregs, int qlen, const uint32_
     const int last_row = tlen - 1 - ((tregs - 1) << 3);
     int score = 0;
     for (int T = 0; T < tregs; T++) {
-        Band bd;
-        bd.load(t[T], sc, false);
+        scr.band(t[T], sc, false);
         int F[8], D[8];
 #pragma unroll
         for (int k = 0; k < 8; k++) {
@@ -249,7 +356,7 @@ __device__ void global_fwd(const uint32_t *q, int qregs, int qlen, const uint32_
 #pragma unroll
             for (int b = 0; b < 8; b++) {
                 const int c = (j << 3) + b;
-                const int rbase = code(qw, b);
+                scr.column(code(qw, b));
                 const uint32_t v = rb.ld(c);
                 const int up0 = sext16(v);
                 int e = hi16(v);
@@ -257,7 +364,7 @@ __device__ void global_fwd(const uint32_t *q, int qregs, int qlen, const uint32_
                 uint32_t dw = 0;
 #pragma unroll
                 for (int k = 0; k < 8; k++) {
-                    const int M = D[k] + bd.s(k, rbase, false);
+                    const int M = D[k] + scr.s(k);
                     const int H = __vimax3_s32(M, F[k], e);
                     if (TB) dw |= dir_nib(M, D[k], H, F[k], e, sc) << (28 - 4 * k);
                     const int t0 = M - sc.oe;
@@ -307,16 +414,15 @@ __device__ void semi_init_rows(int head, int q8, const Scores &sc, RowBuf rb)
 
 /* One sweep over bands T0..tregs-1 of (q, t) as given by the word functions;
  * leaves once acc.best >= stop_at (checked per band and per query word). */
-template <bool SECOND, class QW, class TW>
+template <bool SECOND, class SC, class QW, class TW>
 __device__ void semi_sweep(QW qword, int qregs, int qlen, TW tword, int tregs, int tlen, const Scores &sc,
-                           int head, int tail, int T0, int stop_at, RowBuf rb, SemiAcc &a)
+                           int head, int tail, int T0, int stop_at, RowBuf rb, SC &scr, SemiAcc &a)
 {
     const bool free_head_t = (head == TARGET_ || head == BOTH_);
     const bool free_tail_t = (tail == TARGET_ || tail == BOTH_);
     int R = 0;
     for (int T = T0; T < tregs && a.best < stop_at; T++, R += 8) {
-        Band bd;
-        bd.load(tword(T), sc, true);
+        scr.band(tword(T), sc, true);
         int F[8], D[8], Hc[8];
 #pragma unroll
         for (int k = 0; k < 8; k++) {
@@ -333,8 +439,7 @@ __device__ void semi_sweep(QW qword, int qregs, int qlen, TW tword, int tregs, i
 #pragma unroll
             for (int b = 0; b < 8; b++) {
                 const int c = (j << 3) + b;
-                const int rbase = code(qw, b);
-                const bool rN = rbase == N_CODE4;
+                scr.column(code(qw, b));
                 const uint32_t v = rb.ld(c);
                 const int up0 = sext16(v);
                 int e = hi16(v), up = up0;
@@ -342,7 +447,7 @@ __device__ void semi_sweep(QW qword, int qregs, int qlen, TW tword, int tregs, i
 #pragma unroll
                 for (int k = 0; k < 8; k++) {
                     F[k] = __viaddmax_s32(F[k], -sc.e, Hc[k] - sc.oe);
-                    const int M = D[k] + bd.s(k, rbase, rN);
+                    const int M = D[k] + scr.s(k);
                     e = __viaddmax_s32(e, -sc.e, up - sc.oe);
                     const int H = __vimax3_s32(M, F[k], e);
                     Hn[k] = H;
@@ -382,15 +487,15 @@ __device__ void semi_tail_query(int head, int q8, int qlen, int tlen, int mql, c
     if (SECOND && a.scol != tlen) a.srow = qlen;
 }
 
-template <bool SECOND, bool START>
+template <bool SECOND, bool START, class SC>
 __device__ void semi_global(const uint32_t *q, int qregs, int qlen, const uint32_t *t, int tregs, int tlen,
-                            const Scores &sc, int head, int tail, int mql, RowBuf rb, Res &r)
+                            const Scores &sc, int head, int tail, int mql, RowBuf rb, SC scr, Res &r)
 {
     const int q8 = qregs << 3;
     SemiAcc a = {NEG16, qlen, tlen, NEG16, qlen, tlen};
     semi_init_rows(head, q8, sc, rb);
     semi_sweep<SECOND>([&](int j) { return q[j]; }, qregs, qlen, [&](int T) { return t[T]; }, tregs, tlen, sc,
-                       head, tail, 0, 0x7fffffff, rb, a);
+                       head, tail, 0, 0x7fffffff, rb, scr, a);
     if (tail == QUERY_ || tail == BOTH_) semi_tail_query<SECOND>(head, q8, qlen, tlen, mql, sc, rb, a);
     r.score = a.best, r.t_end = a.brow, r.q_end = a.bcol;
     if (SECOND) r.score2 = a.sec, r.t_end2 = a.srow, r.q_end2 = a.scol;
@@ -406,7 +511,7 @@ __device__ void semi_global(const uint32_t *q, int qregs, int qlen, const uint32
     semi_init_rows(head, q8, sc, rb);
     semi_sweep<false>([&](int j) { return rev_window(q, qlen - 8 - (j << 3)); }, qregs, qlen,
                       [&](int T) { return rev_window(t, tlen - 8 - (T << 3)); }, tregs, tlen, sc, head, tail,
-                      gend_reg, fwd, rb, b);
+                      gend_reg, fwd, rb, scr, b);
     if (tail == QUERY_ || tail == BOTH_) semi_tail_query<false>(head, q8, qlen, tlen, mql, sc, rb, b);
     r.t_start = (tlen - 1) - b.brow;
     r.q_start = (qlen - 1) - b.bcol;
@@ -415,16 +520,16 @@ __device__ void semi_global(const uint32_t *q, int qregs, int qlen, const uint32
 /* =========================== BANDED ===================================== */
 /* Reference src/kernels/banded.h:10-139: local, gaps opened from H, swept
  * per band T over query words max(0,T-k_other+1) .. min(k+T,qregs)-1. */
+template <class SC>
 __device__ void banded(const uint32_t *q, int qregs, const uint32_t *t, int tregs, int kw, const Scores &sc,
-                       RowBuf rb, Res &r)
+                       RowBuf rb, SC scr, Res &r)
 {
     const int q8 = qregs << 3;
     const int k_other = tregs - (qregs - kw);
     for (int c = 0; c < q8; c++) rb.st(c, 0u);
     int best = 0, brow = 0, bcol = 0;
     for (int T = 0; T < tregs; T++) {
-        Band bd;
-        bd.load(t[T], sc, true);
+        scr.band(t[T], sc, true);
         int F[8], D[8], Hc[8];
 #pragma unroll
         for (int k = 0; k < 8; k++) F[k] = 0, D[k] = 0, Hc[k] = 0;
@@ -434,20 +539,18 @@ __device__ void banded(const uint32_t *q, int qregs, const uint32_t *t, int treg
 #pragma unroll
             for (int b = 0; b < 8; b++) {
                 const int c = (j << 3) + b;
-                const int rbase = code(qw, b);
-                const bool rN = rbase == N_CODE4;
+                scr.column(code(qw, b));
                 const uint32_t v = rb.ld(c);
                 const int up0 = sext16(v);
                 int e = hi16(v), up = up0;
-                const int prev = best;
-                int Hn[8];
+                int Hn[8], key[8];
 #pragma unroll
                 for (int k = 0; k < 8; k++) {
                     F[k] = __viaddmax_s32(F[k], -sc.e, Hc[k] - sc.oe);
-                    int H = __vimax3_s32_relu(D[k] + bd.s(k, rbase, rN), F[k], 0);
+                    int H = __vimax3_s32_relu(D[k] + scr.s(k), F[k], 0);
                     e = __viaddmax_s32(e, -sc.e, up - sc.oe);
                     H = max(H, e);
-                    if (best < H) best = H, brow = (T << 3) + k;
+                    key[k] = (H << 3) + (7 - k);
                     Hn[k] = H;
                     up = H;
                 }
@@ -457,7 +560,8 @@ __device__ void banded(const uint32_t *q, int qregs, const uint32_t *t, int treg
                 for (int k = 1; k < 8; k++) D[k] = Hn[k - 1];
 #pragma unroll
                 for (int k = 0; k < 8; k++) Hc[k] = Hn[k];
-                if (prev < best) bcol = c;
+                const int ck = col_key(key);
+                if ((ck >> 3) > best) best = ck >> 3, brow = (T << 3) + 7 - (ck & 7), bcol = c;
             }
         }
     }
@@ -553,10 +657,31 @@ __device__ void ksw(const uint32_t *q, int qlen, const uint32_t *t, int tlen, ui
 }
 
 /* ============================ kernel ==================================== */
+template <int ALGO, int START, bool SECOND, class SC>
+__device__ __forceinline__ void run_pair(const DpArgs &a, const uint32_t *q, int qregs, int qlen, const uint32_t *t,
+                                         int tregs, int tlen, int i, RowBuf rb, uint4 *tb, SC scr, Res &r)
+{
+    if (ALGO == LOCAL_) {
+        local_fwd<SECOND, START == WITH_TB_>(q, qregs, t, tregs, a.sc, rb, tb, scr, r);
+        if (START == WITH_START_) local_start(q, qregs, t, tregs, a.sc, rb, scr, r);
+    } else if (ALGO == GLOBAL_) {
+        global_fwd<START == WITH_TB_>(q, qregs, qlen, t, tregs, tlen, a.sc, rb, tb, scr, r);
+    } else if (ALGO == SEMI_GLOBAL_) {
+        semi_global<SECOND, START == WITH_START_>(q, qregs, qlen, t, tregs, tlen, a.sc, a.head, a.tail, a.mql, rb,
+                                                 scr, r);
+    } else if (ALGO == BANDED_) {
+        banded(q, qregs, t, tregs, a.k_band >> 3, a.sc, rb, scr, r);
+    }
+}
+
 template <int ALGO, int START, bool SECOND, bool SMEM>
 __global__ void __launch_bounds__(128) dp_kernel(DpArgs a)
 {
     extern __shared__ uint32_t smem[];
+    __shared__ uint2 stab[16];
+    build_score_table(stab, a.sc, ALGO != GLOBAL_);
+    __syncthreads();
+    const bool fast_scores = a.sc.match >= -128 && a.sc.match <= 127 && a.sc.mismatch >= -127 && a.sc.mismatch <= 128;
     const uint32_t gtid = blockIdx.x * blockDim.x + threadIdx.x;
     const uint32_t nthr = gridDim.x * blockDim.x;
     RowBuf rb;
@@ -583,18 +708,15 @@ __global__ void __launch_bounds__(128) dp_kernel(DpArgs a)
                 uint4 *z = tb + (size_t)tregs * 2 * qregs;
                 for (int k = 0; k < 4 * qregs; k++) z[k] = make_uint4(0, 0, 0, 0);
             }
-            if (ALGO == LOCAL_) {
-                local_fwd<SECOND, START == WITH_TB_>(q, qregs, t, tregs, a.sc, rb, tb, r);
-                if (START == WITH_START_) local_start(q, qregs, t, tregs, a.sc, rb, r);
-            } else if (ALGO == GLOBAL_) {
-                global_fwd<START == WITH_TB_>(q, qregs, qlen, t, tregs, tlen, a.sc, rb, tb, r);
-            } else if (ALGO == SEMI_GLOBAL_) {
-                semi_global<SECOND, START == WITH_START_>(q, qregs, qlen, t, tregs, tlen, a.sc, a.head, a.tail,
-                                                         a.mql, rb, r);
-            } else if (ALGO == BANDED_) {
-                banded(q, qregs, t, tregs, a.k_band >> 3, a.sc, rb, r);
-            } else if (ALGO == KSW_) {
+            if (ALGO == KSW_) {
                 ksw(q, qlen, t, tlen, a.seed ? a.seed[i] : 0u, a.zdrop, a.sc, rb, r);
+            } else if (fast_scores && plain_words(q, qregs) && plain_words(t, tregs)) {
+                ScFast sf;
+                sf.tab = stab;
+                run_pair<ALGO, START, SECOND>(a, q, qregs, qlen, t, tregs, tlen, i, rb, tb, sf, r);
+            } else {
+                ScCmp scmp{};
+                run_pair<ALGO, START, SECOND>(a, q, qregs, qlen, t, tregs, tlen, i, rb, tb, scmp, r);
             }
         }
         if (a.score) a.score[i] = r.score;
