@@ -229,9 +229,12 @@ __device__ void local_fwd(const uint32_t *q, int qregs, const uint32_t *t, int t
                 const uint32_t v = rb.ld(c);
                 const int up0 = sext16(v);
                 int e = hi16(v);
-                const int prev = best;
                 int Hn[8], key[8];
                 uint32_t dw = 0;
+                /* second best: a cell qualifies when H is below the running
+                 * maximum before it (local_kernel_template.h:145-150); run
+                 * = that running maximum, chained through the column */
+                int run = best, cand[8];
 #pragma unroll
                 for (int k = 0; k < 8; k++) {
                     const int M = D[k] + scr.s(k);
@@ -240,11 +243,11 @@ __device__ void local_fwd(const uint32_t *q, int qregs, const uint32_t *t, int t
                     const int t0 = M - sc.oe;
                     F[k] = __viaddmax_s32(F[k], -sc.e, t0);
                     e = __viaddmax_s32(e, -sc.e, t0);
+                    key[k] = (H << 3) + (7 - k);
                     if (SECOND) {
-                        if (best < H) best = H, brow = (T << 3) + k;
-                        if (sec < H && best > H) sec = H, srow = (T << 3) + k;
-                    } else {
-                        key[k] = (H << 3) + (7 - k);
+                        bool ge;
+                        run = __vibmax_s32(H, run, &ge);
+                        cand[k] = ge ? -1 : key[k];
                     }
                     Hn[k] = H;
                 }
@@ -252,13 +255,13 @@ __device__ void local_fwd(const uint32_t *q, int qregs, const uint32_t *t, int t
                 D[0] = up0;
 #pragma unroll
                 for (int k = 1; k < 8; k++) D[k] = Hn[k - 1];
+                const int ck = col_key(key);
+                if ((ck >> 3) > best) best = ck >> 3, brow = (T << 3) + 7 - (ck & 7), bcol = c;
                 if (SECOND) {
-                    if (prev < best) bcol = c;
+                    const int cs = col_key(cand);
+                    if (cs >= 0 && (cs >> 3) > sec) sec = cs >> 3, srow = (T << 3) + 7 - (cs & 7);
                     if (sprev < best) scol = c;
                     sprev = max(sec, sprev);
-                } else {
-                    const int ck = col_key(key);
-                    if ((ck >> 3) > best) best = ck >> 3, brow = (T << 3) + 7 - (ck & 7), bcol = c;
                 }
                 if (TB) dir[b] = dw;
             }
