@@ -773,6 +773,43 @@ static cudaError_t launch_one(const DpArgs &a, int block, cudaStream_t s)
     return cudaGetLastError();
 }
 
+/* Global-scratch variant on an explicit grid (blocks x block threads must
+ * all fit in a.scratch at a.scratch_cols columns each). */
+template <int ALGO, int START, bool SECOND>
+static cudaError_t launch_scratch_grid(const DpArgs &a, int block, int blocks, cudaStream_t s)
+{
+    dp_kernel<ALGO, START, SECOND, false><<<blocks, block, 0, s>>>(a);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_dp_scratch_grid(int algo, int start, bool second, const DpArgs &a, int block, int blocks,
+                                   cudaStream_t s)
+{
+    if (a.n <= 0) return cudaSuccess;
+    switch (algo) {
+    case LOCAL_:
+        if (start == WITH_START_)
+            return second ? launch_scratch_grid<LOCAL_, WITH_START_, true>(a, block, blocks, s)
+                          : launch_scratch_grid<LOCAL_, WITH_START_, false>(a, block, blocks, s);
+        return second ? launch_scratch_grid<LOCAL_, WITHOUT_START_, true>(a, block, blocks, s)
+                      : launch_scratch_grid<LOCAL_, WITHOUT_START_, false>(a, block, blocks, s);
+    case GLOBAL_:
+        return launch_scratch_grid<GLOBAL_, WITHOUT_START_, false>(a, block, blocks, s);
+    case SEMI_GLOBAL_:
+        if (start == WITH_START_)
+            return second ? launch_scratch_grid<SEMI_GLOBAL_, WITH_START_, true>(a, block, blocks, s)
+                          : launch_scratch_grid<SEMI_GLOBAL_, WITH_START_, false>(a, block, blocks, s);
+        return second ? launch_scratch_grid<SEMI_GLOBAL_, WITHOUT_START_, true>(a, block, blocks, s)
+                      : launch_scratch_grid<SEMI_GLOBAL_, WITHOUT_START_, false>(a, block, blocks, s);
+    case BANDED_:
+        return launch_scratch_grid<BANDED_, WITHOUT_START_, false>(a, block, blocks, s);
+    case KSW_:
+        return launch_scratch_grid<KSW_, WITHOUT_START_, false>(a, block, blocks, s);
+    default:
+        return cudaErrorInvalidValue;
+    }
+}
+
 cudaError_t launch_dp(int algo, int start, bool second, const DpArgs &a, int block, int max_q8, cudaStream_t s)
 {
     (void)max_q8;

@@ -72,6 +72,10 @@ cudaError_t launch_dp(int algo, int start, bool second, const DpArgs &a, int blo
                       cudaStream_t s);
 cudaError_t launch_traceback(const TbArgs &a, cudaStream_t s);
 
+/* the global-scratch DP variant on a caller-chosen grid */
+cudaError_t launch_dp_scratch_grid(int algo, int start, bool second, const DpArgs &a, int block, int blocks,
+                                   cudaStream_t s);
+
 int dp_block_size();
 int dp_scratch_blocks(int n, int block);
 

@@ -79,6 +79,8 @@ SIGNATURES = {
     "gasal_c_is_aln_async_done": (C.c_int, [C.c_void_p]),
     "gb_align": (C.c_int, [C.POINTER(GbParams), C.POINTER(GbBatch), C.POINTER(GbOut)]),
     "gb_align_dev": (C.c_int, [C.POINTER(GbParams), C.POINTER(GbDevBatch), C.POINTER(GbDevOut), C.c_void_p]),
+    "gb_align_dev_noalloc": (C.c_int, [C.POINTER(GbParams), C.POINTER(GbDevBatch), C.POINTER(GbDevOut),
+                                       C.c_void_p]),
     "gb_set_reference_reverse": (C.c_int, [C.c_int]),
     "gb_set_reference_max_query_len": (C.c_int, [C.c_int]),
     "gb_set_tb_budget_mb": (C.c_int, [C.c_int64]),
@@ -148,9 +150,11 @@ def probe_int_peak() -> dict:
     return {"iadd_tops": a.value, "imnmx_tops": b.value, "dpx_tops": c.value}
 
 
-def align_dev(p: Params, dev: dict, h_q_len: np.ndarray, h_t_len: np.ndarray, stream_handle: int = 0):
+def align_dev(p: Params, dev: dict, h_q_len: np.ndarray, h_t_len: np.ndarray, stream_handle: int = 0,
+              noalloc: bool = False):
     """Kernel-level call on device-resident buffers.  ``dev`` maps the
-    gb_dev_batch_t / gb_dev_out_t field names to device addresses (ints)."""
+    gb_dev_batch_t / gb_dev_out_t field names to device addresses (ints).
+    noalloc=True calls gb_align_dev_noalloc, which allocates nothing."""
     b = GbDevBatch()
     b.n = int(h_q_len.shape[0])
     b.q_bytes, b.t_bytes = int(dev["q_bytes"]), int(dev["t_bytes"])
@@ -161,7 +165,12 @@ def align_dev(p: Params, dev: dict, h_q_len: np.ndarray, h_t_len: np.ndarray, st
     for k, _ in GbDevOut._fields_:
         setattr(o, k, dev.get("out_" + k))
     cp = p.to_c()
-    _check(lib().gb_align_dev(C.byref(cp), C.byref(b), C.byref(o), C.c_void_p(stream_handle)), "gb_align_dev")
+    if noalloc:
+        _check(lib().gb_align_dev_noalloc(C.byref(cp), C.byref(b), C.byref(o), C.c_void_p(stream_handle)),
+               "gb_align_dev_noalloc")
+    else:
+        _check(lib().gb_align_dev(C.byref(cp), C.byref(b), C.byref(o), C.c_void_p(stream_handle)),
+               "gb_align_dev")
 
 
 class Streams:

@@ -174,6 +174,17 @@ int gb_align(const gb_params_t *p, const gb_batch_t *b, gb_out_t *o);
  * gasal_aln_async (src/gasal_align.cu:180-264). */
 int gb_align_dev(const gb_params_t *p, const gb_dev_batch_t *b, const gb_dev_out_t *o, void *stream);
 
+/* Allocation-free variant of gb_align_dev, for callers that cannot call
+ * cudaMalloc (inside stream capture, under a device-memory arena, or as a
+ * plugin that must not allocate).  No counterpart in the reference.  The
+ * caller passes every buffer (including pq/pt); the DP row buffers live in a
+ * 32 MiB static device array that each GPU loading the library holds until
+ * exit.  Rejects WITH_TB (GB_ERR_ARG) and batches whose longest query leaves
+ * the array room for fewer than 32 threads (GB_ERR_LIMIT).  Calls share the
+ * array, so calls that overlap on the GPU race.  The first call on a device
+ * resolves the array's address and should precede any stream capture. */
+int gb_align_dev_noalloc(const gb_params_t *p, const gb_dev_batch_t *b, const gb_dev_out_t *o, void *stream);
+
 /* Library settings.
  * reference_reverse: 1 (default) reverses sequences exactly as the
  *   reference's sm_100a build does; 0 reverses the real bases only.
