@@ -56,7 +56,8 @@ def log(*a):
 
 
 class ClockSampler:
-    """nvidia-smi clock / throttle sampling during the timed region."""
+    """nvidia-smi clock / throttle sampling (50 ms) around the timed region;
+    the summary keeps the samples taken between mark_start and mark_end."""
 
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
          "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
@@ -66,11 +67,12 @@ class ClockSampler:
         self.gpu = gpu_index
         self.rows = []
         self.proc = None
+        self.t0 = self.t1 = None
 
     def __enter__(self):
         try:
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.Q}",
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                          "--format=csv,noheader,nounits", "-lms", "50"],
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
@@ -80,7 +82,14 @@ class ClockSampler:
 
     def _read(self):
         for line in self.proc.stdout:
-            self.rows.append([x.strip() for x in line.split(",")])
+            self.rows.append((time.time(), [x.strip() for x in line.split(",")]))
+
+    def mark_start(self):
+        self.t0 = time.time()
+
+    def mark_end(self):
+        self.t1 = time.time()
+        time.sleep(0.12)  # let the sample covering the end arrive
 
     def __exit__(self, *a):
         if self.proc:
@@ -91,14 +100,17 @@ class ClockSampler:
                 self.proc.kill()
 
     def summary(self):
-        if not self.rows:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
-        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
-        mx = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
+        rows = [r for t, r in self.rows if self.t0 is None or (self.t0 - 0.06 <= t <= (self.t1 or t) + 0.06)]
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "samples": 0}
+        num = lambda x: x.replace(".", "").isdigit()
+        sm = [float(r[1]) for r in rows if num(r[1])]
+        mx = [float(r[2]) for r in rows if num(r[2])]
+        pw = [float(r[3]) for r in rows if num(r[3])]
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[i] for r in self.rows for i, v in enumerate(r[5:9]) if v.strip() == "Active"})
+        reasons = sorted({names[i] for r in rows for i, v in enumerate(r[5:9]) if v.strip() == "Active"})
         return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-                "reasons": reasons, "samples": len(self.rows)}
+                "power_w_max": max(pw) if pw else None, "reasons": reasons, "samples": len(rows)}
 
 
 def build_workload(n: int, seed: int):
@@ -162,7 +174,7 @@ def run_reference(args):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--pairs", type=int, default=1_000_000)
@@ -179,9 +191,8 @@ def main():
     import ctypes as C
     from gasal_b200 import lib as gl
 
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    from gasal_b200 import shard
+    rank, world, local_rank = shard.rank_info()
     torch.cuda.set_device(local_rank)
     dist = None
     if world > 1:
@@ -192,7 +203,7 @@ def main():
     gl.lib()
     gl.set_reference_reverse(True)
     peak = gl.probe_int_peak()
-    parts = build_workload(args.pairs, W.SEED_BASE + 1 + 1000 * rank)
+    parts = build_workload(args.pairs, shard.shard_seed(W.SEED_BASE + 1, rank))
     npairs = sum(b.n for _, b in parts)
     dev = torch.device("cuda", local_rank)
 
@@ -226,6 +237,7 @@ def main():
         for p, b, d in dparts:
             gl.align_dev(p, d["map"], b.q_len, b.t_len, stream.cuda_stream)
 
+    clk = ClockSampler(local_rank).__enter__()
     with torch.cuda.stream(stream):
         for _ in range(args.warmup):
             step()
@@ -235,28 +247,26 @@ def main():
     torch.cuda.synchronize()
     gl.kernel_timing(True)
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    with ClockSampler(local_rank) as clk:
-        ev0.record(stream)
-        for _ in range(args.steps):
-            step()
-        ev1.record(stream)
-        torch.cuda.synchronize()
+    clk.mark_start()
+    ev0.record(stream)
+    for _ in range(args.steps):
+        step()
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    clk.mark_end()
+    clk.__exit__()
     kt = gl.kernel_timing_read()
     gl.kernel_timing(False)
-    ms = ev0.elapsed_time(ev1)
+    ms = shard.max_over_ranks(ev0.elapsed_time(ev1), dist, dev)
     if dist:
-        x = torch.tensor([ms], device=dev)
-        dist.all_reduce(x, op=dist.ReduceOp.MAX)
-        ms = float(x.item())
-        if dist:
-            dist.barrier()
+        dist.barrier()
     ms_step = ms / args.steps
-    value = npairs * world * args.steps / (ms * 1e-3)
+    value = shard.job_throughput(npairs, world, args.steps, ms)
     cells = sum(b.cells() for _, b in parts)
     dp_ms, dp_n = kt["dp"]
     alg_ops = sum(b.cells() * OPS_PER_CELL[p.algo] for p, b in parts) * args.steps
     achieved = alg_ops / (dp_ms * 1e-3) / 1e12
-    launches = sum(n for _, n in kt.values())
+    launches = sum(n * gl.KERNELS_PER_MARK[k] for k, (_, n) in kt.items())
 
     # ---------------- end to end through the storage API ----------------
     e2e = None
@@ -290,11 +300,7 @@ def main():
             e2e_times.append(span)
     for _, _, s in streams:
         s.close()
-    e2e_ms = float(np.mean(e2e_times))
-    if dist:
-        x = torch.tensor([e2e_ms], device=dev)
-        dist.all_reduce(x, op=dist.ReduceOp.MAX)
-        e2e_ms = float(x.item())
+    e2e_ms = shard.max_over_ranks(float(np.mean(e2e_times)), dist, dev)
     e2e = {"value": npairs * world / (e2e_ms * 1e-3), "unit": UNIT, "h2d_bytes_per_step": h2d,
            "d2h_bytes_per_step": d2h, "ms_per_step": e2e_ms,
            "path": "gasal_c_aln_async + gasal_c_is_aln_async_done (3 streams), pinned host batches"}

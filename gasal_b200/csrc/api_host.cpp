@@ -220,6 +220,8 @@ void release_state(const gasal_gpu_storage_t *s)
     if (w.h_tb_off) cudaFreeHost(w.h_tb_off);
     if (w.scratch) cudaFree(w.scratch);
     if (w.tb_off_free) cudaEventDestroy(w.tb_off_free);
+    if (w.order) cudaFree(w.order);
+    if (w.bins) cudaFree(w.bins);
     if (p->d_n_cigar) cudaFree(p->d_n_cigar);
 }
 

@@ -26,6 +26,7 @@ Settings &settings()
         Settings v;
         if (const char *e = getenv("GASAL_B200_TB_BUDGET_MB")) v.tb_budget_bytes = (size_t)atoll(e) << 20;
         if (const char *e = getenv("GASAL_B200_BLOCK")) v.block = atoi(e);
+        if (const char *e = getenv("GASAL_B200_MIN_ORDER_PAIRS")) v.min_order_pairs = atoi(e);
         return v;
     }();
     return s;
@@ -141,6 +142,32 @@ static int grow(void **p, size_t *cap, size_t need, size_t elem)
         }                                                                                              \
     } while (0)
 
+/* Length-binned order for pairs [0, n) of the given length arrays; returns
+ * nullptr (identity order) for small batches. */
+static const uint32_t *binned_order(const uint32_t *q_len, const uint32_t *t_len, int n, Workspace &ws,
+                                    cudaStream_t s, int *err)
+{
+    *err = GB_OK;
+    if (n < settings().min_order_pairs) return nullptr;
+    if (grow((void **)&ws.order, &ws.order_cap, (size_t)n, 4) != GB_OK) {
+        *err = GB_ERR_ALLOC;
+        return nullptr;
+    }
+    if (!ws.bins && cudaMalloc((void **)&ws.bins, (size_t)order_bins() * 4) != cudaSuccess) {
+        cudaGetLastError();
+        *err = GB_ERR_ALLOC;
+        return nullptr;
+    }
+    timing_mark(K_ORDER, true, s);
+    const cudaError_t e = launch_order(q_len, t_len, n, ws.bins, ws.order, s);
+    timing_mark(K_ORDER, false, s);
+    if (e != cudaSuccess) {
+        *err = GB_ERR_CUDA;
+        return nullptr;
+    }
+    return ws.order;
+}
+
 int run_batch(const RunCfg &cfg, const DevBatch &b, const DevOut &o, Workspace &ws, cudaStream_t s)
 {
     if (b.n <= 0) return GB_ERR_ARG;
@@ -189,6 +216,9 @@ int run_batch(const RunCfg &cfg, const DevBatch &b, const DevOut &o, Workspace &
     const int start = (cfg.algo == SEMI_GLOBAL_ && cfg.start == WITH_TB_) ? WITHOUT_START_ : cfg.start;
     const bool second = cfg.second && (cfg.algo == LOCAL_ || cfg.algo == SEMI_GLOBAL_);
     if (!tb) {
+        int err = GB_OK;
+        a.order = binned_order(b.q_len, b.t_len, b.n, ws, s, &err);
+        if (err != GB_OK) return err;
         timing_mark(K_DP, true, s);
         GB_CUDA(launch_dp(cfg.algo, start, second, a, block, cols, s));
         timing_mark(K_DP, false, s);
@@ -239,6 +269,9 @@ int run_batch(const RunCfg &cfg, const DevBatch &b, const DevOut &o, Workspace &
         ca.q_start = sh(o.q_start), ca.t_start = sh(o.t_start);
         ca.score2 = sh(o.score2), ca.q_end2 = sh(o.q_end2), ca.t_end2 = sh(o.t_end2);
         ca.tb = ws.tb, ca.tb_off = ws.d_tb_off + p0;
+        int err = GB_OK;
+        ca.order = binned_order(ca.q_len, ca.t_len, ca.n, ws, s, &err);
+        if (err != GB_OK) return err;
         timing_mark(K_DP, true, s);
         GB_CUDA(launch_dp(cfg.algo, start, second, ca, block, cols, s));
         timing_mark(K_DP, false, s);

@@ -55,6 +55,9 @@ struct Workspace {
     uint32_t *scratch = nullptr;
     size_t scratch_cap = 0;     /* uint32 units */
     cudaEvent_t tb_off_free = nullptr;
+    uint32_t *order = nullptr;   /* length-binned visiting order */
+    size_t order_cap = 0;
+    uint32_t *bins = nullptr;    /* order_bins() class counters */
     ~Workspace();
 };
 
@@ -75,11 +78,12 @@ struct Settings {
     int mql = 2048;
     size_t tb_budget_bytes = (size_t)16 << 30;
     int block = 64;
+    int min_order_pairs = 2048; /* batches at least this large visit pairs length-binned */
 };
 Settings &settings();
 
 /* Optional per-kernel CUDA-event timing (off by default).  Kinds: */
-enum KernelKind { K_PACK = 0, K_RC = 1, K_DP = 2, K_TB = 3, K_KINDS = 4 };
+enum KernelKind { K_PACK = 0, K_RC = 1, K_DP = 2, K_TB = 3, K_ORDER = 4, K_KINDS = 5 };
 void timing_enable(bool on);
 void timing_mark(int kind, bool start, cudaStream_t s);
 int timing_read(double ms[K_KINDS], int64_t launches[K_KINDS]);

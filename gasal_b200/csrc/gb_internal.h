@@ -72,6 +72,12 @@ cudaError_t launch_dp(int algo, int start, bool second, const DpArgs &a, int blo
                       cudaStream_t s);
 cudaError_t launch_traceback(const TbArgs &a, cudaStream_t s);
 
+/* length-binned visiting order (sched.cu): bins = order_bins() words of
+ * scratch, order = n words */
+int order_bins();
+cudaError_t launch_order(const uint32_t *q_len, const uint32_t *t_len, int n, uint32_t *bins, uint32_t *order,
+                         cudaStream_t s);
+
 /* the global-scratch DP variant on a caller-chosen grid */
 cudaError_t launch_dp_scratch_grid(int algo, int start, bool second, const DpArgs &a, int block, int blocks,
                                    cudaStream_t s);

@@ -124,6 +124,41 @@ __device__ void revcomp_one(uint32_t *w, uint32_t len, int op, int ref_reverse)
     }
 }
 
+/* Reference-identical reversal, word-parallel: blockDim = (32, 8), one row of
+ * 32 threads per pair, thread x handling word pairs (x, regs-1-x) for
+ * x < ceil(regs/2) in steps of 32.  Each word is read by at most one thread
+ * (its own index, below ceil(regs/2)) and written only after that read, so
+ * the in-place update is race-free; the complement of the untouched words
+ * runs after a row barrier. */
+__device__ __forceinline__ void revcomp_ref_row(uint32_t *w, uint32_t len, int op)
+{
+    const uint32_t regs = (len + 7) >> 3;
+    if (op & 1) {
+        const uint32_t half = (regs + 1) >> 1;
+        for (uint32_t i = threadIdx.x; i < half; i += 32) {
+            const uint32_t head = w[i];
+            uint32_t rev = nib_reverse(head);
+            if (op & 2) rev = complement_word(rev);
+            if (i != regs - 1 - i) w[i] = 0u;
+            w[regs - 1 - i] = rev;
+        }
+    } else if (op & 2) {
+        for (uint32_t i = threadIdx.x; i < regs; i += 32) w[i] = complement_word(w[i]);
+    }
+}
+
+__global__ void __launch_bounds__(256) revcomp_ref_kernel(uint32_t *pq, uint32_t *pt, const uint32_t *q_off,
+                                                          const uint32_t *t_off, const uint32_t *q_len,
+                                                          const uint32_t *t_len, const uint8_t *q_op,
+                                                          const uint8_t *t_op, int32_t n)
+{
+    const int i = blockIdx.x * blockDim.y + threadIdx.y;
+    if (i >= n) return;
+    const int qo = q_op ? q_op[i] : 0, to = t_op ? t_op[i] : 0;
+    if (qo & 3) revcomp_ref_row(pq + (q_off[i] >> 3), q_len[i], qo);
+    if (to & 3) revcomp_ref_row(pt + (t_off[i] >> 3), t_len[i], to);
+}
+
 __global__ void revcomp_kernel(uint32_t *pq, uint32_t *pt, const uint32_t *q_off, const uint32_t *t_off,
                                const uint32_t *q_len, const uint32_t *t_len, const uint8_t *q_op,
                                const uint8_t *t_op, int32_t n, int ref_reverse)
@@ -140,7 +175,12 @@ cudaError_t launch_revcomp(uint32_t *pq, uint32_t *pt, const uint32_t *q_off, co
                            const uint8_t *t_op, int32_t n, int ref_reverse, cudaStream_t s)
 {
     if (n <= 0) return cudaSuccess;
-    revcomp_kernel<<<(n + 127) / 128, 128, 0, s>>>(pq, pt, q_off, t_off, q_len, t_len, q_op, t_op, n, ref_reverse);
+    if (ref_reverse) {
+        const dim3 blk(32, 8);
+        revcomp_ref_kernel<<<(n + 7) / 8, blk, 0, s>>>(pq, pt, q_off, t_off, q_len, t_len, q_op, t_op, n);
+    } else {
+        revcomp_kernel<<<(n + 127) / 128, 128, 0, s>>>(pq, pt, q_off, t_off, q_len, t_len, q_op, t_op, n, 0);
+    }
     return cudaGetLastError();
 }
 

@@ -1,0 +1,98 @@
+/*
+ * sched.cu -- length-binned visiting order for the one-pair-per-thread DP.
+ *
+ * A warp runs until its slowest lane finishes, so pairs of unequal length in
+ * one warp waste lanes (uniform 150-300 bp targets leave a warp ~76% busy).
+ * A counting sort groups pairs with the same (query words, target words) --
+ * identical forward DP work -- and lists the biggest classes first so the
+ * grid's tail holds the short pairs.  Three stream-ordered kernels: class
+ * histogram, exclusive scan over classes, scatter.  Both counting kernels
+ * aggregate per warp (one atomic per distinct class in a warp).  The order
+ * inside a class is not deterministic; results are written per pair, so
+ * output is.
+ */
+#include "gb_internal.h"
+
+namespace gb {
+
+constexpr int ORDER_BITS = 7;
+constexpr int ORDER_BINS = 1 << (2 * ORDER_BITS); /* 128 x 128 classes */
+
+__device__ __forceinline__ uint32_t work_bin(uint32_t qlen, uint32_t tlen)
+{
+    const uint32_t cap = (1u << ORDER_BITS) - 1;
+    const uint32_t qr = min((qlen + 7) >> 3, cap), tr = min((tlen + 7) >> 3, cap);
+    /* descending work -> ascending bin */
+    return (uint32_t)(ORDER_BINS - 1) - ((qr << ORDER_BITS) | tr);
+}
+
+__global__ void __launch_bounds__(256) order_hist_kernel(const uint32_t *q_len, const uint32_t *t_len, int n,
+                                                         uint32_t *hist)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const bool live = i < n;
+    const uint32_t bin = live ? work_bin(q_len[i], t_len[i]) : 0xFFFFFFFFu;
+    const unsigned same = __match_any_sync(0xFFFFFFFFu, bin);
+    const int leader = __ffs(same) - 1;
+    if (live && (int)(threadIdx.x & 31) == leader) atomicAdd(&hist[bin], (uint32_t)__popc(same));
+}
+
+/* one block of 1024 threads: exclusive scan of ORDER_BINS counts in place */
+__global__ void __launch_bounds__(1024) order_scan_kernel(uint32_t *hist)
+{
+    constexpr int PER = ORDER_BINS / 1024;
+    __shared__ uint32_t part[1024];
+    uint32_t v[PER], s = 0;
+    const int base = threadIdx.x * PER;
+#pragma unroll
+    for (int k = 0; k < PER; k++) {
+        v[k] = hist[base + k];
+        s += v[k];
+    }
+    part[threadIdx.x] = s;
+    __syncthreads();
+    for (int off = 1; off < 1024; off <<= 1) {
+        const uint32_t add = threadIdx.x >= (unsigned)off ? part[threadIdx.x - off] : 0u;
+        __syncthreads();
+        part[threadIdx.x] += add;
+        __syncthreads();
+    }
+    uint32_t run = part[threadIdx.x] - s;
+#pragma unroll
+    for (int k = 0; k < PER; k++) {
+        hist[base + k] = run;
+        run += v[k];
+    }
+}
+
+__global__ void __launch_bounds__(256) order_scatter_kernel(const uint32_t *q_len, const uint32_t *t_len, int n,
+                                                            uint32_t *offs, uint32_t *order)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const bool live = i < n;
+    const uint32_t bin = live ? work_bin(q_len[i], t_len[i]) : 0xFFFFFFFFu;
+    const unsigned same = __match_any_sync(0xFFFFFFFFu, bin);
+    const int lane = threadIdx.x & 31;
+    const int leader = __ffs(same) - 1;
+    uint32_t base = 0;
+    if (live && lane == leader) base = atomicAdd(&offs[bin], (uint32_t)__popc(same));
+    base = __shfl_sync(same, base, leader);
+    if (live) order[base + __popc(same & ((1u << lane) - 1u))] = (uint32_t)i;
+}
+
+int order_bins() { return ORDER_BINS; }
+
+cudaError_t launch_order(const uint32_t *q_len, const uint32_t *t_len, int n, uint32_t *bins, uint32_t *order,
+                         cudaStream_t s)
+{
+    if (n <= 0) return cudaSuccess;
+    cudaError_t e = cudaMemsetAsync(bins, 0, ORDER_BINS * sizeof(uint32_t), s);
+    if (e != cudaSuccess) return e;
+    const int blocks = (n + 255) / 256;
+    order_hist_kernel<<<blocks, 256, 0, s>>>(q_len, t_len, n, bins);
+    order_scan_kernel<<<1, 1024, 0, s>>>(bins);
+    order_scatter_kernel<<<blocks, 256, 0, s>>>(q_len, t_len, n, bins, order);
+    return cudaGetLastError();
+}
+
+} // namespace gb

@@ -130,7 +130,8 @@ def set_tb_budget_mb(mb: int):
     _check(lib().gb_set_tb_budget_mb(int(mb)), "gb_set_tb_budget_mb")
 
 
-KERNEL_KINDS = ("pack", "revcomp", "dp", "traceback")
+KERNEL_KINDS = ("pack", "revcomp", "dp", "traceback", "order")
+KERNELS_PER_MARK = {"pack": 1, "revcomp": 1, "dp": 1, "traceback": 1, "order": 3}
 
 
 def kernel_timing(on: bool):
@@ -138,8 +139,8 @@ def kernel_timing(on: bool):
 
 
 def kernel_timing_read() -> dict:
-    ms = (C.c_double * 4)()
-    n = (C.c_int64 * 4)()
+    ms = (C.c_double * 5)()
+    n = (C.c_int64 * 5)()
     _check(lib().gb_kernel_timing_read(ms, n), "gb_kernel_timing_read")
     return {k: (ms[i], n[i]) for i, k in enumerate(KERNEL_KINDS)}
 

@@ -200,8 +200,9 @@ const char *gb_version(void);
 /* Instrumentation (no reference counterpart).  gb_kernel_timing(1) resets
  * and starts recording a CUDA event pair around every kernel the library
  * launches; gb_kernel_timing_read() waits for them and returns, per kind
- * (0 pack, 1 reverse/complement, 2 alignment DP, 3 traceback), the summed
- * milliseconds and the number of launches.  gb_probe_int_peak() times the
+ * (0 pack, 1 reverse/complement, 2 alignment DP, 3 traceback, 4 length-binned
+ * ordering = 3 kernels per mark), the summed milliseconds and the number of
+ * marks, in arrays of 5.  gb_probe_int_peak() times the
  * integer instructions the DP is bound by on the current GPU (tera-ops/s). */
 int gb_kernel_timing(int on);
 int gb_kernel_timing_read(double *ms, int64_t *launches);
