@@ -221,6 +221,9 @@ void release_state(const gasal_gpu_storage_t *s)
     if (w.scratch) cudaFree(w.scratch);
     if (w.tb_off_free) cudaEventDestroy(w.tb_off_free);
     if (w.order) cudaFree(w.order);
+    if (w.aux) cudaStreamDestroy(w.aux);
+    if (w.fork) cudaEventDestroy(w.fork);
+    if (w.join) cudaEventDestroy(w.join);
     if (w.bins) cudaFree(w.bins);
     if (p->d_n_cigar) cudaFree(p->d_n_cigar);
 }

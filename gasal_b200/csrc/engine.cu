@@ -27,6 +27,7 @@ Settings &settings()
         if (const char *e = getenv("GASAL_B200_TB_BUDGET_MB")) v.tb_budget_bytes = (size_t)atoll(e) << 20;
         if (const char *e = getenv("GASAL_B200_BLOCK")) v.block = atoi(e);
         if (const char *e = getenv("GASAL_B200_MIN_ORDER_PAIRS")) v.min_order_pairs = atoi(e);
+        if (const char *e = getenv("GASAL_B200_WC_MIN_QREGS")) v.wc_min_qregs = atoi(e);
         return v;
     }();
     return s;
@@ -145,10 +146,10 @@ static int grow(void **p, size_t *cap, size_t need, size_t elem)
 /* Length-binned order for pairs [0, n) of the given length arrays; returns
  * nullptr (identity order) for small batches. */
 static const uint32_t *binned_order(const uint32_t *q_len, const uint32_t *t_len, int n, Workspace &ws,
-                                    cudaStream_t s, int *err)
+                                    cudaStream_t s, int *err, bool force)
 {
     *err = GB_OK;
-    if (n < settings().min_order_pairs) return nullptr;
+    if (!force && n < settings().min_order_pairs) return nullptr;
     if (grow((void **)&ws.order, &ws.order_cap, (size_t)n, 4) != GB_OK) {
         *err = GB_ERR_ALLOC;
         return nullptr;
@@ -166,6 +167,45 @@ static const uint32_t *binned_order(const uint32_t *q_len, const uint32_t *t_len
         return nullptr;
     }
     return ws.order;
+}
+
+/* DP over pairs [0, a.n) visited in `order` (nullptr: identity): the first
+ * nlong entries of order on the warp-cooperative kernel (auxiliary stream,
+ * forked from and joined back into s), the rest on the one-thread kernel. */
+static int launch_dp_split(int algo, int start, bool second, DpArgs a, const uint32_t *order, int nlong,
+                           int max_q8_long, int max_t8_long, int block, Workspace &ws, cudaStream_t s)
+{
+    if (nlong > 0 && order) {
+        if (!ws.aux) {
+            if (cudaStreamCreateWithFlags(&ws.aux, cudaStreamNonBlocking) != cudaSuccess ||
+                cudaEventCreateWithFlags(&ws.fork, cudaEventDisableTiming) != cudaSuccess ||
+                cudaEventCreateWithFlags(&ws.join, cudaEventDisableTiming) != cudaSuccess) {
+                cudaGetLastError();
+                return GB_ERR_CUDA;
+            }
+        }
+        GB_CUDA(cudaEventRecord(ws.fork, s));
+        GB_CUDA(cudaStreamWaitEvent(ws.aux, ws.fork, 0));
+        timing_mark(K_DP, true, ws.aux);
+        GB_CUDA(launch_dp_wc(algo, start, second, a, order, nlong, max_q8_long, max_t8_long, ws.aux));
+        timing_mark(K_DP, false, ws.aux);
+        GB_CUDA(cudaEventRecord(ws.join, ws.aux));
+        DpArgs rest = a;
+        rest.order = order + nlong;
+        rest.n = a.n - nlong;
+        if (rest.n > 0) {
+            timing_mark(K_DP, true, s);
+            GB_CUDA(launch_dp(algo, start, second, rest, block, 0, s));
+            timing_mark(K_DP, false, s);
+        }
+        GB_CUDA(cudaStreamWaitEvent(s, ws.join, 0));
+        return GB_OK;
+    }
+    a.order = order;
+    timing_mark(K_DP, true, s);
+    GB_CUDA(launch_dp(algo, start, second, a, block, 0, s));
+    timing_mark(K_DP, false, s);
+    return GB_OK;
 }
 
 int run_batch(const RunCfg &cfg, const DevBatch &b, const DevOut &o, Workspace &ws, cudaStream_t s)
@@ -190,9 +230,32 @@ int run_batch(const RunCfg &cfg, const DevBatch &b, const DevOut &o, Workspace &
         timing_mark(K_RC, false, s);
     }
 
-    /* ---- row buffer placement ---- */
-    uint32_t max_q = 0;
-    for (int i = 0; i < b.n; i++) max_q = std::max(max_q, b.h_q_len[i]);
+    /* ---- split: long LOCAL/GLOBAL pairs go warp-cooperative ---- */
+    const bool wc_algo = (cfg.algo == LOCAL_ || cfg.algo == GLOBAL_);
+    uint32_t max_q_short = 0, max_q_long = 0, max_t_long = 0;
+    int nlong = 0;
+    const uint32_t wc_min_q = (uint32_t)st.wc_min_qregs * 8 - 7;
+    for (int i = 0; i < b.n; i++) {
+        const uint32_t ql = b.h_q_len[i];
+        if (wc_algo && ql >= wc_min_q) {
+            nlong++;
+            max_q_long = std::max(max_q_long, ql);
+            max_t_long = std::max(max_t_long, b.h_t_len[i]);
+        } else {
+            max_q_short = std::max(max_q_short, ql);
+        }
+    }
+    /* the warp kernel's shared memory: 4 warps x (ring of q8 words + band maxima) */
+    const size_t wc_smem = 4 * (((size_t)max_q_long + 8) + ((size_t)max_t_long + 8) / 8 + 1) * 4;
+    const bool use_wc = nlong > 0 && b.n >= st.min_order_pairs && ((max_q_long + 7) & ~7u) <= (uint32_t)st.wc_max_q8 &&
+                        wc_smem <= (200u << 10);
+    if (!use_wc) {
+        max_q_short = std::max(max_q_short, max_q_long);
+        nlong = 0;
+    }
+    const uint32_t max_q = max_q_short;
+
+    /* ---- row buffer placement (one-thread kernel) ---- */
     const int cols = cfg.algo == KSW_ ? 2 * ((int)max_q + 2) : (int)((max_q + 7) & ~7u);
     const size_t smem_limit = 160u << 10;
 
@@ -202,8 +265,8 @@ int run_batch(const RunCfg &cfg, const DevBatch &b, const DevOut &o, Workspace &
     a.score = o.score, a.q_end = o.q_end, a.t_end = o.t_end, a.q_start = o.q_start, a.t_start = o.t_start;
     a.score2 = o.score2, a.q_end2 = o.q_end2, a.t_end2 = o.t_end2;
     a.sc = cfg.sc, a.head = cfg.head, a.tail = cfg.tail, a.k_band = cfg.k_band, a.zdrop = cfg.zdrop, a.mql = cfg.mql;
-    if ((size_t)cols * block * 4 <= smem_limit) {
-        a.smem_cols = cols;
+    if ((size_t)std::max(cols, 8) * block * 4 <= smem_limit) {
+        a.smem_cols = std::max(cols, 8);
     } else {
         a.smem_cols = 0;
         const size_t threads = (size_t)dp_scratch_blocks(b.n, block) * block;
@@ -215,14 +278,12 @@ int run_batch(const RunCfg &cfg, const DevBatch &b, const DevOut &o, Workspace &
     const bool tb = cfg.start == WITH_TB_ && (cfg.algo == LOCAL_ || cfg.algo == GLOBAL_);
     const int start = (cfg.algo == SEMI_GLOBAL_ && cfg.start == WITH_TB_) ? WITHOUT_START_ : cfg.start;
     const bool second = cfg.second && (cfg.algo == LOCAL_ || cfg.algo == SEMI_GLOBAL_);
+    const int mq8 = (int)((max_q_long + 7) & ~7u), mt8 = (int)((max_t_long + 7) & ~7u);
     if (!tb) {
         int err = GB_OK;
-        a.order = binned_order(b.q_len, b.t_len, b.n, ws, s, &err);
+        const uint32_t *ord = binned_order(b.q_len, b.t_len, b.n, ws, s, &err, use_wc);
         if (err != GB_OK) return err;
-        timing_mark(K_DP, true, s);
-        GB_CUDA(launch_dp(cfg.algo, start, second, a, block, cols, s));
-        timing_mark(K_DP, false, s);
-        return GB_OK;
+        return launch_dp_split(cfg.algo, start, second, a, ord, ord ? nlong : 0, mq8, mt8, block, ws, s);
     }
 
     /* ---- traceback: chunk pairs so the tiles fit the budget ---- */
@@ -270,11 +331,13 @@ int run_batch(const RunCfg &cfg, const DevBatch &b, const DevOut &o, Workspace &
         ca.score2 = sh(o.score2), ca.q_end2 = sh(o.q_end2), ca.t_end2 = sh(o.t_end2);
         ca.tb = ws.tb, ca.tb_off = ws.d_tb_off + p0;
         int err = GB_OK;
-        ca.order = binned_order(ca.q_len, ca.t_len, ca.n, ws, s, &err);
+        const uint32_t *ord = binned_order(ca.q_len, ca.t_len, ca.n, ws, s, &err, use_wc);
         if (err != GB_OK) return err;
-        timing_mark(K_DP, true, s);
-        GB_CUDA(launch_dp(cfg.algo, start, second, ca, block, cols, s));
-        timing_mark(K_DP, false, s);
+        int nlong_c = 0;
+        if (use_wc && ord)
+            for (int i = p0; i < p1; i++) nlong_c += b.h_q_len[i] >= wc_min_q ? 1 : 0;
+        const int rc = launch_dp_split(cfg.algo, start, second, ca, ord, nlong_c, mq8, mt8, block, ws, s);
+        if (rc != GB_OK) return rc;
         TbArgs t{};
         t.tb = ws.tb, t.tb_off = ws.d_tb_off + p0;
         t.q_off = ca.q_off, t.q_len = ca.q_len, t.t_len = ca.t_len;

@@ -58,6 +58,8 @@ struct Workspace {
     uint32_t *order = nullptr;   /* length-binned visiting order */
     size_t order_cap = 0;
     uint32_t *bins = nullptr;    /* order_bins() class counters */
+    cudaStream_t aux = nullptr;  /* second stream for the warp-cooperative kernel */
+    cudaEvent_t fork = nullptr, join = nullptr;
     ~Workspace();
 };
 
@@ -79,6 +81,8 @@ struct Settings {
     size_t tb_budget_bytes = (size_t)16 << 30;
     int block = 64;
     int min_order_pairs = 2048; /* batches at least this large visit pairs length-binned */
+    int wc_min_qregs = 32;      /* pairs with at least this many query words go warp-cooperative */
+    int wc_max_q8 = 12000;      /* ... while the batch's longest query fits the warp's ring */
 };
 Settings &settings();
 

@@ -78,6 +78,11 @@ int order_bins();
 cudaError_t launch_order(const uint32_t *q_len, const uint32_t *t_len, int n, uint32_t *bins, uint32_t *order,
                          cudaStream_t s);
 
+/* warp-cooperative DP (dp_wc.cu) for the pairs listed in `list`: LOCAL and
+ * GLOBAL; queries of at least 32 words */
+cudaError_t launch_dp_wc(int algo, int start, bool second, const DpArgs &a, const uint32_t *list, int nlist,
+                         int max_q8, int max_t8, cudaStream_t s);
+
 /* the global-scratch DP variant on a caller-chosen grid */
 cudaError_t launch_dp_scratch_grid(int algo, int start, bool second, const DpArgs &a, int block, int blocks,
                                    cudaStream_t s);

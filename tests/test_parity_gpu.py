@@ -153,3 +153,35 @@ def test_streams_api_grows_buffers():
         got = st.results(0, b.n, b)
     exp = oracle_align(p, b).as_dict(p)
     assert_same(got, exp, "grown")
+
+
+# ---- warp-cooperative path (queries of 32+ words in batches of 2048+) ----
+
+def test_wc_local_long_pairs_all_modes():
+    """Long LOCAL pairs (250-2000 bp) on the warp-cooperative kernel: forward,
+    second best (two passes), start pass (reversed sweep), traceback."""
+    b = W.workload3(2100, seed=41)
+    _vs_oracle(Params(algo=LOCAL), b)
+    _vs_oracle(Params(algo=LOCAL, start_pos=WITH_START, second_best=1), b)
+    _vs_oracle(Params(algo=LOCAL, start_pos=WITH_TB), b)
+
+
+def test_wc_global_mixed_lengths_traceback():
+    """Log-uniform 50-1000 bp: short pairs on the one-thread kernel, long ones
+    on the warp kernel, in one launch; GLOBAL score and CIGAR."""
+    b = W.workload2(4000, seed=42)
+    _vs_oracle(Params(algo=GLOBAL), b)
+    _vs_oracle(Params(algo=GLOBAL, start_pos=WITH_TB), b)
+    _vs_oracle(Params(algo=LOCAL, start_pos=WITH_START, second_best=1), b)
+
+
+def test_wc_unrelated_long_pairs():
+    """Random unrelated long pairs: local maxima anywhere, including end cells
+    in the first 31 query words (start pass falls back to one lane)."""
+    rng = np.random.default_rng(43)
+    qs = [bytes(rng.choice(list(b"ACGT"), size=int(rng.integers(260, 700))).tolist()) for _ in range(2200)]
+    ts = [bytes(rng.choice(list(b"ACGT"), size=int(rng.integers(20, 700))).tolist()) for _ in range(2200)]
+    from gasal_b200.capi import Batch
+    b = Batch.from_seqs(qs, ts)
+    _vs_oracle(Params(algo=LOCAL, start_pos=WITH_START, second_best=1), b)
+    _vs_oracle(Params(algo=GLOBAL, start_pos=WITH_TB), b)
