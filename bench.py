@@ -42,10 +42,23 @@ sys.path.insert(0, ROOT)
 from gasal_b200 import workloads as W  # noqa: E402
 from gasal_b200.capi import LOCAL, GLOBAL, SEMI_GLOBAL, Params  # noqa: E402
 
-METRIC = "aligned pairs/s (1M-pair mixed LOCAL/GLOBAL/SEMI_GLOBAL WITH_START batch, RC on 50%)"
 UNIT = "pairs/s"
-# integer ops per cell, per algorithm (LOCAL 11, GLOBAL 9, SEMI_GLOBAL 10)
+# integer ops per cell, per algorithm (LOCAL 11, GLOBAL 9, SEMI_GLOBAL 10; +4 with traceback)
 OPS_PER_CELL = {LOCAL: 11, GLOBAL: 9, SEMI_GLOBAL: 10}
+TB_OPS = 4
+
+WORKLOADS = {
+    "w1": ("aligned pairs/s (1M-pair mixed LOCAL/GLOBAL/SEMI_GLOBAL WITH_START batch, RC on 50%)",
+           "w1: 1M pairs/GPU, thirds LOCAL(second best)/GLOBAL/SEMI_GLOBAL(TARGET,TARGET), WITH_START, q=150, "
+           "t=150-300 (3% subs, 1% indels), RC 50% of queries, scores 1/4/6/1", 1_000_000),
+    "w2": ("aligned pairs/s (2M-pair uneven-length GLOBAL WITH_TB batch, CIGAR out)",
+           "w2: 2M pairs/GPU, GLOBAL WITH_TB, query log-uniform 50-1000, target = query with 1-8% subs and "
+           "0.5-3% indels (len 1-10) per pair, scores 1/4/6/1", 2_000_000),
+    "w0": ("aligned pairs/s (20k-pair LOCAL WITHOUT_START batch)",
+           "w0: 20k pairs, LOCAL WITHOUT_START, q 100-150 with 0.1% N, t = q + 0-20 flanks, 2% subs, 0.5% "
+           "indels", 20_000),
+}
+METRIC = WORKLOADS["w1"][0]
 # DRAM bytes per DP launch of the workload from the committed ncu capture
 # (profiles/dp_kernels_w1.md), scaled to a full launch; None until captured.
 DP_TRAFFIC_BYTES = None
@@ -113,10 +126,16 @@ class ClockSampler:
                 "power_w_max": max(pw) if pw else None, "reasons": reasons, "samples": len(rows)}
 
 
-def build_workload(n: int, seed: int):
+def build_workload(n: int, seed: int, name: str = "w1"):
     t = time.time()
-    parts = W.workload1(n, seed=seed)
-    log(f"workload: {n} pairs generated in {time.time() - t:.1f}s")
+    if name == "w1":
+        parts = W.workload1(n, seed=seed)
+    elif name == "w2":
+        from gasal_b200.capi import WITH_TB
+        parts = [(Params(algo=GLOBAL, start_pos=WITH_TB), W.workload2(n, seed=seed + 1))]
+    else:
+        parts = [(Params(algo=LOCAL), W.workload0(n, seed=seed - 1))]
+    log(f"workload {name}: {n} pairs generated in {time.time() - t:.1f}s")
     return parts
 
 
@@ -126,16 +145,18 @@ def cpu_baseline(parts, budget_s: float = 12.0) -> dict:
     cores = os.cpu_count() or 1
     probe = 3000
     t0 = time.time()
+    k = len(parts)
+    probe = min(probe, min(b.n for _, b in parts))
     for p, b in parts:
-        oracle_align(p, b.subset(np.arange(min(probe, b.n))), threads=cores)
-    per_pair = (time.time() - t0) / (3 * probe)
-    m = int(max(probe, min(parts[0][1].n, budget_s / per_pair / 3)))
+        oracle_align(p, b.subset(np.arange(probe)), threads=cores)
+    per_pair = (time.time() - t0) / (k * probe)
+    m = int(max(probe, min(min(b.n for _, b in parts), budget_s / per_pair / k)))
     t0 = time.time()
     for p, b in parts:
         oracle_align(p, b.subset(np.arange(min(m, b.n))), threads=cores)
     dt = time.time() - t0
-    return {"value": 3 * m / dt, "unit": UNIT, "cores": cores, "kind": "port",
-            "sample": f"first {m} pairs of each of the three launches ({3 * m} pairs), {dt:.1f}s"}
+    return {"value": k * m / dt, "unit": UNIT, "cores": cores, "kind": "port",
+            "sample": f"first {m} pairs of each of the {k} launch(es) ({k * m} pairs), {dt:.1f}s"}
 
 
 def run_reference(args):
@@ -144,7 +165,7 @@ def run_reference(args):
         return
     from oracle.bindings import ref_host_align
     cores = os.cpu_count() or 1
-    parts = build_workload(args.pairs, W.SEED_BASE + 1)
+    parts = build_workload(args.pairs or WORKLOADS[args.workload][2], W.SEED_BASE + 1, args.workload)
     m = args.ref_sample
     sample = [(p, b.subset(np.arange(min(m, b.n)))) for p, b in parts]
     for _ in range(args.warmup):
@@ -158,12 +179,11 @@ def run_reference(args):
         times.append(time.time() - t0)
     npairs = sum(b.n for _, b in sample)
     v = npairs / float(np.mean(times))
-    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus,
+    line = {"impl": "reference", "metric": WORKLOADS[args.workload][0], "value": v, "unit": UNIT, "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * float(np.mean(times)),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int32",
             "data": "synthetic",
-            "config": {"workload": "w1: 1M pairs, thirds LOCAL(second best)/GLOBAL/SEMI_GLOBAL(TARGET,TARGET), "
-                                   "WITH_START, q=150, t=150-300, RC 50%", "pairs_per_step": npairs},
+            "config": {"workload": WORKLOADS[args.workload][1], "pairs_per_step": npairs},
             "cpu_baseline": {"value": v, "unit": UNIT, "cores": cores, "kind": "reference",
                              "sample": f"first {m} pairs of each launch per step ({npairs} pairs); reference "
                                        f"kernel headers compiled for the host, OpenMP over pairs"},
@@ -177,7 +197,8 @@ def main():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--pairs", type=int, default=1_000_000)
+    ap.add_argument("--workload", default="w1", choices=sorted(WORKLOADS))
+    ap.add_argument("--pairs", type=int, default=0, help="pairs per GPU (default: the workload's size)")
     ap.add_argument("--ref-sample", type=int, default=4000)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
@@ -203,7 +224,8 @@ def main():
     gl.lib()
     gl.set_reference_reverse(True)
     peak = gl.probe_int_peak()
-    parts = build_workload(args.pairs, shard.shard_seed(W.SEED_BASE + 1, rank))
+    n_pairs = args.pairs or WORKLOADS[args.workload][2]
+    parts = build_workload(n_pairs, shard.shard_seed(W.SEED_BASE + 1, rank), args.workload)
     npairs = sum(b.n for _, b in parts)
     dev = torch.device("cuda", local_rank)
 
@@ -214,18 +236,24 @@ def main():
     dparts = []
     for p, b in parts:
         d = {"q_t": t_(b.q), "t_t": t_(b.t), "qo": t_(b.q_off, np.int32), "to": t_(b.t_off, np.int32),
-             "ql": t_(b.q_len, np.int32), "tl": t_(b.t_len, np.int32), "qop": t_(b.q_op), "top": t_(b.t_op)}
+             "ql": t_(b.q_len, np.int32), "tl": t_(b.t_len, np.int32),
+             "qop": t_(b.q_op) if b.q_op is not None else None, "top": t_(b.t_op) if b.t_op is not None else None}
         d["pq"] = torch.empty(b.q.shape[0] // 8, dtype=torch.int32, device=dev)
         d["pt"] = torch.empty(b.t.shape[0] // 8, dtype=torch.int32, device=dev)
         outs = {k: torch.empty(b.n, dtype=torch.int32, device=dev) for k in
                 ("score", "q_end", "t_end", "q_start", "t_start", "score2", "q_end2", "t_end2")}
         d["outs"] = outs
+        d["cigar"] = torch.empty(b.q.shape[0], dtype=torch.uint8, device=dev)
+        d["ncig"] = torch.empty(b.n, dtype=torch.int32, device=dev)
         m = {"q_bytes": b.q.shape[0], "t_bytes": b.t.shape[0], "q": d["q_t"].data_ptr(), "t": d["t_t"].data_ptr(),
              "pq": d["pq"].data_ptr(), "pt": d["pt"].data_ptr(), "q_off": d["qo"].data_ptr(),
              "t_off": d["to"].data_ptr(), "q_len": d["ql"].data_ptr(), "t_len": d["tl"].data_ptr(),
-             "q_op": d["qop"].data_ptr(), "t_op": d["top"].data_ptr()}
+             "q_op": d["qop"].data_ptr() if d["qop"] is not None else None,
+             "t_op": d["top"].data_ptr() if d["top"] is not None else None}
         for k, v in outs.items():
             m["out_" + k] = v.data_ptr()
+        m["out_cigar"] = d["cigar"].data_ptr()
+        m["out_n_cigar"] = d["ncig"].data_ptr()
         if not p.second_best:
             m["out_score2"] = m["out_q_end2"] = m["out_t_end2"] = None
         d["map"] = m
@@ -264,7 +292,9 @@ def main():
     value = shard.job_throughput(npairs, world, args.steps, ms)
     cells = sum(b.cells() for _, b in parts)
     dp_ms, dp_n = kt["dp"]
-    alg_ops = sum(b.cells() * OPS_PER_CELL[p.algo] for p, b in parts) * args.steps
+    from gasal_b200.capi import WITH_TB as _TB
+    alg_ops = sum(b.cells() * (OPS_PER_CELL[p.algo] + (TB_OPS if p.start_pos == _TB else 0))
+                  for p, b in parts) * args.steps
     achieved = alg_ops / (dp_ms * 1e-3) / 1e12
     launches = sum(n * gl.KERNELS_PER_MARK[k] for k, (_, n) in kt.items())
 
@@ -272,7 +302,7 @@ def main():
     e2e = None
     streams = []
     for p, b in parts:
-        s = gl.Streams(1, 152, 304, b.n, p)
+        s = gl.Streams(1, int(b.q_len.max()), int(b.t_len.max()), b.n, p)
         streams.append((p, b, s))
     h2d = sum(int(b.q.shape[0] + b.t.shape[0]) + b.n * (4 * 4 + 2) for _, b, _ in streams)
     d2h = 0
@@ -281,9 +311,11 @@ def main():
         if p.algo == GLOBAL:
             nf = 1
         d2h += 4 * b.n * nf
+        if p.start_pos == _TB:
+            d2h += int(b.q.shape[0]) + 4 * b.n
     e2e_times = []
     ext = [torch.cuda.ExternalStream(s.view(0).stream, device=dev) for _, _, s in streams]
-    for it in range(args.warmup + args.steps):
+    for it in range(args.warmup + min(args.steps, 5)):
         sizes = [s.fill_fast(0, b) for _, b, s in streams]
         torch.cuda.synchronize()
         starts = [torch.cuda.Event(enable_timing=True) for _ in streams]
@@ -308,21 +340,20 @@ def main():
     if rank == 0:
         cpu = None if args.no_cpu_baseline else cpu_baseline(parts)
         line = {
-            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "metric": WORKLOADS[args.workload][0], "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "int32", "data": "synthetic (seeded numpy PCG64)",
-            "config": {"workload": "w1: 1M pairs/GPU, thirds LOCAL(second best)/GLOBAL/SEMI_GLOBAL(TARGET,TARGET), "
-                                   "WITH_START, q=150, t=150-300 (3% subs, 1% indels), RC 50% of queries, "
-                                   "scores 1/4/6/1",
+            "config": {"workload": WORKLOADS[args.workload][1],
                        "pairs_per_step_per_gpu": npairs, "cells_per_step_per_gpu": cells,
                        "parallelism": f"pair shards x{world}, no collective in the data path",
                        "l2": "inputs 384 MB > 126 MB L2, no flush"},
             "gcups": cells * world / (ms_step * 1e-3) / 1e9,
             "roofline": {"bound": "int32", "achieved": achieved, "peak": peak["iadd_tops"], "unit": "Tops/s",
-                         "frac": achieved / peak["iadd_tops"], "traffic": DP_TRAFFIC_BYTES,
-                         "kernel": "dp_kernel (LOCAL/GLOBAL/SEMI_GLOBAL, one launch each per step)",
+                         "frac": achieved / peak["iadd_tops"],
+                         "traffic": DP_TRAFFIC_BYTES if args.workload == "w1" else None,
+                         "kernel": "dp_kernel / dp_wc_kernel (one DP launch per algorithm per step)",
                          "dp_ms_per_step": dp_ms / args.steps,
-                         "ops_per_cell": {"local": 11, "global": 9, "semi_global": 10},
+                         "ops_per_cell": {"local": 11, "global": 9, "semi_global": 10, "traceback_extra": 4},
                          "peak_source": "measured live: 2-input int32 add issue rate (gb_probe_int_peak)",
                          "imnmx_tops": peak["imnmx_tops"], "dpx_tops": peak["dpx_tops"]},
             "kernel_ms_per_step": {k: v[0] / args.steps for k, v in kt.items()},

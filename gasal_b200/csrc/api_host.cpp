@@ -222,6 +222,7 @@ void release_state(const gasal_gpu_storage_t *s)
     if (w.tb_off_free) cudaEventDestroy(w.tb_off_free);
     if (w.order) cudaFree(w.order);
     if (w.aux) cudaStreamDestroy(w.aux);
+    if (w.queue) cudaFree(w.queue);
     if (w.fork) cudaEventDestroy(w.fork);
     if (w.join) cudaEventDestroy(w.join);
     if (w.bins) cudaFree(w.bins);

@@ -258,7 +258,8 @@ struct DevWs {
     gb::Workspace ws;
 };
 std::mutex g_dev_mu;
-std::unordered_map<int, DevWs *> g_dev_ws;
+/* one workspace per (device, stream): work on different streams may overlap */
+std::unordered_map<unsigned long long, DevWs *> g_dev_ws;
 } // namespace
 
 extern "C" int gb_align_dev(const gb_params_t *p, const gb_dev_batch_t *b, const gb_dev_out_t *o, void *stream)
@@ -269,7 +270,8 @@ extern "C" int gb_align_dev(const gb_params_t *p, const gb_dev_batch_t *b, const
     DevWs *w;
     {
         std::lock_guard<std::mutex> lk(g_dev_mu);
-        DevWs *&slot = g_dev_ws[dev];
+        const unsigned long long key = ((unsigned long long)(uintptr_t)stream << 8) ^ (unsigned long long)dev;
+        DevWs *&slot = g_dev_ws[key];
         if (!slot) slot = new DevWs();
         w = slot;
     }
@@ -289,7 +291,6 @@ extern "C" int gb_align_dev(const gb_params_t *p, const gb_dev_batch_t *b, const
     dout.score = o->score, dout.q_end = o->q_end, dout.t_end = o->t_end, dout.q_start = o->q_start;
     dout.t_start = o->t_start, dout.score2 = o->score2, dout.q_end2 = o->q_end2, dout.t_end2 = o->t_end2;
     dout.cigar = o->cigar, dout.n_cigar = o->n_cigar;
-    std::lock_guard<std::mutex> lk(g_dev_mu);
     return gb::run_batch(cfg, db, dout, w->ws, (cudaStream_t)stream);
 }
 

@@ -46,6 +46,55 @@ __device__ __forceinline__ void run_pair(const DpArgs &a, const uint32_t *q, int
     }
 }
 
+template <int ALGO, int START, bool SECOND>
+__device__ __forceinline__ void dp_one(const DpArgs &a, uint32_t w, RowBuf rb, const uint2 *stab, bool fast_scores)
+{
+    const int i = a.order ? (int)a.order[w] : (int)w;
+    const int qlen = (int)a.q_len[i], tlen = (int)a.t_len[i];
+    Res r = {0, 0, 0, 0, 0, 0, 0, 0};
+    if (qlen > 0 && tlen > 0) {
+        const uint32_t *q = a.pq + (a.q_off[i] >> 3);
+        const uint32_t *t = a.pt + (a.t_off[i] >> 3);
+        const int qregs = (qlen + 7) >> 3, tregs = (tlen + 7) >> 3;
+        uint4 *tb = nullptr;
+        if (START == WITH_TB_ && (ALGO == LOCAL_ || ALGO == GLOBAL_)) {
+            tb = a.tb + a.tb_off[i];
+            /* two zero tile rows past the matrix: the GLOBAL traceback
+             * starts one past the last cell */
+            uint4 *z = tb + (size_t)tregs * 2 * qregs;
+            for (int k = 0; k < 4 * qregs; k++) z[k] = make_uint4(0, 0, 0, 0);
+        }
+        if (ALGO == KSW_) {
+            ksw(q, qlen, t, tlen, a.seed ? a.seed[i] : 0u, a.zdrop, a.sc, rb, r);
+        } else if (fast_scores && plain_words(q, qregs) && plain_words(t, tregs)) {
+            ScFast sf;
+            sf.tab = stab;
+            run_pair<ALGO, START, SECOND>(a, q, qregs, qlen, t, tregs, tlen, i, rb, tb, sf, r);
+        } else {
+            ScCmp scmp{};
+            run_pair<ALGO, START, SECOND>(a, q, qregs, qlen, t, tregs, tlen, i, rb, tb, scmp, r);
+        }
+    }
+    if (a.score) a.score[i] = r.score;
+    if (ALGO != GLOBAL_) {
+        if (a.q_end) a.q_end[i] = r.q_end;
+        if (a.t_end) a.t_end[i] = r.t_end;
+        if ((ALGO == LOCAL_ || ALGO == SEMI_GLOBAL_) && START == WITH_START_) {
+            if (a.q_start) a.q_start[i] = r.q_start;
+            if (a.t_start) a.t_start[i] = r.t_start;
+        }
+        if (SECOND && (ALGO == LOCAL_ || ALGO == SEMI_GLOBAL_)) {
+            if (a.score2) a.score2[i] = r.score2;
+            if (a.q_end2) a.q_end2[i] = r.q_end2;
+            if (a.t_end2) a.t_end2[i] = r.t_end2;
+        }
+    }
+}
+
+/* One pair per thread.  With a.queue set the launch is persistent: each warp
+ * takes the next 32 entries of the (length-binned) visiting order from a
+ * device counter until the batch is exhausted, so warps that drew short pairs
+ * come back for more instead of idling; without it, a grid-stride loop. */
 template <int ALGO, int START, bool SECOND, bool SMEM>
 __global__ void __launch_bounds__(128) dp_kernel(DpArgs a)
 {
@@ -64,47 +113,18 @@ __global__ void __launch_bounds__(128) dp_kernel(DpArgs a)
         rb.base = a.scratch + gtid;
         rb.stride = nthr;
     }
-    for (uint32_t w = gtid; w < (uint32_t)a.n; w += nthr) {
-        const int i = a.order ? (int)a.order[w] : (int)w;
-        const int qlen = (int)a.q_len[i], tlen = (int)a.t_len[i];
-        Res r = {0, 0, 0, 0, 0, 0, 0, 0};
-        if (qlen > 0 && tlen > 0) {
-            const uint32_t *q = a.pq + (a.q_off[i] >> 3);
-            const uint32_t *t = a.pt + (a.t_off[i] >> 3);
-            const int qregs = (qlen + 7) >> 3, tregs = (tlen + 7) >> 3;
-            uint4 *tb = nullptr;
-            if (START == WITH_TB_ && (ALGO == LOCAL_ || ALGO == GLOBAL_)) {
-                tb = a.tb + a.tb_off[i];
-                /* two zero tile rows past the matrix: the GLOBAL traceback
-                 * starts one past the last cell */
-                uint4 *z = tb + (size_t)tregs * 2 * qregs;
-                for (int k = 0; k < 4 * qregs; k++) z[k] = make_uint4(0, 0, 0, 0);
-            }
-            if (ALGO == KSW_) {
-                ksw(q, qlen, t, tlen, a.seed ? a.seed[i] : 0u, a.zdrop, a.sc, rb, r);
-            } else if (fast_scores && plain_words(q, qregs) && plain_words(t, tregs)) {
-                ScFast sf;
-                sf.tab = stab;
-                run_pair<ALGO, START, SECOND>(a, q, qregs, qlen, t, tregs, tlen, i, rb, tb, sf, r);
-            } else {
-                ScCmp scmp{};
-                run_pair<ALGO, START, SECOND>(a, q, qregs, qlen, t, tregs, tlen, i, rb, tb, scmp, r);
-            }
+    if (a.queue) {
+        const int lane = threadIdx.x & 31;
+        for (;;) {
+            uint32_t base = 0;
+            if (lane == 0) base = atomicAdd(a.queue, 32u);
+            base = __shfl_sync(0xFFFFFFFFu, base, 0);
+            if (base >= (uint32_t)a.n) break;
+            const uint32_t w = base + lane;
+            if (w < (uint32_t)a.n) dp_one<ALGO, START, SECOND>(a, w, rb, stab, fast_scores);
         }
-        if (a.score) a.score[i] = r.score;
-        if (ALGO != GLOBAL_) {
-            if (a.q_end) a.q_end[i] = r.q_end;
-            if (a.t_end) a.t_end[i] = r.t_end;
-            if ((ALGO == LOCAL_ || ALGO == SEMI_GLOBAL_) && START == WITH_START_) {
-                if (a.q_start) a.q_start[i] = r.q_start;
-                if (a.t_start) a.t_start[i] = r.t_start;
-            }
-            if (SECOND && (ALGO == LOCAL_ || ALGO == SEMI_GLOBAL_)) {
-                if (a.score2) a.score2[i] = r.score2;
-                if (a.q_end2) a.q_end2[i] = r.q_end2;
-                if (a.t_end2) a.t_end2[i] = r.t_end2;
-            }
-        }
+    } else {
+        for (uint32_t w = gtid; w < (uint32_t)a.n; w += nthr) dp_one<ALGO, START, SECOND>(a, w, rb, stab, fast_scores);
     }
 }
 
@@ -133,7 +153,14 @@ static cudaError_t launch_one(const DpArgs &a, int block, cudaStream_t s)
         auto k = dp_kernel<ALGO, START, SECOND, true>;
         cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return e;
-        const int blocks = (a.n + block - 1) / block;
+        int blocks = (a.n + block - 1) / block;
+        if (a.queue) {
+            int per_sm = 0;
+            e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, block, smem);
+            if (e != cudaSuccess) return e;
+            if (per_sm < 1) per_sm = 1;
+            if (blocks > per_sm * sms) blocks = per_sm * sms;
+        }
         k<<<blocks, block, smem, s>>>(a);
     } else {
         /* scratch holds scratch_cols columns for every thread of the grid */

@@ -193,6 +193,7 @@ static int launch_dp_split(int algo, int start, bool second, DpArgs a, const uin
         DpArgs rest = a;
         rest.order = order + nlong;
         rest.n = a.n - nlong;
+        if (rest.n > 0 && rest.queue) GB_CUDA(cudaMemsetAsync(rest.queue, 0, 4, s));
         if (rest.n > 0) {
             timing_mark(K_DP, true, s);
             GB_CUDA(launch_dp(algo, start, second, rest, block, 0, s));
@@ -202,6 +203,7 @@ static int launch_dp_split(int algo, int start, bool second, DpArgs a, const uin
         return GB_OK;
     }
     a.order = order;
+    if (a.queue) GB_CUDA(cudaMemsetAsync(a.queue, 0, 4, s));
     timing_mark(K_DP, true, s);
     GB_CUDA(launch_dp(algo, start, second, a, block, 0, s));
     timing_mark(K_DP, false, s);
@@ -265,6 +267,11 @@ int run_batch(const RunCfg &cfg, const DevBatch &b, const DevOut &o, Workspace &
     a.score = o.score, a.q_end = o.q_end, a.t_end = o.t_end, a.q_start = o.q_start, a.t_start = o.t_start;
     a.score2 = o.score2, a.q_end2 = o.q_end2, a.t_end2 = o.t_end2;
     a.sc = cfg.sc, a.head = cfg.head, a.tail = cfg.tail, a.k_band = cfg.k_band, a.zdrop = cfg.zdrop, a.mql = cfg.mql;
+    if (!ws.queue && cudaMalloc((void **)&ws.queue, 64) != cudaSuccess) {
+        cudaGetLastError();
+        return GB_ERR_ALLOC;
+    }
+    a.queue = ws.queue;
     if ((size_t)std::max(cols, 8) * block * 4 <= smem_limit) {
         a.smem_cols = std::max(cols, 8);
     } else {

@@ -59,6 +59,7 @@ struct Workspace {
     size_t order_cap = 0;
     uint32_t *bins = nullptr;    /* order_bins() class counters */
     cudaStream_t aux = nullptr;  /* second stream for the warp-cooperative kernel */
+    uint32_t *queue = nullptr;   /* work counter of the persistent one-thread launch */
     cudaEvent_t fork = nullptr, join = nullptr;
     ~Workspace();
 };

@@ -47,6 +47,7 @@ struct DpArgs {
     Scores sc;
     int32_t head, tail, k_band, zdrop, mql;
     int32_t smem_cols;                  /* columns per thread held in shared memory (0 = use scratch) */
+    uint32_t *queue;                    /* work counter of the persistent launch (zeroed), or null */
 };
 
 struct TbArgs {

@@ -169,9 +169,10 @@ int gb_align(const gb_params_t *p, const gb_batch_t *b, gb_out_t *o);
 
 /* Kernel-level entry point: pack -> reverse/complement -> alignment ->
  * traceback on inputs already in device memory, queued on `stream`
- * (a cudaStream_t, NULL = legacy default stream).  Uses a per-device
- * workspace the library grows on demand.  The device half of
- * gasal_aln_async (src/gasal_align.cu:180-264). */
+ * (a cudaStream_t, NULL = legacy default stream).  Uses a workspace per
+ * (device, stream) that the library grows on demand; calls on one stream must
+ * come from one host thread at a time.  The device half of gasal_aln_async
+ * (src/gasal_align.cu:180-264). */
 int gb_align_dev(const gb_params_t *p, const gb_dev_batch_t *b, const gb_dev_out_t *o, void *stream);
 
 /* Allocation-free variant of gb_align_dev, for callers that cannot call
