@@ -40,11 +40,11 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 from gasal_b200 import workloads as W  # noqa: E402
-from gasal_b200.capi import LOCAL, GLOBAL, SEMI_GLOBAL, Params  # noqa: E402
+from gasal_b200.capi import LOCAL, GLOBAL, SEMI_GLOBAL, KSW, Params  # noqa: E402
 
 UNIT = "pairs/s"
 # integer ops per cell, per algorithm (LOCAL 11, GLOBAL 9, SEMI_GLOBAL 10; +4 with traceback)
-OPS_PER_CELL = {LOCAL: 11, GLOBAL: 9, SEMI_GLOBAL: 10}
+OPS_PER_CELL = {LOCAL: 11, GLOBAL: 9, SEMI_GLOBAL: 10, KSW: 13}
 TB_OPS = 4
 
 WORKLOADS = {
@@ -54,6 +54,9 @@ WORKLOADS = {
     "w2": ("aligned pairs/s (2M-pair uneven-length GLOBAL WITH_TB batch, CIGAR out)",
            "w2: 2M pairs/GPU, GLOBAL WITH_TB, query log-uniform 50-1000, target = query with 1-8% subs and "
            "0.5-3% indels (len 1-10) per pair, scores 1/4/6/1", 2_000_000),
+    "w3": ("aligned pairs/s (ksw seed extension, z-drop 100, query 250-2000 bp)",
+           "w3: ksw extension, query U[250,2000], target = query with indel rate {0.5,2,5,10}% (len 1-3) + "
+           "1-5% subs per pair, h0 U[20,60], zdrop 100, scores 1/4/6/1", 400_000),
     "w0": ("aligned pairs/s (20k-pair LOCAL WITHOUT_START batch)",
            "w0: 20k pairs, LOCAL WITHOUT_START, q 100-150 with 0.1% N, t = q + 0-20 flanks, 2% subs, 0.5% "
            "indels", 20_000),
@@ -133,6 +136,8 @@ def build_workload(n: int, seed: int, name: str = "w1"):
     elif name == "w2":
         from gasal_b200.capi import WITH_TB
         parts = [(Params(algo=GLOBAL, start_pos=WITH_TB), W.workload2(n, seed=seed + 1))]
+    elif name == "w3":
+        parts = [(Params(algo=KSW, zdrop=100), W.workload3(n, seed=seed + 2))]
     else:
         parts = [(Params(algo=LOCAL), W.workload0(n, seed=seed - 1))]
     log(f"workload {name}: {n} pairs generated in {time.time() - t:.1f}s")
@@ -237,7 +242,8 @@ def main():
     for p, b in parts:
         d = {"q_t": t_(b.q), "t_t": t_(b.t), "qo": t_(b.q_off, np.int32), "to": t_(b.t_off, np.int32),
              "ql": t_(b.q_len, np.int32), "tl": t_(b.t_len, np.int32),
-             "qop": t_(b.q_op) if b.q_op is not None else None, "top": t_(b.t_op) if b.t_op is not None else None}
+             "qop": t_(b.q_op) if b.q_op is not None else None, "top": t_(b.t_op) if b.t_op is not None else None,
+             "seed": t_(b.seed, np.int32) if b.seed is not None else None}
         d["pq"] = torch.empty(b.q.shape[0] // 8, dtype=torch.int32, device=dev)
         d["pt"] = torch.empty(b.t.shape[0] // 8, dtype=torch.int32, device=dev)
         outs = {k: torch.empty(b.n, dtype=torch.int32, device=dev) for k in
@@ -249,7 +255,8 @@ def main():
              "pq": d["pq"].data_ptr(), "pt": d["pt"].data_ptr(), "q_off": d["qo"].data_ptr(),
              "t_off": d["to"].data_ptr(), "q_len": d["ql"].data_ptr(), "t_len": d["tl"].data_ptr(),
              "q_op": d["qop"].data_ptr() if d["qop"] is not None else None,
-             "t_op": d["top"].data_ptr() if d["top"] is not None else None}
+             "t_op": d["top"].data_ptr() if d["top"] is not None else None,
+             "seed": d["seed"].data_ptr() if d["seed"] is not None else None}
         for k, v in outs.items():
             m["out_" + k] = v.data_ptr()
         m["out_cigar"] = d["cigar"].data_ptr()
@@ -310,6 +317,9 @@ def main():
         nf = 5 + (3 if p.second_best else 0)
         if p.algo == GLOBAL:
             nf = 1
+        if p.algo == KSW:
+            nf = 3
+            h2d += 4 * b.n
         d2h += 4 * b.n * nf
         if p.start_pos == _TB:
             d2h += int(b.q.shape[0]) + 4 * b.n
@@ -337,6 +347,10 @@ def main():
            "d2h_bytes_per_step": d2h, "ms_per_step": e2e_ms,
            "path": "gasal_c_aln_async + gasal_c_is_aln_async_done (3 streams), pinned host batches"}
 
+    in_mb = sum(int(b.q.shape[0] + b.t.shape[0]) + 16 * b.n for _, b in parts) / 1e6
+    l2_note = (f"inputs {in_mb:.0f} MB > 126 MB L2, no flush" if in_mb > 126 else
+               f"inputs {in_mb:.0f} MB fit the 126 MB L2 (no flush: each step re-reads them, as a caller "
+               f"re-aligning resident batches would)")
     if rank == 0:
         cpu = None if args.no_cpu_baseline else cpu_baseline(parts)
         line = {
@@ -346,14 +360,15 @@ def main():
             "config": {"workload": WORKLOADS[args.workload][1],
                        "pairs_per_step_per_gpu": npairs, "cells_per_step_per_gpu": cells,
                        "parallelism": f"pair shards x{world}, no collective in the data path",
-                       "l2": "inputs 384 MB > 126 MB L2, no flush"},
+                       "l2": l2_note},
             "gcups": cells * world / (ms_step * 1e-3) / 1e9,
             "roofline": {"bound": "int32", "achieved": achieved, "peak": peak["iadd_tops"], "unit": "Tops/s",
                          "frac": achieved / peak["iadd_tops"],
                          "traffic": DP_TRAFFIC_BYTES if args.workload == "w1" else None,
                          "kernel": "dp_kernel / dp_wc_kernel (one DP launch per algorithm per step)",
                          "dp_ms_per_step": dp_ms / args.steps,
-                         "ops_per_cell": {"local": 11, "global": 9, "semi_global": 10, "traceback_extra": 4},
+                         "ops_per_cell": {"local": 11, "global": 9, "semi_global": 10, "ksw": 13,
+                                          "traceback_extra": 4},
                          "peak_source": "measured live: 2-input int32 add issue rate (gb_probe_int_peak)",
                          "imnmx_tops": peak["imnmx_tops"], "dpx_tops": peak["dpx_tops"]},
             "kernel_ms_per_step": {k: v[0] / args.steps for k, v in kt.items()},

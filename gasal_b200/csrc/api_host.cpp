@@ -19,6 +19,7 @@
 #include <cmath>
 #include <cstring>
 #include <memory>
+#include <atomic>
 #include <mutex>
 #include <string>
 #include <unordered_map>
@@ -191,6 +192,8 @@ struct StreamState {
     gb::Workspace ws;
     uint32_t *d_n_cigar = nullptr;
     size_t n_cigar_cap = 0;
+    cudaGraphExec_t exec = nullptr; /* the storage's batch graph */
+    std::vector<uint8_t> sig;       /* what `exec` was captured for */
 };
 
 std::mutex g_mu;
@@ -227,6 +230,112 @@ void release_state(const gasal_gpu_storage_t *s)
     if (w.join) cudaEventDestroy(w.join);
     if (w.bins) cudaFree(w.bins);
     if (p->d_n_cigar) cudaFree(p->d_n_cigar);
+    if (p->exec) cudaGraphExecDestroy(p->exec);
+}
+
+/* graph statistics: 0 relaunched, 1 captured and updated in place,
+ * 2 captured and instantiated, 3 capture failed (ran without a graph) */
+std::atomic<int64_t> g_graph_stats[4];
+void graph_stat(int k) { g_graph_stats[k].fetch_add(1, std::memory_order_relaxed); }
+
+template <class T> void put(std::vector<uint8_t> &v, const T &x)
+{
+    const uint8_t *p = reinterpret_cast<const uint8_t *>(&x);
+    v.insert(v.end(), p, p + sizeof(T));
+}
+
+/* Everything a captured batch graph depends on except the contents of the
+ * buffers it copies: sizes, options, every pointer the copies and kernels
+ * take (host pages included), and the engine plan. */
+void batch_signature(std::vector<uint8_t> &v, const gasal_gpu_storage_t *s, const StreamState &ss,
+                     const Parameters *params, uint32_t n, uint32_t qbytes, uint32_t tbytes, const gb::RunCfg &cfg,
+                     const gb::Plan &plan)
+{
+    v.clear();
+    v.reserve(1024);
+    int dev = -1;
+    cudaGetDevice(&dev);
+    put(v, dev), put(v, n), put(v, qbytes), put(v, tbytes);
+    put(v, params->algo), put(v, params->start_pos), put(v, params->secondBest), put(v, params->isPacked);
+    put(v, params->isReverseComplement), put(v, params->k_band);
+    put(v, params->semiglobal_skipping_head), put(v, params->semiglobal_skipping_tail);
+    put(v, cfg.sc), put(v, cfg.ref_reverse), put(v, cfg.mql), put(v, cfg.zdrop);
+    for (const host_batch_t *p = s->extensible_host_unpacked_query_batch; p; p = p->next)
+        put(v, (const void *)p->data), put(v, p->offset), put(v, p->data_size);
+    put(v, -1);
+    for (const host_batch_t *p = s->extensible_host_unpacked_target_batch; p; p = p->next)
+        put(v, (const void *)p->data), put(v, p->offset), put(v, p->data_size);
+    put(v, -1);
+    const void *ptrs[] = {s->unpacked_query_batch, s->unpacked_target_batch, s->packed_query_batch,
+                          s->packed_target_batch, s->query_batch_offsets, s->target_batch_offsets,
+                          s->query_batch_lens, s->target_batch_lens, s->query_op, s->target_op, s->seed_scores,
+                          s->host_query_batch_lens, s->host_target_batch_lens, s->host_query_batch_offsets,
+                          s->host_target_batch_offsets, s->host_query_op, s->host_target_op, s->host_seed_scores,
+                          ss.d_n_cigar, ss.ws.tb, ss.ws.d_tb_off, ss.ws.h_tb_off, ss.ws.order, ss.ws.bins,
+                          ss.ws.queue, ss.ws.aux, ss.ws.fork, ss.ws.join, (const void *)s->str};
+    for (const void *q : ptrs) put(v, q);
+    const gasal_res_t *rs[] = {s->host_res, s->device_cpy, s->host_res_second, s->device_cpy_second};
+    for (const gasal_res_t *r : rs) {
+        put(v, (const void *)r);
+        if (!r) continue;
+        put(v, (const void *)r->aln_score), put(v, (const void *)r->query_batch_start);
+        put(v, (const void *)r->target_batch_start), put(v, (const void *)r->query_batch_end);
+        put(v, (const void *)r->target_batch_end), put(v, (const void *)r->cigar);
+        put(v, (const void *)r->n_cigar_ops);
+    }
+    put(v, plan.tb), put(v, plan.second), put(v, plan.use_wc), put(v, plan.order_on);
+    put(v, plan.start), put(v, plan.block), put(v, plan.mq8), put(v, plan.mt8), put(v, plan.wc_min_q);
+    put(v, plan.a);
+    for (int c : plan.cut) put(v, c);
+    put(v, -1);
+    for (int c : plan.nlong) put(v, c);
+}
+
+/* Captures issue() on stream st into a graph, updates (or instantiates) the
+ * storage's executable graph from it, and launches that.  When the capture
+ * itself is refused, issue() runs again without a graph. */
+template <class F> cudaError_t capture_and_launch(StreamState &ss, F &issue, cudaStream_t st)
+{
+    cudaError_t ce = cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal);
+    if (ce != cudaSuccess) {
+        cudaGetLastError();
+        graph_stat(3);
+        return issue();
+    }
+    const cudaError_t ie = issue();
+    cudaGraph_t g = nullptr;
+    ce = cudaStreamEndCapture(st, &g);
+    if (ie != cudaSuccess || ce != cudaSuccess || !g) {
+        if (g) cudaGraphDestroy(g);
+        cudaGetLastError();
+        if (ss.exec) cudaGraphExecDestroy(ss.exec);
+        ss.exec = nullptr;
+        graph_stat(3);
+        if (ie != cudaSuccess) return ie; /* a failure of the operations themselves */
+        return issue();
+    }
+    bool updated = false;
+    if (ss.exec) {
+        cudaGraphExecUpdateResultInfo info;
+        if (cudaGraphExecUpdate(ss.exec, g, &info) == cudaSuccess) {
+            updated = true;
+        } else {
+            cudaGetLastError();
+            cudaGraphExecDestroy(ss.exec);
+            ss.exec = nullptr;
+        }
+    }
+    if (!ss.exec) {
+        ce = cudaGraphInstantiate(&ss.exec, g, 0);
+        if (ce != cudaSuccess) {
+            ss.exec = nullptr;
+            cudaGraphDestroy(g);
+            return ce;
+        }
+    }
+    cudaGraphDestroy(g);
+    graph_stat(updated ? 1 : 2);
+    return cudaGraphLaunch(ss.exec, st);
 }
 
 uint32_t round8(uint32_t x) { return (x + 7u) & ~7u; }
@@ -709,7 +818,11 @@ static int grow_dev(void **p, uint32_t old_bytes, uint32_t new_bytes)
     return cudaMalloc(p, new_bytes) == cudaSuccess ? GB_OK : GB_ERR_ALLOC;
 }
 
-int aln_async(gasal_gpu_storage_t *s, uint32_t qbytes, uint32_t tbytes, uint32_t n, Parameters *params, bool fatal)
+/* zdrop: the ksw z-drop threshold.  GASAL2's kernel hard-codes 0
+ * (src/kernels/ksw_kernel_template.h:62), so gasal_aln_async passes 0; the
+ * one-shot C entry point passes its caller's value. */
+int aln_async(gasal_gpu_storage_t *s, uint32_t qbytes, uint32_t tbytes, uint32_t n, Parameters *params, bool fatal,
+              int zdrop)
 {
     Errs E{fatal};
     char msg[512];
@@ -806,44 +919,11 @@ int aln_async(gasal_gpu_storage_t *s, uint32_t qbytes, uint32_t tbytes, uint32_t
     }
 
     cudaStream_t st = s->str;
-    cudaError_t ce = cudaSuccess;
-#define GB_Q(call)                                                                                  \
-    do {                                                                                            \
-        ce = (call);                                                                                \
-        if (ce != cudaSuccess) {                                                                    \
-            snprintf(msg, sizeof msg, "[GASAL CUDA ERROR:] %s(CUDA error no.=%d). Line no. %d in file %s\n", \
-                     cudaGetErrorString(ce), ce, __LINE__, __FILE__);                               \
-            return E.fail(GB_ERR_CUDA, msg);                                                        \
-        }                                                                                           \
-    } while (0)
-
-    /* host pages -> device (src/gasal_align.cu:152-175) */
-    for (host_batch_t *p = s->extensible_host_unpacked_query_batch; p; p = p->next)
-        if (p->data_size) GB_Q(cudaMemcpyAsync(s->unpacked_query_batch + p->offset, p->data, p->data_size, cudaMemcpyHostToDevice, st));
-    for (host_batch_t *p = s->extensible_host_unpacked_target_batch; p; p = p->next)
-        if (p->data_size) GB_Q(cudaMemcpyAsync(s->unpacked_target_batch + p->offset, p->data, p->data_size, cudaMemcpyHostToDevice, st));
-    GB_Q(cudaMemcpyAsync(s->query_batch_lens, s->host_query_batch_lens, n * 4, cudaMemcpyHostToDevice, st));
-    GB_Q(cudaMemcpyAsync(s->target_batch_lens, s->host_target_batch_lens, n * 4, cudaMemcpyHostToDevice, st));
-    GB_Q(cudaMemcpyAsync(s->query_batch_offsets, s->host_query_batch_offsets, n * 4, cudaMemcpyHostToDevice, st));
-    GB_Q(cudaMemcpyAsync(s->target_batch_offsets, s->host_target_batch_offsets, n * 4, cudaMemcpyHostToDevice, st));
-    if (params->algo == KSW) {
-        if (s->seed_scores == NULL || s->host_seed_scores == NULL) {
-            if (s->seed_scores == NULL) fprintf(stderr, "seed_scores == NULL\n");
-            if (s->host_seed_scores == NULL) fprintf(stderr, "host_seed_scores == NULL\n");
-            return E.fail(GB_ERR_ARG, "");
-        }
-        GB_Q(cudaMemcpyAsync(s->seed_scores, s->host_seed_scores, n * 4, cudaMemcpyHostToDevice, st));
-    }
-    if (params->isReverseComplement) {
-        GB_Q(cudaMemcpyAsync(s->query_op, s->host_query_op, n, cudaMemcpyHostToDevice, st));
-        GB_Q(cudaMemcpyAsync(s->target_op, s->host_target_op, n, cudaMemcpyHostToDevice, st));
-    }
-
     const gb::Settings &set = gb::settings();
     gb::RunCfg cfg{};
     cfg.algo = params->algo, cfg.start = params->start_pos, cfg.second = params->secondBest == TRUE;
     cfg.head = params->semiglobal_skipping_head, cfg.tail = params->semiglobal_skipping_tail;
-    cfg.k_band = params->k_band, cfg.zdrop = 0, cfg.sc = set.sc;
+    cfg.k_band = params->k_band, cfg.zdrop = zdrop, cfg.sc = set.sc;
     cfg.ref_reverse = set.ref_reverse, cfg.mql = set.mql, cfg.is_packed = params->isPacked;
     cfg.reverse_complement = params->isReverseComplement;
     gb::DevBatch b{};
@@ -863,29 +943,103 @@ int aln_async(gasal_gpu_storage_t *s, uint32_t qbytes, uint32_t tbytes, uint32_t
         o.t_end2 = s->device_cpy_second->target_batch_end;
     }
     o.cigar = s->unpacked_query_batch, o.n_cigar = ss.d_n_cigar;
-    const int rc = gb::run_batch(cfg, b, o, ss.ws, st);
+    if (params->algo == KSW && (s->seed_scores == NULL || s->host_seed_scores == NULL)) {
+        if (s->seed_scores == NULL) fprintf(stderr, "seed_scores == NULL\n");
+        if (s->host_seed_scores == NULL) fprintf(stderr, "host_seed_scores == NULL\n");
+        return E.fail(GB_ERR_ARG, "");
+    }
+
+    /* every host decision and allocation of the batch */
+    gb::Plan plan;
+    int rc = gb::plan_batch(cfg, b, o, ss.ws, plan);
     if (rc != GB_OK) return E.fail(rc, "[GASAL ERROR:] alignment launch failed\n");
 
-    /* results -> host (src/gasal_align.cu:266-304) */
-    gasal_res_t *h = s->host_res, *d = s->device_cpy;
-    if (h->aln_score && d->aln_score) GB_Q(cudaMemcpyAsync(h->aln_score, d->aln_score, n * 4, cudaMemcpyDeviceToHost, st));
-    if (h->query_batch_start && d->query_batch_start) GB_Q(cudaMemcpyAsync(h->query_batch_start, d->query_batch_start, n * 4, cudaMemcpyDeviceToHost, st));
-    if (h->target_batch_start && d->target_batch_start) GB_Q(cudaMemcpyAsync(h->target_batch_start, d->target_batch_start, n * 4, cudaMemcpyDeviceToHost, st));
-    if (h->query_batch_end && d->query_batch_end) GB_Q(cudaMemcpyAsync(h->query_batch_end, d->query_batch_end, n * 4, cudaMemcpyDeviceToHost, st));
-    if (h->target_batch_end && d->target_batch_end) GB_Q(cudaMemcpyAsync(h->target_batch_end, d->target_batch_end, n * 4, cudaMemcpyDeviceToHost, st));
-    if (params->start_pos == WITH_TB) {
-        if (h->cigar) GB_Q(cudaMemcpyAsync(h->cigar, s->unpacked_query_batch, qbytes, cudaMemcpyDeviceToHost, st));
-        if (h->n_cigar_ops) GB_Q(cudaMemcpyAsync(h->n_cigar_ops, ss.d_n_cigar, n * 4, cudaMemcpyDeviceToHost, st));
-    }
-    if (params->secondBest && s->host_res_second && s->device_cpy_second) {
-        gasal_res_t *h2 = s->host_res_second, *d2 = s->device_cpy_second;
-        if (h2->aln_score && d2->aln_score) GB_Q(cudaMemcpyAsync(h2->aln_score, d2->aln_score, n * 4, cudaMemcpyDeviceToHost, st));
-        if (h2->query_batch_end && d2->query_batch_end) GB_Q(cudaMemcpyAsync(h2->query_batch_end, d2->query_batch_end, n * 4, cudaMemcpyDeviceToHost, st));
-        if (h2->target_batch_end && d2->target_batch_end) GB_Q(cudaMemcpyAsync(h2->target_batch_end, d2->target_batch_end, n * 4, cudaMemcpyDeviceToHost, st));
-    }
+    /* the stream operations of the batch: host pages -> device
+     * (src/gasal_align.cu:152-175), the kernels, results -> host
+     * (src/gasal_align.cu:266-304) */
+    int err_line = 0;
+    auto issue = [&]() -> cudaError_t {
+        cudaError_t ce = cudaSuccess;
+#define GB_Q(call)                                                                                  \
+    do {                                                                                            \
+        ce = (call);                                                                                \
+        if (ce != cudaSuccess) {                                                                    \
+            err_line = __LINE__;                                                                    \
+            return ce;                                                                              \
+        }                                                                                           \
+    } while (0)
+        for (host_batch_t *p = s->extensible_host_unpacked_query_batch; p; p = p->next)
+            if (p->data_size) GB_Q(cudaMemcpyAsync(s->unpacked_query_batch + p->offset, p->data, p->data_size, cudaMemcpyHostToDevice, st));
+        for (host_batch_t *p = s->extensible_host_unpacked_target_batch; p; p = p->next)
+            if (p->data_size) GB_Q(cudaMemcpyAsync(s->unpacked_target_batch + p->offset, p->data, p->data_size, cudaMemcpyHostToDevice, st));
+        GB_Q(cudaMemcpyAsync(s->query_batch_lens, s->host_query_batch_lens, n * 4, cudaMemcpyHostToDevice, st));
+        GB_Q(cudaMemcpyAsync(s->target_batch_lens, s->host_target_batch_lens, n * 4, cudaMemcpyHostToDevice, st));
+        GB_Q(cudaMemcpyAsync(s->query_batch_offsets, s->host_query_batch_offsets, n * 4, cudaMemcpyHostToDevice, st));
+        GB_Q(cudaMemcpyAsync(s->target_batch_offsets, s->host_target_batch_offsets, n * 4, cudaMemcpyHostToDevice, st));
+        if (params->algo == KSW)
+            GB_Q(cudaMemcpyAsync(s->seed_scores, s->host_seed_scores, n * 4, cudaMemcpyHostToDevice, st));
+        if (params->isReverseComplement) {
+            GB_Q(cudaMemcpyAsync(s->query_op, s->host_query_op, n, cudaMemcpyHostToDevice, st));
+            GB_Q(cudaMemcpyAsync(s->target_op, s->host_target_op, n, cudaMemcpyHostToDevice, st));
+        }
+        rc = gb::enqueue_batch(cfg, b, o, ss.ws, plan, st);
+        if (rc != GB_OK) {
+            err_line = __LINE__;
+            return cudaErrorUnknown;
+        }
+        gasal_res_t *h = s->host_res, *d = s->device_cpy;
+        if (h->aln_score && d->aln_score) GB_Q(cudaMemcpyAsync(h->aln_score, d->aln_score, n * 4, cudaMemcpyDeviceToHost, st));
+        if (h->query_batch_start && d->query_batch_start) GB_Q(cudaMemcpyAsync(h->query_batch_start, d->query_batch_start, n * 4, cudaMemcpyDeviceToHost, st));
+        if (h->target_batch_start && d->target_batch_start) GB_Q(cudaMemcpyAsync(h->target_batch_start, d->target_batch_start, n * 4, cudaMemcpyDeviceToHost, st));
+        if (h->query_batch_end && d->query_batch_end) GB_Q(cudaMemcpyAsync(h->query_batch_end, d->query_batch_end, n * 4, cudaMemcpyDeviceToHost, st));
+        if (h->target_batch_end && d->target_batch_end) GB_Q(cudaMemcpyAsync(h->target_batch_end, d->target_batch_end, n * 4, cudaMemcpyDeviceToHost, st));
+        if (params->start_pos == WITH_TB) {
+            if (h->cigar) GB_Q(cudaMemcpyAsync(h->cigar, s->unpacked_query_batch, qbytes, cudaMemcpyDeviceToHost, st));
+            if (h->n_cigar_ops) GB_Q(cudaMemcpyAsync(h->n_cigar_ops, ss.d_n_cigar, n * 4, cudaMemcpyDeviceToHost, st));
+        }
+        if (params->secondBest && s->host_res_second && s->device_cpy_second) {
+            gasal_res_t *h2 = s->host_res_second, *d2 = s->device_cpy_second;
+            if (h2->aln_score && d2->aln_score) GB_Q(cudaMemcpyAsync(h2->aln_score, d2->aln_score, n * 4, cudaMemcpyDeviceToHost, st));
+            if (h2->query_batch_end && d2->query_batch_end) GB_Q(cudaMemcpyAsync(h2->query_batch_end, d2->query_batch_end, n * 4, cudaMemcpyDeviceToHost, st));
+            if (h2->target_batch_end && d2->target_batch_end) GB_Q(cudaMemcpyAsync(h2->target_batch_end, d2->target_batch_end, n * 4, cudaMemcpyDeviceToHost, st));
+        }
 #undef GB_Q
+        return cudaSuccess;
+    };
+
+    cudaError_t ce = cudaSuccess;
+    if (set.graphs && !gb::timing_on()) {
+        /* One CUDA graph per storage: relaunched as is while the batch has the
+         * same signature, else recaptured and updated in place. */
+        std::vector<uint8_t> sig;
+        batch_signature(sig, s, ss, params, n, qbytes, tbytes, cfg, plan);
+        if (ss.exec && sig == ss.sig) {
+            ce = cudaGraphLaunch(ss.exec, st);
+            if (ce == cudaSuccess) graph_stat(0);
+        } else {
+            ce = capture_and_launch(ss, issue, st);
+            if (ce == cudaSuccess) ss.sig.swap(sig);
+            else ss.sig.clear();
+        }
+        if (ce != cudaSuccess && err_line == 0) err_line = __LINE__;
+    } else {
+        ce = issue();
+    }
+    if (ce != cudaSuccess) {
+        if (rc != GB_OK) return E.fail(rc, "[GASAL ERROR:] alignment launch failed\n");
+        snprintf(msg, sizeof msg, "[GASAL CUDA ERROR:] %s(CUDA error no.=%d). Line no. %d in file %s\n",
+                 cudaGetErrorString(ce), ce, err_line, __FILE__);
+        return E.fail(GB_ERR_CUDA, msg);
+    }
+    if (plan.tb && cudaEventRecord(ss.ws.tb_off_free, st) != cudaSuccess)
+        return E.fail(GB_ERR_CUDA, "[GASAL CUDA ERROR:] event record failed\n");
     s->is_free = 0;
     return GB_OK;
+}
+
+void graph_stats(int64_t out[4])
+{
+    for (int k = 0; k < 4; k++) out[k] = g_graph_stats[k].load();
 }
 
 int is_done(gasal_gpu_storage_t *s, bool fatal)
@@ -910,7 +1064,7 @@ int is_done(gasal_gpu_storage_t *s, bool fatal)
 void gasal_aln_async(gasal_gpu_storage_t *gpu_storage, const uint32_t actual_query_batch_bytes,
                      const uint32_t actual_target_batch_bytes, const uint32_t actual_n_alns, Parameters *params)
 {
-    gbapi::aln_async(gpu_storage, actual_query_batch_bytes, actual_target_batch_bytes, actual_n_alns, params, true);
+    gbapi::aln_async(gpu_storage, actual_query_batch_bytes, actual_target_batch_bytes, actual_n_alns, params, true, 0);
 }
 
 int gasal_is_aln_async_done(gasal_gpu_storage_t *gpu_storage) { return gbapi::is_done(gpu_storage, true); }

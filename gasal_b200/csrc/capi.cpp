@@ -14,12 +14,25 @@
 #include <vector>
 
 namespace gbapi {
-int aln_async(gasal_gpu_storage_t *s, uint32_t qbytes, uint32_t tbytes, uint32_t n, Parameters *params, bool fatal);
+int aln_async(gasal_gpu_storage_t *s, uint32_t qbytes, uint32_t tbytes, uint32_t n, Parameters *params, bool fatal,
+              int zdrop);
 int is_done(gasal_gpu_storage_t *s, bool fatal);
+void graph_stats(int64_t out[4]);
 }
 
 static Parameters *P(void *p) { return static_cast<Parameters *>(p); }
 static gasal_gpu_storage_t *S(void *s) { return static_cast<gasal_gpu_storage_t *>(s); }
+
+/* The ksw z-drop of each C parameter object (GASAL2's Parameters has no such
+ * member; its kernel hard-codes 0). */
+static std::mutex g_zdrop_mu;
+static std::unordered_map<const void *, int> g_zdrop;
+static int zdrop_of(const void *params)
+{
+    std::lock_guard<std::mutex> lk(g_zdrop_mu);
+    auto it = g_zdrop.find(params);
+    return it == g_zdrop.end() ? 0 : it->second;
+}
 
 extern "C" {
 
@@ -37,10 +50,19 @@ int gasal_c_params_set(void *params, const gb_params_t *p)
     q->k_band = p->k_band;
     q->isReverseComplement = p->reverse_complement != 0;
     q->sa = p->match, q->sb = p->mismatch, q->gapo = p->gap_open, q->gape = p->gap_extend;
+    std::lock_guard<std::mutex> lk(g_zdrop_mu);
+    g_zdrop[params] = p->zdrop > 0 ? p->zdrop : 0;
     return GB_OK;
 }
 
-void gasal_c_params_free(void *params) { delete P(params); }
+void gasal_c_params_free(void *params)
+{
+    {
+        std::lock_guard<std::mutex> lk(g_zdrop_mu);
+        g_zdrop.erase(params);
+    }
+    delete P(params);
+}
 
 int gasal_c_copy_subst_scores(int32_t match, int32_t mismatch, int32_t gap_open, int32_t gap_extend)
 {
@@ -165,7 +187,7 @@ int gasal_c_set_device(int gpu)
 int gasal_c_aln_async(void *storage, uint32_t qb, uint32_t tb, uint32_t n, void *params)
 {
     if (!storage || !params) return GB_ERR_ARG;
-    return gbapi::aln_async(S(storage), qb, tb, n, P(params), false);
+    return gbapi::aln_async(S(storage), qb, tb, n, P(params), false, zdrop_of(params));
 }
 
 int gasal_c_is_aln_async_done(void *storage)
@@ -216,7 +238,7 @@ int gb_align(const gb_params_t *p, const gb_batch_t *b, gb_out_t *o)
         for (int i = 0; i < n; i++) s->host_seed_scores[i] = b->seed ? b->seed[i] : 0u;
     }
     s->current_n_alns = n;
-    int rc = gbapi::aln_async(s, b->q_bytes, b->t_bytes, n, &params, false);
+    int rc = gbapi::aln_async(s, b->q_bytes, b->t_bytes, n, &params, false, p->zdrop);
     if (rc == GB_OK) {
         cudaError_t e = cudaStreamSynchronize(s->str);
         rc = e == cudaSuccess ? GB_OK : GB_ERR_CUDA;
@@ -262,36 +284,107 @@ std::mutex g_dev_mu;
 std::unordered_map<unsigned long long, DevWs *> g_dev_ws;
 } // namespace
 
-extern "C" int gb_align_dev(const gb_params_t *p, const gb_dev_batch_t *b, const gb_dev_out_t *o, void *stream)
+namespace {
+DevWs *dev_ws(void *stream)
 {
-    if (!p || !b || !o || b->n <= 0 || !b->h_q_len || !b->h_t_len) return GB_ERR_ARG;
     int dev = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess) return GB_ERR_CUDA;
-    DevWs *w;
-    {
-        std::lock_guard<std::mutex> lk(g_dev_mu);
-        const unsigned long long key = ((unsigned long long)(uintptr_t)stream << 8) ^ (unsigned long long)dev;
-        DevWs *&slot = g_dev_ws[key];
-        if (!slot) slot = new DevWs();
-        w = slot;
-    }
+    if (cudaGetDevice(&dev) != cudaSuccess) return nullptr;
+    std::lock_guard<std::mutex> lk(g_dev_mu);
+    const unsigned long long key = ((unsigned long long)(uintptr_t)stream << 8) ^ (unsigned long long)dev;
+    DevWs *&slot = g_dev_ws[key];
+    if (!slot) slot = new DevWs();
+    return slot;
+}
+
+void dev_args(const gb_params_t *p, const gb_dev_batch_t *b, const gb_dev_out_t *o, gb::RunCfg &cfg,
+              gb::DevBatch &db, gb::DevOut &dout)
+{
     const gb::Settings &set = gb::settings();
-    gb::RunCfg cfg{};
+    cfg = gb::RunCfg{};
     cfg.algo = p->algo, cfg.start = p->start_pos, cfg.second = p->second_best != 0;
     cfg.head = p->head, cfg.tail = p->tail, cfg.k_band = p->k_band, cfg.zdrop = p->zdrop;
     cfg.sc = {p->match, p->mismatch, p->gap_open, p->gap_extend, p->gap_open + p->gap_extend};
     cfg.ref_reverse = set.ref_reverse, cfg.mql = set.mql, cfg.is_packed = 0;
     cfg.reverse_complement = p->reverse_complement;
-    gb::DevBatch db{};
+    db = gb::DevBatch{};
     db.n = b->n, db.q_bytes = b->q_bytes, db.t_bytes = b->t_bytes, db.q = b->q, db.t = b->t;
     db.pq = b->pq, db.pt = b->pt, db.q_off = b->q_off, db.t_off = b->t_off, db.q_len = b->q_len;
     db.t_len = b->t_len, db.q_op = b->q_op, db.t_op = b->t_op, db.seed = b->seed;
     db.h_q_len = b->h_q_len, db.h_t_len = b->h_t_len;
-    gb::DevOut dout{};
+    dout = gb::DevOut{};
     dout.score = o->score, dout.q_end = o->q_end, dout.t_end = o->t_end, dout.q_start = o->q_start;
     dout.t_start = o->t_start, dout.score2 = o->score2, dout.q_end2 = o->q_end2, dout.t_end2 = o->t_end2;
     dout.cigar = o->cigar, dout.n_cigar = o->n_cigar;
+}
+} // namespace
+
+extern "C" int gb_align_dev(const gb_params_t *p, const gb_dev_batch_t *b, const gb_dev_out_t *o, void *stream)
+{
+    if (!p || !b || !o || b->n <= 0 || !b->h_q_len || !b->h_t_len) return GB_ERR_ARG;
+    DevWs *w = dev_ws(stream);
+    if (!w) return GB_ERR_CUDA;
+    gb::RunCfg cfg;
+    gb::DevBatch db;
+    gb::DevOut dout;
+    dev_args(p, b, o, cfg, db, dout);
     return gb::run_batch(cfg, db, dout, w->ws, (cudaStream_t)stream);
+}
+
+/* Launch autotuner: times the batch under every candidate setting (CUDA
+ * events on `stream`, `reps` runs after one warm-up run each) and keeps the
+ * fastest.  Candidates: DP block 32/64/128 x warp-cooperative threshold
+ * 32/40/48/64/96 query words (LOCAL/GLOBAL only; other algorithms keep the
+ * current threshold). */
+extern "C" int gb_autotune(const gb_params_t *p, const gb_dev_batch_t *b, const gb_dev_out_t *o, void *stream,
+                           int reps, gb_tuning_t *best, double *best_ms)
+{
+    if (!p || !b || !o || b->n <= 0 || !b->h_q_len || !b->h_t_len || reps <= 0 || !best) return GB_ERR_ARG;
+    DevWs *w = dev_ws(stream);
+    if (!w) return GB_ERR_CUDA;
+    gb::RunCfg cfg;
+    gb::DevBatch db;
+    gb::DevOut dout;
+    dev_args(p, b, o, cfg, db, dout);
+    gb::Settings &st = gb::settings();
+    const gb::Settings saved = st;
+    const cudaStream_t s = (cudaStream_t)stream;
+    std::vector<int> blocks = {32, 64, 128};
+    std::vector<int> wcs = {st.wc_min_qregs};
+    if (p->algo == LOCAL || p->algo == GLOBAL) wcs = {32, 40, 48, 64, 96};
+    cudaEvent_t e0, e1;
+    if (cudaEventCreate(&e0) != cudaSuccess) return GB_ERR_CUDA;
+    if (cudaEventCreate(&e1) != cudaSuccess) {
+        cudaEventDestroy(e0);
+        return GB_ERR_CUDA;
+    }
+    int rc = GB_OK;
+    float best_t = 0.f;
+    gb_tuning_t bt{saved.block, saved.wc_min_qregs, saved.min_order_pairs};
+    for (int blk : blocks) {
+        for (int wc : wcs) {
+            st.block = blk, st.wc_min_qregs = wc;
+            rc = gb::run_batch(cfg, db, dout, w->ws, s);
+            for (int r = 0; r < reps && rc == GB_OK; r++) {
+                if (r == 0 && cudaEventRecord(e0, s) != cudaSuccess) rc = GB_ERR_CUDA;
+                if (rc == GB_OK) rc = gb::run_batch(cfg, db, dout, w->ws, s);
+            }
+            float ms = 0.f;
+            if (rc == GB_OK && (cudaEventRecord(e1, s) != cudaSuccess || cudaEventSynchronize(e1) != cudaSuccess ||
+                                cudaEventElapsedTime(&ms, e0, e1) != cudaSuccess))
+                rc = GB_ERR_CUDA;
+            if (rc != GB_OK) break;
+            if (best_t == 0.f || ms < best_t) best_t = ms, bt.block = blk, bt.wc_min_qregs = wc;
+        }
+        if (rc != GB_OK) break;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    st = saved;
+    if (rc != GB_OK) return rc;
+    st.block = bt.block, st.wc_min_qregs = bt.wc_min_qregs;
+    *best = bt;
+    if (best_ms) *best_ms = best_t / reps;
+    return GB_OK;
 }
 
 extern "C" int gb_set_reference_reverse(int on)
@@ -311,6 +404,37 @@ extern "C" int gb_set_tb_budget_mb(int64_t mb)
 {
     if (mb <= 0) return GB_ERR_ARG;
     gb::settings().tb_budget_bytes = (size_t)mb << 20;
+    return GB_OK;
+}
+
+extern "C" int gb_set_graphs(int on)
+{
+    gb::settings().graphs = on ? 1 : 0;
+    return GB_OK;
+}
+
+extern "C" int gb_graph_stats(int64_t *counts)
+{
+    if (!counts) return GB_ERR_ARG;
+    gbapi::graph_stats(counts);
+    return GB_OK;
+}
+
+extern "C" int gb_set_tuning(const gb_tuning_t *t)
+{
+    if (!t) return GB_ERR_ARG;
+    if (t->block != 32 && t->block != 64 && t->block != 128) return GB_ERR_ARG;
+    if (t->wc_min_qregs < 32 || t->min_order_pairs < 0) return GB_ERR_ARG; /* the warp kernel needs 32+ words */
+    gb::Settings &st = gb::settings();
+    st.block = t->block, st.wc_min_qregs = t->wc_min_qregs, st.min_order_pairs = t->min_order_pairs;
+    return GB_OK;
+}
+
+extern "C" int gb_get_tuning(gb_tuning_t *t)
+{
+    if (!t) return GB_ERR_ARG;
+    const gb::Settings &st = gb::settings();
+    t->block = st.block, t->wc_min_qregs = st.wc_min_qregs, t->min_order_pairs = st.min_order_pairs;
     return GB_OK;
 }
 

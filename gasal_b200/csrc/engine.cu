@@ -143,30 +143,143 @@ static int grow(void **p, size_t *cap, size_t need, size_t elem)
         }                                                                                              \
     } while (0)
 
-/* Length-binned order for pairs [0, n) of the given length arrays; returns
- * nullptr (identity order) for small batches. */
-static const uint32_t *binned_order(const uint32_t *q_len, const uint32_t *t_len, int n, Workspace &ws,
-                                    cudaStream_t s, int *err, bool force)
+/* ---------------------------------------------------------------------- */
+/* Planning: every host-side decision and every allocation of a batch, so
+ * that enqueue_batch() issues stream operations only (and can be captured
+ * into a CUDA graph). */
+
+static int ensure_order_buffers(Workspace &ws, size_t n)
 {
-    *err = GB_OK;
-    if (!force && n < settings().min_order_pairs) return nullptr;
-    if (grow((void **)&ws.order, &ws.order_cap, (size_t)n, 4) != GB_OK) {
-        *err = GB_ERR_ALLOC;
-        return nullptr;
-    }
+    if (grow((void **)&ws.order, &ws.order_cap, n, 4) != GB_OK) return GB_ERR_ALLOC;
     if (!ws.bins && cudaMalloc((void **)&ws.bins, (size_t)order_bins() * 4) != cudaSuccess) {
         cudaGetLastError();
-        *err = GB_ERR_ALLOC;
-        return nullptr;
+        return GB_ERR_ALLOC;
     }
-    timing_mark(K_ORDER, true, s);
-    const cudaError_t e = launch_order(q_len, t_len, n, ws.bins, ws.order, s);
-    timing_mark(K_ORDER, false, s);
-    if (e != cudaSuccess) {
-        *err = GB_ERR_CUDA;
-        return nullptr;
+    return GB_OK;
+}
+
+int plan_batch(const RunCfg &cfg, const DevBatch &b, const DevOut &o, Workspace &ws, Plan &p)
+{
+    if (b.n <= 0) return GB_ERR_ARG;
+    const Settings &st = settings();
+    p = Plan();
+    p.block = st.block;
+
+    /* split: long LOCAL/GLOBAL pairs go warp-cooperative */
+    const bool wc_algo = (cfg.algo == LOCAL_ || cfg.algo == GLOBAL_);
+    uint32_t max_q_short = 0, max_q_long = 0, max_t_long = 0;
+    int nlong = 0;
+    p.wc_min_q = (uint32_t)st.wc_min_qregs * 8 - 7;
+    for (int i = 0; i < b.n; i++) {
+        const uint32_t ql = b.h_q_len[i];
+        if (wc_algo && ql >= p.wc_min_q) {
+            nlong++;
+            max_q_long = std::max(max_q_long, ql);
+            max_t_long = std::max(max_t_long, b.h_t_len[i]);
+        } else {
+            max_q_short = std::max(max_q_short, ql);
+        }
     }
-    return ws.order;
+    /* the warp kernel's shared memory: 4 warps x (ring of q8 words + band maxima) */
+    const size_t wc_smem = 4 * (((size_t)max_q_long + 8) + ((size_t)max_t_long + 8) / 8 + 1) * 4;
+    p.use_wc = nlong > 0 && b.n >= st.min_order_pairs && ((max_q_long + 7) & ~7u) <= (uint32_t)st.wc_max_q8 &&
+               wc_smem <= (200u << 10);
+    if (!p.use_wc) {
+        max_q_short = std::max(max_q_short, max_q_long);
+        nlong = 0;
+    }
+    p.mq8 = (int)((max_q_long + 7) & ~7u), p.mt8 = (int)((max_t_long + 7) & ~7u);
+
+    /* row buffer placement (one-thread kernel) */
+    const uint32_t max_q = max_q_short;
+    const int cols = cfg.algo == KSW_ ? 2 * ((int)max_q + 2) : (int)((max_q + 7) & ~7u);
+    const size_t smem_limit = 160u << 10;
+    DpArgs &a = p.a;
+    a = DpArgs{};
+    a.pq = b.pq, a.pt = b.pt, a.q_off = b.q_off, a.t_off = b.t_off, a.q_len = b.q_len, a.t_len = b.t_len;
+    a.seed = b.seed, a.order = nullptr, a.n = b.n;
+    a.score = o.score, a.q_end = o.q_end, a.t_end = o.t_end, a.q_start = o.q_start, a.t_start = o.t_start;
+    a.score2 = o.score2, a.q_end2 = o.q_end2, a.t_end2 = o.t_end2;
+    a.sc = cfg.sc, a.head = cfg.head, a.tail = cfg.tail, a.k_band = cfg.k_band, a.zdrop = cfg.zdrop, a.mql = cfg.mql;
+    if (!ws.queue && cudaMalloc((void **)&ws.queue, 64) != cudaSuccess) {
+        cudaGetLastError();
+        return GB_ERR_ALLOC;
+    }
+    a.queue = ws.queue;
+    if ((size_t)std::max(cols, 8) * p.block * 4 <= smem_limit) {
+        a.smem_cols = std::max(cols, 8);
+    } else {
+        a.smem_cols = 0;
+        const size_t threads = (size_t)dp_scratch_blocks(b.n, p.block) * p.block;
+        if (grow((void **)&ws.scratch, &ws.scratch_cap, threads * cols, 4) != GB_OK) return GB_ERR_ALLOC;
+        a.scratch = ws.scratch;
+        a.scratch_cols = (uint32_t)cols;
+    }
+    if (p.use_wc && !ws.aux) {
+        if (cudaStreamCreateWithFlags(&ws.aux, cudaStreamNonBlocking) != cudaSuccess ||
+            cudaEventCreateWithFlags(&ws.fork, cudaEventDisableTiming) != cudaSuccess ||
+            cudaEventCreateWithFlags(&ws.join, cudaEventDisableTiming) != cudaSuccess) {
+            cudaGetLastError();
+            return GB_ERR_CUDA;
+        }
+    }
+
+    p.tb = cfg.start == WITH_TB_ && (cfg.algo == LOCAL_ || cfg.algo == GLOBAL_);
+    p.start = (cfg.algo == SEMI_GLOBAL_ && cfg.start == WITH_TB_) ? WITHOUT_START_ : cfg.start;
+    p.second = cfg.second && (cfg.algo == LOCAL_ || cfg.algo == SEMI_GLOBAL_);
+
+    if (!p.tb) {
+        p.cut = {0, b.n};
+        p.nlong = {nlong};
+        p.order_on = p.use_wc || b.n >= st.min_order_pairs;
+        if (p.order_on && ensure_order_buffers(ws, (size_t)b.n) != GB_OK) return GB_ERR_ALLOC;
+        return GB_OK;
+    }
+
+    /* traceback: chunk pairs so the tiles fit the budget */
+    if (ws.tb_off_free && cudaEventSynchronize(ws.tb_off_free) != cudaSuccess) return GB_ERR_CUDA;
+    if (ws.tb_off_cap < (size_t)b.n) {
+        if (ws.h_tb_off) cudaFreeHost(ws.h_tb_off);
+        if (ws.d_tb_off) cudaFree(ws.d_tb_off);
+        ws.h_tb_off = nullptr, ws.d_tb_off = nullptr, ws.tb_off_cap = 0;
+        const size_t want = (size_t)b.n + b.n / 4 + 1024;
+        if (cudaMallocHost((void **)&ws.h_tb_off, want * 8) != cudaSuccess ||
+            cudaMalloc((void **)&ws.d_tb_off, want * 8) != cudaSuccess) {
+            cudaGetLastError();
+            return GB_ERR_ALLOC;
+        }
+        ws.tb_off_cap = want;
+    }
+    if (!ws.tb_off_free && cudaEventCreateWithFlags(&ws.tb_off_free, cudaEventDisableTiming) != cudaSuccess)
+        return GB_ERR_CUDA;
+    const uint64_t budget = std::max<uint64_t>(st.tb_budget_bytes / 16, 1);
+    p.cut = {0};
+    uint64_t run = 0, chunk_max = 0;
+    for (int i = 0; i < b.n; i++) {
+        const uint64_t t = tb_tiles(b.h_q_len[i], b.h_t_len[i]);
+        if (run > 0 && run + t > budget) {
+            chunk_max = std::max(chunk_max, run);
+            p.cut.push_back(i);
+            run = 0;
+        }
+        ws.h_tb_off[i] = run;
+        run += t;
+    }
+    chunk_max = std::max(chunk_max, run);
+    p.cut.push_back(b.n);
+    if (grow((void **)&ws.tb, &ws.tb_cap, chunk_max, sizeof(uint4)) != GB_OK) return GB_ERR_ALLOC;
+    size_t max_chunk = 0;
+    for (size_t c = 0; c + 1 < p.cut.size(); c++) {
+        const int p0 = p.cut[c], p1 = p.cut[c + 1];
+        int nl = 0;
+        if (p.use_wc)
+            for (int i = p0; i < p1; i++) nl += b.h_q_len[i] >= p.wc_min_q ? 1 : 0;
+        p.nlong.push_back(nl);
+        max_chunk = std::max(max_chunk, (size_t)(p1 - p0));
+    }
+    p.order_on = p.use_wc || b.n >= st.min_order_pairs;
+    if (p.order_on && ensure_order_buffers(ws, max_chunk) != GB_OK) return GB_ERR_ALLOC;
+    return GB_OK;
 }
 
 /* DP over pairs [0, a.n) visited in `order` (nullptr: identity): the first
@@ -176,14 +289,6 @@ static int launch_dp_split(int algo, int start, bool second, DpArgs a, const uin
                            int max_q8_long, int max_t8_long, int block, Workspace &ws, cudaStream_t s)
 {
     if (nlong > 0 && order) {
-        if (!ws.aux) {
-            if (cudaStreamCreateWithFlags(&ws.aux, cudaStreamNonBlocking) != cudaSuccess ||
-                cudaEventCreateWithFlags(&ws.fork, cudaEventDisableTiming) != cudaSuccess ||
-                cudaEventCreateWithFlags(&ws.join, cudaEventDisableTiming) != cudaSuccess) {
-                cudaGetLastError();
-                return GB_ERR_CUDA;
-            }
-        }
         GB_CUDA(cudaEventRecord(ws.fork, s));
         GB_CUDA(cudaStreamWaitEvent(ws.aux, ws.fork, 0));
         timing_mark(K_DP, true, ws.aux);
@@ -193,8 +298,8 @@ static int launch_dp_split(int algo, int start, bool second, DpArgs a, const uin
         DpArgs rest = a;
         rest.order = order + nlong;
         rest.n = a.n - nlong;
-        if (rest.n > 0 && rest.queue) GB_CUDA(cudaMemsetAsync(rest.queue, 0, 4, s));
         if (rest.n > 0) {
+            if (rest.queue) GB_CUDA(cudaMemsetAsync(rest.queue, 0, 4, s));
             timing_mark(K_DP, true, s);
             GB_CUDA(launch_dp(algo, start, second, rest, block, 0, s));
             timing_mark(K_DP, false, s);
@@ -210,13 +315,18 @@ static int launch_dp_split(int algo, int start, bool second, DpArgs a, const uin
     return GB_OK;
 }
 
-int run_batch(const RunCfg &cfg, const DevBatch &b, const DevOut &o, Workspace &ws, cudaStream_t s)
+static int enqueue_order(const uint32_t *q_len, const uint32_t *t_len, int n, Workspace &ws, cudaStream_t s)
 {
-    if (b.n <= 0) return GB_ERR_ARG;
-    const Settings &st = settings();
-    const int block = st.block;
+    timing_mark(K_ORDER, true, s);
+    const cudaError_t e = launch_order(q_len, t_len, n, ws.bins, ws.order, s);
+    timing_mark(K_ORDER, false, s);
+    return e == cudaSuccess ? GB_OK : GB_ERR_CUDA;
+}
 
-    /* ---- pack and reverse/complement ---- */
+int enqueue_batch(const RunCfg &cfg, const DevBatch &b, const DevOut &o, Workspace &ws, const Plan &p,
+                  cudaStream_t s)
+{
+    /* pack and reverse/complement */
     if (!cfg.is_packed) {
         timing_mark(K_PACK, true, s);
         GB_CUDA(launch_pack(b.q, b.q_bytes, b.pq, s));
@@ -231,119 +341,35 @@ int run_batch(const RunCfg &cfg, const DevBatch &b, const DevOut &o, Workspace &
                                cfg.ref_reverse, s));
         timing_mark(K_RC, false, s);
     }
-
-    /* ---- split: long LOCAL/GLOBAL pairs go warp-cooperative ---- */
-    const bool wc_algo = (cfg.algo == LOCAL_ || cfg.algo == GLOBAL_);
-    uint32_t max_q_short = 0, max_q_long = 0, max_t_long = 0;
-    int nlong = 0;
-    const uint32_t wc_min_q = (uint32_t)st.wc_min_qregs * 8 - 7;
-    for (int i = 0; i < b.n; i++) {
-        const uint32_t ql = b.h_q_len[i];
-        if (wc_algo && ql >= wc_min_q) {
-            nlong++;
-            max_q_long = std::max(max_q_long, ql);
-            max_t_long = std::max(max_t_long, b.h_t_len[i]);
-        } else {
-            max_q_short = std::max(max_q_short, ql);
+    if (!p.tb) {
+        const uint32_t *ord = nullptr;
+        if (p.order_on) {
+            const int rc = enqueue_order(b.q_len, b.t_len, b.n, ws, s);
+            if (rc != GB_OK) return rc;
+            ord = ws.order;
         }
+        return launch_dp_split(cfg.algo, p.start, p.second, p.a, ord, ord ? p.nlong[0] : 0, p.mq8, p.mt8, p.block,
+                               ws, s);
     }
-    /* the warp kernel's shared memory: 4 warps x (ring of q8 words + band maxima) */
-    const size_t wc_smem = 4 * (((size_t)max_q_long + 8) + ((size_t)max_t_long + 8) / 8 + 1) * 4;
-    const bool use_wc = nlong > 0 && b.n >= st.min_order_pairs && ((max_q_long + 7) & ~7u) <= (uint32_t)st.wc_max_q8 &&
-                        wc_smem <= (200u << 10);
-    if (!use_wc) {
-        max_q_short = std::max(max_q_short, max_q_long);
-        nlong = 0;
-    }
-    const uint32_t max_q = max_q_short;
-
-    /* ---- row buffer placement (one-thread kernel) ---- */
-    const int cols = cfg.algo == KSW_ ? 2 * ((int)max_q + 2) : (int)((max_q + 7) & ~7u);
-    const size_t smem_limit = 160u << 10;
-
-    DpArgs a{};
-    a.pq = b.pq, a.pt = b.pt, a.q_off = b.q_off, a.t_off = b.t_off, a.q_len = b.q_len, a.t_len = b.t_len;
-    a.seed = b.seed, a.order = nullptr, a.n = b.n;
-    a.score = o.score, a.q_end = o.q_end, a.t_end = o.t_end, a.q_start = o.q_start, a.t_start = o.t_start;
-    a.score2 = o.score2, a.q_end2 = o.q_end2, a.t_end2 = o.t_end2;
-    a.sc = cfg.sc, a.head = cfg.head, a.tail = cfg.tail, a.k_band = cfg.k_band, a.zdrop = cfg.zdrop, a.mql = cfg.mql;
-    if (!ws.queue && cudaMalloc((void **)&ws.queue, 64) != cudaSuccess) {
-        cudaGetLastError();
-        return GB_ERR_ALLOC;
-    }
-    a.queue = ws.queue;
-    if ((size_t)std::max(cols, 8) * block * 4 <= smem_limit) {
-        a.smem_cols = std::max(cols, 8);
-    } else {
-        a.smem_cols = 0;
-        const size_t threads = (size_t)dp_scratch_blocks(b.n, block) * block;
-        if (grow((void **)&ws.scratch, &ws.scratch_cap, threads * cols, 4) != GB_OK) return GB_ERR_ALLOC;
-        a.scratch = ws.scratch;
-        a.scratch_cols = (uint32_t)cols;
-    }
-
-    const bool tb = cfg.start == WITH_TB_ && (cfg.algo == LOCAL_ || cfg.algo == GLOBAL_);
-    const int start = (cfg.algo == SEMI_GLOBAL_ && cfg.start == WITH_TB_) ? WITHOUT_START_ : cfg.start;
-    const bool second = cfg.second && (cfg.algo == LOCAL_ || cfg.algo == SEMI_GLOBAL_);
-    const int mq8 = (int)((max_q_long + 7) & ~7u), mt8 = (int)((max_t_long + 7) & ~7u);
-    if (!tb) {
-        int err = GB_OK;
-        const uint32_t *ord = binned_order(b.q_len, b.t_len, b.n, ws, s, &err, use_wc);
-        if (err != GB_OK) return err;
-        return launch_dp_split(cfg.algo, start, second, a, ord, ord ? nlong : 0, mq8, mt8, block, ws, s);
-    }
-
-    /* ---- traceback: chunk pairs so the tiles fit the budget ---- */
-    if (ws.tb_off_free) GB_CUDA(cudaEventSynchronize(ws.tb_off_free));
-    if (ws.tb_off_cap < (size_t)b.n) {
-        if (ws.h_tb_off) cudaFreeHost(ws.h_tb_off);
-        if (ws.d_tb_off) cudaFree(ws.d_tb_off);
-        ws.h_tb_off = nullptr, ws.d_tb_off = nullptr, ws.tb_off_cap = 0;
-        const size_t want = (size_t)b.n + b.n / 4 + 1024;
-        if (cudaMallocHost((void **)&ws.h_tb_off, want * 8) != cudaSuccess ||
-            cudaMalloc((void **)&ws.d_tb_off, want * 8) != cudaSuccess) {
-            cudaGetLastError();
-            return GB_ERR_ALLOC;
-        }
-        ws.tb_off_cap = want;
-    }
-    const uint64_t budget = std::max<uint64_t>(st.tb_budget_bytes / 16, 1);
-    std::vector<int> cut{0};
-    uint64_t run = 0, chunk_max = 0;
-    for (int i = 0; i < b.n; i++) {
-        const uint64_t t = tb_tiles(b.h_q_len[i], b.h_t_len[i]);
-        if (run > 0 && run + t > budget) {
-            chunk_max = std::max(chunk_max, run);
-            cut.push_back(i);
-            run = 0;
-        }
-        ws.h_tb_off[i] = run;
-        run += t;
-    }
-    chunk_max = std::max(chunk_max, run);
-    cut.push_back(b.n);
-    if (grow((void **)&ws.tb, &ws.tb_cap, chunk_max, sizeof(uint4)) != GB_OK) return GB_ERR_ALLOC;
     GB_CUDA(cudaMemcpyAsync(ws.d_tb_off, ws.h_tb_off, (size_t)b.n * 8, cudaMemcpyHostToDevice, s));
-    if (!ws.tb_off_free) GB_CUDA(cudaEventCreateWithFlags(&ws.tb_off_free, cudaEventDisableTiming));
-    GB_CUDA(cudaEventRecord(ws.tb_off_free, s));
-
-    for (size_t c = 0; c + 1 < cut.size(); c++) {
-        const int p0 = cut[c], p1 = cut[c + 1];
-        DpArgs ca = a;
+    for (size_t c = 0; c + 1 < p.cut.size(); c++) {
+        const int p0 = p.cut[c], p1 = p.cut[c + 1];
+        DpArgs ca = p.a;
         ca.n = p1 - p0;
         ca.q_off = b.q_off + p0, ca.t_off = b.t_off + p0, ca.q_len = b.q_len + p0, ca.t_len = b.t_len + p0;
-        auto sh = [p0](int32_t *p) { return p ? p + p0 : p; };
+        auto sh = [p0](int32_t *x) { return x ? x + p0 : x; };
         ca.score = sh(o.score), ca.q_end = sh(o.q_end), ca.t_end = sh(o.t_end);
         ca.q_start = sh(o.q_start), ca.t_start = sh(o.t_start);
         ca.score2 = sh(o.score2), ca.q_end2 = sh(o.q_end2), ca.t_end2 = sh(o.t_end2);
         ca.tb = ws.tb, ca.tb_off = ws.d_tb_off + p0;
-        int err = GB_OK;
-        const uint32_t *ord = binned_order(ca.q_len, ca.t_len, ca.n, ws, s, &err, use_wc);
-        if (err != GB_OK) return err;
-        int nlong_c = 0;
-        if (use_wc && ord)
-            for (int i = p0; i < p1; i++) nlong_c += b.h_q_len[i] >= wc_min_q ? 1 : 0;
-        const int rc = launch_dp_split(cfg.algo, start, second, ca, ord, nlong_c, mq8, mt8, block, ws, s);
+        const uint32_t *ord = nullptr;
+        if (p.order_on) {
+            const int rc = enqueue_order(ca.q_len, ca.t_len, ca.n, ws, s);
+            if (rc != GB_OK) return rc;
+            ord = ws.order;
+        }
+        const int rc = launch_dp_split(cfg.algo, p.start, p.second, ca, ord, ord ? p.nlong[c] : 0, p.mq8, p.mt8,
+                                       p.block, ws, s);
         if (rc != GB_OK) return rc;
         TbArgs t{};
         t.tb = ws.tb, t.tb_off = ws.d_tb_off + p0;
@@ -358,6 +384,23 @@ int run_batch(const RunCfg &cfg, const DevBatch &b, const DevOut &o, Workspace &
         timing_mark(K_TB, false, s);
     }
     return GB_OK;
+}
+
+int run_batch(const RunCfg &cfg, const DevBatch &b, const DevOut &o, Workspace &ws, cudaStream_t s)
+{
+    Plan p;
+    int rc = plan_batch(cfg, b, o, ws, p);
+    if (rc != GB_OK) return rc;
+    rc = enqueue_batch(cfg, b, o, ws, p, s);
+    if (rc == GB_OK && p.tb) GB_CUDA(cudaEventRecord(ws.tb_off_free, s));
+    return rc;
+}
+
+bool timing_on()
+{
+    Timing &t = timing();
+    std::lock_guard<std::mutex> lk(t.mu);
+    return t.on;
 }
 
 } // namespace gb

@@ -13,6 +13,7 @@
 #include <cstddef>
 #include <cstdint>
 #include <cuda_runtime.h>
+#include <vector>
 
 #include "gb_internal.h"
 #include "gasal_b200_capi.h"
@@ -64,7 +65,21 @@ struct Workspace {
     ~Workspace();
 };
 
+/* The decisions and allocations for one batch (plan_batch), so that
+ * enqueue_batch issues stream operations only -- capturable into a graph. */
+struct Plan {
+    bool tb = false, second = false, use_wc = false, order_on = false;
+    int start = 0, block = 64, mq8 = 0, mt8 = 0;
+    uint32_t wc_min_q = 0;
+    DpArgs a{};
+    std::vector<int> cut;   /* pair ranges [cut[c], cut[c+1]) run one after another */
+    std::vector<int> nlong; /* per range: pairs on the warp-cooperative kernel */
+};
+
 /* status codes of gasal_b200_capi.h */
+int plan_batch(const RunCfg &cfg, const DevBatch &b, const DevOut &o, Workspace &ws, Plan &p);
+int enqueue_batch(const RunCfg &cfg, const DevBatch &b, const DevOut &o, Workspace &ws, const Plan &p,
+                  cudaStream_t s);
 int run_batch(const RunCfg &cfg, const DevBatch &b, const DevOut &o, Workspace &ws, cudaStream_t s);
 
 /* Traceback tiles of one pair, in uint4 units (two spare tile rows). */
@@ -84,6 +99,7 @@ struct Settings {
     int min_order_pairs = 2048; /* batches at least this large visit pairs length-binned */
     int wc_min_qregs = 32;      /* pairs with at least this many query words go warp-cooperative */
     int wc_max_q8 = 12000;      /* ... while the batch's longest query fits the warp's ring */
+    int graphs = 1;             /* gasal_aln_async runs each batch as a CUDA graph */
 };
 Settings &settings();
 
@@ -92,6 +108,7 @@ enum KernelKind { K_PACK = 0, K_RC = 1, K_DP = 2, K_TB = 3, K_ORDER = 4, K_KINDS
 void timing_enable(bool on);
 void timing_mark(int kind, bool start, cudaStream_t s);
 int timing_read(double ms[K_KINDS], int64_t launches[K_KINDS]);
+bool timing_on();
 int probe_int_peak(double *iadd, double *imnmx, double *dpx);
 
 } // namespace gb

@@ -47,6 +47,10 @@ class GbDevOut(C.Structure):
                                            "t_end2", "cigar", "n_cigar")]
 
 
+class GbTuning(C.Structure):
+    _fields_ = [("block", C.c_int32), ("wc_min_qregs", C.c_int32), ("min_order_pairs", C.c_int32)]
+
+
 class GbStorageView(C.Structure):
     _fields_ = [(k, C.c_void_p) for k in (
         "host_query_batch_offsets", "host_target_batch_offsets", "host_query_batch_lens",
@@ -85,6 +89,12 @@ SIGNATURES = {
     "gb_set_reference_max_query_len": (C.c_int, [C.c_int]),
     "gb_set_tb_budget_mb": (C.c_int, [C.c_int64]),
     "gb_version": (C.c_char_p, []),
+    "gb_set_graphs": (C.c_int, [C.c_int]),
+    "gb_graph_stats": (C.c_int, [C.POINTER(C.c_int64)]),
+    "gb_set_tuning": (C.c_int, [C.POINTER(GbTuning)]),
+    "gb_get_tuning": (C.c_int, [C.POINTER(GbTuning)]),
+    "gb_autotune": (C.c_int, [C.POINTER(GbParams), C.POINTER(GbDevBatch), C.POINTER(GbDevOut), C.c_void_p, C.c_int,
+                              C.POINTER(GbTuning), C.POINTER(C.c_double)]),
     "gb_kernel_timing": (C.c_int, [C.c_int]),
     "gb_kernel_timing_read": (C.c_int, [C.POINTER(C.c_double), C.POINTER(C.c_int64)]),
     "gb_probe_int_peak": (C.c_int, [C.POINTER(C.c_double)] * 3),
@@ -130,6 +140,31 @@ def set_tb_budget_mb(mb: int):
     _check(lib().gb_set_tb_budget_mb(int(mb)), "gb_set_tb_budget_mb")
 
 
+def set_graphs(on: bool):
+    """Run each gasal_aln_async batch as a CUDA graph (default on)."""
+    _check(lib().gb_set_graphs(1 if on else 0), "gb_set_graphs")
+
+
+def graph_stats() -> dict:
+    c = (C.c_int64 * 4)()
+    _check(lib().gb_graph_stats(c), "gb_graph_stats")
+    return {"relaunched": c[0], "updated": c[1], "instantiated": c[2], "capture_refused": c[3]}
+
+
+def get_tuning() -> dict:
+    t = GbTuning()
+    _check(lib().gb_get_tuning(C.byref(t)), "gb_get_tuning")
+    return {"block": t.block, "wc_min_qregs": t.wc_min_qregs, "min_order_pairs": t.min_order_pairs}
+
+
+def set_tuning(block: int | None = None, wc_min_qregs: int | None = None, min_order_pairs: int | None = None):
+    cur = get_tuning()
+    t = GbTuning(int(block if block is not None else cur["block"]),
+                 int(wc_min_qregs if wc_min_qregs is not None else cur["wc_min_qregs"]),
+                 int(min_order_pairs if min_order_pairs is not None else cur["min_order_pairs"]))
+    _check(lib().gb_set_tuning(C.byref(t)), "gb_set_tuning")
+
+
 KERNEL_KINDS = ("pack", "revcomp", "dp", "traceback", "order")
 KERNELS_PER_MARK = {"pack": 1, "revcomp": 1, "dp": 1, "traceback": 1, "order": 3}
 
@@ -151,11 +186,7 @@ def probe_int_peak() -> dict:
     return {"iadd_tops": a.value, "imnmx_tops": b.value, "dpx_tops": c.value}
 
 
-def align_dev(p: Params, dev: dict, h_q_len: np.ndarray, h_t_len: np.ndarray, stream_handle: int = 0,
-              noalloc: bool = False):
-    """Kernel-level call on device-resident buffers.  ``dev`` maps the
-    gb_dev_batch_t / gb_dev_out_t field names to device addresses (ints).
-    noalloc=True calls gb_align_dev_noalloc, which allocates nothing."""
+def _dev_structs(dev: dict, h_q_len: np.ndarray, h_t_len: np.ndarray):
     b = GbDevBatch()
     b.n = int(h_q_len.shape[0])
     b.q_bytes, b.t_bytes = int(dev["q_bytes"]), int(dev["t_bytes"])
@@ -165,6 +196,29 @@ def align_dev(p: Params, dev: dict, h_q_len: np.ndarray, h_t_len: np.ndarray, st
     o = GbDevOut()
     for k, _ in GbDevOut._fields_:
         setattr(o, k, dev.get("out_" + k))
+    return b, o
+
+
+def autotune(p: Params, dev: dict, h_q_len: np.ndarray, h_t_len: np.ndarray, stream_handle: int = 0,
+             reps: int = 2) -> dict:
+    """gb_autotune on a device-resident batch (same ``dev`` map as
+    align_dev): installs and returns the fastest launch tuning."""
+    b, o = _dev_structs(dev, h_q_len, h_t_len)
+    cp = p.to_c()
+    t = GbTuning()
+    ms = C.c_double()
+    _check(lib().gb_autotune(C.byref(cp), C.byref(b), C.byref(o), C.c_void_p(stream_handle), int(reps),
+                             C.byref(t), C.byref(ms)), "gb_autotune")
+    return {"block": t.block, "wc_min_qregs": t.wc_min_qregs, "min_order_pairs": t.min_order_pairs,
+            "ms": ms.value}
+
+
+def align_dev(p: Params, dev: dict, h_q_len: np.ndarray, h_t_len: np.ndarray, stream_handle: int = 0,
+              noalloc: bool = False):
+    """Kernel-level call on device-resident buffers.  ``dev`` maps the
+    gb_dev_batch_t / gb_dev_out_t field names to device addresses (ints).
+    noalloc=True calls gb_align_dev_noalloc, which allocates nothing."""
+    b, o = _dev_structs(dev, h_q_len, h_t_len)
     cp = p.to_c()
     if noalloc:
         _check(lib().gb_align_dev_noalloc(C.byref(cp), C.byref(b), C.byref(o), C.c_void_p(stream_handle)),
@@ -238,13 +292,20 @@ class Streams:
 
     def fill_fast(self, i: int, b: Batch):
         """Stage a batch whose layout already is GASAL2's (padded, offsets
-        ascending) with two bulk copies instead of one call per sequence."""
+        ascending) with one gasal_host_batch_fill per side: the whole padded
+        buffer is one multiple-of-8 "sequence", so nothing is padded and the
+        page's data size (what gasal_aln_async copies) covers all of it."""
         L = lib()
         s = self.storage(i)
         v = self.view(i)
         n = b.n
-        qi = L.gasal_c_host_batch_add(s, 0, b.q.ctypes.data, int(b.q.shape[0]), QUERY)
-        ti = L.gasal_c_host_batch_add(s, 0, b.t.ctypes.data, int(b.t.shape[0]), TARGET)
+        nq, nt = int(b.q.shape[0]), int(b.t.shape[0])
+        if nq % 8 or nt % 8:
+            raise GasalError("fill_fast needs 8-byte padded buffers")
+        qi = L.gasal_c_host_batch_fill(s, 0, C.c_char_p(b.q.ctypes.data), nq, QUERY)
+        ti = L.gasal_c_host_batch_fill(s, 0, C.c_char_p(b.t.ctypes.data), nt, TARGET)
+        if qi != nq or ti != nt:
+            raise GasalError("host page smaller than the batch; create the storage with larger maxima or use fill()")
         self._arr(v.host_query_batch_offsets, C.c_uint32, n)[:] = b.q_off
         self._arr(v.host_target_batch_offsets, C.c_uint32, n)[:] = b.t_off
         self._arr(v.host_query_batch_lens, C.c_uint32, n)[:] = b.q_len

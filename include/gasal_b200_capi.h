@@ -43,7 +43,9 @@ typedef struct {
     int32_t tail;         /* enum data_source: semi-global skipped tail */
     int32_t k_band;       /* banded: band width in bases (tiles = k_band >> 3) */
     int32_t reverse_complement; /* apply per-sequence ops (isReverseComplement) */
-    int32_t zdrop;        /* ksw z-drop; 0 = off, as the reference hard-codes */
+    int32_t zdrop;        /* ksw z-drop; 0 = off, as the reference hard-codes.  Honoured by every C entry
+                             point (gasal_c_aln_async takes it from gasal_c_params_set); the
+                             C++ gasal_aln_async keeps the reference's 0 */
     int32_t match;        /* gasal_subst_scores (reference src/gasal.h:160-165) */
     int32_t mismatch;
     int32_t gap_open;
@@ -197,6 +199,40 @@ int gb_set_reference_reverse(int on);
 int gb_set_reference_max_query_len(int mql);
 int gb_set_tb_budget_mb(int64_t mb);
 const char *gb_version(void);
+
+/* CUDA graphs for gasal_aln_async / gasal_c_aln_async (no reference
+ * counterpart; on by default).  Each storage keeps one executable graph of
+ * its whole batch (host->device copies, kernels, device->host copies): a batch
+ * with the same sizes, options, buffers and plan relaunches it as is, any
+ * other batch is captured and the graph updated in place.  Graphs are skipped
+ * while gb_kernel_timing is on.  gb_graph_stats() fills counts[4]: batches
+ * that relaunched a graph, that updated it, that instantiated a new one, and
+ * whose capture was refused (those ran without a graph). */
+int gb_set_graphs(int on);
+int gb_graph_stats(int64_t *counts);
+
+/* Launch tuning (no reference counterpart).  block: threads per block of the
+ * one-pair-per-thread DP kernel (32, 64 or 128); wc_min_qregs: pairs
+ * whose query has at least this many 8-base words run warp-cooperative
+ * (LOCAL/GLOBAL; at least 32, which that kernel needs); min_order_pairs: batches with at least this many pairs are
+ * visited length-binned.  Results never depend on these. */
+typedef struct {
+    int32_t block;
+    int32_t wc_min_qregs;
+    int32_t min_order_pairs;
+} gb_tuning_t;
+int gb_set_tuning(const gb_tuning_t *t);
+int gb_get_tuning(gb_tuning_t *t);
+
+/* Autotuner (no reference counterpart): runs gb_align_dev on the caller's
+ * batch under each candidate tuning (block 32/64/128; for LOCAL/GLOBAL also
+ * warp-cooperative thresholds 32/40/48/64/96 words), `reps` timed runs each
+ * after a warm-up run, timed with CUDA events on `stream`; installs and
+ * returns the fastest (best_ms: its mean milliseconds per run; may be NULL).
+ * The outputs hold the batch's results afterwards.  Synchronizes `stream`;
+ * not for use during stream capture. */
+int gb_autotune(const gb_params_t *p, const gb_dev_batch_t *b, const gb_dev_out_t *o, void *stream, int reps,
+                gb_tuning_t *best, double *best_ms);
 
 /* Instrumentation (no reference counterpart).  gb_kernel_timing(1) resets
  * and starts recording a CUDA event pair around every kernel the library

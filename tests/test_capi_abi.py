@@ -102,3 +102,23 @@ def test_product_fails_loudly_without_library(monkeypatch):
     monkeypatch.setattr(gl, "LIB_PATH", "/nonexistent/libgasal_b200.so")
     with pytest.raises(gl.GasalError):
         gl.lib()
+
+
+def test_tuning_and_graph_settings_validate(so):
+    """Launch tuning round-trips and rejects values the kernels cannot take
+    (no GPU needed: these only change library settings)."""
+    from gasal_b200.lib import GbTuning
+    import ctypes as C
+    cur = GbTuning()
+    assert so.gb_get_tuning(C.byref(cur)) == 0
+    for bad in (GbTuning(256, 32, 0), GbTuning(64, 16, 0), GbTuning(64, 32, -1)):
+        assert so.gb_set_tuning(C.byref(bad)) == -1
+    ok = GbTuning(128, 48, 4096)
+    assert so.gb_set_tuning(C.byref(ok)) == 0
+    back = GbTuning()
+    so.gb_get_tuning(C.byref(back))
+    assert (back.block, back.wc_min_qregs, back.min_order_pairs) == (128, 48, 4096)
+    assert so.gb_set_tuning(C.byref(cur)) == 0
+    assert so.gb_set_graphs(0) == 0 and so.gb_set_graphs(1) == 0
+    counts = (C.c_int64 * 4)()
+    assert so.gb_graph_stats(counts) == 0

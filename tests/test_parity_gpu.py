@@ -86,6 +86,22 @@ def test_ksw_long():
     _vs_oracle(Params(algo=KSW), b)
 
 
+@pytest.mark.parametrize("zdrop", [100, 20, 1])
+def test_ksw_zdrop(zdrop):
+    """The z-drop branch the reference leaves dead (its kernel hard-codes
+    zdrop 0): a drop ends the current 8-row target tile.  Workload 3 pairs
+    (250-2000 bp, 0.5-10% indels) plus unrelated pairs, where drops are
+    frequent."""
+    b = W.workload3(600, seed=80 + zdrop)
+    _vs_oracle(Params(algo=KSW, zdrop=zdrop), b)
+    u = W.workload0(600, seed=81)
+    rng = np.random.default_rng(zdrop)
+    u.t = u.t.copy()
+    u.t[:] = np.frombuffer(b"ACGT", dtype=np.uint8)[rng.integers(0, 4, u.t.shape[0])]
+    u.seed = rng.integers(20, 61, u.n).astype(np.uint32)
+    _vs_oracle(Params(algo=KSW, zdrop=zdrop), u)
+
+
 @pytest.mark.parametrize("head", [NONE, QUERY, TARGET, BOTH])
 @pytest.mark.parametrize("tail", [NONE, QUERY, TARGET, BOTH])
 def test_semi_global_variants(head, tail):

@@ -1,0 +1,70 @@
+"""Launch tuning and the autotuner: results never depend on the block size,
+the warp-cooperative threshold or the ordering threshold, and gb_autotune
+installs the fastest candidate it timed."""
+import numpy as np
+import pytest
+
+from gasal_b200 import lib as gl
+from gasal_b200 import workloads as W
+from gasal_b200.capi import Params, LOCAL, GLOBAL, WITH_START, WITH_TB
+from oracle.bindings import oracle_align
+
+pytestmark = pytest.mark.gpu
+
+FIELDS = ("score", "q_end", "t_end", "q_start", "t_start", "score2", "q_end2", "t_end2")
+
+
+def _device(torch, b, dev):
+    def t_(a, dt=None):
+        return torch.from_numpy(np.ascontiguousarray(a).view(dt or a.dtype)).to(dev)
+    keep = {"q": t_(b.q), "t": t_(b.t), "qo": t_(b.q_off, np.int32), "to": t_(b.t_off, np.int32),
+            "ql": t_(b.q_len, np.int32), "tl": t_(b.t_len, np.int32),
+            "pq": torch.zeros(b.q.shape[0] // 8, dtype=torch.int32, device=dev),
+            "pt": torch.zeros(b.t.shape[0] // 8, dtype=torch.int32, device=dev)}
+    keep.update({k: torch.full((b.n,), -7, dtype=torch.int32, device=dev) for k in FIELDS})
+    m = {"q_bytes": b.q.shape[0], "t_bytes": b.t.shape[0]}
+    for k, src in (("q", "q"), ("t", "t"), ("pq", "pq"), ("pt", "pt"), ("q_off", "qo"), ("t_off", "to"),
+                   ("q_len", "ql"), ("t_len", "tl")):
+        m[k] = keep[src].data_ptr()
+    for k in FIELDS:
+        m["out_" + k] = keep[k].data_ptr()
+    return m, keep
+
+
+@pytest.mark.parametrize("tuning", [dict(block=32, wc_min_qregs=32, min_order_pairs=0),
+                                    dict(block=128, wc_min_qregs=64, min_order_pairs=1 << 30),
+                                    dict(block=64, wc_min_qregs=40, min_order_pairs=100)],
+                         ids=["b32_wc32_order_all", "b128_wc64_no_order", "b64_wc40"])
+def test_results_independent_of_tuning(tuning):
+    saved = gl.get_tuning()
+    b = W.workload2(3000, seed=61)
+    try:
+        gl.set_tuning(**tuning)
+        for p in (Params(algo=GLOBAL, start_pos=WITH_TB), Params(algo=LOCAL, start_pos=WITH_START, second_best=1)):
+            got = gl.align(p, b).as_dict(p)
+            exp = oracle_align(p, b).as_dict(p)
+            for k, v in exp.items():
+                assert np.array_equal(got[k], v), f"{tuning} {p.key()} {k}"
+    finally:
+        gl.set_tuning(**saved)
+
+
+def test_autotune_installs_fastest_and_keeps_results():
+    torch = pytest.importorskip("torch")
+    dev = torch.device("cuda", 0)
+    saved = gl.get_tuning()
+    p = Params(algo=LOCAL, start_pos=WITH_START, second_best=1)
+    b = W.workload2(4000, seed=62)
+    m, keep = _device(torch, b, dev)
+    try:
+        best = gl.autotune(p, m, b.q_len, b.t_len, torch.cuda.current_stream().cuda_stream, reps=1)
+        torch.cuda.synchronize()
+        assert best["block"] in (32, 64, 128) and best["wc_min_qregs"] in (32, 40, 48, 64, 96)
+        assert best["ms"] > 0
+        cur = gl.get_tuning()
+        assert (cur["block"], cur["wc_min_qregs"]) == (best["block"], best["wc_min_qregs"])
+        exp = oracle_align(p, b).as_dict(p)
+        for k, v in exp.items():
+            assert np.array_equal(keep[k].cpu().numpy(), v), k
+    finally:
+        gl.set_tuning(**saved)
