@@ -229,6 +229,7 @@ void release_state(const gasal_gpu_storage_t *s)
     if (w.fork) cudaEventDestroy(w.fork);
     if (w.join) cudaEventDestroy(w.join);
     if (w.bins) cudaFree(w.bins);
+    if (w.fb) cudaFree(w.fb);
     if (p->d_n_cigar) cudaFree(p->d_n_cigar);
     if (p->exec) cudaGraphExecDestroy(p->exec);
 }
@@ -272,7 +273,7 @@ void batch_signature(std::vector<uint8_t> &v, const gasal_gpu_storage_t *s, cons
                           s->host_query_batch_lens, s->host_target_batch_lens, s->host_query_batch_offsets,
                           s->host_target_batch_offsets, s->host_query_op, s->host_target_op, s->host_seed_scores,
                           ss.d_n_cigar, ss.ws.tb, ss.ws.d_tb_off, ss.ws.h_tb_off, ss.ws.order, ss.ws.bins,
-                          ss.ws.queue, ss.ws.aux, ss.ws.fork, ss.ws.join, (const void *)s->str};
+                          ss.ws.queue, ss.ws.aux, ss.ws.fork, ss.ws.join, ss.ws.fb, (const void *)s->str};
     for (const void *q : ptrs) put(v, q);
     const gasal_res_t *rs[] = {s->host_res, s->device_cpy, s->host_res_second, s->device_cpy_second};
     for (const gasal_res_t *r : rs) {
@@ -285,6 +286,7 @@ void batch_signature(std::vector<uint8_t> &v, const gasal_gpu_storage_t *s, cons
     }
     put(v, plan.tb), put(v, plan.second), put(v, plan.use_wc), put(v, plan.order_on);
     put(v, plan.start), put(v, plan.block), put(v, plan.mq8), put(v, plan.mt8), put(v, plan.wc_min_q);
+    put(v, plan.ksw_tiles), put(v, plan.fb_blocks);
     put(v, plan.a);
     for (int c : plan.cut) put(v, c);
     put(v, -1);

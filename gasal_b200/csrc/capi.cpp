@@ -359,7 +359,7 @@ extern "C" int gb_autotune(const gb_params_t *p, const gb_dev_batch_t *b, const 
     }
     int rc = GB_OK;
     float best_t = 0.f;
-    gb_tuning_t bt{saved.block, saved.wc_min_qregs, saved.min_order_pairs};
+    gb_tuning_t bt{saved.block, saved.wc_min_qregs, saved.min_order_pairs, saved.ksw_wc};
     for (int blk : blocks) {
         for (int wc : wcs) {
             st.block = blk, st.wc_min_qregs = wc;
@@ -427,6 +427,7 @@ extern "C" int gb_set_tuning(const gb_tuning_t *t)
     if (t->wc_min_qregs < 32 || t->min_order_pairs < 0) return GB_ERR_ARG; /* the warp kernel needs 32+ words */
     gb::Settings &st = gb::settings();
     st.block = t->block, st.wc_min_qregs = t->wc_min_qregs, st.min_order_pairs = t->min_order_pairs;
+    st.ksw_wc = t->ksw_warp ? 1 : 0;
     return GB_OK;
 }
 
@@ -435,6 +436,7 @@ extern "C" int gb_get_tuning(gb_tuning_t *t)
     if (!t) return GB_ERR_ARG;
     const gb::Settings &st = gb::settings();
     t->block = st.block, t->wc_min_qregs = st.wc_min_qregs, t->min_order_pairs = st.min_order_pairs;
+    t->ksw_warp = st.ksw_wc;
     return GB_OK;
 }
 

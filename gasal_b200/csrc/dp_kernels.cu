@@ -52,7 +52,11 @@ __device__ __forceinline__ void dp_one(const DpArgs &a, uint32_t w, RowBuf rb, c
     const int i = a.order ? (int)a.order[w] : (int)w;
     const int qlen = (int)a.q_len[i], tlen = (int)a.t_len[i];
     Res r = {0, 0, 0, 0, 0, 0, 0, 0};
-    if (qlen > 0 && tlen > 0) {
+    if (ALGO == KSW_) {
+        /* empty sequences included: the reference returns h0 for them */
+        ksw(a.pq + (a.q_off[i] >> 3), qlen, a.pt + (a.t_off[i] >> 3), tlen, a.seed ? a.seed[i] : 0u, a.zdrop, a.sc,
+            rb, r);
+    } else if (qlen > 0 && tlen > 0) {
         const uint32_t *q = a.pq + (a.q_off[i] >> 3);
         const uint32_t *t = a.pt + (a.t_off[i] >> 3);
         const int qregs = (qlen + 7) >> 3, tregs = (tlen + 7) >> 3;
@@ -64,9 +68,7 @@ __device__ __forceinline__ void dp_one(const DpArgs &a, uint32_t w, RowBuf rb, c
             uint4 *z = tb + (size_t)tregs * 2 * qregs;
             for (int k = 0; k < 4 * qregs; k++) z[k] = make_uint4(0, 0, 0, 0);
         }
-        if (ALGO == KSW_) {
-            ksw(q, qlen, t, tlen, a.seed ? a.seed[i] : 0u, a.zdrop, a.sc, rb, r);
-        } else if (fast_scores && plain_words(q, qregs) && plain_words(t, tregs)) {
+        if (fast_scores && plain_words(q, qregs) && plain_words(t, tregs)) {
             ScFast sf;
             sf.tab = stab;
             run_pair<ALGO, START, SECOND>(a, q, qregs, qlen, t, tregs, tlen, i, rb, tb, sf, r);
@@ -113,18 +115,19 @@ __global__ void __launch_bounds__(128) dp_kernel(DpArgs a)
         rb.base = a.scratch + gtid;
         rb.stride = nthr;
     }
+    const uint32_t n = a.n_dev ? min(*a.n_dev, (uint32_t)a.n) : (uint32_t)a.n;
     if (a.queue) {
         const int lane = threadIdx.x & 31;
         for (;;) {
             uint32_t base = 0;
             if (lane == 0) base = atomicAdd(a.queue, 32u);
             base = __shfl_sync(0xFFFFFFFFu, base, 0);
-            if (base >= (uint32_t)a.n) break;
+            if (base >= n) break;
             const uint32_t w = base + lane;
-            if (w < (uint32_t)a.n) dp_one<ALGO, START, SECOND>(a, w, rb, stab, fast_scores);
+            if (w < n) dp_one<ALGO, START, SECOND>(a, w, rb, stab, fast_scores);
         }
     } else {
-        for (uint32_t w = gtid; w < (uint32_t)a.n; w += nthr) dp_one<ALGO, START, SECOND>(a, w, rb, stab, fast_scores);
+        for (uint32_t w = gtid; w < n; w += nthr) dp_one<ALGO, START, SECOND>(a, w, rb, stab, fast_scores);
     }
 }
 

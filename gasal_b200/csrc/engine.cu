@@ -206,11 +206,28 @@ int plan_batch(const RunCfg &cfg, const DevBatch &b, const DevOut &o, Workspace 
         return GB_ERR_ALLOC;
     }
     a.queue = ws.queue;
+    /* ksw: warp per pair; the one-thread kernel only takes what that hands
+     * back (queries beyond 2046 bases, huge seed scores) */
+    if (cfg.algo == KSW_ && st.ksw_wc && ksw_wc_scores_ok(cfg.sc)) {
+        uint32_t mq = 0;
+        for (int i = 0; i < b.n; i++)
+            if (b.h_q_len[i] + 2 <= 2048u) mq = std::max(mq, b.h_q_len[i]);
+        p.ksw_tiles = ksw_wc_tiles((int)mq);
+        if (grow((void **)&ws.fb, &ws.fb_cap, (size_t)b.n, 4) != GB_OK) return GB_ERR_ALLOC;
+    }
     if ((size_t)std::max(cols, 8) * p.block * 4 <= smem_limit) {
         a.smem_cols = std::max(cols, 8);
     } else {
         a.smem_cols = 0;
-        const size_t threads = (size_t)dp_scratch_blocks(b.n, p.block) * p.block;
+        int blocks = dp_scratch_blocks(b.n, p.block);
+        if (p.ksw_tiles > 0) {
+            int dev = 0, sms = 148;
+            cudaGetDevice(&dev);
+            cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+            blocks = std::min(blocks, 2 * sms);
+            p.fb_blocks = blocks;
+        }
+        const size_t threads = (size_t)blocks * p.block;
         if (grow((void **)&ws.scratch, &ws.scratch_cap, threads * cols, 4) != GB_OK) return GB_ERR_ALLOC;
         a.scratch = ws.scratch;
         a.scratch_cols = (uint32_t)cols;
@@ -315,6 +332,28 @@ static int launch_dp_split(int algo, int start, bool second, DpArgs a, const uin
     return GB_OK;
 }
 
+/* ksw: every pair (in `order`, or 0..n-1) to the warp-per-pair kernel, then
+ * the pairs it handed back to the one-thread kernel, whose count it reads on
+ * the device.  queue words: [0] one-thread work counter, [1] warp work
+ * counter, [2] handed-back count. */
+static int launch_ksw_split(const Plan &p, const uint32_t *order, int n, Workspace &ws, cudaStream_t s)
+{
+    GB_CUDA(cudaMemsetAsync(ws.queue, 0, 16, s));
+    timing_mark(K_DP, true, s);
+    GB_CUDA(launch_ksw_wc(p.a, order, n, p.ksw_tiles, ws.fb, ws.queue + 2, ws.queue + 1, s));
+    timing_mark(K_DP, false, s);
+    DpArgs fa = p.a;
+    fa.order = ws.fb;
+    fa.n = n;
+    fa.n_dev = ws.queue + 2;
+    fa.queue = ws.queue;
+    timing_mark(K_DP, true, s);
+    if (fa.smem_cols > 0) GB_CUDA(launch_dp(KSW_, WITHOUT_START_, false, fa, p.block, 0, s));
+    else GB_CUDA(launch_dp_scratch_grid(KSW_, WITHOUT_START_, false, fa, p.block, p.fb_blocks, s));
+    timing_mark(K_DP, false, s);
+    return GB_OK;
+}
+
 static int enqueue_order(const uint32_t *q_len, const uint32_t *t_len, int n, Workspace &ws, cudaStream_t s)
 {
     timing_mark(K_ORDER, true, s);
@@ -348,6 +387,7 @@ int enqueue_batch(const RunCfg &cfg, const DevBatch &b, const DevOut &o, Workspa
             if (rc != GB_OK) return rc;
             ord = ws.order;
         }
+        if (p.ksw_tiles > 0) return launch_ksw_split(p, ord, b.n, ws, s);
         return launch_dp_split(cfg.algo, p.start, p.second, p.a, ord, ord ? p.nlong[0] : 0, p.mq8, p.mt8, p.block,
                                ws, s);
     }

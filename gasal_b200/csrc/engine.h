@@ -62,6 +62,8 @@ struct Workspace {
     cudaStream_t aux = nullptr;  /* second stream for the warp-cooperative kernel */
     uint32_t *queue = nullptr;   /* work counter of the persistent one-thread launch */
     cudaEvent_t fork = nullptr, join = nullptr;
+    uint32_t *fb = nullptr;      /* pairs the warp ksw kernel hands back */
+    size_t fb_cap = 0;
     ~Workspace();
 };
 
@@ -71,6 +73,8 @@ struct Plan {
     bool tb = false, second = false, use_wc = false, order_on = false;
     int start = 0, block = 64, mq8 = 0, mt8 = 0;
     uint32_t wc_min_q = 0;
+    int ksw_tiles = 0;      /* > 0: ksw runs warp-per-pair with this many 256-column tiles */
+    int fb_blocks = 0;      /* grid of the one-thread ksw launch for handed-back pairs (scratch rows) */
     DpArgs a{};
     std::vector<int> cut;   /* pair ranges [cut[c], cut[c+1]) run one after another */
     std::vector<int> nlong; /* per range: pairs on the warp-cooperative kernel */
@@ -100,6 +104,7 @@ struct Settings {
     int wc_min_qregs = 32;      /* pairs with at least this many query words go warp-cooperative */
     int wc_max_q8 = 12000;      /* ... while the batch's longest query fits the warp's ring */
     int graphs = 1;             /* gasal_aln_async runs each batch as a CUDA graph */
+    int ksw_wc = 1;             /* ksw pairs run warp-per-pair (ksw_wc.cu) */
 };
 Settings &settings();
 

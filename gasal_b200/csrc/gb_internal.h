@@ -48,6 +48,8 @@ struct DpArgs {
     int32_t head, tail, k_band, zdrop, mql;
     int32_t smem_cols;                  /* columns per thread held in shared memory (0 = use scratch) */
     uint32_t *queue;                    /* work counter of the persistent launch (zeroed), or null */
+    const uint32_t *n_dev;              /* if set, the number of pairs is read here on the device
+                                           (n is then an upper bound, used to size the grid) */
 };
 
 struct TbArgs {
@@ -87,6 +89,17 @@ cudaError_t launch_dp_wc(int algo, int start, bool second, const DpArgs &a, cons
 /* the global-scratch DP variant on a caller-chosen grid */
 cudaError_t launch_dp_scratch_grid(int algo, int start, bool second, const DpArgs &a, int block, int blocks,
                                    cudaStream_t s);
+
+/* warp-per-pair ksw extension (ksw_wc.cu) for the pairs listed in `list`
+ * (null: pairs 0..nlist-1).  Pairs it cannot take (query + 2 above
+ * 256*ksw_wc_tiles(max), seed + match*qlen >= 2^19) are appended to fb,
+ * counted in *fbn, for the one-pair-per-thread kernel.  wq: zeroed work
+ * counter.  Needs gap_extend >= 0, gap_open + gap_extend >= 0 and every
+ * score below 4096 in magnitude (ksw_wc_scores_ok). */
+bool ksw_wc_scores_ok(const Scores &sc);
+int ksw_wc_tiles(int max_qlen); /* 0: no tile count covers it */
+cudaError_t launch_ksw_wc(const DpArgs &a, const uint32_t *list, int nlist, int tiles, uint32_t *fb, uint32_t *fbn,
+                          uint32_t *wq, cudaStream_t s);
 
 int dp_block_size();
 int dp_scratch_blocks(int n, int block);

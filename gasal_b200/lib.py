@@ -48,7 +48,8 @@ class GbDevOut(C.Structure):
 
 
 class GbTuning(C.Structure):
-    _fields_ = [("block", C.c_int32), ("wc_min_qregs", C.c_int32), ("min_order_pairs", C.c_int32)]
+    _fields_ = [("block", C.c_int32), ("wc_min_qregs", C.c_int32), ("min_order_pairs", C.c_int32),
+                ("ksw_warp", C.c_int32)]
 
 
 class GbStorageView(C.Structure):
@@ -154,14 +155,17 @@ def graph_stats() -> dict:
 def get_tuning() -> dict:
     t = GbTuning()
     _check(lib().gb_get_tuning(C.byref(t)), "gb_get_tuning")
-    return {"block": t.block, "wc_min_qregs": t.wc_min_qregs, "min_order_pairs": t.min_order_pairs}
+    return {k: getattr(t, k) for k, _ in GbTuning._fields_}
 
 
-def set_tuning(block: int | None = None, wc_min_qregs: int | None = None, min_order_pairs: int | None = None):
+def set_tuning(**kw):
+    """Change any of block, wc_min_qregs, min_order_pairs, ksw_warp."""
     cur = get_tuning()
-    t = GbTuning(int(block if block is not None else cur["block"]),
-                 int(wc_min_qregs if wc_min_qregs is not None else cur["wc_min_qregs"]),
-                 int(min_order_pairs if min_order_pairs is not None else cur["min_order_pairs"]))
+    bad = set(kw) - set(cur)
+    if bad:
+        raise GasalError(f"unknown tuning keys {sorted(bad)}")
+    cur.update({k: int(v) for k, v in kw.items()})
+    t = GbTuning(*[cur[k] for k, _ in GbTuning._fields_])
     _check(lib().gb_set_tuning(C.byref(t)), "gb_set_tuning")
 
 
@@ -209,8 +213,9 @@ def autotune(p: Params, dev: dict, h_q_len: np.ndarray, h_t_len: np.ndarray, str
     ms = C.c_double()
     _check(lib().gb_autotune(C.byref(cp), C.byref(b), C.byref(o), C.c_void_p(stream_handle), int(reps),
                              C.byref(t), C.byref(ms)), "gb_autotune")
-    return {"block": t.block, "wc_min_qregs": t.wc_min_qregs, "min_order_pairs": t.min_order_pairs,
-            "ms": ms.value}
+    d = {k: getattr(t, k) for k, _ in GbTuning._fields_}
+    d["ms"] = ms.value
+    return d
 
 
 def align_dev(p: Params, dev: dict, h_q_len: np.ndarray, h_t_len: np.ndarray, stream_handle: int = 0,

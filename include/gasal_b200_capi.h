@@ -220,6 +220,7 @@ typedef struct {
     int32_t block;
     int32_t wc_min_qregs;
     int32_t min_order_pairs;
+    int32_t ksw_warp;      /* 1: ksw pairs run one warp per pair (default); 0: one thread per pair */
 } gb_tuning_t;
 int gb_set_tuning(const gb_tuning_t *t);
 int gb_get_tuning(gb_tuning_t *t);

@@ -661,7 +661,9 @@ int oracle_align_ex(const gb_params_t *p, const gb_batch_t *b, gb_out_t *o, int 
                 const int qlen = (int)b->q_len[i], tlen = (int)b->t_len[i];
                 res_t r;
                 memset(&r, 0, sizeof(r));
-                if (qlen > 0 && tlen > 0) {
+                /* ksw runs on empty sequences too: the reference then returns the
+                 * seed score h0 (src/kernels/ksw_kernel_template.h:176-186) */
+                if ((qlen > 0 && tlen > 0) || algo == A_KSW) {
                     const int qregs = (qlen + 7) >> 3, tregs = (tlen + 7) >> 3;
                     const int sb = p->second_best != 0;
                     unpack_codes(pq, b->q_off[i] >> 3, 8 * qregs, qc);

@@ -155,6 +155,22 @@ def case_ksw(seed=17, n=120):
     return W.workload3(n, seed=seed)
 
 
+def case_empty(seed=18):
+    """Empty queries and/or targets among ordinary pairs.  ksw returns the
+    seed score for them; LOCAL returns zeros."""
+    rng = np.random.default_rng(seed)
+    qs, ts = [], []
+    for i in range(48):
+        lq, lt = int(rng.integers(1, 40)), int(rng.integers(1, 40))
+        kind = i % 4
+        q = rand_seq(rng, lq) if kind in (0, 2) else b""
+        t = (mutate_bytes(rng, q) or b"A") if kind == 0 else (rand_seq(rng, lt) if kind == 1 else b"")
+        qs.append(q)
+        ts.append(t)
+    seeds = rng.integers(0, 61, size=len(qs))
+    return Batch.from_seqs(qs, ts, seed=seeds)
+
+
 def semi_start_ok(b: Batch, tail: int) -> np.ndarray:
     """Pairs on which the reference's semi-global start pass stays inside its
     reversed-target array.  With a QUERY/BOTH tail the end row can be set to the
@@ -201,6 +217,9 @@ def configs_for(case: str):
                 Params(algo=SEMI_GLOBAL, start_pos=WITH_START, head=BOTH, tail=BOTH)]
     elif case == "ksw":
         cfg += [Params(algo=KSW), Params(algo=LOCAL, start_pos=WITHOUT_START)]
+    elif case == "empty":
+        cfg += [Params(algo=KSW), Params(algo=KSW, match=2, mismatch=3, gap_open=4, gap_extend=2),
+                Params(algo=LOCAL, start_pos=WITHOUT_START)]
     return cfg
 
 
@@ -212,6 +231,7 @@ CASES = {
     "w1": case_w1,
     "long": case_long,
     "ksw": case_ksw,
+    "empty": case_empty,
 }
 
 
