@@ -206,6 +206,9 @@ def main():
     ap.add_argument("--pairs", type=int, default=0, help="pairs per GPU (default: the workload's size)")
     ap.add_argument("--ref-sample", type=int, default=4000)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--band", default="off", choices=["off", "learned"],
+                    help="ksw (w3): learned band with certificate; the model is trained first on a separate sample")
+    ap.add_argument("--band-train-pairs", type=int, default=100_000)
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -267,6 +270,25 @@ def main():
         dparts.append((p, b, d))
 
     stream = torch.cuda.Stream(device=dev)
+
+    band_info = None
+    if args.band == "learned":
+        if args.workload != "w3":
+            raise SystemExit("--band learned applies to the ksw workload (w3)")
+        from gasal_b200 import band_train as BT
+        t0 = time.time()
+        tp, tb = build_workload(args.band_train_pairs, shard.shard_seed(W.SEED_BASE + 101, rank), "w3")[0]
+        tdb = BT.DeviceBatch(torch, tb, dev)
+        feat = BT.features(torch, tdb)
+        lab = BT.labels(torch, tp, tdb)
+        model = gl.BandModel(seed=11)
+        trace = BT.train(torch, model, feat, lab, steps=600, batch=8192, tau=0.8, lr=3e-3)
+        model.install(16, 1024)
+        band_info = {"train_pairs": tb.n, "train_s": round(time.time() - t0, 1),
+                     "label_hist_log2": {str(k): int(v) for k, v in zip(*np.unique(lab, return_counts=True))},
+                     "loss_first": trace[0], "loss_last": trace[-1]}
+        del tdb, feat
+        log(f"band model trained in {band_info['train_s']} s; loss {trace[0]:.3f} -> {trace[-1]:.3f}")
 
     def step():
         for p, b, d in dparts:
@@ -347,6 +369,16 @@ def main():
            "d2h_bytes_per_step": d2h, "ms_per_step": e2e_ms,
            "path": "gasal_c_aln_async + gasal_c_is_aln_async_done (3 streams), pinned host batches"}
 
+    if args.workload == "w3":
+        # band statistics of one more (untimed) pass: computed cells, and with
+        # a band how many results the certificate kept
+        p3, b3, d3 = dparts[0]
+        wide = None if args.band == "learned" else torch.full((b3.n,), 1 << 20, dtype=torch.int32, device=dev)
+        with torch.cuda.stream(stream):
+            st = gl.ksw_band_align(p3, d3["map"], b3.q_len, b3.t_len, wide.data_ptr() if wide is not None else None,
+                                   None, stream.cuda_stream)
+        band_info = dict(band_info or {}, mode=args.band, **st,
+                         computed_cells_fraction=st["cells"] / max(1, b3.cells()))
     in_mb = sum(int(b.q.shape[0] + b.t.shape[0]) + 16 * b.n for _, b in parts) / 1e6
     l2_note = (f"inputs {in_mb:.0f} MB > 126 MB L2, no flush" if in_mb > 126 else
                f"inputs {in_mb:.0f} MB fit the 126 MB L2 (no flush: each step re-reads them, as a caller "
@@ -376,6 +408,7 @@ def main():
             "cpu_baseline": cpu,
             "e2e": e2e,
             "clocks": clk.summary(),
+            "band": band_info,
         }
         print(json.dumps(line), flush=True)
     if dist:

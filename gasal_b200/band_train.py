@@ -1,0 +1,89 @@
+"""Training the learned ksw band (no reference counterpart).
+
+Labels come from the banded kernel itself: a pair's label is log2 of the
+narrowest band in a ladder whose result the certificate keeps (log2(2048)
+when none does).  The model is trained with the pinball loss at quantile tau
+(tau > 0.5 prefers bands a little wider than needed: a refused band costs a
+full recomputation, a wider one only a few more columns).
+
+Everything runs on the current CUDA device through the C ABI; torch only
+holds the device buffers.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+from . import lib as gl
+from .capi import Batch, Params
+
+LADDER = (16, 32, 64, 128, 256, 512, 1024)
+NO_BAND = 11.0  # log2(2048): no ladder band was kept
+
+
+class DeviceBatch:
+    """A Batch copied to the device, with the gb_dev_batch_t / gb_dev_out_t
+    address map the C ABI wrappers take."""
+
+    def __init__(self, torch, b: Batch, dev, outs=("score", "q_end", "t_end")):
+        def t_(a, dt=None):
+            return torch.from_numpy(np.ascontiguousarray(a).view(dt or a.dtype)).to(dev)
+        self.b = b
+        self.keep = {"q": t_(b.q), "t": t_(b.t), "qo": t_(b.q_off, np.int32), "to": t_(b.t_off, np.int32),
+                     "ql": t_(b.q_len, np.int32), "tl": t_(b.t_len, np.int32),
+                     "pq": torch.zeros(b.q.shape[0] // 8, dtype=torch.int32, device=dev),
+                     "pt": torch.zeros(b.t.shape[0] // 8, dtype=torch.int32, device=dev)}
+        if b.seed is not None:
+            self.keep["seed"] = t_(b.seed, np.int32)
+        for k in outs:
+            self.keep["out_" + k] = torch.zeros(b.n, dtype=torch.int32, device=dev)
+        m = {"q_bytes": b.q.shape[0], "t_bytes": b.t.shape[0]}
+        for k, src in (("q", "q"), ("t", "t"), ("pq", "pq"), ("pt", "pt"), ("q_off", "qo"), ("t_off", "to"),
+                       ("q_len", "ql"), ("t_len", "tl"), ("seed", "seed")):
+            if src in self.keep:
+                m[k] = self.keep[src].data_ptr()
+        for k in outs:
+            m["out_" + k] = self.keep["out_" + k].data_ptr()
+        self.map = m
+
+    def out(self, k):
+        return self.keep["out_" + k]
+
+
+def features(torch, db: DeviceBatch, stream: int = 0):
+    stride = gl.lib().gb_band_feature_stride()
+    f = torch.zeros((db.b.n, stride), dtype=torch.float32, device=db.keep["q"].device)
+    gl.band_features(db.map, db.b.q_len, db.b.t_len, f.data_ptr(), stream)
+    return f
+
+
+def labels(torch, p: Params, db: DeviceBatch, ladder=LADDER, stream: int = 0) -> np.ndarray:
+    """log2 of the narrowest ladder band the certificate keeps, per pair."""
+    n = db.b.n
+    dev = db.keep["q"].device
+    lab = np.full(n, NO_BAND, dtype=np.float32)
+    done = np.zeros(n, dtype=bool)
+    ok = torch.zeros(n, dtype=torch.uint8, device=dev)
+    for w in ladder:
+        band = torch.full((n,), int(w), dtype=torch.int32, device=dev)
+        gl.ksw_band_align(p, db.map, db.b.q_len, db.b.t_len, band.data_ptr(), ok.data_ptr(), stream)
+        kept = ok.cpu().numpy().astype(bool)
+        new = kept & ~done
+        lab[new] = np.log2(w)
+        done |= kept
+    return lab
+
+
+def train(torch, model: "gl.BandModel", feat, lab: np.ndarray, steps: int = 400, batch: int = 8192,
+          tau: float = 0.8, lr: float = 3e-3, seed: int = 0, stream: int = 0) -> list:
+    """Adam on random mini-batches; returns the loss trace."""
+    dev = feat.device
+    y = torch.from_numpy(np.ascontiguousarray(lab, dtype=np.float32)).to(dev)
+    g = torch.Generator(device="cpu").manual_seed(seed)
+    n = feat.shape[0]
+    trace = []
+    for _ in range(steps):
+        idx = torch.randint(0, n, (min(batch, n),), generator=g).to(dev)
+        fb = feat.index_select(0, idx).contiguous()
+        yb = y.index_select(0, idx).contiguous()
+        trace.append(model.train_step(fb.data_ptr(), yb.data_ptr(), fb.shape[0], tau, lr, stream))
+    return trace

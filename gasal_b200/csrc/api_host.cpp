@@ -230,6 +230,10 @@ void release_state(const gasal_gpu_storage_t *s)
     if (w.join) cudaEventDestroy(w.join);
     if (w.bins) cudaFree(w.bins);
     if (w.fb) cudaFree(w.fb);
+    if (w.retry) cudaFree(w.retry);
+    if (w.feat) cudaFree(w.feat);
+    if (w.pred) cudaFree(w.pred);
+    if (w.bandw) cudaFree(w.bandw);
     if (p->d_n_cigar) cudaFree(p->d_n_cigar);
     if (p->exec) cudaGraphExecDestroy(p->exec);
 }
@@ -273,7 +277,8 @@ void batch_signature(std::vector<uint8_t> &v, const gasal_gpu_storage_t *s, cons
                           s->host_query_batch_lens, s->host_target_batch_lens, s->host_query_batch_offsets,
                           s->host_target_batch_offsets, s->host_query_op, s->host_target_op, s->host_seed_scores,
                           ss.d_n_cigar, ss.ws.tb, ss.ws.d_tb_off, ss.ws.h_tb_off, ss.ws.order, ss.ws.bins,
-                          ss.ws.queue, ss.ws.aux, ss.ws.fork, ss.ws.join, ss.ws.fb, (const void *)s->str};
+                          ss.ws.queue, ss.ws.aux, ss.ws.fork, ss.ws.join, ss.ws.fb, ss.ws.retry, ss.ws.feat,
+                          ss.ws.pred, ss.ws.bandw, (const void *)s->str};
     for (const void *q : ptrs) put(v, q);
     const gasal_res_t *rs[] = {s->host_res, s->device_cpy, s->host_res_second, s->device_cpy_second};
     for (const gasal_res_t *r : rs) {
@@ -286,7 +291,9 @@ void batch_signature(std::vector<uint8_t> &v, const gasal_gpu_storage_t *s, cons
     }
     put(v, plan.tb), put(v, plan.second), put(v, plan.use_wc), put(v, plan.order_on);
     put(v, plan.start), put(v, plan.block), put(v, plan.mq8), put(v, plan.mt8), put(v, plan.wc_min_q);
-    put(v, plan.ksw_tiles), put(v, plan.fb_blocks);
+    put(v, plan.ksw_slots), put(v, plan.fb_blocks), put(v, plan.band);
+    put(v, (const void *)cfg.band_w), put(v, cfg.band_model), put(v, cfg.band_min), put(v, cfg.band_max);
+    put(v, (const void *)cfg.band_ok);
     put(v, plan.a);
     for (int c : plan.cut) put(v, c);
     put(v, -1);
@@ -926,6 +933,7 @@ int aln_async(gasal_gpu_storage_t *s, uint32_t qbytes, uint32_t tbytes, uint32_t
     cfg.algo = params->algo, cfg.start = params->start_pos, cfg.second = params->secondBest == TRUE;
     cfg.head = params->semiglobal_skipping_head, cfg.tail = params->semiglobal_skipping_tail;
     cfg.k_band = params->k_band, cfg.zdrop = zdrop, cfg.sc = set.sc;
+    cfg.band_model = set.band_model, cfg.band_min = set.band_min, cfg.band_max = set.band_max;
     cfg.ref_reverse = set.ref_reverse, cfg.mql = set.mql, cfg.is_packed = params->isPacked;
     cfg.reverse_complement = params->isReverseComplement;
     gb::DevBatch b{};

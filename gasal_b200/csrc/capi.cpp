@@ -306,6 +306,7 @@ void dev_args(const gb_params_t *p, const gb_dev_batch_t *b, const gb_dev_out_t 
     cfg.sc = {p->match, p->mismatch, p->gap_open, p->gap_extend, p->gap_open + p->gap_extend};
     cfg.ref_reverse = set.ref_reverse, cfg.mql = set.mql, cfg.is_packed = 0;
     cfg.reverse_complement = p->reverse_complement;
+    cfg.band_model = set.band_model, cfg.band_min = set.band_min, cfg.band_max = set.band_max;
     db = gb::DevBatch{};
     db.n = b->n, db.q_bytes = b->q_bytes, db.t_bytes = b->t_bytes, db.q = b->q, db.t = b->t;
     db.pq = b->pq, db.pt = b->pt, db.q_off = b->q_off, db.t_off = b->t_off, db.q_len = b->q_len;

@@ -11,6 +11,7 @@
  * the same stream, reusing one tile buffer.
  */
 #include "engine.h"
+#include "mlband.h"
 
 #include <algorithm>
 #include <cstdio>
@@ -212,15 +213,26 @@ int plan_batch(const RunCfg &cfg, const DevBatch &b, const DevOut &o, Workspace 
         uint32_t mq = 0;
         for (int i = 0; i < b.n; i++)
             if (b.h_q_len[i] + 2 <= 2048u) mq = std::max(mq, b.h_q_len[i]);
-        p.ksw_tiles = ksw_wc_tiles((int)mq);
+        p.ksw_slots = ksw_wc_slots((int)mq);
         if (grow((void **)&ws.fb, &ws.fb_cap, (size_t)b.n, 4) != GB_OK) return GB_ERR_ALLOC;
+        p.band = cfg.band_w != nullptr || cfg.band_model != nullptr;
+        if (p.band) {
+            if (grow((void **)&ws.retry, &ws.retry_cap, (size_t)b.n, 4) != GB_OK) return GB_ERR_ALLOC;
+            if (cfg.band_model) {
+                if (grow((void **)&ws.feat, &ws.feat_cap, (size_t)b.n * BAND_FEATS_PAD, 4) != GB_OK)
+                    return GB_ERR_ALLOC;
+                size_t cap = ws.pred_cap;
+                if (grow((void **)&ws.pred, &cap, (size_t)b.n, 4) != GB_OK) return GB_ERR_ALLOC;
+                if (grow((void **)&ws.bandw, &ws.pred_cap, (size_t)b.n, 4) != GB_OK) return GB_ERR_ALLOC;
+            }
+        }
     }
     if ((size_t)std::max(cols, 8) * p.block * 4 <= smem_limit) {
         a.smem_cols = std::max(cols, 8);
     } else {
         a.smem_cols = 0;
         int blocks = dp_scratch_blocks(b.n, p.block);
-        if (p.ksw_tiles > 0) {
+        if (p.ksw_slots > 0) {
             int dev = 0, sms = 148;
             cudaGetDevice(&dev);
             cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
@@ -332,15 +344,35 @@ static int launch_dp_split(int algo, int start, bool second, DpArgs a, const uin
     return GB_OK;
 }
 
-/* ksw: every pair (in `order`, or 0..n-1) to the warp-per-pair kernel, then
- * the pairs it handed back to the one-thread kernel, whose count it reads on
- * the device.  queue words: [0] one-thread work counter, [1] warp work
- * counter, [2] handed-back count. */
-static int launch_ksw_split(const Plan &p, const uint32_t *order, int n, Workspace &ws, cudaStream_t s)
+/* ksw: every pair (in `order`, or 0..n-1) to the warp-per-pair kernel --
+ * banded first when a band is given, the certificate's refusals again
+ * without one -- then the pairs it handed back to the one-thread kernel,
+ * whose counts it reads on the device.  queue words: [0] one-thread work
+ * counter, [1] warp work counter, [2] handed-back count, [3] refused count,
+ * [4..5] computed cells (u64), [6] second warp work counter. */
+static int launch_ksw_split(const RunCfg &cfg, const DevBatch &b, const Plan &p, const uint32_t *order, int n,
+                            Workspace &ws, cudaStream_t s)
 {
-    GB_CUDA(cudaMemsetAsync(ws.queue, 0, 16, s));
+    GB_CUDA(cudaMemsetAsync(ws.queue, 0, 32, s));
+    unsigned long long *cells = reinterpret_cast<unsigned long long *>(ws.queue + 4);
     timing_mark(K_DP, true, s);
-    GB_CUDA(launch_ksw_wc(p.a, order, n, p.ksw_tiles, ws.fb, ws.queue + 2, ws.queue + 1, s));
+    if (p.band) {
+        const int32_t *bw = cfg.band_w;
+        if (!bw) {
+            GB_CUDA(launch_band_features(b.pq, b.pt, b.q_off, b.t_off, b.q_len, b.t_len, n, ws.feat, s));
+            GB_CUDA(launch_mlp_forward(static_cast<const __nv_bfloat16 *>(cfg.band_model), ws.feat, n, ws.pred, s));
+            GB_CUDA(launch_band_from_pred(ws.pred, b.q_len, b.t_len, n, cfg.band_min, cfg.band_max, ws.bandw, s));
+            bw = ws.bandw;
+        }
+        GB_CUDA(launch_ksw_band(p.a, order, n, p.ksw_slots, bw, ws.fb, ws.queue + 2, ws.retry, ws.queue + 3, cells,
+                                ws.queue + 1, s));
+        if (cfg.band_ok) GB_CUDA(launch_band_ok(cfg.band_ok, n, ws.retry, ws.queue + 3, s));
+        DpArgs ra = p.a;
+        ra.n_dev = ws.queue + 3;
+        GB_CUDA(launch_ksw_wc(ra, ws.retry, n, p.ksw_slots, ws.fb, ws.queue + 2, ws.queue + 6, cells, s));
+    } else {
+        GB_CUDA(launch_ksw_wc(p.a, order, n, p.ksw_slots, ws.fb, ws.queue + 2, ws.queue + 1, cells, s));
+    }
     timing_mark(K_DP, false, s);
     DpArgs fa = p.a;
     fa.order = ws.fb;
@@ -387,7 +419,7 @@ int enqueue_batch(const RunCfg &cfg, const DevBatch &b, const DevOut &o, Workspa
             if (rc != GB_OK) return rc;
             ord = ws.order;
         }
-        if (p.ksw_tiles > 0) return launch_ksw_split(p, ord, b.n, ws, s);
+        if (p.ksw_slots > 0) return launch_ksw_split(cfg, b, p, ord, b.n, ws, s);
         return launch_dp_split(cfg.algo, p.start, p.second, p.a, ord, ord ? p.nlong[0] : 0, p.mq8, p.mt8, p.block,
                                ws, s);
     }

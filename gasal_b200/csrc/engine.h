@@ -27,6 +27,12 @@ struct RunCfg {
     int mql;         /* reference MAX_QUERY_LEN for the semi-global last-row scan */
     int is_packed;   /* inputs are already 4-bit words */
     int reverse_complement;
+    /* ksw band (warp kernel only): an explicit per-pair half-width array, or
+     * an MLP (BF16 parameters) that predicts it from pair features */
+    const int32_t *band_w = nullptr;
+    const void *band_model = nullptr;
+    int band_min = 16, band_max = 1024;
+    uint8_t *band_ok = nullptr; /* optional: 1 where the banded result was kept */
 };
 
 struct DevBatch {
@@ -64,6 +70,13 @@ struct Workspace {
     cudaEvent_t fork = nullptr, join = nullptr;
     uint32_t *fb = nullptr;      /* pairs the warp ksw kernel hands back */
     size_t fb_cap = 0;
+    uint32_t *retry = nullptr;   /* pairs whose banded result the certificate refused */
+    size_t retry_cap = 0;
+    float *feat = nullptr;       /* band features, BAND_FEATS_PAD per pair */
+    size_t feat_cap = 0;         /* floats */
+    float *pred = nullptr;       /* predicted log2 band */
+    int32_t *bandw = nullptr;    /* per-pair band */
+    size_t pred_cap = 0;
     ~Workspace();
 };
 
@@ -73,7 +86,8 @@ struct Plan {
     bool tb = false, second = false, use_wc = false, order_on = false;
     int start = 0, block = 64, mq8 = 0, mt8 = 0;
     uint32_t wc_min_q = 0;
-    int ksw_tiles = 0;      /* > 0: ksw runs warp-per-pair with this many 256-column tiles */
+    int ksw_slots = 0;      /* > 0: ksw runs warp-per-pair, this many eh columns per warp */
+    bool band = false;      /* ksw through the banded kernel + certificate */
     int fb_blocks = 0;      /* grid of the one-thread ksw launch for handed-back pairs (scratch rows) */
     DpArgs a{};
     std::vector<int> cut;   /* pair ranges [cut[c], cut[c+1]) run one after another */
@@ -105,6 +119,8 @@ struct Settings {
     int wc_max_q8 = 12000;      /* ... while the batch's longest query fits the warp's ring */
     int graphs = 1;             /* gasal_aln_async runs each batch as a CUDA graph */
     int ksw_wc = 1;             /* ksw pairs run warp-per-pair (ksw_wc.cu) */
+    const void *band_model = nullptr; /* installed band MLP (BF16 parameters on the device) */
+    int band_min = 16, band_max = 1024;
 };
 Settings &settings();
 

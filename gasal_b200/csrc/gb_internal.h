@@ -91,15 +91,23 @@ cudaError_t launch_dp_scratch_grid(int algo, int start, bool second, const DpArg
                                    cudaStream_t s);
 
 /* warp-per-pair ksw extension (ksw_wc.cu) for the pairs listed in `list`
- * (null: pairs 0..nlist-1).  Pairs it cannot take (query + 2 above
- * 256*ksw_wc_tiles(max), seed + match*qlen >= 2^19) are appended to fb,
+ * (null: pairs 0..nlist-1; a.n_dev, if set, caps the count on the device).
+ * `slots` = ksw_wc_slots(longest query it should take); pairs it cannot take
+ * (query + 2 above slots, seed + match*qlen >= 2^19) are appended to fb,
  * counted in *fbn, for the one-pair-per-thread kernel.  wq: zeroed work
  * counter.  Needs gap_extend >= 0, gap_open + gap_extend >= 0 and every
  * score below 4096 in magnitude (ksw_wc_scores_ok). */
 bool ksw_wc_scores_ok(const Scores &sc);
-int ksw_wc_tiles(int max_qlen); /* 0: no tile count covers it */
-cudaError_t launch_ksw_wc(const DpArgs &a, const uint32_t *list, int nlist, int tiles, uint32_t *fb, uint32_t *fbn,
-                          uint32_t *wq, cudaStream_t s);
+int ksw_wc_slots(int max_qlen); /* 0: longer than the kernel takes (2046) */
+cudaError_t launch_ksw_wc(const DpArgs &a, const uint32_t *list, int nlist, int slots, uint32_t *fb, uint32_t *fbn,
+                          uint32_t *wq, unsigned long long *cells, cudaStream_t s);
+/* The same with a band: pair p is computed within half-width band_w[p]
+ * (negative: unbanded) and kept only if the band certificate proves it equal
+ * to the unbanded result; otherwise nothing is written and p goes to retry
+ * (count *nretry).  cells (optional) accumulates the computed cells. */
+cudaError_t launch_ksw_band(const DpArgs &a, const uint32_t *list, int nlist, int slots, const int32_t *band_w,
+                            uint32_t *fb, uint32_t *fbn, uint32_t *retry, uint32_t *nretry, unsigned long long *cells,
+                            uint32_t *wq, cudaStream_t s);
 
 int dp_block_size();
 int dp_scratch_blocks(int n, int block);

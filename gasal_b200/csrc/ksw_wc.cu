@@ -36,7 +36,8 @@ namespace gb {
 
 namespace {
 
-constexpr int KT = 256;                 /* columns per tile */
+constexpr int KT = 256;                 /* columns per tile (32 lanes x 8) */
+constexpr int KSW_WC_MAX_COLS = 2048;   /* queries up to 2046 bases stay on this kernel */
 constexpr int KEY_BITS = 12;            /* key = H << 12 | column */
 constexpr int KEY_H_LIMIT = 1 << 19;    /* H must stay below this for the key */
 constexpr unsigned FULL = 0xFFFFFFFFu;
@@ -46,68 +47,87 @@ __device__ __forceinline__ int kslot(int j) { return (j & ~255) | ((j & 7) << 5)
 /* 16-bit prmt selector that sign-extends byte c (class c < 8) */
 __device__ __forceinline__ uint32_t sel16(uint32_t c) { return c * 0x1111u | 0x8880u; }
 
-/* One pair.  NT tiles cover the query (qlen + 2 <= NT*256).  FAST: every code
- * is plain and the scores fit a signed byte (prmt table lookup); otherwise
- * nibble compares. */
-template <int NT, bool FAST>
-__device__ void ksw_pair(const DpArgs &a, uint32_t pid, int2 *eh, const uint2 *stab, int lane, int qlen, int tlen,
-                         const uint32_t *q, const uint32_t *t, int h0)
+/* Band certificate state (BAND mode).  C bounds every value of the
+ * unbanded computation that the banded one does not have: cells outside the
+ * band and band cells whose unbanded value was raised from outside.  Paths
+ * leave the band only through the F chain past its right edge and the E of
+ * its leftmost column (the band moves one column right per row), or start
+ * outside it (the first row's seed-derived entries, the first column's
+ * h0-derived values); a positive value gains at most max(match, 0) per row
+ * and a zero one none ("M ? M + s : 0").  The unbanded computation then has
+ * the banded one's row maximum and position whenever that maximum exceeds C
+ * (or C is 0), the same trimmed range whenever the banded range ends inside
+ * the band only while C is 0, and an end-to-end score that is either known or
+ * bounded by C. */
+struct Cert {
+    int C = 0;          /* carried bound, after the last processed row */
+    int gcert = -1;     /* largest end-to-end score the unbanded run surely took */
+    int gie = -1;       /* its (last) row */
+    int gunc = -1;      /* bound on every end-to-end candidate not known exactly */
+};
+
+/* One pair; `slots` shared-memory columns hold its eh row.  FAST: every
+ * code is plain and the scores fit a signed byte (prmt table lookup),
+ * otherwise nibble compares.  BAND: half-width w >= 0, returns false when
+ * the certificate cannot vouch for the banded result (nothing is written). */
+template <bool FAST, bool BAND>
+__device__ bool ksw_pair(const DpArgs &a, uint32_t pid, int2 *eh, const uint4 *selw, int slots, const uint2 *stab,
+                         int lane, int qlen, int tlen, const uint32_t *q, const uint32_t *t, int h0, int w,
+                         unsigned long long &ncells)
 {
     const int e_del = a.sc.e, oe = a.sc.oe, o_del = a.sc.o;
     const int eK = e_del * 8;
+    const int mpos = max(a.sc.match, 0);
     /* C bounds every substitution score so that min(M + s, M*C) is M + s for
      * M >= 1 and <= 0 for M = 0 (0 and a negative value act alike below:
      * every later use is max(., e>=0, f>=0) or max(. - (o+e), 0)) */
-    const int C = max(max(a.sc.match, -a.sc.mismatch), 0) + 1;
-
-    /* per-lane column codes: FAST = two 16-bit prmt selectors per register,
-     * otherwise the raw packed word */
-    uint32_t cw[NT][4];
-    const int qregs = (qlen + 7) >> 3;
-#pragma unroll
-    for (int tt = 0; tt < NT; tt++) {
-        const int wi = tt * 32 + lane;
-        const uint32_t w = wi < qregs ? q[wi] : 0u;
-        if (FAST) {
-#pragma unroll
-            for (int p = 0; p < 4; p++) {
-                const uint32_t c0 = class_of((w >> (28 - 8 * p)) & 15u), c1 = class_of((w >> (24 - 8 * p)) & 15u);
-                cw[tt][p] = sel16(c0) | (sel16(c1) << 16);
-            }
-        } else {
-            cw[tt][0] = w;
-        }
-    }
+    const int Cmul = max(max(a.sc.match, -a.sc.mismatch), 0) + 1;
 
     /* the reference's first row (ksw_kernel_template.h:75-79) */
-    for (int s = lane; s < NT * KT; s += 32) eh[s] = make_int2(0, 0);
+    for (int s = lane; s < slots; s += 32) eh[s] = make_int2(0, 0);
     __syncwarp();
-    {
-        const long long v1 = (uint32_t)h0 > (uint32_t)oe ? (long long)h0 - oe : 0;
-        for (int j = lane; j <= qlen + 1; j += 32) {
-            long long h = 0;
-            if (j == 0) h = h0;
-            else if (j == 1) h = v1;
-            else if (j <= qlen && v1 - (long long)(j - 2) * e_del > e_del) h = v1 - (long long)(j - 1) * e_del;
-            if (h) eh[kslot(j)].x = (int)h;
-        }
+    const long long v1 = (uint32_t)h0 > (uint32_t)oe ? (long long)h0 - oe : 0;
+    auto init_h = [&](int j) -> long long {
+        if (j == 0) return h0;
+        if (j == 1) return v1;
+        if (j <= qlen && v1 - (long long)(j - 2) * e_del > e_del) return v1 - (long long)(j - 1) * e_del;
+        return 0;
+    };
+    for (int j = lane; j <= qlen + 1; j += 32) {
+        const long long h = init_h(j);
+        if (h) eh[kslot(j)].x = (int)h;
     }
     __syncwarp();
+
+    Cert ct;
+    if (BAND) ct.C = (int)init_h(w + 1); /* the seed-derived entries right of the first row's band */
 
     const int L8 = (qlen >> 3) << 3;
     int mx = h0, max_i = -1, max_j = -1, max_ie = -1, gscore = -1;
     int beg = 0, end = qlen;
+    ncells = 0;
     for (int i = 0; i < tlen;) {
+        bool clipped_r = false;
+        int Cprev = 0;
+        if (BAND) {
+            Cprev = ct.C;
+            /* a trimmed end inside the band is the unbanded end only while C is 0 */
+            if (Cprev > 0 && end < min(i + w + 1, qlen)) return false;
+            clipped_r = end > i + w + 1;
+            if (beg < i - w) beg = i - w;
+            if (end > i + w + 1) end = i + w + 1;
+        }
         const int g = code(__ldg(t + (i >> 3)), i & 7);
         int h1 = 0;
         if (beg == 0) {
             h1 = (int)((uint32_t)h0 - (uint32_t)(o_del + e_del * (i + 1)));
             if (h1 < 0) h1 = 0;
         }
-        int m = 0, mj = -1;
+        int m = 0, mj = -1, fout = 0;
         int tf = -1, tl = -1;
         unsigned mf = 0, ml = 0;
         if (beg < end) {
+            ncells += (unsigned long long)(end - beg);
             uint2 tab = make_uint2(0, 0);
             int sm = 0, sx = 0;
             if (FAST) {
@@ -116,29 +136,33 @@ __device__ void ksw_pair(const DpArgs &a, uint32_t pid, int2 *eh, const uint2 *s
                 sm = g == N_CODE4 ? 0 : a.sc.match;
                 sx = g == N_CODE4 ? 0 : -a.sc.mismatch;
             }
-            int fcarry = 0, hcarry = h1, kmax = -1, hlast = 0;
-            const int tlo = beg >> 8, thi = (end - 1) >> 8;
-#pragma unroll
-            for (int tt = 0; tt < NT; tt++) {
-                if (tt < tlo || tt > thi) continue;
-                const int j0 = tt * KT + lane * 8;
+            int fcarry = 0, hcarry = h1, kmax = -1, hlast = 0, flast = 0;
+            const int c0 = beg & ~7;
+            const int ntiles = (end - c0 + KT - 1) / KT;
+            for (int tt = 0; tt < ntiles; tt++) {
+                const int j0 = c0 + tt * KT + lane * 8;
                 const int nv = min(max(end - j0, 0), 8);
+                /* lanes past the row (nv == 0) read slot group 0 and store nothing */
+                const int jr = j0 < slots ? j0 : 0;
+                const int sb = (jr & ~255) | ((jr >> 3) & 31);
+                const uint4 sw = selw[jr >> 3];
+                const uint32_t swk[4] = {sw.x, sw.y, sw.z, sw.w};
                 int2 v[8];
                 int Mp[8], tv[8];
 #pragma unroll
-                for (int k = 0; k < 8; k++) v[k] = eh[tt * KT + k * 32 + lane];
+                for (int k = 0; k < 8; k++) v[k] = eh[sb + 32 * k];
                 /* pass 1: M', t and the lane's F fold */
                 int agg = 0;
 #pragma unroll
                 for (int k = 0; k < 8; k++) {
                     int s;
                     if (FAST) {
-                        s = (int)prmt(tab.x, tab.y, (k & 1) ? (cw[tt][k >> 1] >> 16) : cw[tt][k >> 1]);
+                        s = (int)prmt(tab.x, tab.y, (k & 1) ? (swk[k >> 1] >> 16) : swk[k >> 1]);
                     } else {
-                        const int c = (int)((cw[tt][0] >> (28 - 4 * k)) & 15u);
+                        const int c = (int)((sw.x >> (28 - 4 * k)) & 15u);
                         s = c == N_CODE4 ? 0 : (c == g ? sm : sx);
                     }
-                    Mp[k] = __viaddmin_s32(v[k].x, s, v[k].x * C);
+                    Mp[k] = __viaddmin_s32(v[k].x, s, v[k].x * Cmul);
                     tv[k] = __viaddmax_s32(Mp[k], -oe, 0);
                     agg = k == 0 ? tv[0] : __viaddmax_s32(agg, -e_del, tv[k]);
                 }
@@ -162,6 +186,7 @@ __device__ void ksw_pair(const DpArgs &a, uint32_t pid, int2 *eh, const uint2 *s
                     if (k < nv) {
                         kmax = max(kmax, H[k] * (1 << KEY_BITS) + (j0 + k));
                         hlast = H[k];
+                        if (BAND) flast = f;
                     }
                 }
                 int hp = __shfl_up_sync(FULL, H[7], 1);
@@ -172,7 +197,7 @@ __device__ void ksw_pair(const DpArgs &a, uint32_t pid, int2 *eh, const uint2 *s
                 for (int k = 0; k < 8; k++) {
                     const int hs = k == 0 ? hp : H[k - 1];
                     if (k < nv) {
-                        eh[tt * KT + k * 32 + lane] = make_int2(hs, v[k].y);
+                        eh[sb + 32 * k] = make_int2(hs, v[k].y);
                         nz |= (uint32_t)(hs | v[k].y);
                     }
                 }
@@ -185,11 +210,48 @@ __device__ void ksw_pair(const DpArgs &a, uint32_t pid, int2 *eh, const uint2 *s
             kmax = __reduce_max_sync(FULL, kmax);
             m = kmax >> KEY_BITS;
             mj = kmax & ((1 << KEY_BITS) - 1);
-            h1 = __shfl_sync(FULL, hlast, ((end - 1) >> 3) & 31);
+            const int owner = ((end - 1 - c0) >> 3) & 31;
+            h1 = __shfl_sync(FULL, hlast, owner);
+            if (BAND) fout = __shfl_sync(FULL, flast, owner);
         }
         if (lane == 0) eh[kslot(end)] = make_int2(h1, 0);
         __syncwarp();
-        if (max(L8, end) == qlen) {
+        if (BAND) {
+            /* bound on this row's values the banded run does not have */
+            int Crow = Cprev > 0 ? Cprev + mpos : 0;
+            if (i > w) { /* the h0-derived column left of the matrix, outside the band */
+                const int hv = h0 - o_del - e_del * i;
+                if (hv > 0) Crow = max(Crow, hv + mpos);
+            }
+            if (end == i + w + 1 && end < qlen) Crow = max(Crow, fout);            /* F past the right edge */
+            if (!(Crow == 0 || m > Crow)) return false;
+            /* end-to-end score candidates (the unbanded end is known when the
+             * row reached qlen, or when nothing was clipped or contaminated) */
+            const bool end_known = end == qlen || (!clipped_r && Cprev == 0);
+            const bool val_known = Crow == 0 || h1 > Crow;
+            bool upd_known = false, upd_maybe = false;
+            if (L8 == qlen) {
+                if (end_known) upd_known = true;
+                else ct.gunc = max(ct.gunc, max(h1, Crow));
+            } else if (end == qlen) {
+                upd_known = true;
+            } else if (!end_known) {
+                upd_maybe = true;
+            }
+            if (upd_known) {
+                if (val_known) {
+                    ct.gie = ct.gcert > h1 ? ct.gie : i;
+                    ct.gcert = max(ct.gcert, h1);
+                } else {
+                    ct.gunc = max(ct.gunc, Crow);
+                }
+            }
+            if (upd_maybe) ct.gunc = max(ct.gunc, Crow);
+            /* E leaving the band's leftmost column into the next row */
+            int Cnext = Crow;
+            if (beg < end && beg == i - w) Cnext = max(Cnext, eh[kslot(i - w)].y);
+            ct.C = Cnext;
+        } else if (max(L8, end) == qlen) {
             max_ie = gscore > h1 ? max_ie : i;
             gscore = max(gscore, h1);
         }
@@ -206,18 +268,19 @@ __device__ void ksw_pair(const DpArgs &a, uint32_t pid, int2 *eh, const uint2 *s
             }
         }
         if (leave) {
+            __syncwarp();
             i = ((i >> 3) + 1) << 3;
             continue;
         }
         /* trimming (ksw_kernel_template.h:188-196) */
         int nbeg = end;
         if (tf >= 0) {
-            const int base = tf * KT + (__ffs(mf) - 1) * 8;
+            const int base = (beg & ~7) + tf * KT + (__ffs(mf) - 1) * 8;
             for (int k = 7; k >= 0; k--) {
                 const int j = base + k;
                 if (j < end) {
-                    const int2 w = eh[kslot(j)];
-                    if (w.x | w.y) nbeg = j;
+                    const int2 x = eh[kslot(j)];
+                    if (x.x | x.y) nbeg = j;
                 }
             }
         }
@@ -225,12 +288,12 @@ __device__ void ksw_pair(const DpArgs &a, uint32_t pid, int2 *eh, const uint2 *s
         if (h1 != 0) {
             lastnz = end;
         } else if (tl >= 0) {
-            const int base = tl * KT + (31 - __clz(ml)) * 8;
+            const int base = (beg & ~7) + tl * KT + (31 - __clz(ml)) * 8;
             for (int k = 0; k < 8; k++) {
                 const int j = base + k;
                 if (j < end) {
-                    const int2 w = eh[kslot(j)];
-                    if (w.x | w.y) lastnz = j;
+                    const int2 x = eh[kslot(j)];
+                    if (x.x | x.y) lastnz = j;
                 }
             }
         }
@@ -238,6 +301,16 @@ __device__ void ksw_pair(const DpArgs &a, uint32_t pid, int2 *eh, const uint2 *s
         end = lastnz + 2 < qlen ? lastnz + 2 : qlen;
         __syncwarp(); /* the scans above read slots their owners rewrite next row */
         i++;
+    }
+    if (BAND) {
+        const int gmax = max(ct.gcert, ct.gunc);
+        if (gmax <= 0 || gmax <= mx - 5) {
+            gscore = -1; /* the maximum is the answer */
+        } else if (ct.gcert > ct.gunc) {
+            gscore = ct.gcert, max_ie = ct.gie;
+        } else {
+            return false;
+        }
     }
     if (lane == 0) {
         int sc, qe, te;
@@ -251,56 +324,97 @@ __device__ void ksw_pair(const DpArgs &a, uint32_t pid, int2 *eh, const uint2 *s
         if (a.t_end) a.t_end[pid] = te;
     }
     __syncwarp();
+    return true;
 }
 
-template <int NT>
-__global__ void __launch_bounds__(128) ksw_wc_kernel(DpArgs a, const uint32_t *list, int nlist, uint32_t *fb,
-                                                     uint32_t *fbn, uint32_t *wq)
+/* band: per-pair half-width (negative = none) or null; retry/nretry collect
+ * the pairs whose banded result the certificate did not accept. */
+struct BandArgs {
+    const int32_t *w;
+    uint32_t *retry, *nretry;
+    unsigned long long *cells; /* computed cells (rows x trimmed range), or null */
+};
+
+template <bool BAND>
+__global__ void __launch_bounds__(32) ksw_wc_kernel(DpArgs a, const uint32_t *list, int nlist, int slots,
+                                                     uint32_t *fb, uint32_t *fbn, uint32_t *wq, BandArgs ba)
 {
     extern __shared__ int2 ksw_smem[];
     __shared__ uint2 stab[16];
     build_score_table(stab, a.sc, true);
     __syncthreads();
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    int2 *eh = ksw_smem + (size_t)warp * NT * KT;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, warps = blockDim.x >> 5;
+    int2 *eh = ksw_smem + (size_t)warp * slots;
+    uint4 *selw = reinterpret_cast<uint4 *>(ksw_smem + (size_t)warps * slots) + (size_t)warp * (slots / 8);
     const bool fast_scores = a.sc.match >= -128 && a.sc.match <= 127 && a.sc.mismatch >= -127 && a.sc.mismatch <= 128;
     const long long mpos = a.sc.match > 0 ? a.sc.match : 0;
+    const uint32_t n = a.n_dev ? min(*a.n_dev, (uint32_t)nlist) : (uint32_t)nlist;
     for (;;) {
         uint32_t idx = 0;
         if (lane == 0) idx = atomicAdd(wq, 1u);
         idx = __shfl_sync(FULL, idx, 0);
-        if (idx >= (uint32_t)nlist) break;
+        if (idx >= n) break;
         const uint32_t pid = list ? list[idx] : idx;
         const int qlen = (int)a.q_len[pid], tlen = (int)a.t_len[pid];
         const uint32_t h0u = a.seed ? a.seed[pid] : 0u;
-        if (qlen + 2 > NT * KT || (long long)h0u + mpos * qlen >= KEY_H_LIMIT) {
+        if (qlen + 2 > slots || (long long)h0u + mpos * qlen >= KEY_H_LIMIT) {
             if (lane == 0) fb[atomicAdd(fbn, 1u)] = pid;
             continue;
         }
         const uint32_t *q = a.pq + (a.q_off[pid] >> 3), *t = a.pt + (a.t_off[pid] >> 3);
         bool plain = fast_scores;
+        const int qregs = (qlen + 7) >> 3;
         if (plain) {
-            const int qregs = (qlen + 7) >> 3, tregs = (tlen + 7) >> 3;
+            const int tregs = (tlen + 7) >> 3;
             uint32_t bad = 0;
-            for (int w = lane; w < qregs + tregs; w += 32) {
-                const uint32_t x = w < qregs ? q[w] : t[w - qregs];
+            for (int x = lane; x < qregs + tregs; x += 32) {
+                const uint32_t y = x < qregs ? q[x] : t[x - qregs];
 #pragma unroll
-                for (int k = 0; k < 8; k++) bad |= ~(PLAIN_CODES >> ((x >> (4 * k)) & 15u)) & 1u;
+                for (int k = 0; k < 8; k++) bad |= ~(PLAIN_CODES >> ((y >> (4 * k)) & 15u)) & 1u;
             }
             plain = __all_sync(FULL, bad == 0);
         }
-        if (plain) ksw_pair<NT, true>(a, pid, eh, stab, lane, qlen, tlen, q, t, (int)h0u);
-        else ksw_pair<NT, false>(a, pid, eh, stab, lane, qlen, tlen, q, t, (int)h0u);
+        /* per 8 query columns: eight 16-bit prmt selectors (plain), or the packed word */
+        for (int gi = lane; gi < slots / 8; gi += 32) {
+            const uint32_t y = gi < qregs ? q[gi] : 0u;
+            uint4 sw;
+            if (plain) {
+                uint32_t c[8];
+#pragma unroll
+                for (int k = 0; k < 8; k++) c[k] = sel16(class_of((y >> (28 - 4 * k)) & 15u));
+                sw = make_uint4(c[0] | (c[1] << 16), c[2] | (c[3] << 16), c[4] | (c[5] << 16), c[6] | (c[7] << 16));
+            } else {
+                sw = make_uint4(y, 0u, 0u, 0u);
+            }
+            selw[gi] = sw;
+        }
+        __syncwarp();
+        const int w = BAND && ba.w ? min(ba.w[pid], 1 << 20) : -1; /* wider than any matrix = unbanded */
+        bool ok;
+        unsigned long long nc = 0;
+        if (BAND && w >= 0) {
+            ok = plain ? ksw_pair<true, true>(a, pid, eh, selw, slots, stab, lane, qlen, tlen, q, t, (int)h0u, w, nc)
+                       : ksw_pair<false, true>(a, pid, eh, selw, slots, stab, lane, qlen, tlen, q, t, (int)h0u, w, nc);
+        } else {
+            ok = plain ? ksw_pair<true, false>(a, pid, eh, selw, slots, stab, lane, qlen, tlen, q, t, (int)h0u, -1, nc)
+                       : ksw_pair<false, false>(a, pid, eh, selw, slots, stab, lane, qlen, tlen, q, t, (int)h0u, -1,
+                                               nc);
+        }
+        if (ba.cells && lane == 0) atomicAdd(ba.cells, nc);
+        if (!ok && lane == 0) ba.retry[atomicAdd(ba.nretry, 1u)] = pid;
+        __syncwarp();
     }
 }
 
-template <int NT>
-cudaError_t launch_nt(const DpArgs &a, const uint32_t *list, int nlist, uint32_t *fb, uint32_t *fbn, uint32_t *wq,
-                      cudaStream_t s)
+/* shared-memory slots per warp for queries up to max_qlen (whole tiles) */
+int slots_for(int max_qlen) { return ((max_qlen + 2 + KT - 1) / KT) * KT; }
+
+cudaError_t launch_slots(const DpArgs &a, const uint32_t *list, int nlist, int slots, uint32_t *fb, uint32_t *fbn,
+                         uint32_t *wq, const BandArgs &ba, bool band, cudaStream_t s)
 {
-    const int block = 128;
-    const size_t smem = (size_t)(block / 32) * NT * KT * sizeof(int2);
-    auto k = ksw_wc_kernel<NT>;
+    const int block = 32, warps = block / 32; /* one warp per block packs shared memory tightest */
+    const size_t smem = (size_t)warps * slots * (sizeof(int2) + 2);
+    auto k = band ? ksw_wc_kernel<true> : ksw_wc_kernel<false>;
     cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     int dev = 0, sms = 148, per_sm = 0;
@@ -309,10 +423,10 @@ cudaError_t launch_nt(const DpArgs &a, const uint32_t *list, int nlist, uint32_t
     e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, block, smem);
     if (e != cudaSuccess) return e;
     if (per_sm < 1) per_sm = 1;
-    int blocks = (nlist + 3) / 4;
+    int blocks = (nlist + warps - 1) / warps;
     if (blocks > per_sm * sms) blocks = per_sm * sms;
     if (blocks < 1) blocks = 1;
-    k<<<blocks, block, smem, s>>>(a, list, nlist, fb, fbn, wq);
+    k<<<blocks, block, smem, s>>>(a, list, nlist, slots, fb, fbn, wq, ba);
     return cudaGetLastError();
 }
 
@@ -324,24 +438,23 @@ bool ksw_wc_scores_ok(const Scores &sc)
            sc.mismatch > -4095;
 }
 
-int ksw_wc_tiles(int max_qlen)
-{
-    for (int nt = 1; nt <= 8; nt <<= 1)
-        if (max_qlen + 2 <= nt * KT) return nt;
-    return 0;
-}
+int ksw_wc_slots(int max_qlen) { return max_qlen + 2 <= KSW_WC_MAX_COLS ? slots_for(max_qlen) : 0; }
 
-cudaError_t launch_ksw_wc(const DpArgs &a, const uint32_t *list, int nlist, int tiles, uint32_t *fb, uint32_t *fbn,
-                          uint32_t *wq, cudaStream_t s)
+cudaError_t launch_ksw_wc(const DpArgs &a, const uint32_t *list, int nlist, int slots, uint32_t *fb, uint32_t *fbn,
+                          uint32_t *wq, unsigned long long *cells, cudaStream_t s)
 {
     if (nlist <= 0) return cudaSuccess;
-    switch (tiles) {
-    case 1: return launch_nt<1>(a, list, nlist, fb, fbn, wq, s);
-    case 2: return launch_nt<2>(a, list, nlist, fb, fbn, wq, s);
-    case 4: return launch_nt<4>(a, list, nlist, fb, fbn, wq, s);
-    case 8: return launch_nt<8>(a, list, nlist, fb, fbn, wq, s);
-    default: return cudaErrorInvalidValue;
-    }
+    BandArgs ba{nullptr, nullptr, nullptr, cells};
+    return launch_slots(a, list, nlist, slots, fb, fbn, wq, ba, false, s);
+}
+
+cudaError_t launch_ksw_band(const DpArgs &a, const uint32_t *list, int nlist, int slots, const int32_t *band_w,
+                            uint32_t *fb, uint32_t *fbn, uint32_t *retry, uint32_t *nretry, unsigned long long *cells,
+                            uint32_t *wq, cudaStream_t s)
+{
+    if (nlist <= 0) return cudaSuccess;
+    BandArgs ba{band_w, retry, nretry, cells};
+    return launch_slots(a, list, nlist, slots, fb, fbn, wq, ba, true, s);
 }
 
 } // namespace gb

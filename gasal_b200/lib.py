@@ -52,6 +52,10 @@ class GbTuning(C.Structure):
                 ("ksw_warp", C.c_int32)]
 
 
+class GbBandStats(C.Structure):
+    _fields_ = [(k, C.c_int64) for k in ("pairs", "accepted", "retried", "handed_back", "cells")]
+
+
 class GbStorageView(C.Structure):
     _fields_ = [(k, C.c_void_p) for k in (
         "host_query_batch_offsets", "host_target_batch_offsets", "host_query_batch_lens",
@@ -94,6 +98,20 @@ SIGNATURES = {
     "gb_graph_stats": (C.c_int, [C.POINTER(C.c_int64)]),
     "gb_set_tuning": (C.c_int, [C.POINTER(GbTuning)]),
     "gb_get_tuning": (C.c_int, [C.POINTER(GbTuning)]),
+    "gb_band_param_count": (C.c_int, []),
+    "gb_band_feature_stride": (C.c_int, []),
+    "gb_band_model_new": (C.c_void_p, [C.c_uint64]),
+    "gb_band_model_free": (None, [C.c_void_p]),
+    "gb_band_model_params": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
+    "gb_band_features": (C.c_int, [C.POINTER(GbDevBatch), C.c_void_p, C.c_void_p]),
+    "gb_band_predict": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p]),
+    "gb_band_grad": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_float, C.c_void_p, C.c_void_p,
+                               C.c_void_p]),
+    "gb_band_train_step": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_float, C.c_float, C.c_void_p,
+                                     C.POINTER(C.c_float)]),
+    "gb_set_band_model": (C.c_int, [C.c_void_p, C.c_int, C.c_int]),
+    "gb_ksw_band_align": (C.c_int, [C.POINTER(GbParams), C.POINTER(GbDevBatch), C.POINTER(GbDevOut), C.c_void_p,
+                                    C.c_void_p, C.c_void_p, C.POINTER(GbBandStats)]),
     "gb_autotune": (C.c_int, [C.POINTER(GbParams), C.POINTER(GbDevBatch), C.POINTER(GbDevOut), C.c_void_p, C.c_int,
                               C.POINTER(GbTuning), C.POINTER(C.c_double)]),
     "gb_kernel_timing": (C.c_int, [C.c_int]),
@@ -216,6 +234,82 @@ def autotune(p: Params, dev: dict, h_q_len: np.ndarray, h_t_len: np.ndarray, str
     d = {k: getattr(t, k) for k, _ in GbTuning._fields_}
     d["ms"] = ms.value
     return d
+
+
+class BandModel:
+    """The learned ksw band MLP (gb_band_model_*): parameters live on the
+    current device; train_step runs the hand-written gradient and Adam
+    kernels."""
+
+    def __init__(self, seed: int = 1):
+        self._m = lib().gb_band_model_new(int(seed))
+        if not self._m:
+            raise GasalError("gb_band_model_new failed")
+        self.n_params = lib().gb_band_param_count()
+
+    @property
+    def handle(self):
+        return self._m
+
+    def params(self) -> np.ndarray:
+        out = np.empty(self.n_params, dtype=np.float32)
+        _check(lib().gb_band_model_params(self._m, out.ctypes.data, None), "gb_band_model_params")
+        return out
+
+    def set_params(self, p: np.ndarray):
+        p = np.ascontiguousarray(p, dtype=np.float32)
+        assert p.shape == (self.n_params,)
+        _check(lib().gb_band_model_params(self._m, None, p.ctypes.data), "gb_band_model_params")
+
+    def predict(self, feat_ptr: int, n: int, out_ptr: int, stream: int = 0):
+        _check(lib().gb_band_predict(self._m, feat_ptr, int(n), out_ptr, stream), "gb_band_predict")
+
+    def grad(self, feat_ptr: int, label_ptr: int, n: int, tau: float, grad_ptr: int, loss_ptr: int, stream: int = 0):
+        _check(lib().gb_band_grad(self._m, feat_ptr, label_ptr, int(n), float(tau), grad_ptr, loss_ptr, stream),
+               "gb_band_grad")
+
+    def train_step(self, feat_ptr: int, label_ptr: int, n: int, tau: float, lr: float, stream: int = 0) -> float:
+        loss = C.c_float()
+        _check(lib().gb_band_train_step(self._m, feat_ptr, label_ptr, int(n), float(tau), float(lr), stream,
+                                        C.byref(loss)), "gb_band_train_step")
+        return loss.value
+
+    def install(self, band_min: int = 16, band_max: int = 1024):
+        _check(lib().gb_set_band_model(self._m, int(band_min), int(band_max)), "gb_set_band_model")
+
+    @staticmethod
+    def uninstall():
+        _check(lib().gb_set_band_model(None, 0, 0), "gb_set_band_model")
+
+    def close(self):
+        if self._m:
+            lib().gb_band_model_free(self._m)
+            self._m = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def band_features(dev: dict, h_q_len: np.ndarray, h_t_len: np.ndarray, feat_ptr: int, stream: int = 0):
+    """gb_band_features: packs dev['q'/'t'] into dev['pq'/'pt'] and writes
+    n x gb_band_feature_stride() floats at feat_ptr."""
+    b, _ = _dev_structs(dev, h_q_len, h_t_len)
+    _check(lib().gb_band_features(C.byref(b), feat_ptr, stream), "gb_band_features")
+
+
+def ksw_band_align(p: Params, dev: dict, h_q_len: np.ndarray, h_t_len: np.ndarray, band_ptr: Optional[int],
+                   ok_ptr: Optional[int] = None, stream: int = 0) -> dict:
+    """gb_ksw_band_align: banded ksw with its certificate and the exact
+    fallback; returns the band statistics (syncs the stream)."""
+    b, o = _dev_structs(dev, h_q_len, h_t_len)
+    cp = p.to_c()
+    st = GbBandStats()
+    _check(lib().gb_ksw_band_align(C.byref(cp), C.byref(b), C.byref(o), band_ptr, ok_ptr, stream, C.byref(st)),
+           "gb_ksw_band_align")
+    return {k: getattr(st, k) for k, _ in GbBandStats._fields_}
 
 
 def align_dev(p: Params, dev: dict, h_q_len: np.ndarray, h_t_len: np.ndarray, stream_handle: int = 0,

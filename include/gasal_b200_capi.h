@@ -242,6 +242,50 @@ int gb_autotune(const gb_params_t *p, const gb_dev_batch_t *b, const gb_dev_out_
  * ordering = 3 kernels per mark), the summed milliseconds and the number of
  * marks, in arrays of 5.  gb_probe_int_peak() times the
  * integer instructions the DP is bound by on the current GPU (tera-ops/s). */
+/* ---- Learned ksw band (no reference counterpart) ----
+ * A small MLP (67 pair features -> 64 -> 64 -> 1, ReLU, BF16 inference,
+ * FP32 training) predicts a log2 band half-width per ksw pair.  The banded
+ * warp kernel keeps a pair's result only when its certificate proves it equal
+ * to the unbanded one; the rest are recomputed without a band, so results
+ * never depend on the model.  Features (gb_band_features): n x
+ * gb_band_feature_stride() device floats: qlen/1024, tlen/1024,
+ * (tlen-qlen)/128, then a 64-bin histogram of the diagonal offsets of shared
+ * 11-mers.  Parameters: gb_band_param_count() floats, layout W1[64][67],
+ * b1[64], W2[64][64], b2[64], W3[64], b3. */
+typedef struct gb_band_model gb_band_model_t;
+typedef struct {
+    int64_t pairs;        /* pairs in the batch */
+    int64_t accepted;     /* banded results the certificate kept */
+    int64_t retried;      /* refused, recomputed without a band */
+    int64_t handed_back;  /* outside the warp kernel's range, one-thread kernel */
+    int64_t cells;        /* computed cells, banded attempts and recomputations included */
+} gb_band_stats_t;
+int gb_band_param_count(void);
+int gb_band_feature_stride(void);
+gb_band_model_t *gb_band_model_new(uint64_t seed);
+void gb_band_model_free(gb_band_model_t *m);
+/* copy parameters out (out) and/or in (in); either may be NULL */
+int gb_band_model_params(gb_band_model_t *m, float *out, const float *in);
+/* packs b->q/b->t (when given) into b->pq/b->pt, then writes the features */
+int gb_band_features(const gb_dev_batch_t *b, float *feat, void *stream);
+int gb_band_predict(gb_band_model_t *m, const float *feat, int n, float *out, void *stream);
+/* gradient of the mean pinball loss (quantile tau) of prediction vs label
+ * into grad (gb_band_param_count() device floats), summed loss into *loss
+ * (one device float) */
+int gb_band_grad(gb_band_model_t *m, const float *feat, const float *label, int n, float tau, float *grad, float *loss,
+                 void *stream);
+/* one Adam step on a batch; loss (host, may be NULL; syncs) = mean loss */
+int gb_band_train_step(gb_band_model_t *m, const float *feat, const float *label, int n, float tau, float lr,
+                       void *stream, float *loss);
+/* install (or with NULL remove) the model for every ksw call; predicted
+ * widths are clamped to [band_min, band_max] */
+int gb_set_band_model(gb_band_model_t *m, int band_min, int band_max);
+/* ksw with a band: band_w (device int32 per pair, negative = none) or, when
+ * NULL, the installed model's prediction.  band_ok (device, optional): 1 where
+ * the banded result was kept.  stats (optional) syncs the stream. */
+int gb_ksw_band_align(const gb_params_t *p, const gb_dev_batch_t *b, const gb_dev_out_t *o, const int32_t *band_w,
+                      uint8_t *band_ok, void *stream, gb_band_stats_t *stats);
+
 int gb_kernel_timing(int on);
 int gb_kernel_timing_read(double *ms, int64_t *launches);
 int gb_probe_int_peak(double *iadd_tops, double *imnmx_tops, double *dpx_tops);

@@ -1,0 +1,134 @@
+"""Learned ksw band on the GPU: feature kernel (exact against the NumPy
+checker), MLP forward (BF16 weights, FP32 accumulation: 1e-3 relative) and
+pinball-loss gradient (FP32 atomics: 1e-3 relative + 1e-6 absolute) against
+NumPy, a training run that lowers the loss, and the band certificate: for
+every band width every result -- kept banded or recomputed -- must equal the
+unbanded oracle bit for bit."""
+import numpy as np
+import pytest
+
+import band_ref as R
+from gasal_b200 import lib as gl
+from gasal_b200 import workloads as W
+from gasal_b200.capi import Params, KSW
+from oracle.bindings import oracle_align
+
+pytestmark = pytest.mark.gpu
+
+torch = pytest.importorskip("torch")
+DEV = torch.device("cuda", 0)
+OUTS = ("score", "q_end", "t_end")
+
+
+def _dev(b):
+    def t_(a, dt=None):
+        return torch.from_numpy(np.ascontiguousarray(a).view(dt or a.dtype)).to(DEV)
+    keep = {"q": t_(b.q), "t": t_(b.t), "qo": t_(b.q_off, np.int32), "to": t_(b.t_off, np.int32),
+            "ql": t_(b.q_len, np.int32), "tl": t_(b.t_len, np.int32), "seed": t_(b.seed, np.int32),
+            "pq": torch.zeros(b.q.shape[0] // 8, dtype=torch.int32, device=DEV),
+            "pt": torch.zeros(b.t.shape[0] // 8, dtype=torch.int32, device=DEV)}
+    for k in OUTS:
+        keep[k] = torch.full((b.n,), -7, dtype=torch.int32, device=DEV)
+    m = {"q_bytes": b.q.shape[0], "t_bytes": b.t.shape[0], "seed": keep["seed"].data_ptr()}
+    for k, src in (("q", "q"), ("t", "t"), ("pq", "pq"), ("pt", "pt"), ("q_off", "qo"), ("t_off", "to"),
+                   ("q_len", "ql"), ("t_len", "tl")):
+        m[k] = keep[src].data_ptr()
+    for k in OUTS:
+        m["out_" + k] = keep[k].data_ptr()
+    return m, keep
+
+
+def _stream():
+    return torch.cuda.current_stream().cuda_stream
+
+
+def test_features_exact():
+    b = W.workload3(60, seed=120)
+    m, keep = _dev(b)
+    feat = torch.zeros((b.n, 68), dtype=torch.float32, device=DEV)
+    gl.band_features(m, b.q_len, b.t_len, feat.data_ptr(), _stream())
+    torch.cuda.synchronize()
+    got = feat.cpu().numpy()
+    exp = R.features(b)
+    assert np.array_equal(got, exp), np.argwhere(got != exp)[:5]
+
+
+def test_forward_and_gradient_match_numpy():
+    rng = np.random.default_rng(121)
+    model = gl.BandModel(seed=5)
+    p = model.params()
+    p = p + rng.normal(0, 0.05, p.shape).astype(np.float32)
+    model.set_params(p)
+    n = 333
+    x = np.abs(rng.normal(0, 0.5, (n, 68))).astype(np.float32)
+    x[:, 67] = 0
+    y = rng.normal(6, 1.5, n).astype(np.float32)
+    xd, yd = torch.from_numpy(x).to(DEV), torch.from_numpy(y).to(DEV)
+    out = torch.zeros(n, dtype=torch.float32, device=DEV)
+    model.predict(xd.data_ptr(), n, out.data_ptr(), _stream())
+    g = torch.zeros(model.n_params, dtype=torch.float32, device=DEV)
+    loss = torch.zeros(1, dtype=torch.float32, device=DEV)
+    model.grad(xd.data_ptr(), yd.data_ptr(), n, 0.9, g.data_ptr(), loss.data_ptr(), _stream())
+    torch.cuda.synchronize()
+    exp_out, _ = R.forward(R.bf16(p), x)
+    assert np.allclose(out.cpu().numpy(), exp_out, rtol=1e-3, atol=1e-3)
+    exp_g, exp_loss = R.grad(p, x, y, 0.9)
+    got_g = g.cpu().numpy()
+    assert np.allclose(got_g, exp_g, rtol=1e-3, atol=1e-6), np.max(np.abs(got_g - exp_g))
+    assert abs(loss.item() - exp_loss) < 1e-3 * abs(exp_loss) + 1e-4
+    model.close()
+
+
+def test_training_lowers_the_loss():
+    rng = np.random.default_rng(122)
+    model = gl.BandModel(seed=6)
+    n = 4096
+    x = np.abs(rng.normal(0, 0.5, (n, 68))).astype(np.float32)
+    y = (4 + 3 * x[:, 0] + 2 * x[:, 5]).astype(np.float32)
+    xd, yd = torch.from_numpy(x).to(DEV), torch.from_numpy(y).to(DEV)
+    first = model.train_step(xd.data_ptr(), yd.data_ptr(), n, 0.5, 1e-2, _stream())
+    for _ in range(300):
+        last = model.train_step(xd.data_ptr(), yd.data_ptr(), n, 0.5, 1e-2, _stream())
+    assert last < 0.25 * first, (first, last)
+    model.close()
+
+
+@pytest.mark.parametrize("zdrop", [0, 100])
+def test_band_certificate_never_changes_a_result(zdrop):
+    """Every band width from 0 to beyond the matrix: the kept banded results
+    and the recomputed ones together equal the unbanded oracle."""
+    b = W.workload3(1200, seed=123 + zdrop)
+    p = Params(algo=KSW, zdrop=zdrop)
+    exp = oracle_align(p, b).as_dict(p)
+    m, keep = _dev(b)
+    kept = {}
+    for w in (0, 8, 24, 64, 128, 256, 512, 4096):
+        for k in OUTS:
+            keep[k].fill_(-7)
+        band = torch.full((b.n,), w, dtype=torch.int32, device=DEV)
+        ok = torch.zeros(b.n, dtype=torch.uint8, device=DEV)
+        st = gl.ksw_band_align(p, m, b.q_len, b.t_len, band.data_ptr(), ok.data_ptr(), _stream())
+        for k in OUTS:
+            got = keep[k].cpu().numpy()
+            bad = np.nonzero(got != exp[k])[0]
+            assert len(bad) == 0, f"w={w} {k}: {len(bad)} differ, first {bad[:5]}"
+        assert st["accepted"] + st["retried"] + st["handed_back"] == b.n
+        assert int(ok.sum().item()) == st["accepted"] + st["handed_back"]
+        kept[w] = st["accepted"]
+    assert kept[4096] == b.n          # a band wider than every matrix keeps everything
+    assert kept[0] < kept[512]        # and narrow bands are refused more often
+
+
+def test_installed_model_path_matches_oracle():
+    b = W.workload3(800, seed=124)
+    p = Params(algo=KSW, zdrop=100)
+    model = gl.BandModel(seed=7)
+    try:
+        model.install(16, 512)
+        got = gl.align(p, b).as_dict(p)
+    finally:
+        gl.BandModel.uninstall()
+        model.close()
+    exp = oracle_align(p, b).as_dict(p)
+    for k in OUTS:
+        assert np.array_equal(got[k], exp[k]), k
