@@ -57,6 +57,11 @@ WORKLOADS = {
     "w3": ("aligned pairs/s (ksw seed extension, z-drop 100, query 250-2000 bp)",
            "w3: ksw extension, query U[250,2000], target = query with indel rate {0.5,2,5,10}% (len 1-3) + "
            "1-5% subs per pair, h0 U[20,60], zdrop 100, scores 1/4/6/1", 400_000),
+    "w4": ("aligned pairs/s (mixed-length LOCAL / LOCAL+traceback / SEMI_GLOBAL / ksw on four streams)",
+           "w4: query lengths log-normal (median 250, clipped 50-5000), 60% short-read-like, 30% long-read-like "
+           "(5-12% errors, indel-dominated), 10% unrelated; LOCAL WITH_START 30%, LOCAL WITH_TB 20%, "
+           "SEMI_GLOBAL(TARGET,TARGET) WITH_START 25%, ksw z-drop 100 25%; one storage/stream per launch, graphs on",
+           1_000_000),
     "w0": ("aligned pairs/s (20k-pair LOCAL WITHOUT_START batch)",
            "w0: 20k pairs, LOCAL WITHOUT_START, q 100-150 with 0.1% N, t = q + 0-20 flanks, 2% subs, 0.5% "
            "indels", 20_000),
@@ -138,6 +143,8 @@ def build_workload(n: int, seed: int, name: str = "w1"):
         parts = [(Params(algo=GLOBAL, start_pos=WITH_TB), W.workload2(n, seed=seed + 1))]
     elif name == "w3":
         parts = [(Params(algo=KSW, zdrop=100), W.workload3(n, seed=seed + 2))]
+    elif name == "w4":
+        parts = W.workload4(n, seed=seed + 3)
     else:
         parts = [(Params(algo=LOCAL), W.workload0(n, seed=seed - 1))]
     log(f"workload {name}: {n} pairs generated in {time.time() - t:.1f}s")
@@ -331,7 +338,8 @@ def main():
     e2e = None
     streams = []
     for p, b in parts:
-        s = gl.Streams(1, int(b.q_len.max()), int(b.t_len.max()), b.n, p)
+        # host pages sized to the batch's own bytes (one bulk gasal_host_batch_fill per side)
+        s = gl.Streams(1, -(-int(b.q.shape[0]) // b.n) + 8, -(-int(b.t.shape[0]) // b.n) + 8, b.n, p)
         streams.append((p, b, s))
     h2d = sum(int(b.q.shape[0] + b.t.shape[0]) + b.n * (4 * 4 + 2) for _, b, _ in streams)
     d2h = 0

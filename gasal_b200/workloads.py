@@ -224,3 +224,43 @@ def workload3(n=4_000_000, seed=SEED_BASE + 3) -> Batch:
     tf, tl = _clip(rng, tf, tl, 1, 1 << 30)
     h0 = rng.integers(20, 61, size=n)
     return _to_batch(qf, ql, tf, tl, seed=h0)
+
+
+WORKLOAD4_PARAMS = [
+    Params(algo=LOCAL, start_pos=WITH_START),
+    Params(algo=LOCAL, start_pos=WITH_TB),
+    Params(algo=SEMI_GLOBAL, start_pos=WITH_START, head=TARGET, tail=TARGET),
+    Params(algo=KSW, zdrop=100),
+]
+WORKLOAD4_SHARES = (0.30, 0.20, 0.25, 0.25)
+
+
+def workload4(n=10_000_000, seed=SEED_BASE + 4):
+    """Workload 4: query lengths log-normal (median 250, sigma 0.8, clipped to
+    [50, 5000]); 60% short-read-like pairs (1-2% substitutions, 0.2% indels),
+    30% long-read-like (5-12% errors, 75% of them indels of length 1-5), 10%
+    unrelated random targets of similar length; split into four launches --
+    LOCAL WITH_START 30%, LOCAL WITH_TB 20%, SEMI_GLOBAL (TARGET, TARGET)
+    WITH_START 25%, ksw (h0 U[20,60], z-drop 100) 25% -- one per stream.
+    Returns [(Params, Batch)]."""
+    rng = np.random.default_rng(seed)
+    ql = np.clip(np.round(250 * np.exp(rng.normal(0, 0.8, size=n))), 50, 5000).astype(np.int64)
+    kind = rng.choice(3, size=n, p=[0.6, 0.3, 0.1])
+    qf = _random_bases(rng, int(ql.sum()))
+    err = np.where(kind == 0, rng.uniform(0.01, 0.02, n), rng.uniform(0.05, 0.12, n))
+    sub = np.where(kind == 0, err, 0.25 * err)
+    ind = np.where(kind == 0, 0.002, 0.75 * err)
+    tf, tl = mutate(rng, qf, ql, sub, ind / 2, ind / 2, 5)
+    tl = tl.astype(np.int64)
+    # unrelated pairs: replace the target by random bases of the same length
+    unrel = np.repeat(kind == 2, tl)
+    tf[unrel] = _random_bases(rng, int(unrel.sum()))
+    tf, tl = _clip(rng, tf, tl, 1, 1 << 30)
+    h0 = rng.integers(20, 61, size=n)
+    b = _to_batch(qf, ql, tf, tl, seed=h0)
+    cuts = np.round(np.cumsum((0,) + WORKLOAD4_SHARES) * n).astype(np.int64)
+    out = []
+    for p, lo, hi in zip(WORKLOAD4_PARAMS, cuts[:-1], cuts[1:]):
+        if hi > lo:
+            out.append((p, _slice_batch(b, np.arange(lo, hi))))
+    return out

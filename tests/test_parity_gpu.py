@@ -201,3 +201,11 @@ def test_wc_unrelated_long_pairs():
     b = Batch.from_seqs(qs, ts)
     _vs_oracle(Params(algo=LOCAL, start_pos=WITH_START, second_best=1), b)
     _vs_oracle(Params(algo=GLOBAL, start_pos=WITH_TB), b)
+
+
+@pytest.mark.parametrize("k", range(4))
+def test_workload4_launches(k):
+    """Workload 4's four launches (mixed 50-5000 bp, short- and long-read-like
+    and unrelated pairs) on 4,000 pairs."""
+    p, b = W.workload4(4000, seed=100)[k]
+    _vs_oracle(p, b)
