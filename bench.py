@@ -67,9 +67,11 @@ WORKLOADS = {
            "indels", 20_000),
 }
 METRIC = WORKLOADS["w1"][0]
-# DRAM bytes per DP launch of the workload from the committed ncu capture
-# (profiles/dp_kernels_w1.md), scaled to a full launch; None until captured.
-DP_TRAFFIC_BYTES = None
+# DRAM bytes (read + write) of one w1 launch of the dominant kernel
+# (dp_kernel, LOCAL third): 28.1 MB measured by ncu on the 133,334-pair launch
+# of a 400k-pair run (profiles/dp_kernel_w1_ncu_full.md), scaled by pairs to
+# the 333,334-pair launch of the full 1M-pair workload.
+DP_TRAFFIC_BYTES = 28.14e6 * 333334 / 133334
 
 
 def log(*a):

@@ -402,8 +402,14 @@ __device__ void semi_init_rows(int head, int q8, const Scores &sc, RowBuf rb)
 }
 
 /* One sweep over bands T0..tregs-1 of (q, t) as given by the word functions;
- * leaves once acc.best >= stop_at (checked per band and per query word). */
-template <bool SECOND, class SC, class QW, class TW>
+ * leaves once acc.best >= stop_at (checked per band and per query word).
+ *
+ * E opens from H here (semiglobal_kernel_template.h:105-107): E_k =
+ * max(E_{k-1} - e, H_{k-1} - (o+e)) with H_{k-1} = max(M, F, E_{k-1}) of the
+ * row above, a chain of three dependent operations per row.  When o >= 0,
+ * E_{k-1} - (o+e) <= E_{k-1} - e, so E_k = max(E_{k-1} - e, max(M, F)_{k-1} -
+ * (o+e)) -- the same value with one operation per row on the chain (OPEN_NN). */
+template <bool SECOND, bool OPEN_NN, class SC, class QW, class TW>
 __device__ void semi_sweep(QW qword, int qregs, int qlen, TW tword, int tregs, int tlen, const Scores &sc,
                            int head, int tail, int T0, int stop_at, RowBuf rb, SC &scr, SemiAcc &a)
 {
@@ -433,14 +439,27 @@ __device__ void semi_sweep(QW qword, int qregs, int qlen, TW tword, int tregs, i
                 const int up0 = sext16(v);
                 int e = hi16(v), up = up0;
                 int Hn[8];
+                if (OPEN_NN) {
+                    int x = up0 - sc.oe; /* H of the row above the band, opened */
 #pragma unroll
-                for (int k = 0; k < 8; k++) {
-                    F[k] = __viaddmax_s32(F[k], -sc.e, Hc[k] - sc.oe);
-                    const int M = D[k] + scr.s(k);
-                    e = __viaddmax_s32(e, -sc.e, up - sc.oe);
-                    const int H = __vimax3_s32(M, F[k], e);
-                    Hn[k] = H;
-                    up = H;
+                    for (int k = 0; k < 8; k++) {
+                        F[k] = __viaddmax_s32(F[k], -sc.e, Hc[k] - sc.oe);
+                        const int M = D[k] + scr.s(k);
+                        e = __viaddmax_s32(e, -sc.e, x);
+                        const int mf = max(M, F[k]);
+                        x = mf - sc.oe;
+                        Hn[k] = max(mf, e);
+                    }
+                } else {
+#pragma unroll
+                    for (int k = 0; k < 8; k++) {
+                        F[k] = __viaddmax_s32(F[k], -sc.e, Hc[k] - sc.oe);
+                        const int M = D[k] + scr.s(k);
+                        e = __viaddmax_s32(e, -sc.e, up - sc.oe);
+                        const int H = __vimax3_s32(M, F[k], e);
+                        Hn[k] = H;
+                        up = H;
+                    }
                 }
                 rb.st(c, pack_he(Hn[7], e));
                 D[0] = up0;
@@ -483,8 +502,12 @@ __device__ void semi_global(const uint32_t *q, int qregs, int qlen, const uint32
     const int q8 = qregs << 3;
     SemiAcc a = {NEG16, qlen, tlen, NEG16, qlen, tlen};
     semi_init_rows(head, q8, sc, rb);
-    semi_sweep<SECOND>([&](int j) { return q[j]; }, qregs, qlen, [&](int T) { return t[T]; }, tregs, tlen, sc,
-                       head, tail, 0, 0x7fffffff, rb, scr, a);
+    if (sc.o >= 0)
+        semi_sweep<SECOND, true>([&](int j) { return q[j]; }, qregs, qlen, [&](int T) { return t[T]; }, tregs, tlen,
+                                 sc, head, tail, 0, 0x7fffffff, rb, scr, a);
+    else
+        semi_sweep<SECOND, false>([&](int j) { return q[j]; }, qregs, qlen, [&](int T) { return t[T]; }, tregs,
+                                  tlen, sc, head, tail, 0, 0x7fffffff, rb, scr, a);
     if (tail == QUERY_ || tail == BOTH_) semi_tail_query<SECOND>(head, q8, qlen, tlen, mql, sc, rb, a);
     r.score = a.best, r.t_end = a.brow, r.q_end = a.bcol;
     if (SECOND) r.score2 = a.sec, r.t_end2 = a.srow, r.q_end2 = a.scol;
@@ -498,9 +521,12 @@ __device__ void semi_global(const uint32_t *q, int qregs, int qlen, const uint32
     const int fwd = a.best;
     SemiAcc b = {NEG16, 0, a.bcol, NEG16, 0, 0};
     semi_init_rows(head, q8, sc, rb);
-    semi_sweep<false>([&](int j) { return rev_window(q, qlen - 8 - (j << 3)); }, qregs, qlen,
-                      [&](int T) { return rev_window(t, tlen - 8 - (T << 3)); }, tregs, tlen, sc, head, tail,
-                      gend_reg, fwd, rb, scr, b);
+    auto rq = [&](int j) { return rev_window(q, qlen - 8 - (j << 3)); };
+    auto rt = [&](int T) { return rev_window(t, tlen - 8 - (T << 3)); };
+    if (sc.o >= 0)
+        semi_sweep<false, true>(rq, qregs, qlen, rt, tregs, tlen, sc, head, tail, gend_reg, fwd, rb, scr, b);
+    else
+        semi_sweep<false, false>(rq, qregs, qlen, rt, tregs, tlen, sc, head, tail, gend_reg, fwd, rb, scr, b);
     if (tail == QUERY_ || tail == BOTH_) semi_tail_query<false>(head, q8, qlen, tlen, mql, sc, rb, b);
     r.t_start = (tlen - 1) - b.brow;
     r.q_start = (qlen - 1) - b.bcol;

@@ -51,6 +51,8 @@ __device__ __forceinline__ void dp_one(const DpArgs &a, uint32_t w, RowBuf rb, c
 {
     const int i = a.order ? (int)a.order[w] : (int)w;
     const int qlen = (int)a.q_len[i], tlen = (int)a.t_len[i];
+    /* a pair outside this launch's length tier belongs to the other launch */
+    if ((uint32_t)qlen < a.q_min || (a.q_max && (uint32_t)qlen > a.q_max)) return;
     Res r = {0, 0, 0, 0, 0, 0, 0, 0};
     if (ALGO == KSW_) {
         /* empty sequences included: the reference returns h0 for them */
@@ -185,28 +187,27 @@ cudaError_t launch_dp_scratch_grid(int algo, int start, bool second, const DpArg
                                    cudaStream_t s)
 {
     if (a.n <= 0) return cudaSuccess;
+#define GB_SG(A, S, B) launch_scratch_grid<A, S, B>(a, block, blocks, s)
     switch (algo) {
     case LOCAL_:
-        if (start == WITH_START_)
-            return second ? launch_scratch_grid<LOCAL_, WITH_START_, true>(a, block, blocks, s)
-                          : launch_scratch_grid<LOCAL_, WITH_START_, false>(a, block, blocks, s);
-        return second ? launch_scratch_grid<LOCAL_, WITHOUT_START_, true>(a, block, blocks, s)
-                      : launch_scratch_grid<LOCAL_, WITHOUT_START_, false>(a, block, blocks, s);
+        if (start == WITH_START_) return second ? GB_SG(LOCAL_, WITH_START_, true) : GB_SG(LOCAL_, WITH_START_, false);
+        if (start == WITH_TB_) return second ? GB_SG(LOCAL_, WITH_TB_, true) : GB_SG(LOCAL_, WITH_TB_, false);
+        return second ? GB_SG(LOCAL_, WITHOUT_START_, true) : GB_SG(LOCAL_, WITHOUT_START_, false);
     case GLOBAL_:
-        return launch_scratch_grid<GLOBAL_, WITHOUT_START_, false>(a, block, blocks, s);
+        if (start == WITH_TB_) return GB_SG(GLOBAL_, WITH_TB_, false);
+        return GB_SG(GLOBAL_, WITHOUT_START_, false);
     case SEMI_GLOBAL_:
         if (start == WITH_START_)
-            return second ? launch_scratch_grid<SEMI_GLOBAL_, WITH_START_, true>(a, block, blocks, s)
-                          : launch_scratch_grid<SEMI_GLOBAL_, WITH_START_, false>(a, block, blocks, s);
-        return second ? launch_scratch_grid<SEMI_GLOBAL_, WITHOUT_START_, true>(a, block, blocks, s)
-                      : launch_scratch_grid<SEMI_GLOBAL_, WITHOUT_START_, false>(a, block, blocks, s);
+            return second ? GB_SG(SEMI_GLOBAL_, WITH_START_, true) : GB_SG(SEMI_GLOBAL_, WITH_START_, false);
+        return second ? GB_SG(SEMI_GLOBAL_, WITHOUT_START_, true) : GB_SG(SEMI_GLOBAL_, WITHOUT_START_, false);
     case BANDED_:
-        return launch_scratch_grid<BANDED_, WITHOUT_START_, false>(a, block, blocks, s);
+        return GB_SG(BANDED_, WITHOUT_START_, false);
     case KSW_:
-        return launch_scratch_grid<KSW_, WITHOUT_START_, false>(a, block, blocks, s);
+        return GB_SG(KSW_, WITHOUT_START_, false);
     default:
         return cudaErrorInvalidValue;
     }
+#undef GB_SG
 }
 
 cudaError_t launch_dp(int algo, int start, bool second, const DpArgs &a, int block, int max_q8, cudaStream_t s)

@@ -210,10 +210,7 @@ int plan_batch(const RunCfg &cfg, const DevBatch &b, const DevOut &o, Workspace 
     /* ksw: warp per pair; the one-thread kernel only takes what that hands
      * back (queries beyond 2046 bases, huge seed scores) */
     if (cfg.algo == KSW_ && st.ksw_wc && ksw_wc_scores_ok(cfg.sc)) {
-        uint32_t mq = 0;
-        for (int i = 0; i < b.n; i++)
-            if (b.h_q_len[i] + 2 <= 2048u) mq = std::max(mq, b.h_q_len[i]);
-        p.ksw_slots = ksw_wc_slots((int)mq);
+        ksw_wc_classes(b.h_q_len, b.n, p.ksw_slots);
         if (grow((void **)&ws.fb, &ws.fb_cap, (size_t)b.n, 4) != GB_OK) return GB_ERR_ALLOC;
         p.band = cfg.band_w != nullptr || cfg.band_model != nullptr;
         if (p.band) {
@@ -227,22 +224,52 @@ int plan_batch(const RunCfg &cfg, const DevBatch &b, const DevOut &o, Workspace 
             }
         }
     }
+    auto cols_of = [&](uint32_t q) {
+        return cfg.algo == KSW_ ? 2 * ((int)q + 2) : (int)((q + 7) & ~7u);
+    };
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     if ((size_t)std::max(cols, 8) * p.block * 4 <= smem_limit) {
         a.smem_cols = std::max(cols, 8);
     } else {
-        a.smem_cols = 0;
-        int blocks = dp_scratch_blocks(b.n, p.block);
-        if (p.ksw_slots > 0) {
-            int dev = 0, sms = 148;
-            cudaGetDevice(&dev);
-            cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-            blocks = std::min(blocks, 2 * sms);
-            p.fb_blocks = blocks;
+        /* the longest query does not leave room for shared-memory rows: split
+         * the one-thread pairs into a shared-memory tier and a long tier with
+         * global rows on a small grid (a long pair needs many cells per
+         * thread, not many threads) */
+        const int fit_cols = (int)(smem_limit / (4 * (size_t)p.block));
+        const uint32_t q_fit = cfg.algo == KSW_ ? (uint32_t)std::max(fit_cols / 2 - 2, 0) : (uint32_t)(fit_cols & ~7);
+        uint32_t max_s = 0, max_l = 0;
+        int n_s = 0, n_l = 0;
+        if (p.ksw_slots[0] == 0) {
+            for (int i = 0; i < b.n; i++) {
+                const uint32_t ql = b.h_q_len[i];
+                if (p.use_wc && ql >= p.wc_min_q) continue;
+                if (ql <= q_fit) n_s++, max_s = std::max(max_s, ql);
+                else n_l++, max_l = std::max(max_l, ql);
+            }
         }
-        const size_t threads = (size_t)blocks * p.block;
-        if (grow((void **)&ws.scratch, &ws.scratch_cap, threads * cols, 4) != GB_OK) return GB_ERR_ALLOC;
-        a.scratch = ws.scratch;
-        a.scratch_cols = (uint32_t)cols;
+        if (n_s > 0 && n_l > 0) {
+            p.tier2 = true;
+            p.tier_q = q_fit;
+            a.smem_cols = std::max(cols_of(max_s), 8);
+            a.q_max = q_fit;
+            p.tier2_cols = cols_of(max_l);
+            p.tier2_blocks = std::min(dp_scratch_blocks(n_l, p.block), 4 * sms);
+            const size_t threads = (size_t)p.tier2_blocks * p.block;
+            if (grow((void **)&ws.scratch, &ws.scratch_cap, threads * p.tier2_cols, 4) != GB_OK) return GB_ERR_ALLOC;
+        } else {
+            a.smem_cols = 0;
+            int blocks = dp_scratch_blocks(b.n, p.block);
+            if (p.ksw_slots[0] > 0) {
+                blocks = std::min(blocks, 2 * sms);
+                p.fb_blocks = blocks;
+            }
+            const size_t threads = (size_t)blocks * p.block;
+            if (grow((void **)&ws.scratch, &ws.scratch_cap, threads * cols, 4) != GB_OK) return GB_ERR_ALLOC;
+            a.scratch = ws.scratch;
+            a.scratch_cols = (uint32_t)cols;
+        }
     }
     if (p.use_wc && !ws.aux) {
         if (cudaStreamCreateWithFlags(&ws.aux, cudaStreamNonBlocking) != cudaSuccess ||
@@ -311,49 +338,67 @@ int plan_batch(const RunCfg &cfg, const DevBatch &b, const DevOut &o, Workspace 
     return GB_OK;
 }
 
+/* The one-thread launch(es) for DpArgs a: with two length tiers, the short
+ * tier from a (shared-memory rows) and the long tier from a's copy with
+ * global rows on a small grid.  queue words 0 and 1 are their counters. */
+static int launch_one_thread(int algo, int start, bool second, const Plan &p, DpArgs a, Workspace &ws,
+                             cudaStream_t s)
+{
+    if (a.queue) GB_CUDA(cudaMemsetAsync(a.queue, 0, 8, s));
+    timing_mark(K_DP, true, s);
+    GB_CUDA(launch_dp(algo, start, second, a, p.block, 0, s));
+    if (p.tier2) {
+        DpArgs l = a;
+        l.smem_cols = 0;
+        l.scratch = ws.scratch;
+        l.scratch_cols = (uint32_t)p.tier2_cols;
+        l.q_min = p.tier_q + 1;
+        l.q_max = 0;
+        l.queue = a.queue ? a.queue + 1 : nullptr;
+        GB_CUDA(launch_dp_scratch_grid(algo, start, second, l, p.block, p.tier2_blocks, s));
+    }
+    timing_mark(K_DP, false, s);
+    return GB_OK;
+}
+
 /* DP over pairs [0, a.n) visited in `order` (nullptr: identity): the first
  * nlong entries of order on the warp-cooperative kernel (auxiliary stream,
  * forked from and joined back into s), the rest on the one-thread kernel. */
-static int launch_dp_split(int algo, int start, bool second, DpArgs a, const uint32_t *order, int nlong,
-                           int max_q8_long, int max_t8_long, int block, Workspace &ws, cudaStream_t s)
+static int launch_dp_split(int algo, int start, bool second, const Plan &p, DpArgs a, const uint32_t *order,
+                           int nlong, Workspace &ws, cudaStream_t s)
 {
     if (nlong > 0 && order) {
         GB_CUDA(cudaEventRecord(ws.fork, s));
         GB_CUDA(cudaStreamWaitEvent(ws.aux, ws.fork, 0));
         timing_mark(K_DP, true, ws.aux);
-        GB_CUDA(launch_dp_wc(algo, start, second, a, order, nlong, max_q8_long, max_t8_long, ws.aux));
+        GB_CUDA(launch_dp_wc(algo, start, second, a, order, nlong, p.mq8, p.mt8, ws.aux));
         timing_mark(K_DP, false, ws.aux);
         GB_CUDA(cudaEventRecord(ws.join, ws.aux));
         DpArgs rest = a;
         rest.order = order + nlong;
         rest.n = a.n - nlong;
         if (rest.n > 0) {
-            if (rest.queue) GB_CUDA(cudaMemsetAsync(rest.queue, 0, 4, s));
-            timing_mark(K_DP, true, s);
-            GB_CUDA(launch_dp(algo, start, second, rest, block, 0, s));
-            timing_mark(K_DP, false, s);
+            const int rc = launch_one_thread(algo, start, second, p, rest, ws, s);
+            if (rc != GB_OK) return rc;
         }
         GB_CUDA(cudaStreamWaitEvent(s, ws.join, 0));
         return GB_OK;
     }
     a.order = order;
-    if (a.queue) GB_CUDA(cudaMemsetAsync(a.queue, 0, 4, s));
-    timing_mark(K_DP, true, s);
-    GB_CUDA(launch_dp(algo, start, second, a, block, 0, s));
-    timing_mark(K_DP, false, s);
-    return GB_OK;
+    return launch_one_thread(algo, start, second, p, a, ws, s);
 }
 
 /* ksw: every pair (in `order`, or 0..n-1) to the warp-per-pair kernel --
  * banded first when a band is given, the certificate's refusals again
  * without one -- then the pairs it handed back to the one-thread kernel,
- * whose counts it reads on the device.  queue words: [0] one-thread work
- * counter, [1] warp work counter, [2] handed-back count, [3] refused count,
- * [4..5] computed cells (u64), [6] second warp work counter. */
+ * whose counts it reads on the device.  queue words: [0..1] one-thread work
+ * counters, [2] handed-back count, [3] refused count, [4..5] computed cells
+ * (u64), [6..7] warp work counters of the two length classes, [8..9] the
+ * same for the recomputation pass. */
 static int launch_ksw_split(const RunCfg &cfg, const DevBatch &b, const Plan &p, const uint32_t *order, int n,
                             Workspace &ws, cudaStream_t s)
 {
-    GB_CUDA(cudaMemsetAsync(ws.queue, 0, 32, s));
+    GB_CUDA(cudaMemsetAsync(ws.queue, 0, 64, s));
     unsigned long long *cells = reinterpret_cast<unsigned long long *>(ws.queue + 4);
     timing_mark(K_DP, true, s);
     if (p.band) {
@@ -365,13 +410,13 @@ static int launch_ksw_split(const RunCfg &cfg, const DevBatch &b, const Plan &p,
             bw = ws.bandw;
         }
         GB_CUDA(launch_ksw_band(p.a, order, n, p.ksw_slots, bw, ws.fb, ws.queue + 2, ws.retry, ws.queue + 3, cells,
-                                ws.queue + 1, s));
+                                ws.queue + 6, s));
         if (cfg.band_ok) GB_CUDA(launch_band_ok(cfg.band_ok, n, ws.retry, ws.queue + 3, s));
         DpArgs ra = p.a;
         ra.n_dev = ws.queue + 3;
-        GB_CUDA(launch_ksw_wc(ra, ws.retry, n, p.ksw_slots, ws.fb, ws.queue + 2, ws.queue + 6, cells, s));
+        GB_CUDA(launch_ksw_wc(ra, ws.retry, n, p.ksw_slots, ws.fb, ws.queue + 2, ws.queue + 8, cells, s));
     } else {
-        GB_CUDA(launch_ksw_wc(p.a, order, n, p.ksw_slots, ws.fb, ws.queue + 2, ws.queue + 1, cells, s));
+        GB_CUDA(launch_ksw_wc(p.a, order, n, p.ksw_slots, ws.fb, ws.queue + 2, ws.queue + 6, cells, s));
     }
     timing_mark(K_DP, false, s);
     DpArgs fa = p.a;
@@ -419,9 +464,8 @@ int enqueue_batch(const RunCfg &cfg, const DevBatch &b, const DevOut &o, Workspa
             if (rc != GB_OK) return rc;
             ord = ws.order;
         }
-        if (p.ksw_slots > 0) return launch_ksw_split(cfg, b, p, ord, b.n, ws, s);
-        return launch_dp_split(cfg.algo, p.start, p.second, p.a, ord, ord ? p.nlong[0] : 0, p.mq8, p.mt8, p.block,
-                               ws, s);
+        if (p.ksw_slots[0] > 0) return launch_ksw_split(cfg, b, p, ord, b.n, ws, s);
+        return launch_dp_split(cfg.algo, p.start, p.second, p, p.a, ord, ord ? p.nlong[0] : 0, ws, s);
     }
     GB_CUDA(cudaMemcpyAsync(ws.d_tb_off, ws.h_tb_off, (size_t)b.n * 8, cudaMemcpyHostToDevice, s));
     for (size_t c = 0; c + 1 < p.cut.size(); c++) {
@@ -440,8 +484,7 @@ int enqueue_batch(const RunCfg &cfg, const DevBatch &b, const DevOut &o, Workspa
             if (rc != GB_OK) return rc;
             ord = ws.order;
         }
-        const int rc = launch_dp_split(cfg.algo, p.start, p.second, ca, ord, ord ? p.nlong[c] : 0, p.mq8, p.mt8,
-                                       p.block, ws, s);
+        const int rc = launch_dp_split(cfg.algo, p.start, p.second, p, ca, ord, ord ? p.nlong[c] : 0, ws, s);
         if (rc != GB_OK) return rc;
         TbArgs t{};
         t.tb = ws.tb, t.tb_off = ws.d_tb_off + p0;

@@ -86,7 +86,11 @@ struct Plan {
     bool tb = false, second = false, use_wc = false, order_on = false;
     int start = 0, block = 64, mq8 = 0, mt8 = 0;
     uint32_t wc_min_q = 0;
-    int ksw_slots = 0;      /* > 0: ksw runs warp-per-pair, this many eh columns per warp */
+    int ksw_slots[2] = {0, 0}; /* [0] > 0: ksw runs warp-per-pair; eh columns per warp of the two length classes */
+    bool tier2 = false;     /* one-thread pairs split: short ones with shared-memory rows (a), long ones
+                               with global rows on a small grid (tier2_* overrides of a) */
+    uint32_t tier_q = 0;    /* queries up to tier_q: shared-memory tier */
+    int tier2_cols = 0, tier2_blocks = 0;
     bool band = false;      /* ksw through the banded kernel + certificate */
     int fb_blocks = 0;      /* grid of the one-thread ksw launch for handed-back pairs (scratch rows) */
     DpArgs a{};

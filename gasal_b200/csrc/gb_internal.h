@@ -50,6 +50,8 @@ struct DpArgs {
     uint32_t *queue;                    /* work counter of the persistent launch (zeroed), or null */
     const uint32_t *n_dev;              /* if set, the number of pairs is read here on the device
                                            (n is then an upper bound, used to size the grid) */
+    uint32_t q_min, q_max;              /* one-thread kernel: only pairs with q_min <= qlen <= q_max
+                                           (q_max 0: no upper limit) */
 };
 
 struct TbArgs {
@@ -92,22 +94,25 @@ cudaError_t launch_dp_scratch_grid(int algo, int start, bool second, const DpArg
 
 /* warp-per-pair ksw extension (ksw_wc.cu) for the pairs listed in `list`
  * (null: pairs 0..nlist-1; a.n_dev, if set, caps the count on the device).
- * `slots` = ksw_wc_slots(longest query it should take); pairs it cannot take
- * (query + 2 above slots, seed + match*qlen >= 2^19) are appended to fb,
- * counted in *fbn, for the one-pair-per-thread kernel.  wq: zeroed work
- * counter.  Needs gap_extend >= 0, gap_open + gap_extend >= 0 and every
- * score below 4096 in magnitude (ksw_wc_scores_ok). */
+ * One launch per length class (wq[0], wq[1]: zeroed work counters); pairs
+ * it cannot take (query above 8190 bases, seed + match*qlen >= 2^15) are
+ * appended to fb, counted in *fbn, for the one-pair-per-thread kernel.
+ * Needs gap_extend >= 0, gap_open + gap_extend >= 0 and every score below
+ * 4096 in magnitude (ksw_wc_scores_ok). */
 bool ksw_wc_scores_ok(const Scores &sc);
-int ksw_wc_slots(int max_qlen); /* 0: longer than the kernel takes (2046) */
-cudaError_t launch_ksw_wc(const DpArgs &a, const uint32_t *list, int nlist, int slots, uint32_t *fb, uint32_t *fbn,
-                          uint32_t *wq, unsigned long long *cells, cudaStream_t s);
+/* Shared-memory slots of the (up to two) length classes of warp launches for
+ * these query lengths: class 0 takes queries up to 2046 bases, class 1 up to
+ * 8190 (0 = no such pairs). */
+void ksw_wc_classes(const uint32_t *h_q_len, int n, int slots[2]);
+cudaError_t launch_ksw_wc(const DpArgs &a, const uint32_t *list, int nlist, const int slots[2], uint32_t *fb,
+                          uint32_t *fbn, uint32_t *wq, unsigned long long *cells, cudaStream_t s);
 /* The same with a band: pair p is computed within half-width band_w[p]
  * (negative: unbanded) and kept only if the band certificate proves it equal
  * to the unbanded result; otherwise nothing is written and p goes to retry
  * (count *nretry).  cells (optional) accumulates the computed cells. */
-cudaError_t launch_ksw_band(const DpArgs &a, const uint32_t *list, int nlist, int slots, const int32_t *band_w,
-                            uint32_t *fb, uint32_t *fbn, uint32_t *retry, uint32_t *nretry, unsigned long long *cells,
-                            uint32_t *wq, cudaStream_t s);
+cudaError_t launch_ksw_band(const DpArgs &a, const uint32_t *list, int nlist, const int slots[2],
+                            const int32_t *band_w, uint32_t *fb, uint32_t *fbn, uint32_t *retry, uint32_t *nretry,
+                            unsigned long long *cells, uint32_t *wq, cudaStream_t s);
 
 int dp_block_size();
 int dp_scratch_blocks(int n, int block);

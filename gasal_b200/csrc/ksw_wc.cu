@@ -10,10 +10,12 @@
  * the columns of one row are spread over the 32 lanes:
  *
  *   eh[] (H of the previous row's column j-1, E entering row i at column j)
- *   lives in shared memory, one int2 per column, tiles of 256 columns; lane L
- *   owns columns 8L..8L+7 of every tile, stored k-major (slot = tile*256 +
- *   k*32 + L) so each of the 8 loads/stores of a tile is one conflict-free
- *   warp access.
+ *   lives in shared memory, one 32-bit word per column (H low, E high half;
+ *   both lie in [0, h0 + match*qlen], so pairs where that reaches 2^15 go to
+ *   the one-thread kernel), in slots of 256 columns; within a row's tile lane
+ *   L takes 8 consecutive columns, stored k-major (slot = (j & ~255) | k*32 |
+ *   (j/8 mod 32)) so each of the tile's 8 loads/stores is one conflict-free
+ *   warp access whatever multiple of 8 the tile starts at.
  *
  *   Within a row, M' (the diagonal score, 0 when the diagonal predecessor is
  *   0) and the E update are per column.  F -- the only left-to-right
@@ -37,9 +39,10 @@ namespace gb {
 namespace {
 
 constexpr int KT = 256;                 /* columns per tile (32 lanes x 8) */
-constexpr int KSW_WC_MAX_COLS = 2048;   /* queries up to 2046 bases stay on this kernel */
+constexpr int KSW_WC_COLS0 = 2048;      /* length class 0: queries up to 2046 bases */
+constexpr int KSW_WC_COLS1 = 8192;      /* length class 1: up to 8190 */
 constexpr int KEY_BITS = 12;            /* key = H << 12 | column */
-constexpr int KEY_H_LIMIT = 1 << 19;    /* H must stay below this for the key */
+constexpr int EH_LIMIT = 1 << 15;       /* H and E are stored as 16-bit halves */
 constexpr unsigned FULL = 0xFFFFFFFFu;
 
 __device__ __forceinline__ int kslot(int j) { return (j & ~255) | ((j & 7) << 5) | ((j >> 3) & 31); }
@@ -71,7 +74,7 @@ struct Cert {
  * otherwise nibble compares.  BAND: half-width w >= 0, returns false when
  * the certificate cannot vouch for the banded result (nothing is written). */
 template <bool FAST, bool BAND>
-__device__ bool ksw_pair(const DpArgs &a, uint32_t pid, int2 *eh, const uint4 *selw, int slots, const uint2 *stab,
+__device__ bool ksw_pair(const DpArgs &a, uint32_t pid, uint32_t *eh, const uint4 *selw, int slots, const uint2 *stab,
                          int lane, int qlen, int tlen, const uint32_t *q, const uint32_t *t, int h0, int w,
                          unsigned long long &ncells)
 {
@@ -84,7 +87,7 @@ __device__ bool ksw_pair(const DpArgs &a, uint32_t pid, int2 *eh, const uint4 *s
     const int Cmul = max(max(a.sc.match, -a.sc.mismatch), 0) + 1;
 
     /* the reference's first row (ksw_kernel_template.h:75-79) */
-    for (int s = lane; s < slots; s += 32) eh[s] = make_int2(0, 0);
+    for (int s = lane; s < slots; s += 32) eh[s] = 0u;
     __syncwarp();
     const long long v1 = (uint32_t)h0 > (uint32_t)oe ? (long long)h0 - oe : 0;
     auto init_h = [&](int j) -> long long {
@@ -95,7 +98,7 @@ __device__ bool ksw_pair(const DpArgs &a, uint32_t pid, int2 *eh, const uint4 *s
     };
     for (int j = lane; j <= qlen + 1; j += 32) {
         const long long h = init_h(j);
-        if (h) eh[kslot(j)].x = (int)h;
+        if (h) eh[kslot(j)] = (uint32_t)h;
     }
     __syncwarp();
 
@@ -150,7 +153,10 @@ __device__ bool ksw_pair(const DpArgs &a, uint32_t pid, int2 *eh, const uint4 *s
                 int2 v[8];
                 int Mp[8], tv[8];
 #pragma unroll
-                for (int k = 0; k < 8; k++) v[k] = eh[sb + 32 * k];
+                for (int k = 0; k < 8; k++) {
+                    const uint32_t pv = eh[sb + 32 * k];
+                    v[k] = make_int2((int)(pv & 0xFFFFu), (int)(pv >> 16));
+                }
                 /* pass 1: M', t and the lane's F fold */
                 int agg = 0;
 #pragma unroll
@@ -197,8 +203,9 @@ __device__ bool ksw_pair(const DpArgs &a, uint32_t pid, int2 *eh, const uint4 *s
                 for (int k = 0; k < 8; k++) {
                     const int hs = k == 0 ? hp : H[k - 1];
                     if (k < nv) {
-                        eh[sb + 32 * k] = make_int2(hs, v[k].y);
-                        nz |= (uint32_t)(hs | v[k].y);
+                        const uint32_t pv = (uint32_t)hs | ((uint32_t)v[k].y << 16);
+                        eh[sb + 32 * k] = pv;
+                        nz |= pv;
                     }
                 }
                 const unsigned bm = __ballot_sync(FULL, nz != 0);
@@ -214,7 +221,7 @@ __device__ bool ksw_pair(const DpArgs &a, uint32_t pid, int2 *eh, const uint4 *s
             h1 = __shfl_sync(FULL, hlast, owner);
             if (BAND) fout = __shfl_sync(FULL, flast, owner);
         }
-        if (lane == 0) eh[kslot(end)] = make_int2(h1, 0);
+        if (lane == 0) eh[kslot(end)] = (uint32_t)h1;
         __syncwarp();
         if (BAND) {
             /* bound on this row's values the banded run does not have */
@@ -249,7 +256,7 @@ __device__ bool ksw_pair(const DpArgs &a, uint32_t pid, int2 *eh, const uint4 *s
             if (upd_maybe) ct.gunc = max(ct.gunc, Crow);
             /* E leaving the band's leftmost column into the next row */
             int Cnext = Crow;
-            if (beg < end && beg == i - w) Cnext = max(Cnext, eh[kslot(i - w)].y);
+            if (beg < end && beg == i - w) Cnext = max(Cnext, (int)(eh[kslot(i - w)] >> 16));
             ct.C = Cnext;
         } else if (max(L8, end) == qlen) {
             max_ie = gscore > h1 ? max_ie : i;
@@ -279,8 +286,7 @@ __device__ bool ksw_pair(const DpArgs &a, uint32_t pid, int2 *eh, const uint4 *s
             for (int k = 7; k >= 0; k--) {
                 const int j = base + k;
                 if (j < end) {
-                    const int2 x = eh[kslot(j)];
-                    if (x.x | x.y) nbeg = j;
+                    if (eh[kslot(j)]) nbeg = j;
                 }
             }
         }
@@ -292,8 +298,7 @@ __device__ bool ksw_pair(const DpArgs &a, uint32_t pid, int2 *eh, const uint4 *s
             for (int k = 0; k < 8; k++) {
                 const int j = base + k;
                 if (j < end) {
-                    const int2 x = eh[kslot(j)];
-                    if (x.x | x.y) lastnz = j;
+                    if (eh[kslot(j)]) lastnz = j;
                 }
             }
         }
@@ -333,18 +338,20 @@ struct BandArgs {
     const int32_t *w;
     uint32_t *retry, *nretry;
     unsigned long long *cells; /* computed cells (rows x trimmed range), or null */
+    int q_lo;                  /* shorter queries belong to an earlier class launch: skipped */
+    int handback;              /* queries too long for this launch: 1 = to fb, 0 = skipped (next class) */
 };
 
 template <bool BAND>
 __global__ void __launch_bounds__(32) ksw_wc_kernel(DpArgs a, const uint32_t *list, int nlist, int slots,
                                                      uint32_t *fb, uint32_t *fbn, uint32_t *wq, BandArgs ba)
 {
-    extern __shared__ int2 ksw_smem[];
+    extern __shared__ __align__(16) uint32_t ksw_smem[];
     __shared__ uint2 stab[16];
     build_score_table(stab, a.sc, true);
     __syncthreads();
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, warps = blockDim.x >> 5;
-    int2 *eh = ksw_smem + (size_t)warp * slots;
+    uint32_t *eh = ksw_smem + (size_t)warp * slots;
     uint4 *selw = reinterpret_cast<uint4 *>(ksw_smem + (size_t)warps * slots) + (size_t)warp * (slots / 8);
     const bool fast_scores = a.sc.match >= -128 && a.sc.match <= 127 && a.sc.mismatch >= -127 && a.sc.mismatch <= 128;
     const long long mpos = a.sc.match > 0 ? a.sc.match : 0;
@@ -357,7 +364,12 @@ __global__ void __launch_bounds__(32) ksw_wc_kernel(DpArgs a, const uint32_t *li
         const uint32_t pid = list ? list[idx] : idx;
         const int qlen = (int)a.q_len[pid], tlen = (int)a.t_len[pid];
         const uint32_t h0u = a.seed ? a.seed[pid] : 0u;
-        if (qlen + 2 > slots || (long long)h0u + mpos * qlen >= KEY_H_LIMIT) {
+        if (qlen < ba.q_lo) continue;
+        if (qlen + 2 > slots) {
+            if (ba.handback && lane == 0) fb[atomicAdd(fbn, 1u)] = pid;
+            continue;
+        }
+        if ((long long)h0u + mpos * qlen >= EH_LIMIT) {
             if (lane == 0) fb[atomicAdd(fbn, 1u)] = pid;
             continue;
         }
@@ -413,7 +425,7 @@ cudaError_t launch_slots(const DpArgs &a, const uint32_t *list, int nlist, int s
                          uint32_t *wq, const BandArgs &ba, bool band, cudaStream_t s)
 {
     const int block = 32, warps = block / 32; /* one warp per block packs shared memory tightest */
-    const size_t smem = (size_t)warps * slots * (sizeof(int2) + 2);
+    const size_t smem = (size_t)warps * slots * (sizeof(uint32_t) + 2);
     auto k = band ? ksw_wc_kernel<true> : ksw_wc_kernel<false>;
     cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
@@ -438,23 +450,45 @@ bool ksw_wc_scores_ok(const Scores &sc)
            sc.mismatch > -4095;
 }
 
-int ksw_wc_slots(int max_qlen) { return max_qlen + 2 <= KSW_WC_MAX_COLS ? slots_for(max_qlen) : 0; }
-
-cudaError_t launch_ksw_wc(const DpArgs &a, const uint32_t *list, int nlist, int slots, uint32_t *fb, uint32_t *fbn,
-                          uint32_t *wq, unsigned long long *cells, cudaStream_t s)
+void ksw_wc_classes(const uint32_t *h_q_len, int n, int slots[2])
 {
-    if (nlist <= 0) return cudaSuccess;
-    BandArgs ba{nullptr, nullptr, nullptr, cells};
-    return launch_slots(a, list, nlist, slots, fb, fbn, wq, ba, false, s);
+    int m0 = 0, m1 = -1;
+    for (int i = 0; i < n; i++) {
+        const int q = (int)h_q_len[i];
+        if (q + 2 <= KSW_WC_COLS0) m0 = q > m0 ? q : m0;
+        else if (q + 2 <= KSW_WC_COLS1) m1 = q > m1 ? q : m1;
+    }
+    slots[0] = slots_for(m0);
+    slots[1] = m1 >= 0 ? slots_for(m1) : 0;
 }
 
-cudaError_t launch_ksw_band(const DpArgs &a, const uint32_t *list, int nlist, int slots, const int32_t *band_w,
-                            uint32_t *fb, uint32_t *fbn, uint32_t *retry, uint32_t *nretry, unsigned long long *cells,
-                            uint32_t *wq, cudaStream_t s)
+/* the class launches over one list; wq[c] is class c's zeroed work counter */
+static cudaError_t launch_classes(const DpArgs &a, const uint32_t *list, int nlist, const int slots[2], uint32_t *fb,
+                                  uint32_t *fbn, uint32_t *wq, BandArgs ba, bool band, cudaStream_t s)
 {
     if (nlist <= 0) return cudaSuccess;
-    BandArgs ba{band_w, retry, nretry, cells};
-    return launch_slots(a, list, nlist, slots, fb, fbn, wq, ba, true, s);
+    ba.q_lo = 0;
+    ba.handback = slots[1] == 0;
+    cudaError_t e = launch_slots(a, list, nlist, slots[0], fb, fbn, wq, ba, band, s);
+    if (e != cudaSuccess || slots[1] == 0) return e;
+    ba.q_lo = slots[0] - 1;
+    ba.handback = 1;
+    return launch_slots(a, list, nlist, slots[1], fb, fbn, wq + 1, ba, band, s);
+}
+
+cudaError_t launch_ksw_wc(const DpArgs &a, const uint32_t *list, int nlist, const int slots[2], uint32_t *fb,
+                          uint32_t *fbn, uint32_t *wq, unsigned long long *cells, cudaStream_t s)
+{
+    BandArgs ba{nullptr, nullptr, nullptr, cells, 0, 1};
+    return launch_classes(a, list, nlist, slots, fb, fbn, wq, ba, false, s);
+}
+
+cudaError_t launch_ksw_band(const DpArgs &a, const uint32_t *list, int nlist, const int slots[2],
+                            const int32_t *band_w, uint32_t *fb, uint32_t *fbn, uint32_t *retry, uint32_t *nretry,
+                            unsigned long long *cells, uint32_t *wq, cudaStream_t s)
+{
+    BandArgs ba{band_w, retry, nretry, cells, 0, 1};
+    return launch_classes(a, list, nlist, slots, fb, fbn, wq, ba, true, s);
 }
 
 } // namespace gb

@@ -98,3 +98,22 @@ def test_empty_sequences():
     b = Batch.from_seqs(qs * 700, ts * 700, seed=np.arange(3500, dtype=np.uint32) % 61)
     got = _check(Params(algo=KSW), b)
     assert got["score"][0] == 0 and got["score"][2] == 2  # the seed score comes back unchanged
+
+
+def test_scores_near_the_16_bit_row_limit():
+    """H and E are stored as 16-bit halves: pairs whose seed + match * qlen
+    reaches 2^15 are handed to the one-thread kernel, the rest stay; both
+    sides of the limit must match the oracle."""
+    rng = np.random.default_rng(95)
+    qs, ts, seeds = [], [], []
+    for i in range(400):
+        n = int(rng.integers(1500, 1700))
+        q = bytes(np.frombuffer(b"ACGT", np.uint8)[rng.integers(0, 4, n)])
+        t = bytearray(q)
+        for _ in range(n // 50):
+            t[int(rng.integers(0, len(t)))] = b"ACGT"[int(rng.integers(0, 4))]
+        qs.append(q)
+        ts.append(bytes(t))
+        seeds.append(int(rng.integers(0, 2000)))
+    b = Batch.from_seqs(qs, ts, seed=np.array(seeds, dtype=np.uint32))
+    _check(Params(algo=KSW, match=20, mismatch=30, gap_open=40, gap_extend=5), b)
