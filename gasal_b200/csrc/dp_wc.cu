@@ -148,7 +148,7 @@ __device__ __forceinline__ uint32_t dnib(int M, int diag, int H, int F, int E, c
 template <int MODE, bool TB, bool SECOND_PASS2, class QW, class TW>
 __device__ void wc_sweep(QW qword, int qregs, TW tword, int tregs, int qlen, int tlen, const Scores &sc,
                          WcScore &S, uint32_t *ring, uint4 *tb, int stop, int *bandmax, bool write_bandmax,
-                         WcRec &best_out, WcRec &sec_out, int &gscore)
+                         WcRec &best_out, WcRec &sec_out, int &gscore, int ctrack = 0x7fffffff)
 {
     const int lane = threadIdx.x & 31;
     const int rounds = (tregs + 31) >> 5;
@@ -251,7 +251,7 @@ __device__ void wc_sweep(QW qword, int qregs, TW tword, int tregs, int qlen, int
                         for (int k = 0; k < 8; k++)
                             if (k == last_row_in_band) gscore = Hn[k];
                     }
-                } else {
+                } else if (c < ctrack) {
                     const int ck = key_max8(key);
                     if ((ck >> 3) > bandbest) bandbest = ck >> 3;
                     if ((ck >> 3) > best.v) {
@@ -291,6 +291,258 @@ __device__ void wc_sweep(QW qword, int qregs, TW tword, int tregs, int qlen, int
     }
     best_out = best;
     sec_out = sec;
+}
+
+/*
+ * SEMI_GLOBAL (reference src/kernels/semiglobal_kernel_template.h:39-388)
+ * with the target tail free (tail TARGET): one sweep of bands T0..tregs-1,
+ * gaps opened from H, the H of the last query column of every row kept in
+ * `lastcol` (indexed by absolute row).  FWD = false: the start pass over the
+ * reversed words, bands counted from T0 for the left boundary, leaving after
+ * the first round whose bands reach `stop` at the last column.
+ */
+template <bool START_PASS, bool OPEN_NN, class QW, class TW>
+__device__ void wc_semi_sweep(QW qword, int qregs, TW tword, int tregs, int T0, int qlen, const Scores &sc,
+                              int head, WcScore &S, uint32_t *ring, int *lastcol, int stop)
+{
+    const int lane = threadIdx.x & 31;
+    const int nb = tregs - T0;
+    if (nb <= 0) return;
+    const int rounds = (nb + 31) >> 5;
+    const bool free_head_t = (head == TARGET_ || head == BOTH_);
+    const bool zero_rows = (head == QUERY_ || head == BOTH_);
+    uint32_t out[8];
+#pragma unroll
+    for (int k = 0; k < 8; k++) out[k] = 0;
+    int F[8], D[8], Hc[8];
+#pragma unroll
+    for (int k = 0; k < 8; k++) F[k] = NEG16W, D[k] = 0, Hc[k] = 0;
+    int up_prev = 0;
+    int hit_round = 0x7fffffff;
+    const int lastw = (qlen - 1) >> 3, lastb = (qlen - 1) & 7;
+    const long steps = (long)rounds * qregs + 31;
+    for (long st = 0; st < steps; st++) {
+        const long rel = st - lane;
+        const int r = rel >= 0 ? (int)(rel / qregs) : -1;
+        const int w = rel >= 0 ? (int)(rel - (long)r * qregs) : 0;
+        const int brel = (r << 5) + lane;
+        const bool active = rel >= 0 && r < rounds && brel < nb;
+        if (START_PASS && hit_round != 0x7fffffff && st >= (long)(hit_round + 1) * qregs + 31) break;
+        uint32_t in[8];
+#pragma unroll
+        for (int k = 0; k < 8; k++) in[k] = __shfl_up_sync(0xFFFFFFFFu, out[k], 1);
+        if (lane == 0 && active) {
+            if (r == 0) {
+#pragma unroll
+                for (int k = 0; k < 8; k++) {
+                    const int c = (w << 3) + k;
+                    in[k] = zero_rows ? 0u : pk(c == 0 ? 0 : (int)(int16_t)(-(sc.o + sc.e * c)), NEG16W);
+                }
+            } else {
+#pragma unroll
+                for (int k = 0; k < 8; k++) in[k] = ring[(w << 3) + k];
+            }
+        }
+        __syncwarp();
+        bool hit = false;
+        if (active) {
+            const int band = T0 + brel;
+            if (w == 0) { /* new band: left boundary (rows counted from T0) */
+                S.band(tword(band), sc);
+#pragma unroll
+                for (int k = 0; k < 8; k++) {
+                    const int R = (brel << 3) + k;
+                    F[k] = NEG16W;
+                    if (free_head_t) {
+                        Hc[k] = 0, D[k] = 0;
+                    } else {
+                        Hc[k] = -(sc.o + sc.e * R);
+                        D[k] = R == 0 ? 0 : -(sc.o + sc.e * R);
+                    }
+                }
+                up_prev = 0;
+            }
+            const uint32_t qw = qword(w);
+#pragma unroll
+            for (int b = 0; b < 8; b++) {
+                const int rbase = cd(qw, b);
+                uint2 tcol = make_uint2(0, 0);
+                if (S.fast) tcol = S.tab[rbase];
+                const bool rz = rbase == 14;
+                const uint32_t v = in[b];
+                const int up0 = sx16(v);
+                int e = hx16(v);
+                if (b > 0 || w > 0) D[0] = up_prev;
+                int Hn[8];
+                int x = up0 - sc.oe, up = up0;
+#pragma unroll
+                for (int k = 0; k < 8; k++) {
+                    int s_;
+                    if (S.fast) s_ = (int)wprmt(tcol.x, tcol.y, S.sel[k]);
+                    else s_ = rz ? 0 : ((rbase == S.g[k]) ? S.ma[k] : S.mm[k]);
+                    F[k] = __viaddmax_s32(F[k], -sc.e, Hc[k] - sc.oe);
+                    const int M = D[k] + s_;
+                    if (OPEN_NN) {
+                        e = __viaddmax_s32(e, -sc.e, x);
+                        const int mf = max(M, F[k]);
+                        x = mf - sc.oe;
+                        Hn[k] = max(mf, e);
+                    } else {
+                        e = __viaddmax_s32(e, -sc.e, up - sc.oe);
+                        Hn[k] = __vimax3_s32(M, F[k], e);
+                        up = Hn[k];
+                    }
+                }
+                out[b] = pk(Hn[7], e);
+#pragma unroll
+                for (int k = 7; k > 0; k--) D[k] = Hn[k - 1];
+#pragma unroll
+                for (int k = 0; k < 8; k++) Hc[k] = Hn[k];
+                up_prev = up0;
+                if (w == lastw && b == lastb) {
+#pragma unroll
+                    for (int k = 0; k < 8; k++) {
+                        lastcol[(band << 3) + k] = Hn[k];
+                        if (START_PASS && Hn[k] >= stop) hit = true;
+                    }
+                }
+            }
+            D[0] = up_prev;
+            if (lane == 31) {
+#pragma unroll
+                for (int k = 0; k < 8; k++) ring[(w << 3) + k] = out[k];
+            }
+        }
+        __syncwarp();
+        if (START_PASS) {
+            const unsigned m = __ballot_sync(0xFFFFFFFFu, hit);
+            if (m) {
+                const int hr = __shfl_sync(0xFFFFFFFFu, r, __ffs(m) - 1);
+                if (hr < hit_round) hit_round = hr;
+            }
+        }
+    }
+    __syncwarp();
+}
+
+/* First maximum (strict >, row order) of lastcol over rows [r0, r1) with the
+ * reference's initial best NEG16 / row `row0`; with SECOND also its second
+ * best (a row qualifies when below every earlier row's value). */
+template <bool SECOND>
+__device__ void wc_lastcol_scan(const int *lastcol, int r0, int r1, int row0, int &best, int &brow, int &sec,
+                                int &srow)
+{
+    const int lane = threadIdx.x & 31;
+    best = NEG16W, brow = row0, sec = NEG16W, srow = row0;
+    int carry = NEG16W; /* max of the rows before the chunk */
+    for (int base = r0; base < r1; base += 32) {
+        const int row = base + lane;
+        const int h = row < r1 ? lastcol[row] : NEG16W - 1;
+        int pm = h; /* inclusive prefix max within the chunk */
+#pragma unroll
+        for (int off = 1; off < 32; off <<= 1) {
+            const int o = __shfl_up_sync(0xFFFFFFFFu, pm, off);
+            if (lane >= off) pm = max(pm, o);
+        }
+        int before = __shfl_up_sync(0xFFFFFFFFu, pm, 1);
+        before = lane == 0 ? carry : max(before, carry);
+        /* chunk argmax, first row on ties */
+        int bv = h, br = row;
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) {
+            const int ov = __shfl_xor_sync(0xFFFFFFFFu, bv, off), orow = __shfl_xor_sync(0xFFFFFFFFu, br, off);
+            if (ov > bv || (ov == bv && orow < br)) bv = ov, br = orow;
+        }
+        if (bv > best) best = bv, brow = br;
+        if (SECOND) {
+            const bool q = row < r1 && h < before && h > NEG16W;
+            int sv = q ? h : NEG16W - 1, sr = row;
+#pragma unroll
+            for (int off = 16; off > 0; off >>= 1) {
+                const int ov = __shfl_xor_sync(0xFFFFFFFFu, sv, off), orow = __shfl_xor_sync(0xFFFFFFFFu, sr, off);
+                if (ov > sv || (ov == sv && orow < sr)) sv = ov, sr = orow;
+            }
+            if (sv > sec) sec = sv, srow = sr;
+        }
+        carry = max(carry, __shfl_sync(0xFFFFFFFFu, pm, 31));
+    }
+}
+
+template <bool SECOND, bool START>
+__global__ void __launch_bounds__(128) dp_wc_semi_kernel(DpArgs a, const uint32_t *list, int nlist, int ring_cols)
+{
+    extern __shared__ uint32_t wc_smem[];
+    __shared__ uint2 tab[16];
+    wc_score_table(tab, a.sc, true);
+    __syncthreads();
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int warps_per_block = blockDim.x >> 5;
+    uint32_t *ring = wc_smem + (size_t)warp * ring_cols;
+    int *lastcol = (int *)(wc_smem + (size_t)warps_per_block * ring_cols) + (size_t)warp * a.scratch_cols;
+    const bool fast_scores = a.sc.match >= -128 && a.sc.match <= 127 && a.sc.mismatch >= -127 && a.sc.mismatch <= 128;
+    const bool open_nn = a.sc.o >= 0;
+    for (int item = blockIdx.x * warps_per_block + warp; item < nlist; item += gridDim.x * warps_per_block) {
+        const int i = (int)list[item];
+        const int qlen = (int)a.q_len[i], tlen = (int)a.t_len[i];
+        const uint32_t *q = a.pq + (a.q_off[i] >> 3);
+        const uint32_t *t = a.pt + (a.t_off[i] >> 3);
+        const int qregs = (qlen + 7) >> 3, tregs = (tlen + 7) >> 3;
+        WcScore S;
+        S.local = true;
+        S.tab = tab;
+        S.fast = fast_scores && wc_plain(q, qregs) && wc_plain(t, tregs);
+        auto qf = [&](int j) { return q[j]; };
+        auto tf = [&](int T) { return t[T]; };
+        if (open_nn) wc_semi_sweep<false, true>(qf, qregs, tf, tregs, 0, qlen, a.sc, a.head, S, ring, lastcol, 0);
+        else wc_semi_sweep<false, false>(qf, qregs, tf, tregs, 0, qlen, a.sc, a.head, S, ring, lastcol, 0);
+        int best, brow, sec, srow;
+        wc_lastcol_scan<SECOND>(lastcol, 0, tlen, qlen, best, brow, sec, srow);
+        int t_start = 0, q_start = 0;
+        if (START) {
+            const int x = tregs - ((brow >> 3) + 1);
+            int gend_reg = x > 0 ? x - 1 : x;
+            if (gend_reg < 0) gend_reg = 0;
+            auto rq = [&](int j) { return rev_window(q, qlen - 8 - (j << 3)); };
+            auto rt = [&](int T) { return rev_window(t, tlen - 8 - (T << 3)); };
+            __syncwarp();
+            if (open_nn)
+                wc_semi_sweep<true, true>(rq, qregs, rt, tregs, gend_reg, qlen, a.sc, a.head, S, ring, lastcol, best);
+            else
+                wc_semi_sweep<true, false>(rq, qregs, rt, tregs, gend_reg, qlen, a.sc, a.head, S, ring, lastcol,
+                                           best);
+            /* rows up to the end of the first band that reached the forward score */
+            const int r0 = gend_reg << 3;
+            int r1 = min(tregs << 3, tlen);
+            for (int base = r0; base < r1; base += 32) {
+                const int row = base + lane;
+                const unsigned m = __ballot_sync(0xFFFFFFFFu, row < r1 && lastcol[row] >= best);
+                if (m) {
+                    const int hit = base + __ffs(m) - 1;
+                    r1 = min(r1, ((hit >> 3) + 1) << 3);
+                    break;
+                }
+            }
+            int bb, bbrow, s2, s2r;
+            wc_lastcol_scan<false>(lastcol, r0, r1, 0, bb, bbrow, s2, s2r);
+            t_start = (tlen - 1) - bbrow;
+            q_start = (qlen - 1) - tlen;
+        }
+        if (lane == 0) {
+            if (a.score) a.score[i] = best;
+            if (a.t_end) a.t_end[i] = brow;
+            if (a.q_end) a.q_end[i] = tlen;
+            if (SECOND) {
+                if (a.score2) a.score2[i] = sec;
+                if (a.t_end2) a.t_end2[i] = srow;
+                if (a.q_end2) a.q_end2[i] = tlen;
+            }
+            if (START) {
+                if (a.t_start) a.t_start[i] = t_start;
+                if (a.q_start) a.q_start[i] = q_start;
+            }
+        }
+        __syncwarp();
+    }
 }
 
 } // namespace
@@ -374,32 +626,20 @@ __global__ void __launch_bounds__(128) dp_wc_kernel(DpArgs a, const uint32_t *li
             auto tr = [&](int T) { return nrev(t[gend_reg - 1 - T]); };
             WcRec bs, ss;
             int g3 = 0;
-            if (rend_reg >= 32) {
-                wc_sweep<1, false, false>(qr, rend_reg, tr, gend_reg, 0, 0, a.sc, S, ring, nullptr, best.v, bandmax,
-                                          false, bs, ss, g3);
-                bs = rec_reduce(bs);
-                /* reversed coordinates -> what the reference records */
-                const int gidx = (gend_reg << 3) - 1 - (bs.band << 3);
-                ts = gidx + (bs.row - (bs.band << 3));
-                qs = (rend_reg << 3) - 1 - bs.col;
-            } else {
-                /* reverse region narrower than 32 words: lane 0 runs the
-                 * one-thread start pass with the warp's ring as row buffer */
-                if (lane == 0) {
-                    RowBuf rb{ring, 1u};
-                    Res rr = {best.v, best.col, best.row, 0, 0, 0, 0, 0};
-                    if (S.fast) {
-                        ScFast sf;
-                        sf.tab = tab;
-                        local_start(q, qregs, t, tregs, a.sc, rb, sf, rr);
-                    } else {
-                        ScCmp sc2{};
-                        local_start(q, qregs, t, tregs, a.sc, rb, sc2, rr);
-                    }
-                    qs = rr.q_start, ts = rr.t_start;
-                }
-                __syncwarp();
-            }
+            /* A reverse region narrower than 32 words (the ring's reader must
+             * trail its writer) is widened with words of code 0 past its end;
+             * cells right of every real column cannot change a real one, and
+             * they are left out of the maximum (ctrack). */
+            const int sweep_regs = rend_reg >= 32 ? rend_reg : 32;
+            auto qrw = [&](int j) { return j < rend_reg ? nrev(q[rend_reg - 1 - j]) : 0u; };
+            wc_sweep<1, false, false>(qrw, sweep_regs, tr, gend_reg, 0, 0, a.sc, S, ring, nullptr, best.v, bandmax,
+                                      false, bs, ss, g3, rend_reg << 3);
+            bs = rec_reduce(bs);
+            /* reversed coordinates -> what the reference records */
+            const int gidx = (gend_reg << 3) - 1 - (bs.band << 3);
+            ts = gidx + (bs.row - (bs.band << 3));
+            qs = (rend_reg << 3) - 1 - bs.col;
+            (void)qr;
         }
         if (lane == 0) {
             if (a.score) a.score[i] = best.v;
@@ -439,10 +679,38 @@ static cudaError_t launch_wc_one(const DpArgs &a, const uint32_t *list, int nlis
     return cudaGetLastError();
 }
 
+template <bool SECOND, bool START>
+static cudaError_t launch_wc_semi(const DpArgs &a, const uint32_t *list, int nlist, int max_q8, int max_t8,
+                                  cudaStream_t s)
+{
+    const int warps = 4, block = warps * 32;
+    const int ring_cols = max_q8;
+    DpArgs b = a;
+    b.scratch_cols = (uint32_t)(max_t8 + 8); /* lastcol stride per warp */
+    const size_t smem = (size_t)warps * ring_cols * 4 + (size_t)warps * b.scratch_cols * 4;
+    auto k = dp_wc_semi_kernel<SECOND, START>;
+    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    int blocks = (nlist + warps - 1) / warps;
+    if (blocks > sms * 16) blocks = sms * 16;
+    k<<<blocks, block, smem, s>>>(b, list, nlist, ring_cols);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_dp_wc(int algo, int start, bool second, const DpArgs &a, const uint32_t *list, int nlist,
                          int max_q8, int max_t8, cudaStream_t s)
 {
     if (nlist <= 0) return cudaSuccess;
+    if (algo == SEMI_GLOBAL_) {
+        if (start == WITH_START_)
+            return second ? launch_wc_semi<true, true>(a, list, nlist, max_q8, max_t8, s)
+                          : launch_wc_semi<false, true>(a, list, nlist, max_q8, max_t8, s);
+        return second ? launch_wc_semi<true, false>(a, list, nlist, max_q8, max_t8, s)
+                      : launch_wc_semi<false, false>(a, list, nlist, max_q8, max_t8, s);
+    }
     if (algo == GLOBAL_)
         return start == WITH_TB_ ? launch_wc_one<GLOBAL_, WITH_TB_, false>(a, list, nlist, max_q8, max_t8, s)
                                  : launch_wc_one<GLOBAL_, WITHOUT_START_, false>(a, list, nlist, max_q8, max_t8, s);

@@ -166,8 +166,8 @@ int plan_batch(const RunCfg &cfg, const DevBatch &b, const DevOut &o, Workspace 
     p = Plan();
     p.block = st.block;
 
-    /* split: long LOCAL/GLOBAL pairs go warp-cooperative */
-    const bool wc_algo = (cfg.algo == LOCAL_ || cfg.algo == GLOBAL_);
+    /* split: long LOCAL/GLOBAL (and target-tail SEMI_GLOBAL) pairs go warp-cooperative */
+    const bool wc_algo = cfg.algo == LOCAL_ || cfg.algo == GLOBAL_ || (cfg.algo == SEMI_GLOBAL_ && cfg.tail == TARGET_);
     uint32_t max_q_short = 0, max_q_long = 0, max_t_long = 0;
     int nlong = 0;
     p.wc_min_q = (uint32_t)st.wc_min_qregs * 8 - 7;
@@ -181,8 +181,10 @@ int plan_batch(const RunCfg &cfg, const DevBatch &b, const DevOut &o, Workspace 
             max_q_short = std::max(max_q_short, ql);
         }
     }
-    /* the warp kernel's shared memory: 4 warps x (ring of q8 words + band maxima) */
-    const size_t wc_smem = 4 * (((size_t)max_q_long + 8) + ((size_t)max_t_long + 8) / 8 + 1) * 4;
+    /* the warp kernel's shared memory: 4 warps x (ring of q8 words + band
+     * maxima, or for SEMI_GLOBAL the last-column H of every row) */
+    const size_t t_words = cfg.algo == SEMI_GLOBAL_ ? (size_t)max_t_long + 16 : ((size_t)max_t_long + 8) / 8 + 1;
+    const size_t wc_smem = 4 * (((size_t)max_q_long + 8) + t_words) * 4;
     p.use_wc = nlong > 0 && b.n >= st.min_order_pairs && ((max_q_long + 7) & ~7u) <= (uint32_t)st.wc_max_q8 &&
                wc_smem <= (200u << 10);
     if (!p.use_wc) {

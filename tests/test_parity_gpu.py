@@ -209,3 +209,22 @@ def test_workload4_launches(k):
     and unrelated pairs) on 4,000 pairs."""
     p, b = W.workload4(4000, seed=100)[k]
     _vs_oracle(p, b)
+
+
+@pytest.mark.parametrize("head", [NONE, QUERY, TARGET, BOTH])
+def test_wc_semi_global_target_tail(head):
+    """Long target-tail SEMI_GLOBAL pairs (queries of 32+ words in a batch of
+    2048+) on the warp-cooperative kernel: forward with second best, and the
+    reversed start pass; every head mode."""
+    b = W.workload2(3000, seed=60 + head)
+    _vs_oracle(Params(algo=SEMI_GLOBAL, head=head, tail=TARGET, second_best=1), b)
+    _vs_oracle(Params(algo=SEMI_GLOBAL, head=head, tail=TARGET, start_pos=WITH_START), b)
+
+
+def test_wc_semi_global_scores_and_open_forms():
+    """Other scores, a zero gap open (the shortened E chain's edge) and a
+    negative one (the literal chain), on long pairs."""
+    b = W.workload3(2100, seed=64)
+    for sc in (dict(match=2, mismatch=3, gap_open=5, gap_extend=2), dict(gap_open=0, gap_extend=2),
+               dict(gap_open=-1, gap_extend=3)):
+        _vs_oracle(Params(algo=SEMI_GLOBAL, head=TARGET, tail=TARGET, start_pos=WITH_START, second_best=1, **sc), b)
