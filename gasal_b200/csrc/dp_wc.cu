@@ -148,7 +148,7 @@ __device__ __forceinline__ uint32_t dnib(int M, int diag, int H, int F, int E, c
 template <int MODE, bool TB, bool SECOND_PASS2, class QW, class TW>
 __device__ void wc_sweep(QW qword, int qregs, TW tword, int tregs, int qlen, int tlen, const Scores &sc,
                          WcScore &S, uint32_t *ring, uint4 *tb, int stop, int *bandmax, bool write_bandmax,
-                         WcRec &best_out, WcRec &sec_out, int &gscore, int ctrack = 0x7fffffff)
+                         WcRec &best_out, WcRec &sec_out, int &gscore)
 {
     const int lane = threadIdx.x & 31;
     const int rounds = (tregs + 31) >> 5;
@@ -251,7 +251,7 @@ __device__ void wc_sweep(QW qword, int qregs, TW tword, int tregs, int qlen, int
                         for (int k = 0; k < 8; k++)
                             if (k == last_row_in_band) gscore = Hn[k];
                     }
-                } else if (c < ctrack) {
+                } else {
                     const int ck = key_max8(key);
                     if ((ck >> 3) > bandbest) bandbest = ck >> 3;
                     if ((ck >> 3) > best.v) {
@@ -626,20 +626,36 @@ __global__ void __launch_bounds__(128) dp_wc_kernel(DpArgs a, const uint32_t *li
             auto tr = [&](int T) { return nrev(t[gend_reg - 1 - T]); };
             WcRec bs, ss;
             int g3 = 0;
-            /* A reverse region narrower than 32 words (the ring's reader must
-             * trail its writer) is widened with words of code 0 past its end;
-             * cells right of every real column cannot change a real one, and
-             * they are left out of the maximum (ctrack). */
-            const int sweep_regs = rend_reg >= 32 ? rend_reg : 32;
-            auto qrw = [&](int j) { return j < rend_reg ? nrev(q[rend_reg - 1 - j]) : 0u; };
-            wc_sweep<1, false, false>(qrw, sweep_regs, tr, gend_reg, 0, 0, a.sc, S, ring, nullptr, best.v, bandmax,
-                                      false, bs, ss, g3, rend_reg << 3);
-            bs = rec_reduce(bs);
-            /* reversed coordinates -> what the reference records */
-            const int gidx = (gend_reg << 3) - 1 - (bs.band << 3);
-            ts = gidx + (bs.row - (bs.band << 3));
-            qs = (rend_reg << 3) - 1 - bs.col;
-            (void)qr;
+            if (rend_reg >= 32) {
+                wc_sweep<1, false, false>(qr, rend_reg, tr, gend_reg, 0, 0, a.sc, S, ring, nullptr, best.v, bandmax,
+                                          false, bs, ss, g3);
+                bs = rec_reduce(bs);
+                /* reversed coordinates -> what the reference records */
+                const int gidx = (gend_reg << 3) - 1 - (bs.band << 3);
+                ts = gidx + (bs.row - (bs.band << 3));
+                qs = (rend_reg << 3) - 1 - bs.col;
+            } else {
+                /* reverse region narrower than 32 words (the ring's reader
+                 * must trail its writer): lane 0 runs the one-thread start
+                 * pass with the warp's ring as row buffer.  It stops at the
+                 * first cell reaching the score -- for the short local hits
+                 * that end this early, a few bands -- where the warp would
+                 * finish a 32-band round. */
+                if (lane == 0) {
+                    RowBuf rb{ring, 1u};
+                    Res rr = {best.v, best.col, best.row, 0, 0, 0, 0, 0};
+                    if (S.fast) {
+                        ScFast sf;
+                        sf.tab = tab;
+                        local_start(q, qregs, t, tregs, a.sc, rb, sf, rr);
+                    } else {
+                        ScCmp sc2{};
+                        local_start(q, qregs, t, tregs, a.sc, rb, sc2, rr);
+                    }
+                    qs = rr.q_start, ts = rr.t_start;
+                }
+                __syncwarp();
+            }
         }
         if (lane == 0) {
             if (a.score) a.score[i] = best.v;
