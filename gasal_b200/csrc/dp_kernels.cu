@@ -133,8 +133,6 @@ __global__ void __launch_bounds__(128) dp_kernel(DpArgs a)
     }
 }
 
-int dp_block_size() { return 64; }
-
 /* Grid of the scratch (global row buffer) variant: at most what the GPU holds
  * resident, each thread looping over pairs. */
 int dp_scratch_blocks(int n, int block)

@@ -117,7 +117,7 @@ struct Settings {
     int ref_reverse = 1;
     int mql = 2048;
     size_t tb_budget_bytes = (size_t)16 << 30;
-    int block = 64;
+    int block = 32;             /* one-pair-per-thread block: 32 packs the most row buffers per SM */
     int min_order_pairs = 2048; /* batches at least this large visit pairs length-binned */
     int wc_min_qregs = 32;      /* pairs with at least this many query words go warp-cooperative */
     int wc_max_q8 = 12000;      /* ... while the batch's longest query fits the warp's ring */

@@ -114,7 +114,6 @@ cudaError_t launch_ksw_band(const DpArgs &a, const uint32_t *list, int nlist, co
                             const int32_t *band_w, uint32_t *fb, uint32_t *fbn, uint32_t *retry, uint32_t *nretry,
                             unsigned long long *cells, uint32_t *wq, cudaStream_t s);
 
-int dp_block_size();
 int dp_scratch_blocks(int n, int block);
 
 } // namespace gb
