@@ -224,6 +224,7 @@ void release_state(const gasal_gpu_storage_t *s)
     if (w.scratch) cudaFree(w.scratch);
     if (w.tb_off_free) cudaEventDestroy(w.tb_off_free);
     if (w.order) cudaFree(w.order);
+    if (w.order2) cudaFree(w.order2);
     if (w.aux) cudaStreamDestroy(w.aux);
     if (w.queue) cudaFree(w.queue);
     if (w.fork) cudaEventDestroy(w.fork);
@@ -277,7 +278,7 @@ void batch_signature(std::vector<uint8_t> &v, const gasal_gpu_storage_t *s, cons
                           s->host_query_batch_lens, s->host_target_batch_lens, s->host_query_batch_offsets,
                           s->host_target_batch_offsets, s->host_query_op, s->host_target_op, s->host_seed_scores,
                           ss.d_n_cigar, ss.ws.tb, ss.ws.d_tb_off, ss.ws.h_tb_off, ss.ws.order, ss.ws.bins,
-                          ss.ws.queue, ss.ws.aux, ss.ws.fork, ss.ws.join, ss.ws.fb, ss.ws.retry, ss.ws.feat,
+                          ss.ws.queue, ss.ws.aux, ss.ws.fork, ss.ws.join, ss.ws.fb, ss.ws.retry, ss.ws.feat, ss.ws.order2,
                           ss.ws.pred, ss.ws.bandw, (const void *)s->str};
     for (const void *q : ptrs) put(v, q);
     const gasal_res_t *rs[] = {s->host_res, s->device_cpy, s->host_res_second, s->device_cpy_second};
@@ -293,6 +294,7 @@ void batch_signature(std::vector<uint8_t> &v, const gasal_gpu_storage_t *s, cons
     put(v, plan.start), put(v, plan.block), put(v, plan.mq8), put(v, plan.mt8), put(v, plan.wc_min_q);
     put(v, plan.ksw_slots), put(v, plan.fb_blocks), put(v, plan.band);
     put(v, plan.tier2), put(v, plan.tier_q), put(v, plan.tier2_cols), put(v, plan.tier2_blocks);
+    put(v, plan.split_start);
     put(v, (const void *)cfg.band_w), put(v, cfg.band_model), put(v, cfg.band_min), put(v, cfg.band_max);
     put(v, (const void *)cfg.band_ok);
     put(v, plan.a);

@@ -8,6 +8,7 @@
 #include "gasal_b200_capi.h"
 #include "engine.h"
 
+#include <cstdio>
 #include <cstring>
 #include <mutex>
 #include <unordered_map>
@@ -336,6 +337,16 @@ extern "C" int gb_align_dev(const gb_params_t *p, const gb_dev_batch_t *b, const
  * fastest.  Candidates: DP block 32/64/128 x warp-cooperative threshold
  * 32/40/48/64/96 query words (LOCAL/GLOBAL only; other algorithms keep the
  * current threshold). */
+namespace {
+thread_local char g_last_error[256] = "";
+void set_last_error(const char *where, cudaError_t e)
+{
+    snprintf(g_last_error, sizeof g_last_error, "%s: %s", where, cudaGetErrorString(e));
+}
+} // namespace
+
+extern "C" const char *gb_last_error(void) { return g_last_error; }
+
 extern "C" int gb_autotune(const gb_params_t *p, const gb_dev_batch_t *b, const gb_dev_out_t *o, void *stream,
                            int reps, gb_tuning_t *best, double *best_ms)
 {
@@ -360,19 +371,25 @@ extern "C" int gb_autotune(const gb_params_t *p, const gb_dev_batch_t *b, const 
     }
     int rc = GB_OK;
     float best_t = 0.f;
-    gb_tuning_t bt{saved.block, saved.wc_min_qregs, saved.min_order_pairs, saved.ksw_wc};
+    gb_tuning_t bt{saved.block, saved.wc_min_qregs, saved.min_order_pairs, saved.ksw_wc, saved.split_start};
+    char where[96];
     for (int blk : blocks) {
         for (int wc : wcs) {
             st.block = blk, st.wc_min_qregs = wc;
+            snprintf(where, sizeof where, "gb_autotune block %d threshold %d", blk, wc);
             rc = gb::run_batch(cfg, db, dout, w->ws, s);
             for (int r = 0; r < reps && rc == GB_OK; r++) {
                 if (r == 0 && cudaEventRecord(e0, s) != cudaSuccess) rc = GB_ERR_CUDA;
                 if (rc == GB_OK) rc = gb::run_batch(cfg, db, dout, w->ws, s);
             }
+            if (rc != GB_OK) set_last_error(where, cudaGetLastError());
             float ms = 0.f;
-            if (rc == GB_OK && (cudaEventRecord(e1, s) != cudaSuccess || cudaEventSynchronize(e1) != cudaSuccess ||
-                                cudaEventElapsedTime(&ms, e0, e1) != cudaSuccess))
+            cudaError_t ce = cudaSuccess;
+            if (rc == GB_OK && ((ce = cudaEventRecord(e1, s)) != cudaSuccess || (ce = cudaEventSynchronize(e1)) != cudaSuccess ||
+                                (ce = cudaEventElapsedTime(&ms, e0, e1)) != cudaSuccess)) {
                 rc = GB_ERR_CUDA;
+                set_last_error(where, ce);
+            }
             if (rc != GB_OK) break;
             if (best_t == 0.f || ms < best_t) best_t = ms, bt.block = blk, bt.wc_min_qregs = wc;
         }
@@ -429,6 +446,7 @@ extern "C" int gb_set_tuning(const gb_tuning_t *t)
     gb::Settings &st = gb::settings();
     st.block = t->block, st.wc_min_qregs = t->wc_min_qregs, st.min_order_pairs = t->min_order_pairs;
     st.ksw_wc = t->ksw_warp ? 1 : 0;
+    st.split_start = t->split_start ? 1 : 0;
     return GB_OK;
 }
 
@@ -438,6 +456,7 @@ extern "C" int gb_get_tuning(gb_tuning_t *t)
     const gb::Settings &st = gb::settings();
     t->block = st.block, t->wc_min_qregs = st.wc_min_qregs, t->min_order_pairs = st.min_order_pairs;
     t->ksw_warp = st.ksw_wc;
+    t->split_start = st.split_start;
     return GB_OK;
 }
 

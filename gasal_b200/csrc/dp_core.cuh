@@ -495,6 +495,32 @@ __device__ void semi_tail_query(int head, int q8, int qlen, int tlen, int mql, c
     if (SECOND && a.scol != tlen) a.srow = qlen;
 }
 
+/* The start pass alone: both sequences reversed base by base, pads as code
+ * 0 (:227-381), from the forward pass's score (best), end row (brow) and end
+ * column (bcol). */
+template <class SC>
+__device__ void semi_start(const uint32_t *q, int qregs, int qlen, const uint32_t *t, int tregs, int tlen,
+                           const Scores &sc, int head, int tail, int mql, RowBuf rb, SC &scr, int best, int brow,
+                           int bcol, Res &r)
+{
+    const int q8 = qregs << 3;
+    const int x = tregs - ((brow >> 3) + 1);
+    int gend_reg = x > 0 ? x - 1 : x;
+    if (gend_reg < 0) gend_reg = 0; /* reference reads before its array here */
+    const int fwd = best;
+    SemiAcc b = {NEG16, 0, bcol, NEG16, 0, 0};
+    semi_init_rows(head, q8, sc, rb);
+    auto rq = [&](int j) { return rev_window(q, qlen - 8 - (j << 3)); };
+    auto rt = [&](int T) { return rev_window(t, tlen - 8 - (T << 3)); };
+    if (sc.o >= 0)
+        semi_sweep<false, true>(rq, qregs, qlen, rt, tregs, tlen, sc, head, tail, gend_reg, fwd, rb, scr, b);
+    else
+        semi_sweep<false, false>(rq, qregs, qlen, rt, tregs, tlen, sc, head, tail, gend_reg, fwd, rb, scr, b);
+    if (tail == QUERY_ || tail == BOTH_) semi_tail_query<false>(head, q8, qlen, tlen, mql, sc, rb, b);
+    r.t_start = (tlen - 1) - b.brow;
+    r.q_start = (qlen - 1) - b.bcol;
+}
+
 template <bool SECOND, bool START, class SC>
 __device__ void semi_global(const uint32_t *q, int qregs, int qlen, const uint32_t *t, int tregs, int tlen,
                             const Scores &sc, int head, int tail, int mql, RowBuf rb, SC scr, Res &r)
@@ -512,24 +538,7 @@ __device__ void semi_global(const uint32_t *q, int qregs, int qlen, const uint32
     r.score = a.best, r.t_end = a.brow, r.q_end = a.bcol;
     if (SECOND) r.score2 = a.sec, r.t_end2 = a.srow, r.q_end2 = a.scol;
     if (!START) return;
-
-    /* start: both sequences reversed base by base, pads as code 0,
-     * :227-381 */
-    const int x = tregs - ((a.brow >> 3) + 1);
-    int gend_reg = x > 0 ? x - 1 : x;
-    if (gend_reg < 0) gend_reg = 0; /* reference reads before its array here */
-    const int fwd = a.best;
-    SemiAcc b = {NEG16, 0, a.bcol, NEG16, 0, 0};
-    semi_init_rows(head, q8, sc, rb);
-    auto rq = [&](int j) { return rev_window(q, qlen - 8 - (j << 3)); };
-    auto rt = [&](int T) { return rev_window(t, tlen - 8 - (T << 3)); };
-    if (sc.o >= 0)
-        semi_sweep<false, true>(rq, qregs, qlen, rt, tregs, tlen, sc, head, tail, gend_reg, fwd, rb, scr, b);
-    else
-        semi_sweep<false, false>(rq, qregs, qlen, rt, tregs, tlen, sc, head, tail, gend_reg, fwd, rb, scr, b);
-    if (tail == QUERY_ || tail == BOTH_) semi_tail_query<false>(head, q8, qlen, tlen, mql, sc, rb, b);
-    r.t_start = (tlen - 1) - b.brow;
-    r.q_start = (qlen - 1) - b.bcol;
+    semi_start(q, qregs, qlen, t, tregs, tlen, sc, head, tail, mql, rb, scr, a.best, a.brow, a.bcol, r);
 }
 
 /* =========================== BANDED ===================================== */

@@ -33,6 +33,16 @@ template <int ALGO, int START, bool SECOND, class SC>
 __device__ __forceinline__ void run_pair(const DpArgs &a, const uint32_t *q, int qregs, int qlen, const uint32_t *t,
                                          int tregs, int tlen, int i, RowBuf rb, uint4 *tb, SC scr, Res &r)
 {
+    if (START == START_ONLY_) { /* the forward outputs are already in place */
+        if (ALGO == LOCAL_) {
+            r.score = a.score[i], r.q_end = a.q_end[i], r.t_end = a.t_end[i];
+            local_start(q, qregs, t, tregs, a.sc, rb, scr, r);
+        } else if (ALGO == SEMI_GLOBAL_) {
+            semi_start(q, qregs, qlen, t, tregs, tlen, a.sc, a.head, a.tail, a.mql, rb, scr, a.score[i], a.t_end[i],
+                       a.q_end[i], r);
+        }
+        return;
+    }
     if (ALGO == LOCAL_) {
         local_fwd<SECOND, START == WITH_TB_>(q, qregs, t, tregs, a.sc, rb, tb, scr, r);
         if (START == WITH_START_) local_start(q, qregs, t, tregs, a.sc, rb, scr, r);
@@ -47,12 +57,17 @@ __device__ __forceinline__ void run_pair(const DpArgs &a, const uint32_t *q, int
 }
 
 template <int ALGO, int START, bool SECOND>
-__device__ __forceinline__ void dp_one(const DpArgs &a, uint32_t w, RowBuf rb, const uint2 *stab, bool fast_scores)
+__device__ __forceinline__ void dp_one(const DpArgs &a, uint32_t w, RowBuf rb, const uint2 *stab, bool fast_scores,
+                                       uint32_t row_cols)
 {
     const int i = a.order ? (int)a.order[w] : (int)w;
     const int qlen = (int)a.q_len[i], tlen = (int)a.t_len[i];
     /* a pair outside this launch's length tier belongs to the other launch */
     if ((uint32_t)qlen < a.q_min || (a.q_max && (uint32_t)qlen > a.q_max)) return;
+    /* rows that would not fit the row buffer are never written (the engine
+     * sizes buffers for every pair it routes here; this only guards memory) */
+    const uint32_t need = ALGO == KSW_ ? 2u * ((uint32_t)qlen + 2u) : (((uint32_t)qlen + 7u) & ~7u);
+    if (need > row_cols) return;
     Res r = {0, 0, 0, 0, 0, 0, 0, 0};
     if (ALGO == KSW_) {
         /* empty sequences included: the reference returns h0 for them */
@@ -78,6 +93,11 @@ __device__ __forceinline__ void dp_one(const DpArgs &a, uint32_t w, RowBuf rb, c
             ScCmp scmp{};
             run_pair<ALGO, START, SECOND>(a, q, qregs, qlen, t, tregs, tlen, i, rb, tb, scmp, r);
         }
+    }
+    if (START == START_ONLY_) {
+        if (a.q_start) a.q_start[i] = r.q_start;
+        if (a.t_start) a.t_start[i] = r.t_start;
+        return;
     }
     if (a.score) a.score[i] = r.score;
     if (ALGO != GLOBAL_) {
@@ -110,12 +130,15 @@ __global__ void __launch_bounds__(128) dp_kernel(DpArgs a)
     const uint32_t gtid = blockIdx.x * blockDim.x + threadIdx.x;
     const uint32_t nthr = gridDim.x * blockDim.x;
     RowBuf rb;
+    uint32_t row_cols;
     if (SMEM) {
         rb.base = smem + threadIdx.x;
         rb.stride = blockDim.x;
+        row_cols = (uint32_t)a.smem_cols;
     } else {
         rb.base = a.scratch + gtid;
         rb.stride = nthr;
+        row_cols = a.scratch_cols;
     }
     const uint32_t n = a.n_dev ? min(*a.n_dev, (uint32_t)a.n) : (uint32_t)a.n;
     if (a.queue) {
@@ -126,10 +149,10 @@ __global__ void __launch_bounds__(128) dp_kernel(DpArgs a)
             base = __shfl_sync(0xFFFFFFFFu, base, 0);
             if (base >= n) break;
             const uint32_t w = base + lane;
-            if (w < n) dp_one<ALGO, START, SECOND>(a, w, rb, stab, fast_scores);
+            if (w < n) dp_one<ALGO, START, SECOND>(a, w, rb, stab, fast_scores, row_cols);
         }
     } else {
-        for (uint32_t w = gtid; w < n; w += nthr) dp_one<ALGO, START, SECOND>(a, w, rb, stab, fast_scores);
+        for (uint32_t w = gtid; w < n; w += nthr) dp_one<ALGO, START, SECOND>(a, w, rb, stab, fast_scores, row_cols);
     }
 }
 
@@ -188,6 +211,7 @@ cudaError_t launch_dp_scratch_grid(int algo, int start, bool second, const DpArg
 #define GB_SG(A, S, B) launch_scratch_grid<A, S, B>(a, block, blocks, s)
     switch (algo) {
     case LOCAL_:
+        if (start == START_ONLY_) return GB_SG(LOCAL_, START_ONLY_, false);
         if (start == WITH_START_) return second ? GB_SG(LOCAL_, WITH_START_, true) : GB_SG(LOCAL_, WITH_START_, false);
         if (start == WITH_TB_) return second ? GB_SG(LOCAL_, WITH_TB_, true) : GB_SG(LOCAL_, WITH_TB_, false);
         return second ? GB_SG(LOCAL_, WITHOUT_START_, true) : GB_SG(LOCAL_, WITHOUT_START_, false);
@@ -195,6 +219,7 @@ cudaError_t launch_dp_scratch_grid(int algo, int start, bool second, const DpArg
         if (start == WITH_TB_) return GB_SG(GLOBAL_, WITH_TB_, false);
         return GB_SG(GLOBAL_, WITHOUT_START_, false);
     case SEMI_GLOBAL_:
+        if (start == START_ONLY_) return GB_SG(SEMI_GLOBAL_, START_ONLY_, false);
         if (start == WITH_START_)
             return second ? GB_SG(SEMI_GLOBAL_, WITH_START_, true) : GB_SG(SEMI_GLOBAL_, WITH_START_, false);
         return second ? GB_SG(SEMI_GLOBAL_, WITHOUT_START_, true) : GB_SG(SEMI_GLOBAL_, WITHOUT_START_, false);
@@ -214,6 +239,7 @@ cudaError_t launch_dp(int algo, int start, bool second, const DpArgs &a, int blo
     if (a.n <= 0) return cudaSuccess;
     switch (algo) {
     case LOCAL_:
+        if (start == START_ONLY_) return launch_one<LOCAL_, START_ONLY_, false>(a, block, s);
         if (start == WITH_START_)
             return second ? launch_one<LOCAL_, WITH_START_, true>(a, block, s) : launch_one<LOCAL_, WITH_START_, false>(a, block, s);
         if (start == WITH_TB_)
@@ -223,6 +249,7 @@ cudaError_t launch_dp(int algo, int start, bool second, const DpArgs &a, int blo
         if (start == WITH_TB_) return launch_one<GLOBAL_, WITH_TB_, false>(a, block, s);
         return launch_one<GLOBAL_, WITHOUT_START_, false>(a, block, s);
     case SEMI_GLOBAL_:
+        if (start == START_ONLY_) return launch_one<SEMI_GLOBAL_, START_ONLY_, false>(a, block, s);
         if (start == WITH_START_)
             return second ? launch_one<SEMI_GLOBAL_, WITH_START_, true>(a, block, s) : launch_one<SEMI_GLOBAL_, WITH_START_, false>(a, block, s);
         return second ? launch_one<SEMI_GLOBAL_, WITHOUT_START_, true>(a, block, s) : launch_one<SEMI_GLOBAL_, WITHOUT_START_, false>(a, block, s);

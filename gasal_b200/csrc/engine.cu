@@ -285,6 +285,15 @@ int plan_batch(const RunCfg &cfg, const DevBatch &b, const DevOut &o, Workspace 
     p.tb = cfg.start == WITH_TB_ && (cfg.algo == LOCAL_ || cfg.algo == GLOBAL_);
     p.start = (cfg.algo == SEMI_GLOBAL_ && cfg.start == WITH_TB_) ? WITHOUT_START_ : cfg.start;
     p.second = cfg.second && (cfg.algo == LOCAL_ || cfg.algo == SEMI_GLOBAL_);
+    p.split_start = st.split_start && p.start == WITH_START_ && (cfg.algo == LOCAL_ || cfg.algo == SEMI_GLOBAL_) &&
+                    b.n >= st.min_order_pairs && o.score && o.q_end && o.t_end;
+    if (p.split_start) {
+        if (grow((void **)&ws.order2, &ws.order2_cap, (size_t)b.n, 4) != GB_OK) return GB_ERR_ALLOC;
+        if (!ws.bins && cudaMalloc((void **)&ws.bins, (size_t)order_bins() * 4) != cudaSuccess) {
+            cudaGetLastError();
+            return GB_ERR_ALLOC;
+        }
+    }
 
     if (!p.tb) {
         p.cut = {0, b.n};
@@ -343,8 +352,10 @@ int plan_batch(const RunCfg &cfg, const DevBatch &b, const DevOut &o, Workspace 
 /* The one-thread launch(es) for DpArgs a: with two length tiers, the short
  * tier from a (shared-memory rows) and the long tier from a's copy with
  * global rows on a small grid.  queue words 0 and 1 are their counters. */
-static int launch_one_thread(int algo, int start, bool second, const Plan &p, DpArgs a, Workspace &ws,
-                             cudaStream_t s)
+/* `upper` (0: none) bounds the query lengths of the long tier: the start
+ * pass launch visits every pair and must skip the warp-cooperative ones. */
+static int launch_tiers(int algo, int start, bool second, const Plan &p, DpArgs a, Workspace &ws, cudaStream_t s,
+                        uint32_t upper = 0)
 {
     if (a.queue) GB_CUDA(cudaMemsetAsync(a.queue, 0, 8, s));
     timing_mark(K_DP, true, s);
@@ -355,12 +366,36 @@ static int launch_one_thread(int algo, int start, bool second, const Plan &p, Dp
         l.scratch = ws.scratch;
         l.scratch_cols = (uint32_t)p.tier2_cols;
         l.q_min = p.tier_q + 1;
-        l.q_max = 0;
+        l.q_max = upper;
         l.queue = a.queue ? a.queue + 1 : nullptr;
         GB_CUDA(launch_dp_scratch_grid(algo, start, second, l, p.block, p.tier2_blocks, s));
     }
     timing_mark(K_DP, false, s);
     return GB_OK;
+}
+
+/* With split_start the forward pass runs first; then the start passes of the
+ * same pairs, visited by (reverse-region words, forward score) so the lanes
+ * of a warp stop at similar bands (a start pass runs until it reaches the
+ * forward score).  Pairs the warp-cooperative kernel owns are skipped by
+ * their length. */
+static int launch_one_thread(int algo, int start, bool second, const Plan &p, DpArgs a, Workspace &ws,
+                             cudaStream_t s)
+{
+    if (!(p.split_start && start == WITH_START_)) return launch_tiers(algo, start, second, p, a, ws, s);
+    int rc = launch_tiers(algo, WITHOUT_START_, second, p, a, ws, s);
+    if (rc != GB_OK) return rc;
+    timing_mark(K_ORDER, true, s);
+    /* the warp-cooperative pairs' outputs may still be in flight on the
+     * auxiliary stream: the order must not read them */
+    const uint32_t cut = p.use_wc ? (uint32_t)p.wc_min_q : 0u;
+    GB_CUDA(launch_start_order(p.a.q_len, p.a.q_end, p.a.score, p.a.n, cut, ws.bins, ws.order2, s));
+    timing_mark(K_ORDER, false, s);
+    DpArgs st = p.a;
+    st.order = ws.order2;
+    const uint32_t upper = cut ? cut - 1 : 0;
+    if (upper && (st.q_max == 0 || st.q_max > upper)) st.q_max = upper;
+    return launch_tiers(algo, START_ONLY_, false, p, st, ws, s, upper);
 }
 
 /* DP over pairs [0, a.n) visited in `order` (nullptr: identity): the first

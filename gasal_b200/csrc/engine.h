@@ -64,6 +64,8 @@ struct Workspace {
     cudaEvent_t tb_off_free = nullptr;
     uint32_t *order = nullptr;   /* length-binned visiting order */
     size_t order_cap = 0;
+    uint32_t *order2 = nullptr;  /* visiting order of the separate start passes */
+    size_t order2_cap = 0;
     uint32_t *bins = nullptr;    /* order_bins() class counters */
     cudaStream_t aux = nullptr;  /* second stream for the warp-cooperative kernel */
     uint32_t *queue = nullptr;   /* work counter of the persistent one-thread launch */
@@ -92,6 +94,7 @@ struct Plan {
     uint32_t tier_q = 0;    /* queries up to tier_q: shared-memory tier */
     int tier2_cols = 0, tier2_blocks = 0;
     bool band = false;      /* ksw through the banded kernel + certificate */
+    bool split_start = false; /* one-thread start passes as a second launch (order2) */
     int fb_blocks = 0;      /* grid of the one-thread ksw launch for handed-back pairs (scratch rows) */
     DpArgs a{};
     std::vector<int> cut;   /* pair ranges [cut[c], cut[c+1]) run one after another */
@@ -123,6 +126,8 @@ struct Settings {
     int wc_max_q8 = 12000;      /* ... while the batch's longest query fits the warp's ring */
     int graphs = 1;             /* gasal_aln_async runs each batch as a CUDA graph */
     int ksw_wc = 1;             /* ksw pairs run warp-per-pair (ksw_wc.cu) */
+    int split_start = 1;        /* one-thread LOCAL/SEMI_GLOBAL start passes run as their own launch,
+                                   pairs re-ordered by forward score */
     const void *band_model = nullptr; /* installed band MLP (BF16 parameters on the device) */
     int band_min = 16, band_max = 1024;
 };

@@ -22,7 +22,8 @@
 namespace gb {
 
 enum Algo { GLOBAL_ = 1, SEMI_GLOBAL_ = 2, LOCAL_ = 3, BANDED_ = 5, KSW_ = 6 };
-enum Start { WITHOUT_START_ = 0, WITH_START_ = 1, WITH_TB_ = 2 };
+enum Start { WITHOUT_START_ = 0, WITH_START_ = 1, WITH_TB_ = 2,
+             START_ONLY_ = 3 /* engine-internal: the start pass alone, from the forward outputs */ };
 enum Src { NONE_ = 0, QUERY_ = 1, TARGET_ = 2, BOTH_ = 3 };
 
 struct Scores {
@@ -82,6 +83,11 @@ cudaError_t launch_traceback(const TbArgs &a, cudaStream_t s);
 int order_bins();
 cudaError_t launch_order(const uint32_t *q_len, const uint32_t *t_len, int n, uint32_t *bins, uint32_t *order,
                          cudaStream_t s);
+/* order for the start passes: by query words of the reverse region and the
+ * forward score (a proxy for how far the start pass runs), most work first.
+ * Pairs of q_cut+ bases (0: none) go last without their outputs being read. */
+cudaError_t launch_start_order(const uint32_t *q_len, const int32_t *q_end, const int32_t *score, int n,
+                               uint32_t q_cut, uint32_t *bins, uint32_t *order, cudaStream_t s);
 
 /* warp-cooperative DP (dp_wc.cu) for the pairs listed in `list`: LOCAL and
  * GLOBAL; queries of at least 32 words */

@@ -49,7 +49,7 @@ class GbDevOut(C.Structure):
 
 class GbTuning(C.Structure):
     _fields_ = [("block", C.c_int32), ("wc_min_qregs", C.c_int32), ("min_order_pairs", C.c_int32),
-                ("ksw_warp", C.c_int32)]
+                ("ksw_warp", C.c_int32), ("split_start", C.c_int32)]
 
 
 class GbBandStats(C.Structure):
@@ -112,6 +112,7 @@ SIGNATURES = {
     "gb_set_band_model": (C.c_int, [C.c_void_p, C.c_int, C.c_int]),
     "gb_ksw_band_align": (C.c_int, [C.POINTER(GbParams), C.POINTER(GbDevBatch), C.POINTER(GbDevOut), C.c_void_p,
                                     C.c_void_p, C.c_void_p, C.POINTER(GbBandStats)]),
+    "gb_last_error": (C.c_char_p, []),
     "gb_autotune": (C.c_int, [C.POINTER(GbParams), C.POINTER(GbDevBatch), C.POINTER(GbDevOut), C.c_void_p, C.c_int,
                               C.POINTER(GbTuning), C.POINTER(C.c_double)]),
     "gb_kernel_timing": (C.c_int, [C.c_int]),
@@ -229,8 +230,10 @@ def autotune(p: Params, dev: dict, h_q_len: np.ndarray, h_t_len: np.ndarray, str
     cp = p.to_c()
     t = GbTuning()
     ms = C.c_double()
-    _check(lib().gb_autotune(C.byref(cp), C.byref(b), C.byref(o), C.c_void_p(stream_handle), int(reps),
-                             C.byref(t), C.byref(ms)), "gb_autotune")
+    rc = lib().gb_autotune(C.byref(cp), C.byref(b), C.byref(o), C.c_void_p(stream_handle), int(reps), C.byref(t),
+                           C.byref(ms))
+    if rc != 0:
+        raise GasalError(f"gb_autotune failed: {GB_STATUS.get(rc, rc)} ({lib().gb_last_error().decode()})")
     d = {k: getattr(t, k) for k, _ in GbTuning._fields_}
     d["ms"] = ms.value
     return d

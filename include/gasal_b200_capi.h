@@ -221,6 +221,8 @@ typedef struct {
     int32_t wc_min_qregs;
     int32_t min_order_pairs;
     int32_t ksw_warp;      /* 1: ksw pairs run one warp per pair (default); 0: one thread per pair */
+    int32_t split_start;   /* 1: LOCAL / SEMI_GLOBAL start passes run as their own launch, pairs re-ordered
+                              by forward score (default); 0: in the forward launch */
 } gb_tuning_t;
 int gb_set_tuning(const gb_tuning_t *t);
 int gb_get_tuning(gb_tuning_t *t);
@@ -234,6 +236,8 @@ int gb_get_tuning(gb_tuning_t *t);
  * not for use during stream capture. */
 int gb_autotune(const gb_params_t *p, const gb_dev_batch_t *b, const gb_dev_out_t *o, void *stream, int reps,
                 gb_tuning_t *best, double *best_ms);
+/* Text of the last CUDA failure the calling thread met in gb_autotune ("" if none). */
+const char *gb_last_error(void);
 
 /* Instrumentation (no reference counterpart).  gb_kernel_timing(1) resets
  * and starts recording a CUDA event pair around every kernel the library

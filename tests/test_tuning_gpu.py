@@ -6,7 +6,7 @@ import pytest
 
 from gasal_b200 import lib as gl
 from gasal_b200 import workloads as W
-from gasal_b200.capi import Params, LOCAL, GLOBAL, WITH_START, WITH_TB
+from gasal_b200.capi import Params, LOCAL, GLOBAL, SEMI_GLOBAL, WITH_START, WITH_TB, TARGET, QUERY, NONE
 from oracle.bindings import oracle_align
 
 pytestmark = pytest.mark.gpu
@@ -66,5 +66,29 @@ def test_autotune_installs_fastest_and_keeps_results():
         exp = oracle_align(p, b).as_dict(p)
         for k, v in exp.items():
             assert np.array_equal(keep[k].cpu().numpy(), v), k
+    finally:
+        gl.set_tuning(**saved)
+
+
+@pytest.mark.parametrize("split", [0, 1])
+def test_start_pass_split_keeps_results(split):
+    """Start passes in the forward launch or as their own score-ordered
+    launch give the same starts (batches of 2048+ pairs; the w2 batch also
+    has warp-cooperative long pairs, whose starts the split leaves alone)."""
+    saved = gl.get_tuning()
+    try:
+        gl.set_tuning(split_start=split)
+        cases = [(Params(algo=LOCAL, start_pos=WITH_START, second_best=1, reverse_complement=1),
+                  W.workload1(9000, seed=66)[0][1]),
+                 (Params(algo=SEMI_GLOBAL, start_pos=WITH_START, head=TARGET, tail=TARGET, reverse_complement=1),
+                  W.workload1(9000, seed=67)[2][1]),
+                 (Params(algo=SEMI_GLOBAL, start_pos=WITH_START, head=QUERY, tail=NONE), W.workload0(3000, seed=68)),
+                 (Params(algo=LOCAL, start_pos=WITH_START), W.workload2(3000, seed=69)),
+                 (Params(algo=SEMI_GLOBAL, start_pos=WITH_START, head=TARGET, tail=TARGET), W.workload2(3000, seed=70))]
+        for p, b in cases:
+            got = gl.align(p, b).as_dict(p)
+            exp = oracle_align(p, b).as_dict(p)
+            for k, v in exp.items():
+                assert np.array_equal(got[k], v), f"split={split} {p.key()} {k}"
     finally:
         gl.set_tuning(**saved)
