@@ -216,7 +216,12 @@ def main():
     ap.add_argument("--ref-sample", type=int, default=4000)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--band", default="off", choices=["off", "learned"],
-                    help="ksw (w3): learned band with certificate; the model is trained first on a separate sample")
+                    help="ksw launches (w3, w4): learned band with certificate; the model is trained first on a "
+                         "separate sample")
+    ap.add_argument("--no-plain", action="store_true",
+                    help="skip timing the plain full-DP form (one pair per thread, input order) on the same batch")
+    ap.add_argument("--plain-budget-s", type=float, default=15.0,
+                    help="device time the plain form's timed steps may take (at least one step)")
     ap.add_argument("--band-train-pairs", type=int, default=100_000)
     args = ap.parse_args()
     if args.warmup < 3:
@@ -281,12 +286,16 @@ def main():
     stream = torch.cuda.Stream(device=dev)
 
     band_info = None
+    model = None
     if args.band == "learned":
-        if args.workload != "w3":
-            raise SystemExit("--band learned applies to the ksw workload (w3)")
+        if args.workload not in ("w3", "w4"):
+            raise SystemExit("--band learned applies to the workloads with ksw launches (w3, w4)")
         from gasal_b200 import band_train as BT
         t0 = time.time()
-        tp, tb = build_workload(args.band_train_pairs, shard.shard_seed(W.SEED_BASE + 101, rank), "w3")[0]
+        # a separate sample of the same workload; w4's ksw launch is a quarter of it
+        n_train = args.band_train_pairs * (4 if args.workload == "w4" else 1)
+        tparts = build_workload(n_train, shard.shard_seed(W.SEED_BASE + 101, rank), args.workload)
+        tp, tb = next((p, b) for p, b in tparts if p.algo == KSW)
         tdb = BT.DeviceBatch(torch, tb, dev)
         feat = BT.features(torch, tdb)
         lab = BT.labels(torch, tp, tdb)
@@ -379,16 +388,55 @@ def main():
            "d2h_bytes_per_step": d2h, "ms_per_step": e2e_ms,
            "path": "gasal_c_aln_async + gasal_c_is_aln_async_done (3 streams), pinned host batches"}
 
-    if args.workload == "w3":
-        # band statistics of one more (untimed) pass: computed cells, and with
-        # a band how many results the certificate kept
-        p3, b3, d3 = dparts[0]
+    kparts = [x for x in dparts if x[0].algo == KSW]
+    if kparts:
+        # band statistics of one more (untimed) pass over the ksw launch:
+        # computed cells, and with a band how many results the certificate kept
+        p3, b3, d3 = kparts[0]
         wide = None if args.band == "learned" else torch.full((b3.n,), 1 << 20, dtype=torch.int32, device=dev)
         with torch.cuda.stream(stream):
             st = gl.ksw_band_align(p3, d3["map"], b3.q_len, b3.t_len, wide.data_ptr() if wide is not None else None,
                                    None, stream.cuda_stream)
         band_info = dict(band_info or {}, mode=args.band, **st,
                          computed_cells_fraction=st["cells"] / max(1, b3.cells()))
+    # ---------------- the plain full-DP form on the same batch ----------------
+    plain = None
+    if not args.no_plain:
+        want = [[v.clone() for v in list(d["outs"].values()) + [d["cigar"], d["ncig"]]] for _, _, d in dparts]
+        saved = gl.get_tuning()
+        if model is not None:
+            gl.BandModel.uninstall()
+        gl.set_tuning(**gl.PLAIN_FORM)
+        try:
+            p0, p1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            p0.record(stream)
+            step()  # warm-up; its time sizes the timed leg
+            p1.record(stream)
+            torch.cuda.synchronize()
+            t1 = shard.max_over_ranks(p0.elapsed_time(p1), dist, dev)
+            k_plain = int(max(1, min(args.steps, args.plain_budget_s * 1e3 // max(t1, 1e-3))))
+            if dist:
+                dist.barrier()
+            torch.cuda.synchronize()
+            p0.record(stream)
+            for _ in range(k_plain):
+                step()
+            p1.record(stream)
+            torch.cuda.synchronize()
+            pms = shard.max_over_ranks(p0.elapsed_time(p1), dist, dev)
+        finally:
+            gl.set_tuning(**saved)
+            if model is not None:
+                model.install(16, 1024)
+        got = [list(d["outs"].values()) + [d["cigar"], d["ncig"]] for _, _, d in dparts]
+        same = all(torch.equal(g, w) for gs, ws in zip(got, want) for g, w in zip(gs, ws))
+        pval = shard.job_throughput(npairs, world, k_plain, pms)
+        plain = {"value": pval, "unit": UNIT, "ms_per_step": pms / k_plain, "steps": k_plain, "warmup": 1,
+                 "gcups": cells * world / (pms / k_plain * 1e-3) / 1e9,
+                 "form": "every pair one per thread in input order on a grid over the batch: no device work "
+                         "counter, no length ordering, no warp-cooperative or warp-per-pair kernels, no band, "
+                         "start passes in the forward launch",
+                 "value_over_plain": value / pval, "bit_exact_vs_plain": bool(same)}
     in_mb = sum(int(b.q.shape[0] + b.t.shape[0]) + 16 * b.n for _, b in parts) / 1e6
     l2_note = (f"inputs {in_mb:.0f} MB > 126 MB L2, no flush" if in_mb > 126 else
                f"inputs {in_mb:.0f} MB fit the 126 MB L2 (no flush: each step re-reads them, as a caller "
@@ -419,6 +467,7 @@ def main():
             "e2e": e2e,
             "clocks": clk.summary(),
             "band": band_info,
+            "plain": plain,
         }
         print(json.dumps(line), flush=True)
     if dist:

@@ -371,7 +371,8 @@ extern "C" int gb_autotune(const gb_params_t *p, const gb_dev_batch_t *b, const 
     }
     int rc = GB_OK;
     float best_t = 0.f;
-    gb_tuning_t bt{saved.block, saved.wc_min_qregs, saved.min_order_pairs, saved.ksw_wc, saved.split_start};
+    gb_tuning_t bt{saved.block, saved.wc_min_qregs, saved.min_order_pairs, saved.ksw_wc, saved.split_start,
+                   saved.persistent};
     char where[96];
     for (int blk : blocks) {
         for (int wc : wcs) {
@@ -447,6 +448,7 @@ extern "C" int gb_set_tuning(const gb_tuning_t *t)
     st.block = t->block, st.wc_min_qregs = t->wc_min_qregs, st.min_order_pairs = t->min_order_pairs;
     st.ksw_wc = t->ksw_warp ? 1 : 0;
     st.split_start = t->split_start ? 1 : 0;
+    st.persistent = t->persistent ? 1 : 0;
     return GB_OK;
 }
 
@@ -457,6 +459,7 @@ extern "C" int gb_get_tuning(gb_tuning_t *t)
     t->block = st.block, t->wc_min_qregs = st.wc_min_qregs, t->min_order_pairs = st.min_order_pairs;
     t->ksw_warp = st.ksw_wc;
     t->split_start = st.split_start;
+    t->persistent = st.persistent;
     return GB_OK;
 }
 

@@ -208,7 +208,7 @@ int plan_batch(const RunCfg &cfg, const DevBatch &b, const DevOut &o, Workspace 
         cudaGetLastError();
         return GB_ERR_ALLOC;
     }
-    a.queue = ws.queue;
+    a.queue = st.persistent ? ws.queue : nullptr;
     /* ksw: warp per pair; the one-thread kernel only takes what that hands
      * back (queries beyond 2046 bases, huge seed scores) */
     if (cfg.algo == KSW_ && st.ksw_wc && ksw_wc_scores_ok(cfg.sc)) {

@@ -128,6 +128,8 @@ struct Settings {
     int ksw_wc = 1;             /* ksw pairs run warp-per-pair (ksw_wc.cu) */
     int split_start = 1;        /* one-thread LOCAL/SEMI_GLOBAL start passes run as their own launch,
                                    pairs re-ordered by forward score */
+    int persistent = 1;         /* one-thread launches pull pairs from a device counter; 0: one thread per
+                                   pair on a grid over the batch */
     const void *band_model = nullptr; /* installed band MLP (BF16 parameters on the device) */
     int band_min = 16, band_max = 1024;
 };

@@ -25,7 +25,7 @@
  *   the lane applies its carry in a second pass over the same registers.
  *
  *   The row maximum and its last column come from one warp max-reduction of
- *   the key H*4096 + j; the trimming scan from one ballot per tile and a
+ *   the key H*8192 + j; the trimming scan from one ballot per tile and a
  *   broadcast re-read of the boundary lane's 8 entries.
  *
  * Columns left of beg are computed too (they hold zeros and stay zero, which
@@ -41,8 +41,10 @@ namespace {
 constexpr int KT = 256;                 /* columns per tile (32 lanes x 8) */
 constexpr int KSW_WC_COLS0 = 2048;      /* length class 0: queries up to 2046 bases */
 constexpr int KSW_WC_COLS1 = 8192;      /* length class 1: up to 8190 */
-constexpr int KEY_BITS = 12;            /* key = H << 12 | column */
 constexpr int EH_LIMIT = 1 << 15;       /* H and E are stored as 16-bit halves */
+constexpr int KEY_BITS = 13;            /* key = H << 13 | column: columns up to 8191, H below EH_LIMIT */
+static_assert((1 << KEY_BITS) >= KSW_WC_COLS1, "the row-maximum key must hold every column of a length class");
+static_assert((long long)EH_LIMIT << KEY_BITS <= 0x7FFFFFFFll, "the row-maximum key must fit in 32 bits");
 constexpr unsigned FULL = 0xFFFFFFFFu;
 
 __device__ __forceinline__ int kslot(int j) { return (j & ~255) | ((j & 7) << 5) | ((j >> 3) & 31); }

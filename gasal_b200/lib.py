@@ -49,7 +49,7 @@ class GbDevOut(C.Structure):
 
 class GbTuning(C.Structure):
     _fields_ = [("block", C.c_int32), ("wc_min_qregs", C.c_int32), ("min_order_pairs", C.c_int32),
-                ("ksw_warp", C.c_int32), ("split_start", C.c_int32)]
+                ("ksw_warp", C.c_int32), ("split_start", C.c_int32), ("persistent", C.c_int32)]
 
 
 class GbBandStats(C.Structure):
@@ -177,8 +177,14 @@ def get_tuning() -> dict:
     return {k: getattr(t, k) for k, _ in GbTuning._fields_}
 
 
+# The plain full-DP form: every pair one per thread, in input order, on a grid
+# over the batch (no device work counter, no length ordering, no warp kernels,
+# start passes inside the forward launch).
+PLAIN_FORM = dict(min_order_pairs=1 << 30, ksw_warp=0, split_start=0, persistent=0)
+
+
 def set_tuning(**kw):
-    """Change any of block, wc_min_qregs, min_order_pairs, ksw_warp."""
+    """Change any of block, wc_min_qregs, min_order_pairs, ksw_warp, split_start, persistent."""
     cur = get_tuning()
     bad = set(kw) - set(cur)
     if bad:

@@ -223,6 +223,10 @@ typedef struct {
     int32_t ksw_warp;      /* 1: ksw pairs run one warp per pair (default); 0: one thread per pair */
     int32_t split_start;   /* 1: LOCAL / SEMI_GLOBAL start passes run as their own launch, pairs re-ordered
                               by forward score (default); 0: in the forward launch */
+    int32_t persistent;    /* 1: one-pair-per-thread launches are persistent, warps pulling pairs from a
+                              device counter (default); 0: one thread per pair on a grid over the batch.
+                              With min_order_pairs above the batch size, ksw_warp 0 and split_start 0
+                              this is the plain full-DP form: every pair one per thread, in input order */
 } gb_tuning_t;
 int gb_set_tuning(const gb_tuning_t *t);
 int gb_get_tuning(gb_tuning_t *t);

@@ -117,3 +117,24 @@ def test_scores_near_the_16_bit_row_limit():
         seeds.append(int(rng.integers(0, 2000)))
     b = Batch.from_seqs(qs, ts, seed=np.array(seeds, dtype=np.uint32))
     _check(Params(algo=KSW, match=20, mismatch=30, gap_open=40, gap_extend=5), b)
+
+
+def test_long_class_columns_past_4095():
+    """Queries of 4,100-8,190 bases run in the 8192-column length class; the
+    row maximum's key must carry columns past 4095 (near-identical pairs
+    put the maximum in the last columns)."""
+    rng = np.random.default_rng(96)
+    qs, ts, seeds = [], [], []
+    for i in range(90):
+        n = int(rng.integers(4100, 8191)) if i % 3 else int(rng.integers(4100, 4400))
+        q = bytes(np.frombuffer(b"ACGT", np.uint8)[rng.integers(0, 4, n)])
+        t = bytearray(q)
+        for _ in range(n // 200):
+            t[int(rng.integers(0, len(t)))] = b"ACGT"[int(rng.integers(0, 4))]
+        qs.append(q)
+        ts.append(bytes(t) + bytes(np.frombuffer(b"ACGT", np.uint8)[rng.integers(0, 4, int(rng.integers(0, 40)))]))
+        seeds.append(int(rng.integers(20, 61)))
+    b = Batch.from_seqs(qs, ts, seed=np.array(seeds, dtype=np.uint32))
+    got = _check(Params(algo=KSW, zdrop=100), b)
+    assert int((got["q_end"] > 4096).sum()) > 45  # the maxima sit past column 4096
+    _check(Params(algo=KSW), b)

@@ -92,3 +92,26 @@ def test_start_pass_split_keeps_results(split):
                 assert np.array_equal(got[k], v), f"split={split} {p.key()} {k}"
     finally:
         gl.set_tuning(**saved)
+
+
+def test_plain_form_matches_oracle():
+    """The plain full-DP form (every pair one per thread in input order, no
+    device work counter, no ordering, no warp kernels) gives the same results:
+    it is the baseline the batched form is measured against."""
+    from gasal_b200.capi import KSW, WITH_TB as TB
+    saved = gl.get_tuning()
+    try:
+        gl.set_tuning(**gl.PLAIN_FORM)
+        assert gl.get_tuning()["persistent"] == 0
+        cases = [(Params(algo=LOCAL, start_pos=WITH_START, second_best=1), W.workload2(2500, seed=71)),
+                 (Params(algo=GLOBAL, start_pos=TB), W.workload2(2500, seed=72)),
+                 (Params(algo=SEMI_GLOBAL, start_pos=WITH_START, head=TARGET, tail=TARGET, second_best=1),
+                  W.workload1(3000, seed=73)[2][1]),
+                 (Params(algo=KSW, zdrop=100), W.workload3(300, seed=74))]
+        for p, b in cases:
+            got = gl.align(p, b).as_dict(p)
+            exp = oracle_align(p, b).as_dict(p)
+            for k, v in exp.items():
+                assert np.array_equal(got[k], v), f"plain {p.key()} {k}"
+    finally:
+        gl.set_tuning(**saved)
