@@ -132,3 +132,44 @@ def test_installed_model_path_matches_oracle():
     exp = oracle_align(p, b).as_dict(p)
     for k in OUTS:
         assert np.array_equal(got[k], exp[k]), k
+
+
+def test_trained_band_beats_a_fixed_band_of_the_same_width():
+    """What the trained network gains over the banded method without it: on
+    held-out pairs its per-pair bands keep more banded results (fewer exact
+    recomputations) and compute fewer cells than one fixed band of the same
+    mean width -- and every result still equals the oracle."""
+    from gasal_b200 import band_train as BT
+    p = Params(algo=KSW, zdrop=100)
+    tb = W.workload3(16000, seed=130)
+    tdb = BT.DeviceBatch(torch, tb, DEV)
+    feat = BT.features(torch, tdb)
+    lab = BT.labels(torch, p, tdb)
+    model = gl.BandModel(seed=13)
+    BT.train(torch, model, feat, lab, steps=400, batch=4096, tau=0.8, lr=3e-3)
+    eb = W.workload3(12000, seed=131)
+    edb = BT.DeviceBatch(torch, eb, DEV)
+    ef = BT.features(torch, edb)
+    pred = torch.zeros(eb.n, dtype=torch.float32, device=DEV)
+    model.predict(ef.data_ptr(), eb.n, pred.data_ptr(), _stream())
+    torch.cuda.synchronize()
+    model.close()
+    # the same transform as band_from_pred_kernel: ceil(2^y), multiple of 8, [16, 1024]
+    w = np.ceil(np.exp2(np.clip(pred.cpu().numpy(), 0, 20))).astype(np.int64)
+    w = np.clip((w + 7) & ~7, 16, 1024)
+    cover = np.maximum(eb.q_len, eb.t_len).astype(np.int64)
+    learned = np.where(w >= cover, -1, w).astype(np.int32)
+    mean_w = int(np.mean(np.where(learned < 0, cover, learned)))
+    fixed = np.full(eb.n, (mean_w + 7) & ~7, np.int32)
+    exp = oracle_align(p, eb).as_dict(p)
+    stats = {}
+    for name, band in (("learned", learned), ("fixed", fixed)):
+        bt = torch.from_numpy(band).to(DEV)
+        for k in OUTS:
+            edb.out(k).fill_(-7)
+        stats[name] = gl.ksw_band_align(p, edb.map, eb.q_len, eb.t_len, bt.data_ptr(), None, _stream())
+        for k in OUTS:
+            assert np.array_equal(edb.out(k).cpu().numpy(), exp[k]), (name, k)
+    kept = {k: v["accepted"] / eb.n for k, v in stats.items()}
+    assert kept["learned"] > kept["fixed"] + 0.03, (kept, mean_w)
+    assert stats["learned"]["cells"] < stats["fixed"]["cells"], stats
