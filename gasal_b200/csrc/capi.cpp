@@ -335,7 +335,8 @@ extern "C" int gb_align_dev(const gb_params_t *p, const gb_dev_batch_t *b, const
 /* Launch autotuner: times the batch under every candidate setting (CUDA
  * events on `stream`, `reps` runs after one warm-up run each) and keeps the
  * fastest.  Candidates: DP block 32/64/128 x warp-cooperative threshold
- * 32/40/48/64/96 query words (LOCAL/GLOBAL only; other algorithms keep the
+ * 16/32/48/64 query words x lane groups automatic/8/16/32 (LOCAL, GLOBAL and
+ * target-tail SEMI_GLOBAL; other algorithms keep the
  * current threshold). */
 namespace {
 thread_local char g_last_error[256] = "";
@@ -362,7 +363,11 @@ extern "C" int gb_autotune(const gb_params_t *p, const gb_dev_batch_t *b, const 
     const cudaStream_t s = (cudaStream_t)stream;
     std::vector<int> blocks = {32, 64, 128};
     std::vector<int> wcs = {st.wc_min_qregs};
-    if (p->algo == LOCAL || p->algo == GLOBAL) wcs = {32, 40, 48, 64, 96};
+    std::vector<int> groups = {st.wc_group};
+    if (p->algo == LOCAL || p->algo == GLOBAL || (p->algo == SEMI_GLOBAL && p->tail == TARGET)) {
+        wcs = {16, 32, 48, 64};
+        groups = {0, 8, 16, 32};
+    }
     cudaEvent_t e0, e1;
     if (cudaEventCreate(&e0) != cudaSuccess) return GB_ERR_CUDA;
     if (cudaEventCreate(&e1) != cudaSuccess) {
@@ -372,12 +377,14 @@ extern "C" int gb_autotune(const gb_params_t *p, const gb_dev_batch_t *b, const 
     int rc = GB_OK;
     float best_t = 0.f;
     gb_tuning_t bt{saved.block, saved.wc_min_qregs, saved.min_order_pairs, saved.ksw_wc, saved.split_start,
-                   saved.persistent};
+                   saved.persistent, saved.wc_group};
     char where[96];
     for (int blk : blocks) {
-        for (int wc : wcs) {
-            st.block = blk, st.wc_min_qregs = wc;
-            snprintf(where, sizeof where, "gb_autotune block %d threshold %d", blk, wc);
+        for (size_t c = 0; c < wcs.size() * groups.size() && rc == GB_OK; c++) {
+            const int wc = wcs[c % wcs.size()], grp = groups[c / wcs.size()];
+            if (groups.size() > 1 && wc < grp) continue; /* the threshold is at least the group */
+            st.block = blk, st.wc_min_qregs = wc, st.wc_group = grp;
+            snprintf(where, sizeof where, "gb_autotune block %d threshold %d group %d", blk, wc, grp);
             rc = gb::run_batch(cfg, db, dout, w->ws, s);
             for (int r = 0; r < reps && rc == GB_OK; r++) {
                 if (r == 0 && cudaEventRecord(e0, s) != cudaSuccess) rc = GB_ERR_CUDA;
@@ -392,7 +399,7 @@ extern "C" int gb_autotune(const gb_params_t *p, const gb_dev_batch_t *b, const 
                 set_last_error(where, ce);
             }
             if (rc != GB_OK) break;
-            if (best_t == 0.f || ms < best_t) best_t = ms, bt.block = blk, bt.wc_min_qregs = wc;
+            if (best_t == 0.f || ms < best_t) best_t = ms, bt.block = blk, bt.wc_min_qregs = wc, bt.wc_group = grp;
         }
         if (rc != GB_OK) break;
     }
@@ -400,7 +407,7 @@ extern "C" int gb_autotune(const gb_params_t *p, const gb_dev_batch_t *b, const 
     cudaEventDestroy(e1);
     st = saved;
     if (rc != GB_OK) return rc;
-    st.block = bt.block, st.wc_min_qregs = bt.wc_min_qregs;
+    st.block = bt.block, st.wc_min_qregs = bt.wc_min_qregs, st.wc_group = bt.wc_group;
     *best = bt;
     if (best_ms) *best_ms = best_t / reps;
     return GB_OK;
@@ -443,12 +450,14 @@ extern "C" int gb_set_tuning(const gb_tuning_t *t)
 {
     if (!t) return GB_ERR_ARG;
     if (t->block != 32 && t->block != 64 && t->block != 128) return GB_ERR_ARG;
-    if (t->wc_min_qregs < 32 || t->min_order_pairs < 0) return GB_ERR_ARG; /* the warp kernel needs 32+ words */
+    if (t->wc_min_qregs < 8 || t->min_order_pairs < 0) return GB_ERR_ARG;
+    if (t->wc_group != 0 && t->wc_group != 8 && t->wc_group != 16 && t->wc_group != 32) return GB_ERR_ARG;
     gb::Settings &st = gb::settings();
     st.block = t->block, st.wc_min_qregs = t->wc_min_qregs, st.min_order_pairs = t->min_order_pairs;
     st.ksw_wc = t->ksw_warp ? 1 : 0;
     st.split_start = t->split_start ? 1 : 0;
     st.persistent = t->persistent ? 1 : 0;
+    st.wc_group = t->wc_group;
     return GB_OK;
 }
 
@@ -460,6 +469,7 @@ extern "C" int gb_get_tuning(gb_tuning_t *t)
     t->ksw_warp = st.ksw_wc;
     t->split_start = st.split_start;
     t->persistent = st.persistent;
+    t->wc_group = st.wc_group;
     return GB_OK;
 }
 

@@ -13,9 +13,19 @@
  * (bands, then columns, then rows) through per-lane records of
  * (value, band, column, row) reduced first by value and then by band.
  *
+ * Lane groups: with G = 16 or 8 a warp sweeps 32/G pairs side by side, each
+ * on its own G lanes with its own ring (shuffles of width G, ballots masked
+ * to the group).  A pair's sweep takes rounds*qregs + G-1 steps on G lanes,
+ * so the G-1 steps of pipeline fill and drain cost less: on w2's 250-1000 bp
+ * pairs 72% of lane-steps do work at G = 32, 88% at 16, 95% at 8.
+ * Neighbouring pairs of the length-ordered list have about the same lengths,
+ * so the groups of a warp finish together.  Every loop that contains a warp
+ * operation runs the same trip count on all lanes (the warp's maximum) with
+ * per-group predicates.
+ *
  * Replaces, for long pairs, reference src/kernels/local_kernel_template.h and
  * src/kernels/global.h (one thread per pair there).  The pairs handled here
- * need at least 32 query words (the ring's reader must trail its writer).
+ * need at least G query words (the ring's reader must trail its writer).
  */
 #include "dp_core.cuh"
 
@@ -48,15 +58,24 @@ constexpr uint64_t WC_CLASS = (5ull << 0) | (0ull << 4) | (6ull << 8) | (1ull <<
                               (6ull << 44) | (6ull << 48) | (6ull << 52) | (4ull << 56) | (6ull << 60);
 constexpr uint32_t WC_PLAIN = (1u << 0) | (1u << 1) | (1u << 3) | (1u << 4) | (1u << 7) | (1u << 14);
 
-__device__ bool wc_plain(const uint32_t *w, int n)
+/* lanes of a group of G: its first lane and its ballot mask */
+template <int G> __device__ __forceinline__ int gbase_of(int lane) { return lane & ~(G - 1); }
+template <int G> __device__ __forceinline__ unsigned gmask_of(int lane)
 {
+    return G == 32 ? 0xFFFFFFFFu : (((1u << G) - 1u) << (lane & ~(G - 1)));
+}
+
+/* all codes of the group's words plain (A, C, G, T and the like)? */
+template <int G> __device__ bool wc_plain(const uint32_t *w, int n)
+{
+    const int lane = threadIdx.x & 31;
     uint32_t bad = 0;
-    for (int i = threadIdx.x & 31; i < n; i += 32) {
+    for (int i = lane & (G - 1); i < n; i += G) {
         const uint32_t x = w[i];
 #pragma unroll
         for (int k = 0; k < 8; k++) bad |= ~(WC_PLAIN >> ((x >> (4 * k)) & 15u)) & 1u;
     }
-    return __all_sync(0xFFFFFFFFu, bad == 0);
+    return (__ballot_sync(0xFFFFFFFFu, bad != 0) & gmask_of<G>(lane)) == 0;
 }
 
 __device__ void wc_score_table(uint2 *tab, const Scores &sc, bool local)
@@ -106,10 +125,10 @@ __device__ __forceinline__ bool rec_before(const WcRec &a, const WcRec &b)
     return a.v > b.v || (a.v == b.v && a.band < b.band);
 }
 
-__device__ __forceinline__ WcRec rec_reduce(WcRec r)
+template <int G> __device__ __forceinline__ WcRec rec_reduce(WcRec r)
 {
 #pragma unroll
-    for (int off = 16; off > 0; off >>= 1) {
+    for (int off = G / 2; off > 0; off >>= 1) {
         WcRec o;
         o.v = __shfl_xor_sync(0xFFFFFFFFu, r.v, off);
         o.band = __shfl_xor_sync(0xFFFFFFFFu, r.band, off);
@@ -145,13 +164,14 @@ __device__ __forceinline__ uint32_t dnib(int M, int diag, int H, int F, int E, c
  * qword(j), tword(T): the words the sweep reads (reversed for MODE 1).
  * bandmax: per-band maxima (written when SECOND pass 1, read in pass 2).
  */
-template <int MODE, bool TB, bool SECOND_PASS2, class QW, class TW>
+template <int G, int MODE, bool TB, bool SECOND_PASS2, class QW, class TW>
 __device__ void wc_sweep(QW qword, int qregs, TW tword, int tregs, int qlen, int tlen, const Scores &sc,
                          WcScore &S, uint32_t *ring, uint4 *tb, int stop, int *bandmax, bool write_bandmax,
                          WcRec &best_out, WcRec &sec_out, int &gscore)
 {
-    const int lane = threadIdx.x & 31;
-    const int rounds = (tregs + 31) >> 5;
+    const int lane = threadIdx.x & 31, gl = lane & (G - 1);
+    const unsigned gmask = gmask_of<G>(lane);
+    const int rounds = (tregs + G - 1) / G; /* 0 for a group without a pair */
     const bool local = MODE != 2;
     const int last_band = tregs - 1, last_row_in_band = tlen - 1 - ((tregs - 1) << 3);
     uint32_t out[8];
@@ -164,21 +184,24 @@ __device__ void wc_sweep(QW qword, int qregs, TW tword, int tregs, int qlen, int
     if (MODE == 2) best.v = 0;
     int bandbest = 0;
     int hit_round = 0x7fffffff;
-    const long steps = (long)rounds * qregs + 31;
+    const long gsteps = rounds > 0 && qregs > 0 ? (long)rounds * qregs + G - 1 : 0;
+    const long steps = G == 32 ? gsteps : (long)__reduce_max_sync(0xFFFFFFFFu, (unsigned)gsteps);
     for (long s = 0; s < steps; s++) {
-        const long rel = s - lane;
-        const int r = rel >= 0 ? (int)(rel / qregs) : -1;
+        const long rel = s - gl;
+        const int r = rel >= 0 && qregs > 0 ? (int)(rel / qregs) : -1;
         const int w = rel >= 0 ? (int)(rel - (long)r * qregs) : 0;
-        const int band = (r << 5) + lane;
-        const bool active = rel >= 0 && r < rounds && band < tregs;
-        /* stop once every lane is past the first round with a hit (s-based,
-         * so the whole warp leaves together) */
-        if (MODE == 1 && hit_round != 0x7fffffff && s >= (long)(hit_round + 1) * qregs + 31) break;
+        const int band = r * G + gl;
+        /* a group is done once its lanes are past the first round with a
+         * hit (MODE 1) or its sweep has ended; the warp leaves together */
+        const bool gdone = s >= gsteps || (MODE == 1 && hit_round != 0x7fffffff &&
+                                           s >= (long)(hit_round + 1) * qregs + G - 1);
+        if (MODE == 1 && (G == 32 ? gdone : __all_sync(0xFFFFFFFFu, gdone))) break;
+        const bool active = !gdone && rel >= 0 && r < rounds && band < tregs;
         /* inputs: bottom H/E of the band above at the 8 columns of word w */
         uint32_t in[8];
 #pragma unroll
-        for (int k = 0; k < 8; k++) in[k] = __shfl_up_sync(0xFFFFFFFFu, out[k], 1);
-        if (lane == 0 && active) {
+        for (int k = 0; k < 8; k++) in[k] = __shfl_up_sync(0xFFFFFFFFu, out[k], 1, G);
+        if (gl == 0 && active) {
             if (r == 0) {
 #pragma unroll
                 for (int k = 0; k < 8; k++) {
@@ -272,7 +295,7 @@ __device__ void wc_sweep(QW qword, int qregs, TW tword, int tregs, int qlen, int
                 tp[0] = make_uint4(dir[0], dir[1], dir[2], dir[3]);
                 tp[1] = make_uint4(dir[4], dir[5], dir[6], dir[7]);
             }
-            if (lane == 31) {
+            if (gl == G - 1) {
 #pragma unroll
                 for (int k = 0; k < 8; k++) ring[(w << 3) + k] = out[k];
             }
@@ -280,13 +303,11 @@ __device__ void wc_sweep(QW qword, int qregs, TW tword, int tregs, int qlen, int
         }
         __syncwarp();
         if (MODE == 1) {
-            /* a band reaching the forward score ends the sweep after its round */
+            /* a band reaching the forward score ends the group's sweep after its round */
             const bool hit = active && w == qregs - 1 && bandbest >= stop;
-            const unsigned m = __ballot_sync(0xFFFFFFFFu, hit);
-            if (m) {
-                const int hr = __shfl_sync(0xFFFFFFFFu, r, __ffs(m) - 1);
-                if (hr < hit_round) hit_round = hr;
-            }
+            const unsigned m = __ballot_sync(0xFFFFFFFFu, hit) & gmask;
+            const int hr = __shfl_sync(0xFFFFFFFFu, r, m ? __ffs(m) - 1 : lane);
+            if (m && hr < hit_round) hit_round = hr;
         }
     }
     best_out = best;
@@ -301,14 +322,15 @@ __device__ void wc_sweep(QW qword, int qregs, TW tword, int tregs, int qlen, int
  * reversed words, bands counted from T0 for the left boundary, leaving after
  * the first round whose bands reach `stop` at the last column.
  */
-template <bool START_PASS, bool OPEN_NN, class QW, class TW>
+template <int G, bool START_PASS, bool OPEN_NN, class QW, class TW>
 __device__ void wc_semi_sweep(QW qword, int qregs, TW tword, int tregs, int T0, int qlen, const Scores &sc,
                               int head, WcScore &S, uint32_t *ring, int *lastcol, int stop)
 {
-    const int lane = threadIdx.x & 31;
+    const int lane = threadIdx.x & 31, gl = lane & (G - 1);
+    const unsigned gmask = gmask_of<G>(lane);
     const int nb = tregs - T0;
-    if (nb <= 0) return;
-    const int rounds = (nb + 31) >> 5;
+    if (G == 32 && nb <= 0) return;
+    const int rounds = nb > 0 ? (nb + G - 1) / G : 0;
     const bool free_head_t = (head == TARGET_ || head == BOTH_);
     const bool zero_rows = (head == QUERY_ || head == BOTH_);
     uint32_t out[8];
@@ -320,18 +342,21 @@ __device__ void wc_semi_sweep(QW qword, int qregs, TW tword, int tregs, int T0, 
     int up_prev = 0;
     int hit_round = 0x7fffffff;
     const int lastw = (qlen - 1) >> 3, lastb = (qlen - 1) & 7;
-    const long steps = (long)rounds * qregs + 31;
+    const long gsteps = rounds > 0 && qregs > 0 ? (long)rounds * qregs + G - 1 : 0;
+    const long steps = G == 32 ? gsteps : (long)__reduce_max_sync(0xFFFFFFFFu, (unsigned)gsteps);
     for (long st = 0; st < steps; st++) {
-        const long rel = st - lane;
-        const int r = rel >= 0 ? (int)(rel / qregs) : -1;
+        const long rel = st - gl;
+        const int r = rel >= 0 && qregs > 0 ? (int)(rel / qregs) : -1;
         const int w = rel >= 0 ? (int)(rel - (long)r * qregs) : 0;
-        const int brel = (r << 5) + lane;
-        const bool active = rel >= 0 && r < rounds && brel < nb;
-        if (START_PASS && hit_round != 0x7fffffff && st >= (long)(hit_round + 1) * qregs + 31) break;
+        const int brel = r * G + gl;
+        const bool gdone = st >= gsteps || (START_PASS && hit_round != 0x7fffffff &&
+                                            st >= (long)(hit_round + 1) * qregs + G - 1);
+        if (START_PASS && (G == 32 ? gdone : __all_sync(0xFFFFFFFFu, gdone))) break;
+        const bool active = !gdone && rel >= 0 && r < rounds && brel < nb;
         uint32_t in[8];
 #pragma unroll
-        for (int k = 0; k < 8; k++) in[k] = __shfl_up_sync(0xFFFFFFFFu, out[k], 1);
-        if (lane == 0 && active) {
+        for (int k = 0; k < 8; k++) in[k] = __shfl_up_sync(0xFFFFFFFFu, out[k], 1, G);
+        if (gl == 0 && active) {
             if (r == 0) {
 #pragma unroll
                 for (int k = 0; k < 8; k++) {
@@ -408,18 +433,16 @@ __device__ void wc_semi_sweep(QW qword, int qregs, TW tword, int tregs, int T0, 
                 }
             }
             D[0] = up_prev;
-            if (lane == 31) {
+            if (gl == G - 1) {
 #pragma unroll
                 for (int k = 0; k < 8; k++) ring[(w << 3) + k] = out[k];
             }
         }
         __syncwarp();
         if (START_PASS) {
-            const unsigned m = __ballot_sync(0xFFFFFFFFu, hit);
-            if (m) {
-                const int hr = __shfl_sync(0xFFFFFFFFu, r, __ffs(m) - 1);
-                if (hr < hit_round) hit_round = hr;
-            }
+            const unsigned m = __ballot_sync(0xFFFFFFFFu, hit) & gmask;
+            const int hr = __shfl_sync(0xFFFFFFFFu, r, m ? __ffs(m) - 1 : lane);
+            if (m && hr < hit_round) hit_round = hr;
         }
     }
     __syncwarp();
@@ -428,28 +451,31 @@ __device__ void wc_semi_sweep(QW qword, int qregs, TW tword, int tregs, int T0, 
 /* First maximum (strict >, row order) of lastcol over rows [r0, r1) with the
  * reference's initial best NEG16 / row `row0`; with SECOND also its second
  * best (a row qualifies when below every earlier row's value). */
-template <bool SECOND>
+template <int G, bool SECOND>
 __device__ void wc_lastcol_scan(const int *lastcol, int r0, int r1, int row0, int &best, int &brow, int &sec,
                                 int &srow)
 {
-    const int lane = threadIdx.x & 31;
+    const int lane = threadIdx.x & 31, gl = lane & (G - 1);
     best = NEG16W, brow = row0, sec = NEG16W, srow = row0;
     int carry = NEG16W; /* max of the rows before the chunk */
-    for (int base = r0; base < r1; base += 32) {
-        const int row = base + lane;
+    const int chunks = r1 > r0 ? (r1 - r0 + G - 1) / G : 0;
+    const int nchunks = G == 32 ? chunks : (int)__reduce_max_sync(0xFFFFFFFFu, (unsigned)chunks);
+    for (int ch = 0; ch < nchunks; ch++) {
+        const int base = r0 + ch * G;
+        const int row = base + gl;
         const int h = row < r1 ? lastcol[row] : NEG16W - 1;
         int pm = h; /* inclusive prefix max within the chunk */
 #pragma unroll
-        for (int off = 1; off < 32; off <<= 1) {
-            const int o = __shfl_up_sync(0xFFFFFFFFu, pm, off);
-            if (lane >= off) pm = max(pm, o);
+        for (int off = 1; off < G; off <<= 1) {
+            const int o = __shfl_up_sync(0xFFFFFFFFu, pm, off, G);
+            if (gl >= off) pm = max(pm, o);
         }
-        int before = __shfl_up_sync(0xFFFFFFFFu, pm, 1);
-        before = lane == 0 ? carry : max(before, carry);
+        int before = __shfl_up_sync(0xFFFFFFFFu, pm, 1, G);
+        before = gl == 0 ? carry : max(before, carry);
         /* chunk argmax, first row on ties */
         int bv = h, br = row;
 #pragma unroll
-        for (int off = 16; off > 0; off >>= 1) {
+        for (int off = G / 2; off > 0; off >>= 1) {
             const int ov = __shfl_xor_sync(0xFFFFFFFFu, bv, off), orow = __shfl_xor_sync(0xFFFFFFFFu, br, off);
             if (ov > bv || (ov == bv && orow < br)) bv = ov, br = orow;
         }
@@ -458,45 +484,55 @@ __device__ void wc_lastcol_scan(const int *lastcol, int r0, int r1, int row0, in
             const bool q = row < r1 && h < before && h > NEG16W;
             int sv = q ? h : NEG16W - 1, sr = row;
 #pragma unroll
-            for (int off = 16; off > 0; off >>= 1) {
+            for (int off = G / 2; off > 0; off >>= 1) {
                 const int ov = __shfl_xor_sync(0xFFFFFFFFu, sv, off), orow = __shfl_xor_sync(0xFFFFFFFFu, sr, off);
                 if (ov > sv || (ov == sv && orow < sr)) sv = ov, sr = orow;
             }
             if (sv > sec) sec = sv, srow = sr;
         }
-        carry = max(carry, __shfl_sync(0xFFFFFFFFu, pm, 31));
+        carry = max(carry, __shfl_sync(0xFFFFFFFFu, pm, gbase_of<G>(lane) + G - 1));
     }
 }
 
-template <bool SECOND, bool START>
+template <int G, bool SECOND, bool START>
 __global__ void __launch_bounds__(128) dp_wc_semi_kernel(DpArgs a, const uint32_t *list, int nlist, int ring_cols)
 {
+    constexpr int NG = 32 / G; /* pairs per warp */
     extern __shared__ uint32_t wc_smem[];
     __shared__ uint2 tab[16];
     wc_score_table(tab, a.sc, true);
     __syncthreads();
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, gl = lane & (G - 1), gi = lane / G;
+    const unsigned gmask = gmask_of<G>(lane);
     const int warps_per_block = blockDim.x >> 5;
-    uint32_t *ring = wc_smem + (size_t)warp * ring_cols;
-    int *lastcol = (int *)(wc_smem + (size_t)warps_per_block * ring_cols) + (size_t)warp * a.scratch_cols;
+    const int slot = warp * NG + gi; /* this group's ring and last-column buffer */
+    uint32_t *ring = wc_smem + (size_t)slot * ring_cols;
+    int *lastcol = (int *)(wc_smem + (size_t)warps_per_block * NG * ring_cols) + (size_t)slot * a.scratch_cols;
     const bool fast_scores = a.sc.match >= -128 && a.sc.match <= 127 && a.sc.mismatch >= -127 && a.sc.mismatch <= 128;
     const bool open_nn = a.sc.o >= 0;
-    for (int item = blockIdx.x * warps_per_block + warp; item < nlist; item += gridDim.x * warps_per_block) {
-        const int i = (int)list[item];
-        const int qlen = (int)a.q_len[i], tlen = (int)a.t_len[i];
-        const uint32_t *q = a.pq + (a.q_off[i] >> 3);
-        const uint32_t *t = a.pt + (a.t_off[i] >> 3);
+    for (int item0 = (blockIdx.x * warps_per_block + warp) * NG; item0 < nlist;
+         item0 += gridDim.x * warps_per_block * NG) {
+        const int item = item0 + gi;
+        const bool has = item < nlist; /* the last warp may have groups without a pair */
+        const int i = has ? (int)list[item] : 0;
+        const int qlen = has ? (int)a.q_len[i] : 0, tlen = has ? (int)a.t_len[i] : 0;
+        const uint32_t *q = a.pq + (has ? (a.q_off[i] >> 3) : 0);
+        const uint32_t *t = a.pt + (has ? (a.t_off[i] >> 3) : 0);
         const int qregs = (qlen + 7) >> 3, tregs = (tlen + 7) >> 3;
         WcScore S;
         S.local = true;
         S.tab = tab;
-        S.fast = fast_scores && wc_plain(q, qregs) && wc_plain(t, tregs);
+        S.fast = fast_scores;
+        S.fast = wc_plain<G>(q, qregs) && S.fast;
+        S.fast = wc_plain<G>(t, tregs) && S.fast;
         auto qf = [&](int j) { return q[j]; };
         auto tf = [&](int T) { return t[T]; };
-        if (open_nn) wc_semi_sweep<false, true>(qf, qregs, tf, tregs, 0, qlen, a.sc, a.head, S, ring, lastcol, 0);
-        else wc_semi_sweep<false, false>(qf, qregs, tf, tregs, 0, qlen, a.sc, a.head, S, ring, lastcol, 0);
+        if (open_nn)
+            wc_semi_sweep<G, false, true>(qf, qregs, tf, tregs, 0, qlen, a.sc, a.head, S, ring, lastcol, 0);
+        else
+            wc_semi_sweep<G, false, false>(qf, qregs, tf, tregs, 0, qlen, a.sc, a.head, S, ring, lastcol, 0);
         int best, brow, sec, srow;
-        wc_lastcol_scan<SECOND>(lastcol, 0, tlen, qlen, best, brow, sec, srow);
+        wc_lastcol_scan<G, SECOND>(lastcol, 0, tlen, qlen, best, brow, sec, srow);
         int t_start = 0, q_start = 0;
         if (START) {
             const int x = tregs - ((brow >> 3) + 1);
@@ -506,28 +542,35 @@ __global__ void __launch_bounds__(128) dp_wc_semi_kernel(DpArgs a, const uint32_
             auto rt = [&](int T) { return rev_window(t, tlen - 8 - (T << 3)); };
             __syncwarp();
             if (open_nn)
-                wc_semi_sweep<true, true>(rq, qregs, rt, tregs, gend_reg, qlen, a.sc, a.head, S, ring, lastcol, best);
+                wc_semi_sweep<G, true, true>(rq, qregs, rt, tregs, gend_reg, qlen, a.sc, a.head, S, ring, lastcol,
+                                             best);
             else
-                wc_semi_sweep<true, false>(rq, qregs, rt, tregs, gend_reg, qlen, a.sc, a.head, S, ring, lastcol,
-                                           best);
+                wc_semi_sweep<G, true, false>(rq, qregs, rt, tregs, gend_reg, qlen, a.sc, a.head, S, ring, lastcol,
+                                              best);
             /* rows up to the end of the first band that reached the forward score */
             const int r0 = gend_reg << 3;
             int r1 = min(tregs << 3, tlen);
-            for (int base = r0; base < r1; base += 32) {
-                const int row = base + lane;
-                const unsigned m = __ballot_sync(0xFFFFFFFFu, row < r1 && lastcol[row] >= best);
+            const int chunks = r1 > r0 ? (r1 - r0 + G - 1) / G : 0;
+            const int nchunks = G == 32 ? chunks : (int)__reduce_max_sync(0xFFFFFFFFu, (unsigned)chunks);
+            bool found = false;
+            for (int ch = 0; ch < nchunks; ch++) {
+                const int base = r0 + ch * G;
+                const int row = base + gl;
+                const unsigned m =
+                    __ballot_sync(0xFFFFFFFFu, !found && row < r1 && lastcol[row] >= best) & gmask;
                 if (m) {
-                    const int hit = base + __ffs(m) - 1;
+                    const int hit = base + (__ffs(m) - 1 - gbase_of<G>(lane));
                     r1 = min(r1, ((hit >> 3) + 1) << 3);
-                    break;
+                    found = true;
                 }
+                if (G == 32 && found) break;
             }
             int bb, bbrow, s2, s2r;
-            wc_lastcol_scan<false>(lastcol, r0, r1, 0, bb, bbrow, s2, s2r);
+            wc_lastcol_scan<G, false>(lastcol, r0, r1, 0, bb, bbrow, s2, s2r);
             t_start = (tlen - 1) - bbrow;
             q_start = (qlen - 1) - tlen;
         }
-        if (lane == 0) {
+        if (gl == 0 && has) {
             if (a.score) a.score[i] = best;
             if (a.t_end) a.t_end[i] = brow;
             if (a.q_end) a.q_end[i] = tlen;
@@ -549,99 +592,111 @@ __global__ void __launch_bounds__(128) dp_wc_semi_kernel(DpArgs a, const uint32_
 
 /* ---------------------------------------------------------------------- */
 
-template <int ALGO, int START, bool SECOND>
+template <int G, int ALGO, int START, bool SECOND>
 __global__ void __launch_bounds__(128) dp_wc_kernel(DpArgs a, const uint32_t *list, int nlist, int ring_cols)
 {
+    constexpr int NG = 32 / G; /* pairs per warp */
     extern __shared__ uint32_t wc_smem[];
     __shared__ uint2 tab[16];
     wc_score_table(tab, a.sc, ALGO == LOCAL_);
     __syncthreads();
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, gl = lane & (G - 1), gi = lane / G;
     const int warps_per_block = blockDim.x >> 5;
-    uint32_t *ring = wc_smem + (size_t)warp * ring_cols;
-    int *bandmax = (int *)(wc_smem + (size_t)warps_per_block * ring_cols) + (size_t)warp * a.scratch_cols;
+    const int slot = warp * NG + gi; /* this group's ring and band maxima */
+    uint32_t *ring = wc_smem + (size_t)slot * ring_cols;
+    int *bandmax = (int *)(wc_smem + (size_t)warps_per_block * NG * ring_cols) + (size_t)slot * a.scratch_cols;
     const bool fast_scores = a.sc.match >= -128 && a.sc.match <= 127 && a.sc.mismatch >= -127 && a.sc.mismatch <= 128;
-    for (int item = blockIdx.x * warps_per_block + warp; item < nlist; item += gridDim.x * warps_per_block) {
-        const int i = (int)list[item];
-        const int qlen = (int)a.q_len[i], tlen = (int)a.t_len[i];
-        const uint32_t *q = a.pq + (a.q_off[i] >> 3);
-        const uint32_t *t = a.pt + (a.t_off[i] >> 3);
+    for (int item0 = (blockIdx.x * warps_per_block + warp) * NG; item0 < nlist;
+         item0 += gridDim.x * warps_per_block * NG) {
+        const int item = item0 + gi;
+        const bool has = item < nlist; /* the last warp may have groups without a pair */
+        const int i = has ? (int)list[item] : 0;
+        const int qlen = has ? (int)a.q_len[i] : 0, tlen = has ? (int)a.t_len[i] : 0;
+        const uint32_t *q = a.pq + (has ? (a.q_off[i] >> 3) : 0);
+        const uint32_t *t = a.pt + (has ? (a.t_off[i] >> 3) : 0);
         const int qregs = (qlen + 7) >> 3, tregs = (tlen + 7) >> 3;
         WcScore S;
         S.local = ALGO == LOCAL_;
         S.tab = tab;
-        S.fast = fast_scores && wc_plain(q, qregs) && wc_plain(t, tregs);
+        S.fast = fast_scores;
+        S.fast = wc_plain<G>(q, qregs) && S.fast;
+        S.fast = wc_plain<G>(t, tregs) && S.fast;
         uint4 *tb = nullptr;
-        if (START == WITH_TB_) {
+        if (START == WITH_TB_ && has) {
             tb = a.tb + a.tb_off[i];
             uint4 *z = tb + (size_t)tregs * 2 * qregs;
-            for (int k = lane; k < 4 * qregs; k += 32) z[k] = make_uint4(0, 0, 0, 0);
+            for (int k = gl; k < 4 * qregs; k += G) z[k] = make_uint4(0, 0, 0, 0);
         }
         auto qf = [&](int j) { return q[j]; };
         auto tf = [&](int T) { return t[T]; };
         WcRec best, sec;
         int gscore = 0;
         if (ALGO == GLOBAL_) {
-            wc_sweep<2, START == WITH_TB_, false>(qf, qregs, tf, tregs, qlen, tlen, a.sc, S, ring, tb, 0, bandmax,
-                                                  false, best, sec, gscore);
+            wc_sweep<G, 2, START == WITH_TB_, false>(qf, qregs, tf, tregs, qlen, tlen, a.sc, S, ring, tb, 0,
+                                                     bandmax, false, best, sec, gscore);
             /* the owner lane of the last band holds the score */
-            const int owner = (tregs - 1) & 31;
+            const int owner = gbase_of<G>(lane) + ((tregs - 1) & (G - 1));
             gscore = __shfl_sync(0xFFFFFFFFu, gscore, owner);
-            if (lane == 0 && a.score) a.score[i] = gscore;
+            if (gl == 0 && has && a.score) a.score[i] = gscore;
             continue;
         }
         /* LOCAL forward (pass 1 also records per-band maxima for second best) */
-        wc_sweep<0, START == WITH_TB_, false>(qf, qregs, tf, tregs, qlen, tlen, a.sc, S, ring, tb, 0, bandmax,
-                                              SECOND, best, sec, gscore);
-        best = rec_reduce(best);
+        wc_sweep<G, 0, START == WITH_TB_, false>(qf, qregs, tf, tregs, qlen, tlen, a.sc, S, ring, tb, 0, bandmax,
+                                                 SECOND, best, sec, gscore);
+        best = rec_reduce<G>(best);
         WcRec secr = {0, 0x7fffffff, 0, 0};
         if (SECOND) {
             __syncwarp();
             /* exclusive prefix maximum over bands, in place */
             int carry = 0;
-            for (int base = 0; base < tregs; base += 32) {
-                const int b = base + lane;
+            const int chunks = (tregs + G - 1) / G;
+            const int nchunks = G == 32 ? chunks : (int)__reduce_max_sync(0xFFFFFFFFu, (unsigned)chunks);
+            for (int ch = 0; ch < nchunks; ch++) {
+                const int b = ch * G + gl;
                 int v = b < tregs ? bandmax[b] : 0;
 #pragma unroll
-                for (int off = 1; off < 32; off <<= 1) {
-                    const int o = __shfl_up_sync(0xFFFFFFFFu, v, off);
-                    if (lane >= off) v = max(v, o);
+                for (int off = 1; off < G; off <<= 1) {
+                    const int o = __shfl_up_sync(0xFFFFFFFFu, v, off, G);
+                    if (gl >= off) v = max(v, o);
                 }
                 v = max(v, carry);
                 if (b < tregs) bandmax[b] = v;
-                carry = __shfl_sync(0xFFFFFFFFu, v, 31);
+                carry = __shfl_sync(0xFFFFFFFFu, v, gbase_of<G>(lane) + G - 1);
             }
             __syncwarp();
             WcRec b2, s2;
             int g2 = 0;
-            wc_sweep<0, false, true>(qf, qregs, tf, tregs, qlen, tlen, a.sc, S, ring, nullptr, 0, bandmax, false,
-                                     b2, s2, g2);
-            secr = rec_reduce(s2);
+            wc_sweep<G, 0, false, true>(qf, qregs, tf, tregs, qlen, tlen, a.sc, S, ring, nullptr, 0, bandmax, false,
+                                        b2, s2, g2);
+            secr = rec_reduce<G>(s2);
         }
         int qs = 0, ts = 0;
-        if (START == WITH_START_ && best.v > 0) {
-            const int rend_reg = min((best.col >> 3) + 1, qregs);
-            const int gend_reg = min((best.row >> 3) + 1, tregs);
+        if (START == WITH_START_) {
+            /* groups whose reverse region spans at least G words sweep it;
+             * the others (and groups without a hit) pass an empty sweep */
+            const int rend_reg = best.v > 0 ? min((best.col >> 3) + 1, qregs) : 0;
+            const int gend_reg = best.v > 0 ? min((best.row >> 3) + 1, tregs) : 0;
+            const bool sweep = rend_reg >= G;
             auto qr = [&](int j) { return nrev(q[rend_reg - 1 - j]); };
             auto tr = [&](int T) { return nrev(t[gend_reg - 1 - T]); };
             WcRec bs, ss;
             int g3 = 0;
-            if (rend_reg >= 32) {
-                wc_sweep<1, false, false>(qr, rend_reg, tr, gend_reg, 0, 0, a.sc, S, ring, nullptr, best.v, bandmax,
-                                          false, bs, ss, g3);
-                bs = rec_reduce(bs);
+            wc_sweep<G, 1, false, false>(qr, sweep ? rend_reg : 0, tr, sweep ? gend_reg : 0, 0, 0, a.sc, S, ring,
+                                         nullptr, best.v, bandmax, false, bs, ss, g3);
+            bs = rec_reduce<G>(bs);
+            if (sweep) {
                 /* reversed coordinates -> what the reference records */
                 const int gidx = (gend_reg << 3) - 1 - (bs.band << 3);
                 ts = gidx + (bs.row - (bs.band << 3));
                 qs = (rend_reg << 3) - 1 - bs.col;
-            } else {
-                /* reverse region narrower than 32 words (the ring's reader
-                 * must trail its writer): lane 0 runs the one-thread start
-                 * pass with the warp's ring as row buffer.  It stops at the
-                 * first cell reaching the score -- for the short local hits
-                 * that end this early, a few bands -- where the warp would
-                 * finish a 32-band round. */
-                if (lane == 0) {
+            } else if (best.v > 0) {
+                /* reverse region narrower than G words (the ring's reader
+                 * must trail its writer): the group's first lane runs the
+                 * one-thread start pass with the group's ring as row buffer.
+                 * It stops at the first cell reaching the score -- for the
+                 * short local hits that end this early, a few bands -- where
+                 * the group would finish a G-band round. */
+                if (gl == 0) {
                     RowBuf rb{ring, 1u};
                     Res rr = {best.v, best.col, best.row, 0, 0, 0, 0, 0};
                     if (S.fast) {
@@ -654,10 +709,10 @@ __global__ void __launch_bounds__(128) dp_wc_kernel(DpArgs a, const uint32_t *li
                     }
                     qs = rr.q_start, ts = rr.t_start;
                 }
-                __syncwarp();
             }
+            __syncwarp();
         }
-        if (lane == 0) {
+        if (gl == 0 && has) {
             if (a.score) a.score[i] = best.v;
             if (a.q_end) a.q_end[i] = best.v > 0 ? best.col : 0;
             if (a.t_end) a.t_end[i] = best.v > 0 ? best.row : 0;
@@ -674,72 +729,155 @@ __global__ void __launch_bounds__(128) dp_wc_kernel(DpArgs a, const uint32_t *li
     }
 }
 
-template <int ALGO, int START, bool SECOND>
+/* Shared memory of one block of the warp-cooperative kernels: 4 warps x 32/G
+ * groups, each with a ring of max_q8 words and, for LOCAL/GLOBAL, band
+ * maxima (max_t8/8 + 1 words) or, for SEMI_GLOBAL, the last column's H of
+ * every row (max_t8 + 8 words). */
+size_t wc_smem_bytes(int algo, int group, int max_q8, int max_t8)
+{
+    const size_t per = (size_t)max_q8 + (algo == SEMI_GLOBAL_ ? (size_t)max_t8 + 8 : (size_t)max_t8 / 8 + 1);
+    return (size_t)4 * (32 / group) * per * 4;
+}
+
+template <int G, int ALGO, int START, bool SECOND>
 static cudaError_t launch_wc_one(const DpArgs &a, const uint32_t *list, int nlist, int max_q8, int max_t8,
                                  cudaStream_t s)
 {
+    constexpr int NG = 32 / G;
     const int warps = 4, block = warps * 32;
     const int ring_cols = max_q8;
-    const size_t smem = (size_t)warps * ring_cols * 4 + (size_t)warps * (max_t8 / 8 + 1) * 4;
+    const size_t smem = wc_smem_bytes(ALGO, G, max_q8, max_t8);
     DpArgs b = a;
-    b.scratch_cols = (uint32_t)(max_t8 / 8 + 1); /* bandmax stride per warp */
-    auto k = dp_wc_kernel<ALGO, START, SECOND>;
+    b.scratch_cols = (uint32_t)(max_t8 / 8 + 1); /* bandmax stride per group */
+    auto k = dp_wc_kernel<G, ALGO, START, SECOND>;
     cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     int dev = 0, sms = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    int blocks = (nlist + warps - 1) / warps;
+    int blocks = (nlist + warps * NG - 1) / (warps * NG);
     if (blocks > sms * 16) blocks = sms * 16;
     k<<<blocks, block, smem, s>>>(b, list, nlist, ring_cols);
     return cudaGetLastError();
 }
 
-template <bool SECOND, bool START>
+template <int G, bool SECOND, bool START>
 static cudaError_t launch_wc_semi(const DpArgs &a, const uint32_t *list, int nlist, int max_q8, int max_t8,
                                   cudaStream_t s)
 {
+    constexpr int NG = 32 / G;
     const int warps = 4, block = warps * 32;
     const int ring_cols = max_q8;
     DpArgs b = a;
-    b.scratch_cols = (uint32_t)(max_t8 + 8); /* lastcol stride per warp */
-    const size_t smem = (size_t)warps * ring_cols * 4 + (size_t)warps * b.scratch_cols * 4;
-    auto k = dp_wc_semi_kernel<SECOND, START>;
+    b.scratch_cols = (uint32_t)(max_t8 + 8); /* lastcol stride per group */
+    const size_t smem = wc_smem_bytes(SEMI_GLOBAL_, G, max_q8, max_t8);
+    auto k = dp_wc_semi_kernel<G, SECOND, START>;
     cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     int dev = 0, sms = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    int blocks = (nlist + warps - 1) / warps;
+    int blocks = (nlist + warps * NG - 1) / (warps * NG);
     if (blocks > sms * 16) blocks = sms * 16;
     k<<<blocks, block, smem, s>>>(b, list, nlist, ring_cols);
     return cudaGetLastError();
 }
 
-cudaError_t launch_dp_wc(int algo, int start, bool second, const DpArgs &a, const uint32_t *list, int nlist,
-                         int max_q8, int max_t8, cudaStream_t s)
+template <int G>
+static cudaError_t launch_dp_wc_g(int algo, int start, bool second, const DpArgs &a, const uint32_t *list,
+                                  int nlist, int max_q8, int max_t8, cudaStream_t s)
 {
-    if (nlist <= 0) return cudaSuccess;
     if (algo == SEMI_GLOBAL_) {
         if (start == WITH_START_)
-            return second ? launch_wc_semi<true, true>(a, list, nlist, max_q8, max_t8, s)
-                          : launch_wc_semi<false, true>(a, list, nlist, max_q8, max_t8, s);
-        return second ? launch_wc_semi<true, false>(a, list, nlist, max_q8, max_t8, s)
-                      : launch_wc_semi<false, false>(a, list, nlist, max_q8, max_t8, s);
+            return second ? launch_wc_semi<G, true, true>(a, list, nlist, max_q8, max_t8, s)
+                          : launch_wc_semi<G, false, true>(a, list, nlist, max_q8, max_t8, s);
+        return second ? launch_wc_semi<G, true, false>(a, list, nlist, max_q8, max_t8, s)
+                      : launch_wc_semi<G, false, false>(a, list, nlist, max_q8, max_t8, s);
     }
     if (algo == GLOBAL_)
-        return start == WITH_TB_ ? launch_wc_one<GLOBAL_, WITH_TB_, false>(a, list, nlist, max_q8, max_t8, s)
-                                 : launch_wc_one<GLOBAL_, WITHOUT_START_, false>(a, list, nlist, max_q8, max_t8, s);
+        return start == WITH_TB_ ? launch_wc_one<G, GLOBAL_, WITH_TB_, false>(a, list, nlist, max_q8, max_t8, s)
+                                 : launch_wc_one<G, GLOBAL_, WITHOUT_START_, false>(a, list, nlist, max_q8, max_t8,
+                                                                                    s);
     if (algo == LOCAL_) {
         if (start == WITH_START_)
-            return second ? launch_wc_one<LOCAL_, WITH_START_, true>(a, list, nlist, max_q8, max_t8, s)
-                          : launch_wc_one<LOCAL_, WITH_START_, false>(a, list, nlist, max_q8, max_t8, s);
+            return second ? launch_wc_one<G, LOCAL_, WITH_START_, true>(a, list, nlist, max_q8, max_t8, s)
+                          : launch_wc_one<G, LOCAL_, WITH_START_, false>(a, list, nlist, max_q8, max_t8, s);
         if (start == WITH_TB_)
-            return second ? launch_wc_one<LOCAL_, WITH_TB_, true>(a, list, nlist, max_q8, max_t8, s)
-                          : launch_wc_one<LOCAL_, WITH_TB_, false>(a, list, nlist, max_q8, max_t8, s);
-        return second ? launch_wc_one<LOCAL_, WITHOUT_START_, true>(a, list, nlist, max_q8, max_t8, s)
-                      : launch_wc_one<LOCAL_, WITHOUT_START_, false>(a, list, nlist, max_q8, max_t8, s);
+            return second ? launch_wc_one<G, LOCAL_, WITH_TB_, true>(a, list, nlist, max_q8, max_t8, s)
+                          : launch_wc_one<G, LOCAL_, WITH_TB_, false>(a, list, nlist, max_q8, max_t8, s);
+        return second ? launch_wc_one<G, LOCAL_, WITHOUT_START_, true>(a, list, nlist, max_q8, max_t8, s)
+                      : launch_wc_one<G, LOCAL_, WITHOUT_START_, false>(a, list, nlist, max_q8, max_t8, s);
     }
+    return cudaErrorInvalidValue;
+}
+
+/* resident blocks per SM of the warp-cooperative kernel for these options */
+template <int G>
+static int wc_blocks_g(int algo, int start, bool second, size_t smem)
+{
+    int n = 0;
+    cudaError_t e = cudaErrorInvalidValue;
+    auto occ = [&](auto k) {
+        if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) return;
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k, 128, smem);
+    };
+    if (algo == SEMI_GLOBAL_) {
+        if (start == WITH_START_) second ? occ(dp_wc_semi_kernel<G, true, true>) : occ(dp_wc_semi_kernel<G, false, true>);
+        else second ? occ(dp_wc_semi_kernel<G, true, false>) : occ(dp_wc_semi_kernel<G, false, false>);
+    } else if (algo == GLOBAL_) {
+        start == WITH_TB_ ? occ(dp_wc_kernel<G, GLOBAL_, WITH_TB_, false>)
+                          : occ(dp_wc_kernel<G, GLOBAL_, WITHOUT_START_, false>);
+    } else if (algo == LOCAL_) {
+        if (start == WITH_START_)
+            second ? occ(dp_wc_kernel<G, LOCAL_, WITH_START_, true>) : occ(dp_wc_kernel<G, LOCAL_, WITH_START_, false>);
+        else if (start == WITH_TB_)
+            second ? occ(dp_wc_kernel<G, LOCAL_, WITH_TB_, true>) : occ(dp_wc_kernel<G, LOCAL_, WITH_TB_, false>);
+        else
+            second ? occ(dp_wc_kernel<G, LOCAL_, WITHOUT_START_, true>)
+                   : occ(dp_wc_kernel<G, LOCAL_, WITHOUT_START_, false>);
+    }
+    if (e != cudaSuccess) {
+        cudaGetLastError(); /* a size the kernel cannot take: no resident block */
+        return 0;
+    }
+    return n;
+}
+
+int wc_blocks_per_sm(int algo, int start, bool second, int group, int max_q8, int max_t8)
+{
+    const size_t smem = wc_smem_bytes(algo, group, max_q8, max_t8);
+    if (smem > (200u << 10)) return 0;
+    if (group == 8) return wc_blocks_g<8>(algo, start, second, smem);
+    if (group == 16) return wc_blocks_g<16>(algo, start, second, smem);
+    if (group == 32) return wc_blocks_g<32>(algo, start, second, smem);
+    return 0;
+}
+
+/* Lane group for a launch: the smallest of 8 / 16 / 32 (at most max_group)
+ * that keeps at least 3/4 of the resident blocks the 32-lane kernel has --
+ * narrower groups waste fewer lanes on pipeline fill and drain but hold one
+ * ring (and band or last-column buffer) per pair, so long queries can cost
+ * occupancy.  SEMI_GLOBAL keeps 32 lanes: its per-group last-column buffer
+ * made the narrower groups slower on 250-1000 bp pairs.  0: none fits. */
+int wc_pick_group(int algo, int start, bool second, int max_q8, int max_t8, int max_group)
+{
+    const int b32 = max_group >= 32 ? wc_blocks_per_sm(algo, start, second, 32, max_q8, max_t8) : 0;
+    if (algo == SEMI_GLOBAL_) return b32 > 0 ? 32 : 0;
+    for (int g : {8, 16}) {
+        if (g > max_group) break;
+        const int bg = wc_blocks_per_sm(algo, start, second, g, max_q8, max_t8);
+        if (bg > 0 && (b32 == 0 || 4 * bg >= 3 * b32)) return g;
+    }
+    return b32 > 0 ? 32 : 0;
+}
+
+cudaError_t launch_dp_wc(int algo, int start, bool second, const DpArgs &a, const uint32_t *list, int nlist,
+                         int max_q8, int max_t8, int group, cudaStream_t s)
+{
+    if (nlist <= 0) return cudaSuccess;
+    if (group == 8) return launch_dp_wc_g<8>(algo, start, second, a, list, nlist, max_q8, max_t8, s);
+    if (group == 16) return launch_dp_wc_g<16>(algo, start, second, a, list, nlist, max_q8, max_t8, s);
+    if (group == 32) return launch_dp_wc_g<32>(algo, start, second, a, list, nlist, max_q8, max_t8, s);
     return cudaErrorInvalidValue;
 }
 

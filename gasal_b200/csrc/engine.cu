@@ -170,7 +170,10 @@ int plan_batch(const RunCfg &cfg, const DevBatch &b, const DevOut &o, Workspace 
     const bool wc_algo = cfg.algo == LOCAL_ || cfg.algo == GLOBAL_ || (cfg.algo == SEMI_GLOBAL_ && cfg.tail == TARGET_);
     uint32_t max_q_short = 0, max_q_long = 0, max_t_long = 0;
     int nlong = 0;
-    p.wc_min_q = (uint32_t)st.wc_min_qregs * 8 - 7;
+    /* a pair needs at least as many query words as its lane group (the
+     * group's ring reader must trail its writer) */
+    const int min_words = std::max(st.wc_min_qregs, st.wc_group > 0 ? st.wc_group : 8);
+    p.wc_min_q = (uint32_t)min_words * 8 - 7;
     for (int i = 0; i < b.n; i++) {
         const uint32_t ql = b.h_q_len[i];
         if (wc_algo && ql >= p.wc_min_q) {
@@ -181,12 +184,22 @@ int plan_batch(const RunCfg &cfg, const DevBatch &b, const DevOut &o, Workspace 
             max_q_short = std::max(max_q_short, ql);
         }
     }
-    /* the warp kernel's shared memory: 4 warps x (ring of q8 words + band
-     * maxima, or for SEMI_GLOBAL the last-column H of every row) */
-    const size_t t_words = cfg.algo == SEMI_GLOBAL_ ? (size_t)max_t_long + 16 : ((size_t)max_t_long + 8) / 8 + 1;
-    const size_t wc_smem = 4 * (((size_t)max_q_long + 8) + t_words) * 4;
-    p.use_wc = nlong > 0 && b.n >= st.min_order_pairs && ((max_q_long + 7) & ~7u) <= (uint32_t)st.wc_max_q8 &&
-               wc_smem <= (200u << 10);
+    /* lane group of the warp kernel: forced, or the narrowest that keeps its
+     * occupancy (each group holds a ring of q8 words and band maxima, or for
+     * SEMI_GLOBAL the last-column H of every row, in shared memory) */
+    {
+        const int wstart = (cfg.algo == SEMI_GLOBAL_ && cfg.start == WITH_TB_) ? WITHOUT_START_ : cfg.start;
+        const bool wsecond = cfg.second && (cfg.algo == LOCAL_ || cfg.algo == SEMI_GLOBAL_);
+        const int mq8 = (int)((max_q_long + 7) & ~7u), mt8 = (int)((max_t_long + 7) & ~7u);
+        p.wc_group = 0;
+        if (nlong > 0 && b.n >= st.min_order_pairs && mq8 <= st.wc_max_q8) {
+            if (st.wc_group > 0)
+                p.wc_group = wc_blocks_per_sm(cfg.algo, wstart, wsecond, st.wc_group, mq8, mt8) > 0 ? st.wc_group : 0;
+            else
+                p.wc_group = wc_pick_group(cfg.algo, wstart, wsecond, mq8, mt8, min_words >= 32 ? 32 : min_words >= 16 ? 16 : 8);
+        }
+    }
+    p.use_wc = p.wc_group > 0;
     if (!p.use_wc) {
         max_q_short = std::max(max_q_short, max_q_long);
         nlong = 0;
@@ -408,7 +421,7 @@ static int launch_dp_split(int algo, int start, bool second, const Plan &p, DpAr
         GB_CUDA(cudaEventRecord(ws.fork, s));
         GB_CUDA(cudaStreamWaitEvent(ws.aux, ws.fork, 0));
         timing_mark(K_DP, true, ws.aux);
-        GB_CUDA(launch_dp_wc(algo, start, second, a, order, nlong, p.mq8, p.mt8, ws.aux));
+        GB_CUDA(launch_dp_wc(algo, start, second, a, order, nlong, p.mq8, p.mt8, p.wc_group, ws.aux));
         timing_mark(K_DP, false, ws.aux);
         GB_CUDA(cudaEventRecord(ws.join, ws.aux));
         DpArgs rest = a;

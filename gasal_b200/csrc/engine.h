@@ -88,6 +88,7 @@ struct Plan {
     bool tb = false, second = false, use_wc = false, order_on = false;
     int start = 0, block = 64, mq8 = 0, mt8 = 0;
     uint32_t wc_min_q = 0;
+    int wc_group = 32;
     int ksw_slots[2] = {0, 0}; /* [0] > 0: ksw runs warp-per-pair; eh columns per warp of the two length classes */
     bool tier2 = false;     /* one-thread pairs split: short ones with shared-memory rows (a), long ones
                                with global rows on a small grid (tier2_* overrides of a) */
@@ -128,6 +129,8 @@ struct Settings {
     int ksw_wc = 1;             /* ksw pairs run warp-per-pair (ksw_wc.cu) */
     int split_start = 1;        /* one-thread LOCAL/SEMI_GLOBAL start passes run as their own launch,
                                    pairs re-ordered by forward score */
+    int wc_group = 0;           /* lanes per pair in the warp-cooperative kernels: 32, 16 or 8, or 0 to pick
+                                   per launch from the kernel's occupancy */
     int persistent = 1;         /* one-thread launches pull pairs from a device counter; 0: one thread per
                                    pair on a grid over the batch */
     const void *band_model = nullptr; /* installed band MLP (BF16 parameters on the device) */

@@ -89,10 +89,17 @@ cudaError_t launch_order(const uint32_t *q_len, const uint32_t *t_len, int n, ui
 cudaError_t launch_start_order(const uint32_t *q_len, const int32_t *q_end, const int32_t *score, int n,
                                uint32_t q_cut, uint32_t *bins, uint32_t *order, cudaStream_t s);
 
-/* warp-cooperative DP (dp_wc.cu) for the pairs listed in `list`: LOCAL and
- * GLOBAL; queries of at least 32 words */
+/* warp-cooperative DP (dp_wc.cu) for the pairs listed in `list`: LOCAL,
+ * GLOBAL and target-tail SEMI_GLOBAL, each pair on `group` lanes (32, 16 or
+ * 8; queries of at least `group` words) */
 cudaError_t launch_dp_wc(int algo, int start, bool second, const DpArgs &a, const uint32_t *list, int nlist,
-                         int max_q8, int max_t8, cudaStream_t s);
+                         int max_q8, int max_t8, int group, cudaStream_t s);
+/* dynamic shared memory of one warp-cooperative block */
+size_t wc_smem_bytes(int algo, int group, int max_q8, int max_t8);
+/* resident blocks per SM of that kernel (0: it cannot run at these sizes) */
+int wc_blocks_per_sm(int algo, int start, bool second, int group, int max_q8, int max_t8);
+/* the lane group a launch uses when none is forced (0: none fits) */
+int wc_pick_group(int algo, int start, bool second, int max_q8, int max_t8, int max_group);
 
 /* the global-scratch DP variant on a caller-chosen grid */
 cudaError_t launch_dp_scratch_grid(int algo, int start, bool second, const DpArgs &a, int block, int blocks,

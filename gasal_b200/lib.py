@@ -49,7 +49,8 @@ class GbDevOut(C.Structure):
 
 class GbTuning(C.Structure):
     _fields_ = [("block", C.c_int32), ("wc_min_qregs", C.c_int32), ("min_order_pairs", C.c_int32),
-                ("ksw_warp", C.c_int32), ("split_start", C.c_int32), ("persistent", C.c_int32)]
+                ("ksw_warp", C.c_int32), ("split_start", C.c_int32), ("persistent", C.c_int32),
+                ("wc_group", C.c_int32)]
 
 
 class GbBandStats(C.Structure):
@@ -184,7 +185,7 @@ PLAIN_FORM = dict(min_order_pairs=1 << 30, ksw_warp=0, split_start=0, persistent
 
 
 def set_tuning(**kw):
-    """Change any of block, wc_min_qregs, min_order_pairs, ksw_warp, split_start, persistent."""
+    """Change any of block, wc_min_qregs, min_order_pairs, ksw_warp, split_start, persistent, wc_group."""
     cur = get_tuning()
     bad = set(kw) - set(cur)
     if bad:

@@ -214,7 +214,8 @@ int gb_graph_stats(int64_t *counts);
 /* Launch tuning (no reference counterpart).  block: threads per block of the
  * one-pair-per-thread DP kernel (32, 64 or 128); wc_min_qregs: pairs
  * whose query has at least this many 8-base words run warp-cooperative
- * (LOCAL/GLOBAL; at least 32, which that kernel needs); min_order_pairs: batches with at least this many pairs are
+ * (LOCAL/GLOBAL/target-tail SEMI_GLOBAL; at least 8, and never fewer than
+ * wc_group, which that kernel needs); min_order_pairs: batches with at least this many pairs are
  * visited length-binned.  Results never depend on these. */
 typedef struct {
     int32_t block;
@@ -227,13 +228,18 @@ typedef struct {
                               device counter (default); 0: one thread per pair on a grid over the batch.
                               With min_order_pairs above the batch size, ksw_warp 0 and split_start 0
                               this is the plain full-DP form: every pair one per thread, in input order */
+    int32_t wc_group;      /* lanes per pair in the warp-cooperative kernels: 32, 16 or 8 (a warp sweeps
+                              32/wc_group pairs side by side), or 0 (default) to pick per launch the
+                              narrowest group that keeps 3/4 of the 32-lane kernel's resident blocks.
+                              Pairs go warp-cooperative from max(wc_min_qregs, wc_group) query words */
 } gb_tuning_t;
 int gb_set_tuning(const gb_tuning_t *t);
 int gb_get_tuning(gb_tuning_t *t);
 
 /* Autotuner (no reference counterpart): runs gb_align_dev on the caller's
- * batch under each candidate tuning (block 32/64/128; for LOCAL/GLOBAL also
- * warp-cooperative thresholds 32/40/48/64/96 words), `reps` timed runs each
+ * batch under each candidate tuning (block 32/64/128; for LOCAL, GLOBAL and
+ * target-tail SEMI_GLOBAL also warp-cooperative thresholds 16/32/48/64 words
+ * x lane groups automatic/8/16/32, thresholds below the group skipped), `reps` timed runs each
  * after a warm-up run, timed with CUDA events on `stream`; installs and
  * returns the fastest (best_ms: its mean milliseconds per run; may be NULL).
  * The outputs hold the batch's results afterwards.  Synchronizes `stream`;

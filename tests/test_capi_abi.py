@@ -111,14 +111,15 @@ def test_tuning_and_graph_settings_validate(so):
     import ctypes as C
     cur = GbTuning()
     assert so.gb_get_tuning(C.byref(cur)) == 0
-    for bad in (GbTuning(256, 32, 0, 1, 1, 1), GbTuning(64, 16, 0, 1, 1, 1), GbTuning(64, 32, -1, 1, 1, 1)):
+    for bad in (GbTuning(256, 32, 0, 1, 1, 1, 16), GbTuning(64, 4, 0, 1, 1, 1, 16), GbTuning(64, 32, -1, 1, 1, 1, 16),
+                GbTuning(64, 32, 0, 1, 1, 1, 4), GbTuning(64, 32, 0, 1, 1, 1, 24)):
         assert so.gb_set_tuning(C.byref(bad)) == -1
-    ok = GbTuning(128, 48, 4096, 0, 0, 0)
+    ok = GbTuning(128, 48, 4096, 0, 0, 0, 8)
     assert so.gb_set_tuning(C.byref(ok)) == 0
     back = GbTuning()
     so.gb_get_tuning(C.byref(back))
     assert (back.block, back.wc_min_qregs, back.min_order_pairs, back.ksw_warp, back.split_start,
-            back.persistent) == (128, 48, 4096, 0, 0, 0)
+            back.persistent, back.wc_group) == (128, 48, 4096, 0, 0, 0, 8)
     assert so.gb_set_tuning(C.byref(cur)) == 0
     assert so.gb_set_graphs(0) == 0 and so.gb_set_graphs(1) == 0
     counts = (C.c_int64 * 4)()

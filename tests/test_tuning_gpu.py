@@ -59,10 +59,12 @@ def test_autotune_installs_fastest_and_keeps_results():
     try:
         best = gl.autotune(p, m, b.q_len, b.t_len, torch.cuda.current_stream().cuda_stream, reps=1)
         torch.cuda.synchronize()
-        assert best["block"] in (32, 64, 128) and best["wc_min_qregs"] in (32, 40, 48, 64, 96)
+        assert best["block"] in (32, 64, 128) and best["wc_min_qregs"] in (16, 32, 48, 64)
+        assert best["wc_group"] in (0, 8, 16, 32) and best["wc_min_qregs"] >= best["wc_group"]
         assert best["ms"] > 0
         cur = gl.get_tuning()
-        assert (cur["block"], cur["wc_min_qregs"]) == (best["block"], best["wc_min_qregs"])
+        assert (cur["block"], cur["wc_min_qregs"], cur["wc_group"]) == \
+            (best["block"], best["wc_min_qregs"], best["wc_group"])
         exp = oracle_align(p, b).as_dict(p)
         for k, v in exp.items():
             assert np.array_equal(keep[k].cpu().numpy(), v), k
@@ -113,5 +115,39 @@ def test_plain_form_matches_oracle():
             exp = oracle_align(p, b).as_dict(p)
             for k, v in exp.items():
                 assert np.array_equal(got[k], v), f"plain {p.key()} {k}"
+    finally:
+        gl.set_tuning(**saved)
+
+
+@pytest.mark.parametrize("group", [0, 8, 16, 32])
+def test_wc_lane_groups_match_oracle(group):
+    """Warp-cooperative kernels with 32/group pairs per warp: every mode on
+    mixed 50-1000 bp pairs with the cut at `group` words (so the shortest
+    warp-cooperative pairs just meet the ring's bound), unrelated long pairs
+    (start regions narrower than the group fall back to one lane), and batch
+    sizes that leave groups of the last warp without a pair.  Group 0 picks
+    the group per launch."""
+    saved = gl.get_tuning()
+    try:
+        gl.set_tuning(wc_group=group, wc_min_qregs=group or 32)
+        rng = np.random.default_rng(80 + group)
+        from gasal_b200.capi import Batch
+        qs = [bytes(rng.choice(list(b"ACGT"), size=int(rng.integers(260, 700))).tolist()) for _ in range(2101)]
+        ts = [bytes(rng.choice(list(b"ACGT"), size=int(rng.integers(20, 700))).tolist()) for _ in range(2101)]
+        unrelated = Batch.from_seqs(qs, ts)
+        cases = [(Params(algo=LOCAL, start_pos=WITH_START, second_best=1), W.workload2(3003, seed=81)),
+                 (Params(algo=LOCAL, start_pos=WITH_TB, second_best=1), W.workload2(2053, seed=82)),
+                 (Params(algo=GLOBAL, start_pos=WITH_TB), W.workload2(3001, seed=83)),
+                 (Params(algo=SEMI_GLOBAL, start_pos=WITH_START, head=TARGET, tail=TARGET, second_best=1),
+                  W.workload2(3005, seed=84)),
+                 (Params(algo=SEMI_GLOBAL, start_pos=WITH_START, head=QUERY, tail=TARGET), W.workload3(2051, seed=85)),
+                 (Params(algo=LOCAL, start_pos=WITH_START, second_best=1), unrelated),
+                 (Params(algo=GLOBAL), unrelated)]
+        for p, b in cases:
+            got = gl.align(p, b).as_dict(p)
+            exp = oracle_align(p, b).as_dict(p)
+            for k, v in exp.items():
+                bad = np.nonzero(got[k] != v)[0]
+                assert len(bad) == 0, f"group {group} {p.key()} {k}: {len(bad)} differ, first {bad[:5]}"
     finally:
         gl.set_tuning(**saved)
