@@ -294,13 +294,16 @@ void batch_signature(std::vector<uint8_t> &v, const gasal_gpu_storage_t *s, cons
     put(v, plan.start), put(v, plan.block), put(v, plan.mq8), put(v, plan.mt8), put(v, plan.wc_min_q);
     put(v, plan.ksw_slots), put(v, plan.fb_blocks), put(v, plan.band);
     put(v, plan.tier2), put(v, plan.tier_q), put(v, plan.tier2_cols), put(v, plan.tier2_blocks);
-    put(v, plan.split_start), put(v, plan.wc_group);
+    put(v, plan.split_start), put(v, plan.wc_group), put(v, plan.wc_group_big), put(v, plan.mq8_big);
+    put(v, plan.mt8_big);
     put(v, (const void *)cfg.band_w), put(v, cfg.band_model), put(v, cfg.band_min), put(v, cfg.band_max);
     put(v, (const void *)cfg.band_ok);
     put(v, plan.a);
     for (int c : plan.cut) put(v, c);
     put(v, -1);
     for (int c : plan.nlong) put(v, c);
+    put(v, -1);
+    for (int c : plan.nbig) put(v, c);
 }
 
 /* Captures issue() on stream st into a graph, updates (or instantiates) the

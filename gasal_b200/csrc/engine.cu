@@ -168,8 +168,9 @@ int plan_batch(const RunCfg &cfg, const DevBatch &b, const DevOut &o, Workspace 
 
     /* split: long LOCAL/GLOBAL (and target-tail SEMI_GLOBAL) pairs go warp-cooperative */
     const bool wc_algo = cfg.algo == LOCAL_ || cfg.algo == GLOBAL_ || (cfg.algo == SEMI_GLOBAL_ && cfg.tail == TARGET_);
-    uint32_t max_q_short = 0, max_q_long = 0, max_t_long = 0;
-    int nlong = 0;
+    uint32_t max_q_short = 0, max_q_long = 0, max_t_long = 0, max_q_big = 0, max_t_big = 0;
+    int nlong = 0, nbig = 0;
+    const uint32_t big_q = ORDER_CAP_WORDS * 8 - 7;
     /* a pair needs at least as many query words as its lane group (the
      * group's ring reader must trail its writer) */
     const int min_words = std::max(st.wc_min_qregs, st.wc_group > 0 ? st.wc_group : 8);
@@ -178,8 +179,14 @@ int plan_batch(const RunCfg &cfg, const DevBatch &b, const DevOut &o, Workspace 
         const uint32_t ql = b.h_q_len[i];
         if (wc_algo && ql >= p.wc_min_q) {
             nlong++;
-            max_q_long = std::max(max_q_long, ql);
-            max_t_long = std::max(max_t_long, b.h_t_len[i]);
+            if (ql >= big_q) {
+                nbig++;
+                max_q_big = std::max(max_q_big, ql);
+                max_t_big = std::max(max_t_big, b.h_t_len[i]);
+            } else {
+                max_q_long = std::max(max_q_long, ql);
+                max_t_long = std::max(max_t_long, b.h_t_len[i]);
+            }
         } else {
             max_q_short = std::max(max_q_short, ql);
         }
@@ -190,21 +197,26 @@ int plan_batch(const RunCfg &cfg, const DevBatch &b, const DevOut &o, Workspace 
     {
         const int wstart = (cfg.algo == SEMI_GLOBAL_ && cfg.start == WITH_TB_) ? WITHOUT_START_ : cfg.start;
         const bool wsecond = cfg.second && (cfg.algo == LOCAL_ || cfg.algo == SEMI_GLOBAL_);
-        const int mq8 = (int)((max_q_long + 7) & ~7u), mt8 = (int)((max_t_long + 7) & ~7u);
-        p.wc_group = 0;
-        if (nlong > 0 && b.n >= st.min_order_pairs && mq8 <= st.wc_max_q8) {
+        const int max_group = min_words >= 32 ? 32 : min_words >= 16 ? 16 : 8;
+        auto group_for = [&](uint32_t mq, uint32_t mt) {
+            const int mq8 = (int)((mq + 7) & ~7u), mt8 = (int)((mt + 7) & ~7u);
+            if (mq8 > st.wc_max_q8) return 0;
             if (st.wc_group > 0)
-                p.wc_group = wc_blocks_per_sm(cfg.algo, wstart, wsecond, st.wc_group, mq8, mt8) > 0 ? st.wc_group : 0;
-            else
-                p.wc_group = wc_pick_group(cfg.algo, wstart, wsecond, mq8, mt8, min_words >= 32 ? 32 : min_words >= 16 ? 16 : 8);
-        }
+                return wc_blocks_per_sm(cfg.algo, wstart, wsecond, st.wc_group, mq8, mt8) > 0 ? st.wc_group : 0;
+            return wc_pick_group(cfg.algo, wstart, wsecond, mq8, mt8, max_group);
+        };
+        const int nsmall = nlong - nbig;
+        p.wc_group = nsmall > 0 ? group_for(max_q_long, max_t_long) : 0;
+        p.wc_group_big = nbig > 0 ? group_for(max_q_big, max_t_big) : 0;
+        p.use_wc = nlong > 0 && b.n >= st.min_order_pairs && (nsmall == 0 || p.wc_group > 0) &&
+                   (nbig == 0 || p.wc_group_big > 0);
     }
-    p.use_wc = p.wc_group > 0;
     if (!p.use_wc) {
-        max_q_short = std::max(max_q_short, max_q_long);
-        nlong = 0;
+        max_q_short = std::max({max_q_short, max_q_long, max_q_big});
+        nlong = 0, nbig = 0;
     }
     p.mq8 = (int)((max_q_long + 7) & ~7u), p.mt8 = (int)((max_t_long + 7) & ~7u);
+    p.mq8_big = (int)((max_q_big + 7) & ~7u), p.mt8_big = (int)((max_t_big + 7) & ~7u);
 
     /* row buffer placement (one-thread kernel) */
     const uint32_t max_q = max_q_short;
@@ -311,6 +323,7 @@ int plan_batch(const RunCfg &cfg, const DevBatch &b, const DevOut &o, Workspace 
     if (!p.tb) {
         p.cut = {0, b.n};
         p.nlong = {nlong};
+        p.nbig = {nbig};
         p.order_on = p.use_wc || b.n >= st.min_order_pairs;
         if (p.order_on && ensure_order_buffers(ws, (size_t)b.n) != GB_OK) return GB_ERR_ALLOC;
         return GB_OK;
@@ -351,10 +364,14 @@ int plan_batch(const RunCfg &cfg, const DevBatch &b, const DevOut &o, Workspace 
     size_t max_chunk = 0;
     for (size_t c = 0; c + 1 < p.cut.size(); c++) {
         const int p0 = p.cut[c], p1 = p.cut[c + 1];
-        int nl = 0;
+        int nl = 0, nb = 0;
         if (p.use_wc)
-            for (int i = p0; i < p1; i++) nl += b.h_q_len[i] >= p.wc_min_q ? 1 : 0;
+            for (int i = p0; i < p1; i++) {
+                nl += b.h_q_len[i] >= p.wc_min_q ? 1 : 0;
+                nb += b.h_q_len[i] >= big_q ? 1 : 0;
+            }
         p.nlong.push_back(nl);
+        p.nbig.push_back(nb);
         max_chunk = std::max(max_chunk, (size_t)(p1 - p0));
     }
     p.order_on = p.use_wc || b.n >= st.min_order_pairs;
@@ -412,16 +429,22 @@ static int launch_one_thread(int algo, int start, bool second, const Plan &p, Dp
 }
 
 /* DP over pairs [0, a.n) visited in `order` (nullptr: identity): the first
- * nlong entries of order on the warp-cooperative kernel (auxiliary stream,
+ * nlong entries of order on the warp-cooperative kernel (auxiliary stream;
+ * the leading nbig of them, ORDER_CAP_WORDS+ query words, as a launch of
+ * their own,
  * forked from and joined back into s), the rest on the one-thread kernel. */
 static int launch_dp_split(int algo, int start, bool second, const Plan &p, DpArgs a, const uint32_t *order,
-                           int nlong, Workspace &ws, cudaStream_t s)
+                           int nlong, int nbig, Workspace &ws, cudaStream_t s)
 {
     if (nlong > 0 && order) {
         GB_CUDA(cudaEventRecord(ws.fork, s));
         GB_CUDA(cudaStreamWaitEvent(ws.aux, ws.fork, 0));
         timing_mark(K_DP, true, ws.aux);
-        GB_CUDA(launch_dp_wc(algo, start, second, a, order, nlong, p.mq8, p.mt8, p.wc_group, ws.aux));
+        if (nbig > 0)
+            GB_CUDA(launch_dp_wc(algo, start, second, a, order, nbig, p.mq8_big, p.mt8_big, p.wc_group_big, ws.aux));
+        if (nlong > nbig)
+            GB_CUDA(launch_dp_wc(algo, start, second, a, order + nbig, nlong - nbig, p.mq8, p.mt8, p.wc_group,
+                                 ws.aux));
         timing_mark(K_DP, false, ws.aux);
         GB_CUDA(cudaEventRecord(ws.join, ws.aux));
         DpArgs rest = a;
@@ -515,7 +538,8 @@ int enqueue_batch(const RunCfg &cfg, const DevBatch &b, const DevOut &o, Workspa
             ord = ws.order;
         }
         if (p.ksw_slots[0] > 0) return launch_ksw_split(cfg, b, p, ord, b.n, ws, s);
-        return launch_dp_split(cfg.algo, p.start, p.second, p, p.a, ord, ord ? p.nlong[0] : 0, ws, s);
+        return launch_dp_split(cfg.algo, p.start, p.second, p, p.a, ord, ord ? p.nlong[0] : 0, ord ? p.nbig[0] : 0,
+                               ws, s);
     }
     GB_CUDA(cudaMemcpyAsync(ws.d_tb_off, ws.h_tb_off, (size_t)b.n * 8, cudaMemcpyHostToDevice, s));
     for (size_t c = 0; c + 1 < p.cut.size(); c++) {
@@ -534,7 +558,8 @@ int enqueue_batch(const RunCfg &cfg, const DevBatch &b, const DevOut &o, Workspa
             if (rc != GB_OK) return rc;
             ord = ws.order;
         }
-        const int rc = launch_dp_split(cfg.algo, p.start, p.second, p, ca, ord, ord ? p.nlong[c] : 0, ws, s);
+        const int rc = launch_dp_split(cfg.algo, p.start, p.second, p, ca, ord, ord ? p.nlong[c] : 0,
+                                       ord ? p.nbig[c] : 0, ws, s);
         if (rc != GB_OK) return rc;
         TbArgs t{};
         t.tb = ws.tb, t.tb_off = ws.d_tb_off + p0;

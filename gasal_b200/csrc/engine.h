@@ -89,6 +89,10 @@ struct Plan {
     int start = 0, block = 64, mq8 = 0, mt8 = 0;
     uint32_t wc_min_q = 0;
     int wc_group = 32;
+    /* warp-cooperative pairs of ORDER_CAP_WORDS+ query words (the order's
+     * prefix) run as a launch of their own with their own lane group and
+     * buffer sizes, so their long rings leave the shorter pairs' groups alone */
+    int wc_group_big = 0, mq8_big = 0, mt8_big = 0;
     int ksw_slots[2] = {0, 0}; /* [0] > 0: ksw runs warp-per-pair; eh columns per warp of the two length classes */
     bool tier2 = false;     /* one-thread pairs split: short ones with shared-memory rows (a), long ones
                                with global rows on a small grid (tier2_* overrides of a) */
@@ -100,6 +104,7 @@ struct Plan {
     DpArgs a{};
     std::vector<int> cut;   /* pair ranges [cut[c], cut[c+1]) run one after another */
     std::vector<int> nlong; /* per range: pairs on the warp-cooperative kernel */
+    std::vector<int> nbig;  /* per range: of those, the leading ORDER_CAP_WORDS+ word ones */
 };
 
 /* status codes of gasal_b200_capi.h */

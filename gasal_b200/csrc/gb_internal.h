@@ -78,6 +78,10 @@ cudaError_t launch_dp(int algo, int start, bool second, const DpArgs &a, int blo
                       cudaStream_t s);
 cudaError_t launch_traceback(const TbArgs &a, cudaStream_t s);
 
+/* the length order's classes stop at this many query (and target) words:
+ * pairs of at least ORDER_CAP_WORDS query words form the order's prefix */
+constexpr uint32_t ORDER_CAP_WORDS = 127;
+
 /* length-binned visiting order (sched.cu): bins = order_bins() words of
  * scratch, order = n words */
 int order_bins();

@@ -19,6 +19,7 @@ namespace gb {
 
 constexpr int ORDER_BITS = 7;
 constexpr int ORDER_BINS = 1 << (2 * ORDER_BITS); /* 128 x 128 classes */
+static_assert((1u << ORDER_BITS) - 1 == ORDER_CAP_WORDS, "class cap of the length order");
 
 __device__ __forceinline__ uint32_t work_bin(uint32_t qlen, uint32_t tlen)
 {

@@ -151,3 +151,31 @@ def test_wc_lane_groups_match_oracle(group):
                 assert len(bad) == 0, f"group {group} {p.key()} {k}: {len(bad)} differ, first {bad[:5]}"
     finally:
         gl.set_tuning(**saved)
+
+
+def test_long_prefix_runs_its_own_wc_launch():
+    """Warp-cooperative pairs of 127+ query words (the length order's prefix)
+    run as their own launch with their own lane group; mixed 50-5000 bp
+    batches cover both launches, with traceback chunks of a small tile
+    budget splitting the prefix across chunks."""
+    saved = gl.get_tuning()
+    try:
+        gl.set_tuning(wc_group=0)
+        parts = W.workload4(12000, seed=101)[:3]  # each launch above the ordering threshold
+        for p, b in parts:
+            assert int((b.q_len >= 1009).sum()) > 0 and int(((b.q_len >= 249) & (b.q_len < 1009)).sum()) > 0
+            exp = oracle_align(p, b).as_dict(p)
+            got = gl.align(p, b).as_dict(p)
+            for k, v in exp.items():
+                assert np.array_equal(got[k], v), f"{p.key()} {k}"
+        p, b = parts[1]
+        gl.set_tb_budget_mb(8)
+        try:
+            got = gl.align(p, b).as_dict(p)
+        finally:
+            gl.set_tb_budget_mb(16384)
+        exp = oracle_align(p, b).as_dict(p)
+        for k, v in exp.items():
+            assert np.array_equal(got[k], v), f"chunked {p.key()} {k}"
+    finally:
+        gl.set_tuning(**saved)
