@@ -177,7 +177,7 @@ static cudaError_t launch_one(const DpArgs &a, int block, cudaStream_t s)
     if (a.smem_cols > 0) {
         const size_t smem = (size_t)a.smem_cols * block * sizeof(uint32_t);
         auto k = dp_kernel<ALGO, START, SECOND, true>;
-        cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        cudaError_t e = allow_dyn_smem(k);
         if (e != cudaSuccess) return e;
         int blocks = (a.n + block - 1) / block;
         if (a.queue) {

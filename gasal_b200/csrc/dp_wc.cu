@@ -750,7 +750,7 @@ static cudaError_t launch_wc_one(const DpArgs &a, const uint32_t *list, int nlis
     DpArgs b = a;
     b.scratch_cols = (uint32_t)(max_t8 / 8 + 1); /* bandmax stride per group */
     auto k = dp_wc_kernel<G, ALGO, START, SECOND>;
-    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaError_t e = allow_dyn_smem(k);
     if (e != cudaSuccess) return e;
     int dev = 0, sms = 148;
     cudaGetDevice(&dev);
@@ -772,7 +772,7 @@ static cudaError_t launch_wc_semi(const DpArgs &a, const uint32_t *list, int nli
     b.scratch_cols = (uint32_t)(max_t8 + 8); /* lastcol stride per group */
     const size_t smem = wc_smem_bytes(SEMI_GLOBAL_, G, max_q8, max_t8);
     auto k = dp_wc_semi_kernel<G, SECOND, START>;
-    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaError_t e = allow_dyn_smem(k);
     if (e != cudaSuccess) return e;
     int dev = 0, sms = 148;
     cudaGetDevice(&dev);
@@ -818,7 +818,7 @@ static int wc_blocks_g(int algo, int start, bool second, size_t smem)
     int n = 0;
     cudaError_t e = cudaErrorInvalidValue;
     auto occ = [&](auto k) {
-        if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) return;
+        if (allow_dyn_smem(k) != cudaSuccess) return;
         e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k, 128, smem);
     };
     if (algo == SEMI_GLOBAL_) {

@@ -78,6 +78,15 @@ cudaError_t launch_dp(int algo, int start, bool second, const DpArgs &a, int blo
                       cudaStream_t s);
 cudaError_t launch_traceback(const TbArgs &a, cudaStream_t s);
 
+/* Lets a kernel use the most dynamic shared memory the device gives a block
+ * (set once per kernel and device).  Kernels launched with different sizes
+ * -- the length classes of one batch, other storages, occupancy queries --
+ * then never depend on which size an earlier call set: a launch captured in
+ * a CUDA graph and replayed later (or profiled node by node) finds the
+ * attribute still covering it. */
+cudaError_t allow_dyn_smem_fn(const void *fn);
+template <class K> inline cudaError_t allow_dyn_smem(K *k) { return allow_dyn_smem_fn((const void *)k); }
+
 /* the length order's classes stop at this many query (and target) words:
  * pairs of at least ORDER_CAP_WORDS query words form the order's prefix */
 constexpr uint32_t ORDER_CAP_WORDS = 127;

@@ -429,7 +429,7 @@ cudaError_t launch_slots(const DpArgs &a, const uint32_t *list, int nlist, int s
     const int block = 32, warps = block / 32; /* one warp per block packs shared memory tightest */
     const size_t smem = (size_t)warps * slots * (sizeof(uint32_t) + 2);
     auto k = band ? ksw_wc_kernel<true> : ksw_wc_kernel<false>;
-    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaError_t e = allow_dyn_smem(k);
     if (e != cudaSuccess) return e;
     int dev = 0, sms = 148, per_sm = 0;
     cudaGetDevice(&dev);
