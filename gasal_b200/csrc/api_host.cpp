@@ -225,6 +225,7 @@ void release_state(const gasal_gpu_storage_t *s)
     if (w.tb_off_free) cudaEventDestroy(w.tb_off_free);
     if (w.order) cudaFree(w.order);
     if (w.order2) cudaFree(w.order2);
+    if (w.wc_rows) cudaFree(w.wc_rows);
     if (w.aux) cudaStreamDestroy(w.aux);
     if (w.queue) cudaFree(w.queue);
     if (w.fork) cudaEventDestroy(w.fork);
@@ -294,8 +295,8 @@ void batch_signature(std::vector<uint8_t> &v, const gasal_gpu_storage_t *s, cons
     put(v, plan.start), put(v, plan.block), put(v, plan.mq8), put(v, plan.mt8), put(v, plan.wc_min_q);
     put(v, plan.ksw_slots), put(v, plan.fb_blocks), put(v, plan.band);
     put(v, plan.tier2), put(v, plan.tier_q), put(v, plan.tier2_cols), put(v, plan.tier2_blocks);
-    put(v, plan.split_start), put(v, plan.wc_group), put(v, plan.wc_group_big), put(v, plan.mq8_big);
-    put(v, plan.mt8_big);
+    put(v, plan.split_start), put(v, plan.wc), put(v, plan.wc_big), put(v, plan.mq8_big);
+    put(v, plan.mt8_big), put(v, (const void *)ss.ws.wc_rows);
     put(v, (const void *)cfg.band_w), put(v, cfg.band_model), put(v, cfg.band_min), put(v, cfg.band_max);
     put(v, (const void *)cfg.band_ok);
     put(v, plan.a);

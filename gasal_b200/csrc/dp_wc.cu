@@ -507,7 +507,7 @@ __global__ void __launch_bounds__(128) dp_wc_semi_kernel(DpArgs a, const uint32_
     const int warps_per_block = blockDim.x >> 5;
     const int slot = warp * NG + gi; /* this group's ring and last-column buffer */
     uint32_t *ring = wc_smem + (size_t)slot * ring_cols;
-    int *lastcol = (int *)(wc_smem + (size_t)warps_per_block * NG * ring_cols) + (size_t)slot * a.scratch_cols;
+    int *lastcol = a.lastcol + ((size_t)blockIdx.x * warps_per_block * NG + slot) * a.scratch_cols;
     const bool fast_scores = a.sc.match >= -128 && a.sc.match <= 127 && a.sc.mismatch >= -127 && a.sc.mismatch <= 128;
     const bool open_nn = a.sc.o >= 0;
     for (int item0 = (blockIdx.x * warps_per_block + warp) * NG; item0 < nlist;
@@ -729,113 +729,55 @@ __global__ void __launch_bounds__(128) dp_wc_kernel(DpArgs a, const uint32_t *li
     }
 }
 
-/* Shared memory of one block of the warp-cooperative kernels: 4 warps x 32/G
- * groups, each with a ring of max_q8 words and, for LOCAL/GLOBAL, band
- * maxima (max_t8/8 + 1 words) or, for SEMI_GLOBAL, the last column's H of
- * every row (max_t8 + 8 words). */
-size_t wc_smem_bytes(int algo, int group, int max_q8, int max_t8)
+/* Shared memory of one warp-cooperative block: `warps` warps x 32/G groups,
+ * each with a ring of max_q8 words and, for LOCAL/GLOBAL, band maxima
+ * (max_t8/8 + 1 words).  SEMI_GLOBAL's last-column rows live in global
+ * scratch (`DpArgs::lastcol`), one slot per group of the grid. */
+size_t wc_smem_bytes(int algo, int group, int warps, int max_q8, int max_t8)
 {
-    const size_t per = (size_t)max_q8 + (algo == SEMI_GLOBAL_ ? (size_t)max_t8 + 8 : (size_t)max_t8 / 8 + 1);
-    return (size_t)4 * (32 / group) * per * 4;
+    const size_t per = (size_t)max_q8 + (algo == SEMI_GLOBAL_ ? 0 : (size_t)max_t8 / 8 + 1);
+    return (size_t)warps * (32 / group) * per * 4;
 }
 
-template <int G, int ALGO, int START, bool SECOND>
-static cudaError_t launch_wc_one(const DpArgs &a, const uint32_t *list, int nlist, int max_q8, int max_t8,
-                                 cudaStream_t s)
-{
-    constexpr int NG = 32 / G;
-    const int warps = 4, block = warps * 32;
-    const int ring_cols = max_q8;
-    const size_t smem = wc_smem_bytes(ALGO, G, max_q8, max_t8);
-    DpArgs b = a;
-    b.scratch_cols = (uint32_t)(max_t8 / 8 + 1); /* bandmax stride per group */
-    auto k = dp_wc_kernel<G, ALGO, START, SECOND>;
-    cudaError_t e = allow_dyn_smem(k);
-    if (e != cudaSuccess) return e;
-    int dev = 0, sms = 148;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    int blocks = (nlist + warps * NG - 1) / (warps * NG);
-    if (blocks > sms * 16) blocks = sms * 16;
-    k<<<blocks, block, smem, s>>>(b, list, nlist, ring_cols);
-    return cudaGetLastError();
-}
-
-template <int G, bool SECOND, bool START>
-static cudaError_t launch_wc_semi(const DpArgs &a, const uint32_t *list, int nlist, int max_q8, int max_t8,
-                                  cudaStream_t s)
-{
-    constexpr int NG = 32 / G;
-    const int warps = 4, block = warps * 32;
-    const int ring_cols = max_q8;
-    DpArgs b = a;
-    b.scratch_cols = (uint32_t)(max_t8 + 8); /* lastcol stride per group */
-    const size_t smem = wc_smem_bytes(SEMI_GLOBAL_, G, max_q8, max_t8);
-    auto k = dp_wc_semi_kernel<G, SECOND, START>;
-    cudaError_t e = allow_dyn_smem(k);
-    if (e != cudaSuccess) return e;
-    int dev = 0, sms = 148;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    int blocks = (nlist + warps * NG - 1) / (warps * NG);
-    if (blocks > sms * 16) blocks = sms * 16;
-    k<<<blocks, block, smem, s>>>(b, list, nlist, ring_cols);
-    return cudaGetLastError();
-}
-
-template <int G>
-static cudaError_t launch_dp_wc_g(int algo, int start, bool second, const DpArgs &a, const uint32_t *list,
-                                  int nlist, int max_q8, int max_t8, cudaStream_t s)
+/* one kernel instantiation per (group, algo, start, second best) */
+template <int G, class F> static cudaError_t with_wc_kernel(int algo, int start, bool second, F &&f)
 {
     if (algo == SEMI_GLOBAL_) {
         if (start == WITH_START_)
-            return second ? launch_wc_semi<G, true, true>(a, list, nlist, max_q8, max_t8, s)
-                          : launch_wc_semi<G, false, true>(a, list, nlist, max_q8, max_t8, s);
-        return second ? launch_wc_semi<G, true, false>(a, list, nlist, max_q8, max_t8, s)
-                      : launch_wc_semi<G, false, false>(a, list, nlist, max_q8, max_t8, s);
+            return second ? f(dp_wc_semi_kernel<G, true, true>) : f(dp_wc_semi_kernel<G, false, true>);
+        return second ? f(dp_wc_semi_kernel<G, true, false>) : f(dp_wc_semi_kernel<G, false, false>);
     }
     if (algo == GLOBAL_)
-        return start == WITH_TB_ ? launch_wc_one<G, GLOBAL_, WITH_TB_, false>(a, list, nlist, max_q8, max_t8, s)
-                                 : launch_wc_one<G, GLOBAL_, WITHOUT_START_, false>(a, list, nlist, max_q8, max_t8,
-                                                                                    s);
+        return start == WITH_TB_ ? f(dp_wc_kernel<G, GLOBAL_, WITH_TB_, false>)
+                                 : f(dp_wc_kernel<G, GLOBAL_, WITHOUT_START_, false>);
     if (algo == LOCAL_) {
         if (start == WITH_START_)
-            return second ? launch_wc_one<G, LOCAL_, WITH_START_, true>(a, list, nlist, max_q8, max_t8, s)
-                          : launch_wc_one<G, LOCAL_, WITH_START_, false>(a, list, nlist, max_q8, max_t8, s);
+            return second ? f(dp_wc_kernel<G, LOCAL_, WITH_START_, true>) : f(dp_wc_kernel<G, LOCAL_, WITH_START_, false>);
         if (start == WITH_TB_)
-            return second ? launch_wc_one<G, LOCAL_, WITH_TB_, true>(a, list, nlist, max_q8, max_t8, s)
-                          : launch_wc_one<G, LOCAL_, WITH_TB_, false>(a, list, nlist, max_q8, max_t8, s);
-        return second ? launch_wc_one<G, LOCAL_, WITHOUT_START_, true>(a, list, nlist, max_q8, max_t8, s)
-                      : launch_wc_one<G, LOCAL_, WITHOUT_START_, false>(a, list, nlist, max_q8, max_t8, s);
+            return second ? f(dp_wc_kernel<G, LOCAL_, WITH_TB_, true>) : f(dp_wc_kernel<G, LOCAL_, WITH_TB_, false>);
+        return second ? f(dp_wc_kernel<G, LOCAL_, WITHOUT_START_, true>)
+                      : f(dp_wc_kernel<G, LOCAL_, WITHOUT_START_, false>);
     }
     return cudaErrorInvalidValue;
 }
-
-/* resident blocks per SM of the warp-cooperative kernel for these options */
-template <int G>
-static int wc_blocks_g(int algo, int start, bool second, size_t smem)
+template <class F> static cudaError_t with_wc_kernel(int group, int algo, int start, bool second, F &&f)
 {
+    if (group == 8) return with_wc_kernel<8>(algo, start, second, f);
+    if (group == 16) return with_wc_kernel<16>(algo, start, second, f);
+    if (group == 32) return with_wc_kernel<32>(algo, start, second, f);
+    return cudaErrorInvalidValue;
+}
+
+/* resident blocks per SM of one launch shape (0: it cannot run) */
+static int wc_blocks_per_sm(int algo, int start, bool second, int group, int warps, size_t smem)
+{
+    if (smem > (200u << 10)) return 0;
     int n = 0;
-    cudaError_t e = cudaErrorInvalidValue;
-    auto occ = [&](auto k) {
-        if (allow_dyn_smem(k) != cudaSuccess) return;
-        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k, 128, smem);
-    };
-    if (algo == SEMI_GLOBAL_) {
-        if (start == WITH_START_) second ? occ(dp_wc_semi_kernel<G, true, true>) : occ(dp_wc_semi_kernel<G, false, true>);
-        else second ? occ(dp_wc_semi_kernel<G, true, false>) : occ(dp_wc_semi_kernel<G, false, false>);
-    } else if (algo == GLOBAL_) {
-        start == WITH_TB_ ? occ(dp_wc_kernel<G, GLOBAL_, WITH_TB_, false>)
-                          : occ(dp_wc_kernel<G, GLOBAL_, WITHOUT_START_, false>);
-    } else if (algo == LOCAL_) {
-        if (start == WITH_START_)
-            second ? occ(dp_wc_kernel<G, LOCAL_, WITH_START_, true>) : occ(dp_wc_kernel<G, LOCAL_, WITH_START_, false>);
-        else if (start == WITH_TB_)
-            second ? occ(dp_wc_kernel<G, LOCAL_, WITH_TB_, true>) : occ(dp_wc_kernel<G, LOCAL_, WITH_TB_, false>);
-        else
-            second ? occ(dp_wc_kernel<G, LOCAL_, WITHOUT_START_, true>)
-                   : occ(dp_wc_kernel<G, LOCAL_, WITHOUT_START_, false>);
-    }
+    const cudaError_t e = with_wc_kernel(group, algo, start, second, [&](auto k) {
+        cudaError_t r = allow_dyn_smem(k);
+        if (r == cudaSuccess) r = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k, 32 * warps, smem);
+        return r;
+    });
     if (e != cudaSuccess) {
         cudaGetLastError(); /* a size the kernel cannot take: no resident block */
         return 0;
@@ -843,42 +785,85 @@ static int wc_blocks_g(int algo, int start, bool second, size_t smem)
     return n;
 }
 
-int wc_blocks_per_sm(int algo, int start, bool second, int group, int max_q8, int max_t8)
+/* the shape with the most resident warps for this group (4, 2 or 1 warps
+ * per block; long rings fit better in small blocks) */
+static WcLaunch wc_shape(int algo, int start, bool second, int group, int max_q8, int max_t8)
 {
-    const size_t smem = wc_smem_bytes(algo, group, max_q8, max_t8);
-    if (smem > (200u << 10)) return 0;
-    if (group == 8) return wc_blocks_g<8>(algo, start, second, smem);
-    if (group == 16) return wc_blocks_g<16>(algo, start, second, smem);
-    if (group == 32) return wc_blocks_g<32>(algo, start, second, smem);
-    return 0;
+    WcLaunch best;
+    int best_res = 0;
+    for (int warps : {4, 2, 1}) {
+        const size_t smem = wc_smem_bytes(algo, group, warps, max_q8, max_t8);
+        const int res = wc_blocks_per_sm(algo, start, second, group, warps, smem) * warps;
+        if (res > best_res) {
+            best_res = res;
+            best.group = group, best.warps = warps, best.smem = smem, best.resident_warps = res;
+        }
+    }
+    return best;
 }
 
-/* Lane group for a launch: the smallest of 8 / 16 / 32 (at most max_group)
- * that keeps at least 3/4 of the resident blocks the 32-lane kernel has --
- * narrower groups waste fewer lanes on pipeline fill and drain but hold one
- * ring (and band or last-column buffer) per pair, so long queries can cost
- * occupancy.  SEMI_GLOBAL keeps 32 lanes: its per-group last-column buffer
- * made the narrower groups slower on 250-1000 bp pairs.  0: none fits. */
-int wc_pick_group(int algo, int start, bool second, int max_q8, int max_t8, int max_group)
+WcLaunch wc_plan(int algo, int start, bool second, int nlist, int max_q8, int max_t8, int forced_group,
+                 int max_group)
 {
-    const int b32 = max_group >= 32 ? wc_blocks_per_sm(algo, start, second, 32, max_q8, max_t8) : 0;
-    if (algo == SEMI_GLOBAL_) return b32 > 0 ? 32 : 0;
-    for (int g : {8, 16}) {
-        if (g > max_group) break;
-        const int bg = wc_blocks_per_sm(algo, start, second, g, max_q8, max_t8);
-        if (bg > 0 && (b32 == 0 || 4 * bg >= 3 * b32)) return g;
+    WcLaunch l;
+    if (nlist <= 0) return l;
+    if (forced_group > 0) {
+        l = wc_shape(algo, start, second, forced_group, max_q8, max_t8);
+    } else {
+        /* the narrowest group that keeps 3/4 of the 32-lane kernel's
+         * resident warps: narrower groups waste fewer lanes on each pair's
+         * pipeline fill and drain but hold one ring per pair */
+        const WcLaunch w32 = max_group >= 32 ? wc_shape(algo, start, second, 32, max_q8, max_t8) : WcLaunch{};
+        for (int g : {8, 16}) {
+            if (g > max_group) break;
+            /* SEMI_GLOBAL measured slower at 8 lanes than at 16 (250-1000 bp:
+             * 93 against 87 ms), its last-column writes and row scans
+             * weighing more on narrow groups */
+            if (algo == SEMI_GLOBAL_ && g == 8 && max_group >= 16) continue;
+            const WcLaunch wg = wc_shape(algo, start, second, g, max_q8, max_t8);
+            if (wg.group > 0 && (w32.group == 0 || 4 * wg.resident_warps >= 3 * w32.resident_warps)) {
+                l = wg;
+                break;
+            }
+        }
+        if (l.group == 0) l = w32;
     }
-    return b32 > 0 ? 32 : 0;
+    if (l.group == 0) return l;
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const int per_block = l.warps * (32 / l.group);
+    l.blocks = (nlist + per_block - 1) / per_block;
+    const int cap = sms * 64 / l.warps; /* at most 64 warps per SM's worth of blocks; warps loop over pairs */
+    if (l.blocks > cap) l.blocks = cap;
+    return l;
+}
+
+size_t wc_scratch_words(int algo, const WcLaunch &l, int max_t8)
+{
+    if (algo != SEMI_GLOBAL_ || l.group == 0) return 0;
+    return (size_t)l.blocks * l.warps * (32 / l.group) * ((size_t)max_t8 + 8);
 }
 
 cudaError_t launch_dp_wc(int algo, int start, bool second, const DpArgs &a, const uint32_t *list, int nlist,
-                         int max_q8, int max_t8, int group, cudaStream_t s)
+                         int max_q8, int max_t8, const WcLaunch &l, int32_t *rows, cudaStream_t s)
 {
     if (nlist <= 0) return cudaSuccess;
-    if (group == 8) return launch_dp_wc_g<8>(algo, start, second, a, list, nlist, max_q8, max_t8, s);
-    if (group == 16) return launch_dp_wc_g<16>(algo, start, second, a, list, nlist, max_q8, max_t8, s);
-    if (group == 32) return launch_dp_wc_g<32>(algo, start, second, a, list, nlist, max_q8, max_t8, s);
-    return cudaErrorInvalidValue;
+    if (l.group == 0) return cudaErrorInvalidValue;
+    DpArgs b = a;
+    if (algo == SEMI_GLOBAL_) {
+        b.scratch_cols = (uint32_t)(max_t8 + 8); /* last-column rows per group */
+        b.lastcol = rows;
+    } else {
+        b.scratch_cols = (uint32_t)(max_t8 / 8 + 1); /* band maxima per group */
+    }
+    const int ring_cols = max_q8;
+    return with_wc_kernel(l.group, algo, start, second, [&](auto k) {
+        cudaError_t e = allow_dyn_smem(k);
+        if (e != cudaSuccess) return e;
+        k<<<l.blocks, 32 * l.warps, l.smem, s>>>(b, list, nlist, ring_cols);
+        return cudaGetLastError();
+    });
 }
 
 } // namespace gb

@@ -220,18 +220,25 @@ int plan_batch(const RunCfg &cfg, const DevBatch &b, const DevOut &o, Workspace 
         const int wstart = (cfg.algo == SEMI_GLOBAL_ && cfg.start == WITH_TB_) ? WITHOUT_START_ : cfg.start;
         const bool wsecond = cfg.second && (cfg.algo == LOCAL_ || cfg.algo == SEMI_GLOBAL_);
         const int max_group = min_words >= 32 ? 32 : min_words >= 16 ? 16 : 8;
-        auto group_for = [&](uint32_t mq, uint32_t mt) {
+        auto shape_for = [&](int n, uint32_t mq, uint32_t mt) {
             const int mq8 = (int)((mq + 7) & ~7u), mt8 = (int)((mt + 7) & ~7u);
-            if (mq8 > st.wc_max_q8) return 0;
-            if (st.wc_group > 0)
-                return wc_blocks_per_sm(cfg.algo, wstart, wsecond, st.wc_group, mq8, mt8) > 0 ? st.wc_group : 0;
-            return wc_pick_group(cfg.algo, wstart, wsecond, mq8, mt8, max_group);
+            if (n <= 0 || mq8 > st.wc_max_q8) return WcLaunch{};
+            return wc_plan(cfg.algo, wstart, wsecond, n, mq8, mt8, st.wc_group, max_group);
         };
         const int nsmall = nlong - nbig;
-        p.wc_group = nsmall > 0 ? group_for(max_q_long, max_t_long) : 0;
-        p.wc_group_big = nbig > 0 ? group_for(max_q_big, max_t_big) : 0;
-        p.use_wc = nlong > 0 && b.n >= st.min_order_pairs && (nsmall == 0 || p.wc_group > 0) &&
-                   (nbig == 0 || p.wc_group_big > 0);
+        if (nlong > 0 && b.n >= st.min_order_pairs) {
+            p.wc = shape_for(nsmall, max_q_long, max_t_long);
+            p.wc_big = shape_for(nbig, max_q_big, max_t_big);
+        }
+        p.use_wc = nlong > 0 && b.n >= st.min_order_pairs && (nsmall == 0 || p.wc.group > 0) &&
+                   (nbig == 0 || p.wc_big.group > 0);
+        if (p.use_wc) {
+            /* the two launches run one after the other on one stream: one
+             * last-column scratch serves both */
+            const size_t rows = std::max(wc_scratch_words(cfg.algo, p.wc, (int)((max_t_long + 7) & ~7u)),
+                                         wc_scratch_words(cfg.algo, p.wc_big, (int)((max_t_big + 7) & ~7u)));
+            if (rows > 0 && grow((void **)&ws.wc_rows, &ws.wc_rows_cap, rows, 4) != GB_OK) return GB_ERR_ALLOC;
+        }
     }
     if (!p.use_wc) {
         max_q_short = std::max({max_q_short, max_q_long, max_q_big});
@@ -463,9 +470,10 @@ static int launch_dp_split(int algo, int start, bool second, const Plan &p, DpAr
         GB_CUDA(cudaStreamWaitEvent(ws.aux, ws.fork, 0));
         timing_mark(K_DP, true, ws.aux);
         if (nbig > 0)
-            GB_CUDA(launch_dp_wc(algo, start, second, a, order, nbig, p.mq8_big, p.mt8_big, p.wc_group_big, ws.aux));
+            GB_CUDA(launch_dp_wc(algo, start, second, a, order, nbig, p.mq8_big, p.mt8_big, p.wc_big, ws.wc_rows,
+                                 ws.aux));
         if (nlong > nbig)
-            GB_CUDA(launch_dp_wc(algo, start, second, a, order + nbig, nlong - nbig, p.mq8, p.mt8, p.wc_group,
+            GB_CUDA(launch_dp_wc(algo, start, second, a, order + nbig, nlong - nbig, p.mq8, p.mt8, p.wc, ws.wc_rows,
                                  ws.aux));
         timing_mark(K_DP, false, ws.aux);
         GB_CUDA(cudaEventRecord(ws.join, ws.aux));

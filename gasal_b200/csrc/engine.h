@@ -64,6 +64,8 @@ struct Workspace {
     cudaEvent_t tb_off_free = nullptr;
     uint32_t *order = nullptr;   /* length-binned visiting order */
     size_t order_cap = 0;
+    int32_t *wc_rows = nullptr;  /* warp-cooperative SEMI_GLOBAL last-column rows */
+    size_t wc_rows_cap = 0;
     uint32_t *order2 = nullptr;  /* visiting order of the separate start passes */
     size_t order2_cap = 0;
     uint32_t *bins = nullptr;    /* order_bins() class counters */
@@ -88,11 +90,12 @@ struct Plan {
     bool tb = false, second = false, use_wc = false, order_on = false;
     int start = 0, block = 64, mq8 = 0, mt8 = 0;
     uint32_t wc_min_q = 0;
-    int wc_group = 32;
+    WcLaunch wc;                 /* shape of the warp-cooperative launch */
     /* warp-cooperative pairs of ORDER_CAP_WORDS+ query words (the order's
-     * prefix) run as a launch of their own with their own lane group and
-     * buffer sizes, so their long rings leave the shorter pairs' groups alone */
-    int wc_group_big = 0, mq8_big = 0, mt8_big = 0;
+     * prefix) run as a launch of their own with their own shape and buffer
+     * sizes, so their long rings leave the shorter pairs' groups alone */
+    WcLaunch wc_big;
+    int mq8_big = 0, mt8_big = 0;
     int ksw_slots[2] = {0, 0}; /* [0] > 0: ksw runs warp-per-pair; eh columns per warp of the two length classes */
     bool tier2 = false;     /* one-thread pairs split: short ones with shared-memory rows (a), long ones
                                with global rows on a small grid (tier2_* overrides of a) */

@@ -53,6 +53,15 @@ struct DpArgs {
                                            (n is then an upper bound, used to size the grid) */
     uint32_t q_min, q_max;              /* one-thread kernel: only pairs with q_min <= qlen <= q_max
                                            (q_max 0: no upper limit) */
+    int32_t *lastcol;                   /* warp-cooperative SEMI_GLOBAL: last-column H of every row,
+                                           one slot of scratch_cols words per lane group of the grid */
+};
+
+/* Shape of one warp-cooperative launch: lanes per pair (0: it cannot run),
+ * warps per block, grid, dynamic shared memory, resident warps per SM. */
+struct WcLaunch {
+    int group = 0, warps = 4, blocks = 0, resident_warps = 0;
+    size_t smem = 0;
 };
 
 struct TbArgs {
@@ -103,16 +112,21 @@ cudaError_t launch_start_order(const uint32_t *q_len, const int32_t *q_end, cons
                                uint32_t q_cut, uint32_t *bins, uint32_t *order, cudaStream_t s);
 
 /* warp-cooperative DP (dp_wc.cu) for the pairs listed in `list`: LOCAL,
- * GLOBAL and target-tail SEMI_GLOBAL, each pair on `group` lanes (32, 16 or
- * 8; queries of at least `group` words) */
+ * GLOBAL and target-tail SEMI_GLOBAL, each pair on `l.group` lanes (32, 16
+ * or 8; queries of at least that many words); `rows`: SEMI_GLOBAL's
+ * last-column scratch of wc_scratch_words(...) words */
 cudaError_t launch_dp_wc(int algo, int start, bool second, const DpArgs &a, const uint32_t *list, int nlist,
-                         int max_q8, int max_t8, int group, cudaStream_t s);
+                         int max_q8, int max_t8, const WcLaunch &l, int32_t *rows, cudaStream_t s);
 /* dynamic shared memory of one warp-cooperative block */
-size_t wc_smem_bytes(int algo, int group, int max_q8, int max_t8);
-/* resident blocks per SM of that kernel (0: it cannot run at these sizes) */
-int wc_blocks_per_sm(int algo, int start, bool second, int group, int max_q8, int max_t8);
-/* the lane group a launch uses when none is forced (0: none fits) */
-int wc_pick_group(int algo, int start, bool second, int max_q8, int max_t8, int max_group);
+size_t wc_smem_bytes(int algo, int group, int warps, int max_q8, int max_t8);
+/* launch shape for nlist pairs: the forced group, or (forced_group 0) the
+ * narrowest group up to max_group that keeps 3/4 of the 32-lane kernel's
+ * resident warps; per group the warps per block with the most resident
+ * warps.  group 0: no shape fits. */
+WcLaunch wc_plan(int algo, int start, bool second, int nlist, int max_q8, int max_t8, int forced_group,
+                 int max_group);
+/* global scratch words a launch of that shape needs */
+size_t wc_scratch_words(int algo, const WcLaunch &l, int max_t8);
 
 /* the global-scratch DP variant on a caller-chosen grid */
 cudaError_t launch_dp_scratch_grid(int algo, int start, bool second, const DpArgs &a, int block, int blocks,
