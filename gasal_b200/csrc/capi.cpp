@@ -473,6 +473,15 @@ extern "C" int gb_get_tuning(gb_tuning_t *t)
     return GB_OK;
 }
 
+extern "C" int gb_cigar_text(const uint8_t *cigar, const uint32_t *q_off, const uint32_t *n_cigar, int n, char *text,
+                             int stride, int32_t *text_len, void *stream)
+{
+    if (n < 0 || stride <= 0 || (n > 0 && (!cigar || !q_off || !n_cigar || !text || !text_len))) return GB_ERR_ARG;
+    return gb::launch_cigar_text(cigar, q_off, n_cigar, n, text, stride, text_len, (cudaStream_t)stream) == cudaSuccess
+               ? GB_OK
+               : GB_ERR_CUDA;
+}
+
 extern "C" const char *gb_version(void) { return "gasal-b200 0.1 (sm_100a)"; }
 
 extern "C" int gb_kernel_timing(int on)

@@ -96,6 +96,10 @@ cudaError_t launch_traceback(const TbArgs &a, cudaStream_t s);
 cudaError_t allow_dyn_smem_fn(const void *fn);
 template <class K> inline cudaError_t allow_dyn_smem(K *k) { return allow_dyn_smem_fn((const void *)k); }
 
+/* forward CIGAR text of every pair (cigar_text.cu) */
+cudaError_t launch_cigar_text(const uint8_t *cigar, const uint32_t *q_off, const uint32_t *n_cigar, int n,
+                              char *text, int stride, int32_t *text_len, cudaStream_t s);
+
 /* the length order's classes stop at this many query (and target) words:
  * pairs of at least ORDER_CAP_WORDS query words form the order's prefix */
 constexpr uint32_t ORDER_CAP_WORDS = 127;

@@ -114,6 +114,8 @@ SIGNATURES = {
     "gb_ksw_band_align": (C.c_int, [C.POINTER(GbParams), C.POINTER(GbDevBatch), C.POINTER(GbDevOut), C.c_void_p,
                                     C.c_void_p, C.c_void_p, C.POINTER(GbBandStats)]),
     "gb_last_error": (C.c_char_p, []),
+    "gb_cigar_text": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_int, C.c_void_p,
+                                C.c_void_p]),
     "gb_autotune": (C.c_int, [C.POINTER(GbParams), C.POINTER(GbDevBatch), C.POINTER(GbDevOut), C.c_void_p, C.c_int,
                               C.POINTER(GbTuning), C.POINTER(C.c_double)]),
     "gb_kernel_timing": (C.c_int, [C.c_int]),
@@ -320,6 +322,15 @@ def ksw_band_align(p: Params, dev: dict, h_q_len: np.ndarray, h_t_len: np.ndarra
     _check(lib().gb_ksw_band_align(C.byref(cp), C.byref(b), C.byref(o), band_ptr, ok_ptr, stream, C.byref(st)),
            "gb_ksw_band_align")
     return {k: getattr(st, k) for k, _ in GbBandStats._fields_}
+
+
+def cigar_text_dev(cigar_ptr: int, q_off_ptr: int, n_cigar_ptr: int, n: int, text_ptr: int, stride: int,
+                   text_len_ptr: int, stream_handle: int = 0):
+    """gb_cigar_text on device buffers: forward CIGAR strings in stride-byte
+    slots, lengths (-1: did not fit) in text_len."""
+    _check(lib().gb_cigar_text(C.c_void_p(cigar_ptr), C.c_void_p(q_off_ptr), C.c_void_p(n_cigar_ptr), int(n),
+                               C.c_void_p(text_ptr), int(stride), C.c_void_p(text_len_ptr), C.c_void_p(stream_handle)),
+           "gb_cigar_text")
 
 
 def align_dev(p: Params, dev: dict, h_q_len: np.ndarray, h_t_len: np.ndarray, stream_handle: int = 0,

@@ -188,6 +188,18 @@ int gb_align_dev(const gb_params_t *p, const gb_dev_batch_t *b, const gb_dev_out
  * resolves the array's address and should precede any stream capture. */
 int gb_align_dev_noalloc(const gb_params_t *p, const gb_dev_batch_t *b, const gb_dev_out_t *o, void *stream);
 
+/* Forward CIGAR text on the device (no counterpart in the reference
+ * library; its test program decodes on the host, test_prog/test_prog.cpp:
+ * 382-428).  Input: the traceback's run-length bytes (count << 2 | op, last
+ * operation first) at each pair's query offset -- gb_dev_out_t::cigar /
+ * n_cigar, or GASAL2's device CIGAR buffer -- all device pointers.  Pair i's
+ * text (neighbouring runs of one operation merged, each run as its count and
+ * M / X / D / I, NUL-terminated) goes to text + i * stride; text_len[i] is its
+ * length, or -1 when it needs more than stride - 1 characters (the slot then
+ * holds ""); a pair without operations gets "".  Asynchronous on `stream`. */
+int gb_cigar_text(const uint8_t *cigar, const uint32_t *q_off, const uint32_t *n_cigar, int n, char *text, int stride,
+                  int32_t *text_len, void *stream);
+
 /* Library settings.
  * reference_reverse: 1 (default) reverses sequences exactly as the
  *   reference's sm_100a build does; 0 reverses the real bases only.

@@ -51,6 +51,24 @@ def oracle_align(p: Params, b: Batch, threads: int = 0, want_packed=False, compa
     return _call(fn, p, b, want_packed, (C.c_int(threads), C.c_int(compat), C.c_int(mql)))
 
 
+def oracle_cigar_text(cigar: np.ndarray, q_off: np.ndarray, n_cigar: np.ndarray, stride: int):
+    """Forward CIGAR strings (the reference test program's decode); returns
+    (list of str, int32 lengths with -1 where stride was too small)."""
+    lib = _load("liboracle_gasal.so")
+    n = len(n_cigar)
+    cig = np.ascontiguousarray(cigar, dtype=np.uint8)
+    qo = np.ascontiguousarray(q_off, dtype=np.uint32)
+    nc = np.ascontiguousarray(n_cigar, dtype=np.uint32)
+    text = np.zeros(n * stride, dtype=np.uint8)
+    lens = np.zeros(n, dtype=np.int32)
+    fn = lib.oracle_cigar_text
+    fn.restype = None
+    fn.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_int, C.c_void_p]
+    fn(cig.ctypes.data, qo.ctypes.data, nc.ctypes.data, n, text.ctypes.data, stride, lens.ctypes.data)
+    strs = [bytes(text[i * stride:i * stride + max(int(lens[i]), 0)]).decode() for i in range(n)]
+    return strs, lens
+
+
 def ref_host_align(p: Params, b: Batch, threads: int = 0, want_packed=False) -> Outputs:
     lib = _load(os.path.join("_ref", "libgasal_ref_host.so"))
     fn = lib.ref_host_align

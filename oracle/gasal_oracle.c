@@ -736,3 +736,36 @@ int oracle_align_ex(const gb_params_t *p, const gb_batch_t *b, gb_out_t *o, int 
     free(pq), free(pt);
     return err ? GB_ERR_ALLOC : GB_OK;
 }
+
+/* ---------------- forward CIGAR text (test_prog/test_prog.cpp:382-428) ---------------- */
+void oracle_cigar_text(const uint8_t *cigar, const uint32_t *q_off, const uint32_t *n_cigar, int n, char *text,
+                       int stride, int32_t *text_len)
+{
+    static const char OPS[4] = {'M', 'X', 'D', 'I'};
+    for (int i = 0; i < n; i++) {
+        char *out = text + (size_t)i * stride;
+        const uint8_t *c = cigar + q_off[i];
+        int len = 0, ok = 1;
+        /* runs in forward order: the bytes from last to first */
+        int u = (int)n_cigar[i] - 1;
+        while (u >= 0 && ok) {
+            const int op = c[u] & 3;
+            long count = 0;
+            while (u >= 0 && (c[u] & 3) == op) count += c[u--] >> 2;
+            char digits[24];
+            int nd = 0;
+            do {
+                digits[nd++] = (char)('0' + count % 10);
+                count /= 10;
+            } while (count > 0);
+            if (len + nd + 1 > stride - 1) {
+                ok = 0;
+                break;
+            }
+            while (nd > 0) out[len++] = digits[--nd];
+            out[len++] = OPS[op];
+        }
+        if (stride > 0) out[ok ? len : 0] = 0;
+        text_len[i] = ok ? len : -1;
+    }
+}

@@ -50,6 +50,17 @@ int oracle_align(const gb_params_t *p, const gb_batch_t *b, gb_out_t *o, int thr
 void oracle_pack(const uint8_t *ascii, uint32_t nbytes, uint32_t *words);
 void oracle_revcomp(uint32_t *words, uint32_t word_off, uint32_t len, int op, int compat);
 
+/* Forward CIGAR text of every pair from the run-length bytes the traceback
+ * wrote (count << 2 | op, last operation first, at each pair's query offset),
+ * as the reference's test program prints it (test_prog/test_prog.cpp:382-428):
+ * bytes read from last to first, neighbouring runs of one operation merged,
+ * each run printed as its count and M / X / D / I.  Pair i's text goes to
+ * text + i * stride, NUL-terminated; text_len[i] = its length, or -1 when
+ * it needs more than stride - 1 characters.  A pair without operations gets
+ * "" (the reference's loop would read the byte before the pair's slot). */
+void oracle_cigar_text(const uint8_t *cigar, const uint32_t *q_off, const uint32_t *n_cigar, int n, char *text,
+                       int stride, int32_t *text_len);
+
 #ifdef __cplusplus
 }
 #endif
