@@ -570,6 +570,8 @@ __global__ void __launch_bounds__(128) dp_wc_semi_kernel(DpArgs a, const uint32_
             t_start = (tlen - 1) - bbrow;
             q_start = (qlen - 1) - tlen;
         }
+        if (tlen == 0) /* an empty target: every result 0, as on the one-pair-per-thread path */
+            best = 0, brow = 0, sec = 0, srow = 0, t_start = 0, q_start = 0;
         if (gl == 0 && has) {
             if (a.score) a.score[i] = best;
             if (a.t_end) a.t_end[i] = brow;

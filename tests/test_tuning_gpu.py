@@ -179,3 +179,53 @@ def test_long_prefix_runs_its_own_wc_launch():
             assert np.array_equal(got[k], v), f"chunked {p.key()} {k}"
     finally:
         gl.set_tuning(**saved)
+
+
+@pytest.mark.parametrize("group", [0, 8, 16, 32])
+def test_wc_boundary_shapes(group):
+    """Shapes at the edges of the warp-cooperative split, per lane group:
+    queries of exactly 249/256 bases (the 32-word cut) and 1009/1016 bases
+    (the 127-word cut of the separate long launch), targets of 0, 1 and 7
+    bases, and a batch size that leaves groups of the last warp empty."""
+    from gasal_b200.capi import Batch
+    saved = gl.get_tuning()
+    rng = np.random.default_rng(160 + group)
+
+    def seq(n):
+        return bytes(np.frombuffer(b"ACGT", np.uint8)[rng.integers(0, 4, n)])
+    qs, ts = [], []
+    for i in range(2081):
+        ql = [249, 256, 1009, 1016, 300, 5000][i % 6]
+        q = seq(ql)
+        k = i % 5
+        if k == 0:
+            t = b""
+        elif k == 1:
+            t = seq(1)
+        elif k == 2:
+            t = seq(7)
+        else:
+            t = bytearray(q[: int(rng.integers(1, ql))])
+            for _ in range(len(t) // 30 + 1):
+                t[int(rng.integers(0, len(t)))] = b"ACGT"[int(rng.integers(0, 4))]
+            t = bytes(t)
+        qs.append(q)
+        ts.append(t)
+    b = Batch.from_seqs(qs, ts)
+    try:
+        gl.set_tuning(wc_group=group, wc_min_qregs=32)
+        for p in (Params(algo=LOCAL, start_pos=WITH_START, second_best=1), Params(algo=GLOBAL, start_pos=WITH_TB),
+                  Params(algo=LOCAL, start_pos=WITH_TB),
+                  Params(algo=SEMI_GLOBAL, start_pos=WITH_START, head=TARGET, tail=TARGET, second_best=1)):
+            got = gl.align(p, b).as_dict(p)
+            exp = oracle_align(p, b).as_dict(p)
+            for k, v in exp.items():
+                if p.algo == GLOBAL and k == "score":
+                    keep = b.t_len > 0  # the reference leaves empty-target GLOBAL scores undefined
+                    assert np.array_equal(got[k][keep], v[keep]), f"group {group} {p.key()} {k}"
+                elif k in ("cigar",):
+                    continue
+                else:
+                    assert np.array_equal(got[k], v), f"group {group} {p.key()} {k}"
+    finally:
+        gl.set_tuning(**saved)
