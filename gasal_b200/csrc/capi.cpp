@@ -451,7 +451,8 @@ extern "C" int gb_set_tuning(const gb_tuning_t *t)
     if (!t) return GB_ERR_ARG;
     if (t->block != 32 && t->block != 64 && t->block != 128) return GB_ERR_ARG;
     if (t->wc_min_qregs < 8 || t->min_order_pairs < 0) return GB_ERR_ARG;
-    if (t->wc_group != 0 && t->wc_group != 8 && t->wc_group != 16 && t->wc_group != 32) return GB_ERR_ARG;
+    if (t->wc_group != 0 && t->wc_group != 8 && t->wc_group != 16 && t->wc_group != 32 && t->wc_group != 64)
+        return GB_ERR_ARG;
     gb::Settings &st = gb::settings();
     st.block = t->block, st.wc_min_qregs = t->wc_min_qregs, st.min_order_pairs = t->min_order_pairs;
     st.ksw_wc = t->ksw_warp ? 1 : 0;

@@ -58,11 +58,108 @@ constexpr uint64_t WC_CLASS = (5ull << 0) | (0ull << 4) | (6ull << 8) | (1ull <<
                               (6ull << 44) | (6ull << 48) | (6ull << 52) | (4ull << 56) | (6ull << 60);
 constexpr uint32_t WC_PLAIN = (1u << 0) | (1u << 1) | (1u << 3) | (1u << 4) | (1u << 7) | (1u << 14);
 
-/* lanes of a group of G: its first lane and its ballot mask */
-template <int G> __device__ __forceinline__ int gbase_of(int lane) { return lane & ~(G - 1); }
+/* lanes of a group of G <= 32: its first lane and its ballot mask (a group
+ * of 64 is a whole block of two warps: every lane of each warp) */
+template <int G> __device__ __forceinline__ int gbase_of(int lane) { return G >= 32 ? 0 : lane & ~(G - 1); }
 template <int G> __device__ __forceinline__ unsigned gmask_of(int lane)
 {
-    return G == 32 ? 0xFFFFFFFFu : (((1u << G) - 1u) << (lane & ~(G - 1)));
+    return G >= 32 ? 0xFFFFFFFFu : (((1u << G) - 1u) << (lane & ~(G - 1)));
+}
+/* a lane's index in its group */
+template <int G> __device__ __forceinline__ int glane_of() { return G > 32 ? (int)threadIdx.x : (int)(threadIdx.x & (G - 1)); }
+
+/* Block-wide pieces of the 64-lane (two-warp) groups; each ends with the
+ * block barrier so its shared slots can be reused at once. */
+template <int G> __device__ __forceinline__ int grp_max(int v)
+{
+#pragma unroll
+    for (int off = (G > 32 ? 32 : G) / 2; off > 0; off >>= 1) v = max(v, __shfl_xor_sync(0xFFFFFFFFu, v, off));
+    if constexpr (G > 32) {
+        __shared__ int x[2];
+        if ((threadIdx.x & 31) == 0) x[threadIdx.x >> 5] = v;
+        __syncthreads();
+        v = max(x[0], x[1]);
+        __syncthreads();
+    }
+    return v;
+}
+/* inclusive prefix maximum over the group's lanes in lane order */
+template <int G> __device__ __forceinline__ int grp_prefix_max(int v)
+{
+    const int gl = glane_of<G>(), wl = threadIdx.x & 31;
+#pragma unroll
+    for (int off = 1; off < (G > 32 ? 32 : G); off <<= 1) {
+        const int o = __shfl_up_sync(0xFFFFFFFFu, v, off, G > 32 ? 32 : G);
+        if ((G > 32 ? wl : gl) >= off) v = max(v, o);
+    }
+    if constexpr (G > 32) {
+        __shared__ int x;
+        if (threadIdx.x == 31) x = v;
+        __syncthreads();
+        if (threadIdx.x >= 32) v = max(v, x);
+        __syncthreads();
+    }
+    return v;
+}
+/* value of lane `src` of the group */
+template <int G> __device__ __forceinline__ int grp_bcast(int v, int src)
+{
+    if constexpr (G > 32) {
+        __shared__ int x;
+        if ((int)threadIdx.x == src) x = v;
+        __syncthreads();
+        v = x;
+        __syncthreads();
+        return v;
+    } else {
+        return __shfl_sync(0xFFFFFFFFu, v, gbase_of<G>(threadIdx.x & 31) + src);
+    }
+}
+/* the value of the group's previous lane (`fill` for lane 0) */
+template <int G> __device__ __forceinline__ int grp_shift_up1(int v, int fill)
+{
+    const int gl = glane_of<G>();
+    int o = __shfl_up_sync(0xFFFFFFFFu, v, 1, G > 32 ? 32 : G);
+    if constexpr (G > 32) {
+        __shared__ int x;
+        if (threadIdx.x == 31) x = v;
+        __syncthreads();
+        if (threadIdx.x == 32) o = x;
+        __syncthreads();
+    }
+    return gl == 0 ? fill : o;
+}
+/* largest value, then smallest index, over the group */
+template <int G> __device__ __forceinline__ void grp_argmax(int &v, int &idx)
+{
+#pragma unroll
+    for (int off = (G > 32 ? 32 : G) / 2; off > 0; off >>= 1) {
+        const int ov = __shfl_xor_sync(0xFFFFFFFFu, v, off), oi = __shfl_xor_sync(0xFFFFFFFFu, idx, off);
+        if (ov > v || (ov == v && oi < idx)) v = ov, idx = oi;
+    }
+    if constexpr (G > 32) {
+        __shared__ int xv[2], xi[2];
+        if ((threadIdx.x & 31) == 0) xv[threadIdx.x >> 5] = v, xi[threadIdx.x >> 5] = idx;
+        __syncthreads();
+        const int o = (threadIdx.x >> 5) ^ 1;
+        if (xv[o] > v || (xv[o] == v && xi[o] < idx)) v = xv[o], idx = xi[o];
+        __syncthreads();
+    }
+}
+/* first lane of the group (lowest index) with `hit`, or -1 */
+template <int G> __device__ __forceinline__ int grp_first(bool hit)
+{
+    const unsigned m = __ballot_sync(0xFFFFFFFFu, hit) & gmask_of<G>(threadIdx.x & 31);
+    if constexpr (G > 32) {
+        __shared__ int x[2];
+        if ((threadIdx.x & 31) == 0) x[threadIdx.x >> 5] = m ? (int)(threadIdx.x & ~31u) + __ffs(m) - 1 : -1;
+        __syncthreads();
+        const int f = x[0] >= 0 ? x[0] : x[1];
+        __syncthreads();
+        return f;
+    } else {
+        return m ? __ffs(m) - 1 - gbase_of<G>(threadIdx.x & 31) : -1;
+    }
 }
 
 /* all codes of the group's words plain (A, C, G, T and the like)? */
@@ -70,11 +167,12 @@ template <int G> __device__ bool wc_plain(const uint32_t *w, int n)
 {
     const int lane = threadIdx.x & 31;
     uint32_t bad = 0;
-    for (int i = lane & (G - 1); i < n; i += G) {
+    for (int i = glane_of<G>(); i < n; i += G) {
         const uint32_t x = w[i];
 #pragma unroll
         for (int k = 0; k < 8; k++) bad |= ~(WC_PLAIN >> ((x >> (4 * k)) & 15u)) & 1u;
     }
+    if constexpr (G > 32) return grp_first<G>(bad != 0) < 0;
     return (__ballot_sync(0xFFFFFFFFu, bad != 0) & gmask_of<G>(lane)) == 0;
 }
 
@@ -128,13 +226,21 @@ __device__ __forceinline__ bool rec_before(const WcRec &a, const WcRec &b)
 template <int G> __device__ __forceinline__ WcRec rec_reduce(WcRec r)
 {
 #pragma unroll
-    for (int off = G / 2; off > 0; off >>= 1) {
+    for (int off = (G > 32 ? 32 : G) / 2; off > 0; off >>= 1) {
         WcRec o;
         o.v = __shfl_xor_sync(0xFFFFFFFFu, r.v, off);
         o.band = __shfl_xor_sync(0xFFFFFFFFu, r.band, off);
         o.col = __shfl_xor_sync(0xFFFFFFFFu, r.col, off);
         o.row = __shfl_xor_sync(0xFFFFFFFFu, r.row, off);
         if (rec_before(o, r)) r = o;
+    }
+    if constexpr (G > 32) {
+        __shared__ WcRec x[2];
+        if ((threadIdx.x & 31) == 0) x[threadIdx.x >> 5] = r;
+        __syncthreads();
+        const WcRec o = x[(threadIdx.x >> 5) ^ 1];
+        if (rec_before(o, r)) r = o;
+        __syncthreads();
     }
     return r;
 }
@@ -169,8 +275,14 @@ __device__ void wc_sweep(QW qword, int qregs, TW tword, int tregs, int qlen, int
                          WcScore &S, uint32_t *ring, uint4 *tb, int stop, int *bandmax, bool write_bandmax,
                          WcRec &best_out, WcRec &sec_out, int &gscore)
 {
-    const int lane = threadIdx.x & 31, gl = lane & (G - 1);
+    const int lane = threadIdx.x & 31, gl = glane_of<G>();
     const unsigned gmask = gmask_of<G>(lane);
+    constexpr int SW = G > 32 ? 32 : G; /* shuffle width */
+    /* G = 64: warp 0's last lane hands its outputs to warp 1's first lane
+     * through shared memory, double-buffered by step parity, one block
+     * barrier per step; hits are combined the same way */
+    __shared__ uint32_t xch[2][8];
+    __shared__ int xhit[2][2];
     const int rounds = (tregs + G - 1) / G; /* 0 for a group without a pair */
     const bool local = MODE != 2;
     const int last_band = tregs - 1, last_row_in_band = tlen - 1 - ((tregs - 1) << 3);
@@ -185,22 +297,27 @@ __device__ void wc_sweep(QW qword, int qregs, TW tword, int tregs, int qlen, int
     int bandbest = 0;
     int hit_round = 0x7fffffff;
     const long gsteps = rounds > 0 && qregs > 0 ? (long)rounds * qregs + G - 1 : 0;
-    const long steps = G == 32 ? gsteps : (long)__reduce_max_sync(0xFFFFFFFFu, (unsigned)gsteps);
+    const long steps = G >= 32 ? gsteps : (long)__reduce_max_sync(0xFFFFFFFFu, (unsigned)gsteps);
     for (long s = 0; s < steps; s++) {
         const long rel = s - gl;
         const int r = rel >= 0 && qregs > 0 ? (int)(rel / qregs) : -1;
         const int w = rel >= 0 ? (int)(rel - (long)r * qregs) : 0;
         const int band = r * G + gl;
         /* a group is done once its lanes are past the first round with a
-         * hit (MODE 1) or its sweep has ended; the warp leaves together */
+         * hit (MODE 1) or its sweep has ended; the warp (block for G = 64)
+         * leaves together */
         const bool gdone = s >= gsteps || (MODE == 1 && hit_round != 0x7fffffff &&
                                            s >= (long)(hit_round + 1) * qregs + G - 1);
-        if (MODE == 1 && (G == 32 ? gdone : __all_sync(0xFFFFFFFFu, gdone))) break;
+        if (MODE == 1 && (G >= 32 ? gdone : __all_sync(0xFFFFFFFFu, gdone))) break;
         const bool active = !gdone && rel >= 0 && r < rounds && band < tregs;
         /* inputs: bottom H/E of the band above at the 8 columns of word w */
         uint32_t in[8];
 #pragma unroll
-        for (int k = 0; k < 8; k++) in[k] = __shfl_up_sync(0xFFFFFFFFu, out[k], 1, G);
+        for (int k = 0; k < 8; k++) in[k] = __shfl_up_sync(0xFFFFFFFFu, out[k], 1, SW);
+        if (G > 32 && gl == 32) {
+#pragma unroll
+            for (int k = 0; k < 8; k++) in[k] = xch[(s + 1) & 1][k];
+        }
         if (gl == 0 && active) {
             if (r == 0) {
 #pragma unroll
@@ -302,7 +419,24 @@ __device__ void wc_sweep(QW qword, int qregs, TW tword, int tregs, int qlen, int
             if (w == qregs - 1 && write_bandmax) bandmax[band] = bandbest;
         }
         __syncwarp();
-        if (MODE == 1) {
+        if constexpr (G > 32) {
+            if (gl == 31) {
+#pragma unroll
+                for (int k = 0; k < 8; k++) xch[s & 1][k] = out[k];
+            }
+            if (MODE == 1) {
+                const bool hit = active && w == qregs - 1 && bandbest >= stop;
+                const unsigned m = __ballot_sync(0xFFFFFFFFu, hit);
+                const int hr = __shfl_sync(0xFFFFFFFFu, r, m ? __ffs(m) - 1 : lane);
+                if (lane == 0) xhit[s & 1][threadIdx.x >> 5] = m ? hr : 0x7fffffff;
+            }
+            __syncthreads();
+            if (MODE == 1) {
+                const int h0 = xhit[s & 1][0], h1 = xhit[s & 1][1];
+                const int hr = h0 != 0x7fffffff ? h0 : h1;
+                if (hr < hit_round) hit_round = hr;
+            }
+        } else if (MODE == 1) {
             /* a band reaching the forward score ends the group's sweep after its round */
             const bool hit = active && w == qregs - 1 && bandbest >= stop;
             const unsigned m = __ballot_sync(0xFFFFFFFFu, hit) & gmask;
@@ -326,10 +460,13 @@ template <int G, bool START_PASS, bool OPEN_NN, class QW, class TW>
 __device__ void wc_semi_sweep(QW qword, int qregs, TW tword, int tregs, int T0, int qlen, const Scores &sc,
                               int head, WcScore &S, uint32_t *ring, int *lastcol, int stop)
 {
-    const int lane = threadIdx.x & 31, gl = lane & (G - 1);
+    const int lane = threadIdx.x & 31, gl = glane_of<G>();
     const unsigned gmask = gmask_of<G>(lane);
+    constexpr int SW = G > 32 ? 32 : G; /* shuffle width */
+    __shared__ uint32_t xch[2][8];      /* G = 64: warp 0's last lane -> warp 1's first, by step parity */
+    __shared__ int xhit[2][2];
     const int nb = tregs - T0;
-    if (G == 32 && nb <= 0) return;
+    if (G >= 32 && nb <= 0) return;
     const int rounds = nb > 0 ? (nb + G - 1) / G : 0;
     const bool free_head_t = (head == TARGET_ || head == BOTH_);
     const bool zero_rows = (head == QUERY_ || head == BOTH_);
@@ -343,7 +480,7 @@ __device__ void wc_semi_sweep(QW qword, int qregs, TW tword, int tregs, int T0, 
     int hit_round = 0x7fffffff;
     const int lastw = (qlen - 1) >> 3, lastb = (qlen - 1) & 7;
     const long gsteps = rounds > 0 && qregs > 0 ? (long)rounds * qregs + G - 1 : 0;
-    const long steps = G == 32 ? gsteps : (long)__reduce_max_sync(0xFFFFFFFFu, (unsigned)gsteps);
+    const long steps = G >= 32 ? gsteps : (long)__reduce_max_sync(0xFFFFFFFFu, (unsigned)gsteps);
     for (long st = 0; st < steps; st++) {
         const long rel = st - gl;
         const int r = rel >= 0 && qregs > 0 ? (int)(rel / qregs) : -1;
@@ -351,11 +488,15 @@ __device__ void wc_semi_sweep(QW qword, int qregs, TW tword, int tregs, int T0, 
         const int brel = r * G + gl;
         const bool gdone = st >= gsteps || (START_PASS && hit_round != 0x7fffffff &&
                                             st >= (long)(hit_round + 1) * qregs + G - 1);
-        if (START_PASS && (G == 32 ? gdone : __all_sync(0xFFFFFFFFu, gdone))) break;
+        if (START_PASS && (G >= 32 ? gdone : __all_sync(0xFFFFFFFFu, gdone))) break;
         const bool active = !gdone && rel >= 0 && r < rounds && brel < nb;
         uint32_t in[8];
 #pragma unroll
-        for (int k = 0; k < 8; k++) in[k] = __shfl_up_sync(0xFFFFFFFFu, out[k], 1, G);
+        for (int k = 0; k < 8; k++) in[k] = __shfl_up_sync(0xFFFFFFFFu, out[k], 1, SW);
+        if (G > 32 && gl == 32) {
+#pragma unroll
+            for (int k = 0; k < 8; k++) in[k] = xch[(st + 1) & 1][k];
+        }
         if (gl == 0 && active) {
             if (r == 0) {
 #pragma unroll
@@ -439,13 +580,30 @@ __device__ void wc_semi_sweep(QW qword, int qregs, TW tword, int tregs, int T0, 
             }
         }
         __syncwarp();
-        if (START_PASS) {
+        if constexpr (G > 32) {
+            if (gl == 31) {
+#pragma unroll
+                for (int k = 0; k < 8; k++) xch[st & 1][k] = out[k];
+            }
+            if (START_PASS) {
+                const unsigned m = __ballot_sync(0xFFFFFFFFu, hit);
+                const int hr = __shfl_sync(0xFFFFFFFFu, r, m ? __ffs(m) - 1 : lane);
+                if (lane == 0) xhit[st & 1][threadIdx.x >> 5] = m ? hr : 0x7fffffff;
+            }
+            __syncthreads();
+            if (START_PASS) {
+                const int h0 = xhit[st & 1][0], h1 = xhit[st & 1][1];
+                const int hr = h0 != 0x7fffffff ? h0 : h1;
+                if (hr < hit_round) hit_round = hr;
+            }
+        } else if (START_PASS) {
             const unsigned m = __ballot_sync(0xFFFFFFFFu, hit) & gmask;
             const int hr = __shfl_sync(0xFFFFFFFFu, r, m ? __ffs(m) - 1 : lane);
             if (m && hr < hit_round) hit_round = hr;
         }
     }
-    __syncwarp();
+    if constexpr (G > 32) __syncthreads();
+    else __syncwarp();
 }
 
 /* First maximum (strict >, row order) of lastcol over rows [r0, r1) with the
@@ -455,64 +613,49 @@ template <int G, bool SECOND>
 __device__ void wc_lastcol_scan(const int *lastcol, int r0, int r1, int row0, int &best, int &brow, int &sec,
                                 int &srow)
 {
-    const int lane = threadIdx.x & 31, gl = lane & (G - 1);
+    const int gl = glane_of<G>();
     best = NEG16W, brow = row0, sec = NEG16W, srow = row0;
     int carry = NEG16W; /* max of the rows before the chunk */
     const int chunks = r1 > r0 ? (r1 - r0 + G - 1) / G : 0;
-    const int nchunks = G == 32 ? chunks : (int)__reduce_max_sync(0xFFFFFFFFu, (unsigned)chunks);
+    const int nchunks = G >= 32 ? chunks : (int)__reduce_max_sync(0xFFFFFFFFu, (unsigned)chunks);
     for (int ch = 0; ch < nchunks; ch++) {
         const int base = r0 + ch * G;
         const int row = base + gl;
         const int h = row < r1 ? lastcol[row] : NEG16W - 1;
-        int pm = h; /* inclusive prefix max within the chunk */
-#pragma unroll
-        for (int off = 1; off < G; off <<= 1) {
-            const int o = __shfl_up_sync(0xFFFFFFFFu, pm, off, G);
-            if (gl >= off) pm = max(pm, o);
-        }
-        int before = __shfl_up_sync(0xFFFFFFFFu, pm, 1, G);
-        before = gl == 0 ? carry : max(before, carry);
+        const int pm = grp_prefix_max<G>(h); /* inclusive prefix max within the chunk */
+        const int before = max(grp_shift_up1<G>(pm, carry), carry);
         /* chunk argmax, first row on ties */
         int bv = h, br = row;
-#pragma unroll
-        for (int off = G / 2; off > 0; off >>= 1) {
-            const int ov = __shfl_xor_sync(0xFFFFFFFFu, bv, off), orow = __shfl_xor_sync(0xFFFFFFFFu, br, off);
-            if (ov > bv || (ov == bv && orow < br)) bv = ov, br = orow;
-        }
+        grp_argmax<G>(bv, br);
         if (bv > best) best = bv, brow = br;
         if (SECOND) {
             const bool q = row < r1 && h < before && h > NEG16W;
             int sv = q ? h : NEG16W - 1, sr = row;
-#pragma unroll
-            for (int off = G / 2; off > 0; off >>= 1) {
-                const int ov = __shfl_xor_sync(0xFFFFFFFFu, sv, off), orow = __shfl_xor_sync(0xFFFFFFFFu, sr, off);
-                if (ov > sv || (ov == sv && orow < sr)) sv = ov, sr = orow;
-            }
+            grp_argmax<G>(sv, sr);
             if (sv > sec) sec = sv, srow = sr;
         }
-        carry = max(carry, __shfl_sync(0xFFFFFFFFu, pm, gbase_of<G>(lane) + G - 1));
+        carry = max(carry, grp_bcast<G>(pm, G - 1));
     }
 }
 
 template <int G, bool SECOND, bool START>
 __global__ void __launch_bounds__(128) dp_wc_semi_kernel(DpArgs a, const uint32_t *list, int nlist, int ring_cols)
 {
-    constexpr int NG = 32 / G; /* pairs per warp */
     extern __shared__ uint32_t wc_smem[];
     __shared__ uint2 tab[16];
     wc_score_table(tab, a.sc, true);
     __syncthreads();
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, gl = lane & (G - 1), gi = lane / G;
-    const unsigned gmask = gmask_of<G>(lane);
-    const int warps_per_block = blockDim.x >> 5;
-    const int slot = warp * NG + gi; /* this group's ring and last-column buffer */
+    const int gl = glane_of<G>();
+    /* groups per block: 32/G per warp, or one two-warp group (G = 64) */
+    const int gpb = G > 32 ? 1 : (int)(blockDim.x >> 5) * (32 / G);
+    const int slot = G > 32 ? 0 : (int)(threadIdx.x / G); /* this group's ring and last-column buffer */
     uint32_t *ring = wc_smem + (size_t)slot * ring_cols;
-    int *lastcol = a.lastcol + ((size_t)blockIdx.x * warps_per_block * NG + slot) * a.scratch_cols;
+    int *lastcol = a.lastcol + ((size_t)blockIdx.x * gpb + slot) * a.scratch_cols;
     const bool fast_scores = a.sc.match >= -128 && a.sc.match <= 127 && a.sc.mismatch >= -127 && a.sc.mismatch <= 128;
     const bool open_nn = a.sc.o >= 0;
-    for (int item0 = (blockIdx.x * warps_per_block + warp) * NG; item0 < nlist;
-         item0 += gridDim.x * warps_per_block * NG) {
-        const int item = item0 + gi;
+    for (int item0 = blockIdx.x * gpb; item0 < nlist; item0 += gridDim.x * gpb) {
+        if constexpr (G > 32) __syncthreads(); /* both warps are done with the previous pair */
+        const int item = item0 + slot;
         const bool has = item < nlist; /* the last warp may have groups without a pair */
         const int i = has ? (int)list[item] : 0;
         const int qlen = has ? (int)a.q_len[i] : 0, tlen = has ? (int)a.t_len[i] : 0;
@@ -540,7 +683,8 @@ __global__ void __launch_bounds__(128) dp_wc_semi_kernel(DpArgs a, const uint32_
             if (gend_reg < 0) gend_reg = 0;
             auto rq = [&](int j) { return rev_window(q, qlen - 8 - (j << 3)); };
             auto rt = [&](int T) { return rev_window(t, tlen - 8 - (T << 3)); };
-            __syncwarp();
+            if constexpr (G > 32) __syncthreads();
+            else __syncwarp();
             if (open_nn)
                 wc_semi_sweep<G, true, true>(rq, qregs, rt, tregs, gend_reg, qlen, a.sc, a.head, S, ring, lastcol,
                                              best);
@@ -551,19 +695,18 @@ __global__ void __launch_bounds__(128) dp_wc_semi_kernel(DpArgs a, const uint32_
             const int r0 = gend_reg << 3;
             int r1 = min(tregs << 3, tlen);
             const int chunks = r1 > r0 ? (r1 - r0 + G - 1) / G : 0;
-            const int nchunks = G == 32 ? chunks : (int)__reduce_max_sync(0xFFFFFFFFu, (unsigned)chunks);
+            const int nchunks = G >= 32 ? chunks : (int)__reduce_max_sync(0xFFFFFFFFu, (unsigned)chunks);
             bool found = false;
             for (int ch = 0; ch < nchunks; ch++) {
                 const int base = r0 + ch * G;
                 const int row = base + gl;
-                const unsigned m =
-                    __ballot_sync(0xFFFFFFFFu, !found && row < r1 && lastcol[row] >= best) & gmask;
-                if (m) {
-                    const int hit = base + (__ffs(m) - 1 - gbase_of<G>(lane));
+                const int f = grp_first<G>(!found && row < r1 && lastcol[row] >= best);
+                if (f >= 0 && !found) {
+                    const int hit = base + f;
                     r1 = min(r1, ((hit >> 3) + 1) << 3);
                     found = true;
                 }
-                if (G == 32 && found) break;
+                if (G >= 32 && found) break;
             }
             int bb, bbrow, s2, s2r;
             wc_lastcol_scan<G, false>(lastcol, r0, r1, 0, bb, bbrow, s2, s2r);
@@ -597,20 +740,20 @@ __global__ void __launch_bounds__(128) dp_wc_semi_kernel(DpArgs a, const uint32_
 template <int G, int ALGO, int START, bool SECOND>
 __global__ void __launch_bounds__(128) dp_wc_kernel(DpArgs a, const uint32_t *list, int nlist, int ring_cols)
 {
-    constexpr int NG = 32 / G; /* pairs per warp */
     extern __shared__ uint32_t wc_smem[];
     __shared__ uint2 tab[16];
     wc_score_table(tab, a.sc, ALGO == LOCAL_);
     __syncthreads();
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, gl = lane & (G - 1), gi = lane / G;
-    const int warps_per_block = blockDim.x >> 5;
-    const int slot = warp * NG + gi; /* this group's ring and band maxima */
+    const int gl = glane_of<G>();
+    /* groups per block: 32/G per warp, or one two-warp group (G = 64) */
+    const int gpb = G > 32 ? 1 : (int)(blockDim.x >> 5) * (32 / G);
+    const int slot = G > 32 ? 0 : (int)(threadIdx.x / G); /* this group's ring and band maxima */
     uint32_t *ring = wc_smem + (size_t)slot * ring_cols;
-    int *bandmax = (int *)(wc_smem + (size_t)warps_per_block * NG * ring_cols) + (size_t)slot * a.scratch_cols;
+    int *bandmax = (int *)(wc_smem + (size_t)gpb * ring_cols) + (size_t)slot * a.scratch_cols;
     const bool fast_scores = a.sc.match >= -128 && a.sc.match <= 127 && a.sc.mismatch >= -127 && a.sc.mismatch <= 128;
-    for (int item0 = (blockIdx.x * warps_per_block + warp) * NG; item0 < nlist;
-         item0 += gridDim.x * warps_per_block * NG) {
-        const int item = item0 + gi;
+    for (int item0 = blockIdx.x * gpb; item0 < nlist; item0 += gridDim.x * gpb) {
+        if constexpr (G > 32) __syncthreads(); /* both warps are done with the previous pair */
+        const int item = item0 + slot;
         const bool has = item < nlist; /* the last warp may have groups without a pair */
         const int i = has ? (int)list[item] : 0;
         const int qlen = has ? (int)a.q_len[i] : 0, tlen = has ? (int)a.t_len[i] : 0;
@@ -637,8 +780,7 @@ __global__ void __launch_bounds__(128) dp_wc_kernel(DpArgs a, const uint32_t *li
             wc_sweep<G, 2, START == WITH_TB_, false>(qf, qregs, tf, tregs, qlen, tlen, a.sc, S, ring, tb, 0,
                                                      bandmax, false, best, sec, gscore);
             /* the owner lane of the last band holds the score */
-            const int owner = gbase_of<G>(lane) + ((tregs - 1) & (G - 1));
-            gscore = __shfl_sync(0xFFFFFFFFu, gscore, owner);
+            gscore = grp_bcast<G>(gscore, (tregs - 1) & (G - 1));
             if (gl == 0 && has && a.score) a.score[i] = gscore;
             continue;
         }
@@ -648,24 +790,21 @@ __global__ void __launch_bounds__(128) dp_wc_kernel(DpArgs a, const uint32_t *li
         best = rec_reduce<G>(best);
         WcRec secr = {0, 0x7fffffff, 0, 0};
         if (SECOND) {
-            __syncwarp();
-            /* exclusive prefix maximum over bands, in place */
+            if constexpr (G > 32) __syncthreads();
+            else __syncwarp();
+            /* inclusive prefix maximum over bands, in place */
             int carry = 0;
             const int chunks = (tregs + G - 1) / G;
-            const int nchunks = G == 32 ? chunks : (int)__reduce_max_sync(0xFFFFFFFFu, (unsigned)chunks);
+            const int nchunks = G >= 32 ? chunks : (int)__reduce_max_sync(0xFFFFFFFFu, (unsigned)chunks);
             for (int ch = 0; ch < nchunks; ch++) {
                 const int b = ch * G + gl;
-                int v = b < tregs ? bandmax[b] : 0;
-#pragma unroll
-                for (int off = 1; off < G; off <<= 1) {
-                    const int o = __shfl_up_sync(0xFFFFFFFFu, v, off, G);
-                    if (gl >= off) v = max(v, o);
-                }
+                int v = grp_prefix_max<G>(b < tregs ? bandmax[b] : 0);
                 v = max(v, carry);
                 if (b < tregs) bandmax[b] = v;
-                carry = __shfl_sync(0xFFFFFFFFu, v, gbase_of<G>(lane) + G - 1);
+                carry = grp_bcast<G>(v, G - 1);
             }
-            __syncwarp();
+            if constexpr (G > 32) __syncthreads();
+            else __syncwarp();
             WcRec b2, s2;
             int g2 = 0;
             wc_sweep<G, 0, false, true>(qf, qregs, tf, tregs, qlen, tlen, a.sc, S, ring, nullptr, 0, bandmax, false,
@@ -692,13 +831,31 @@ __global__ void __launch_bounds__(128) dp_wc_kernel(DpArgs a, const uint32_t *li
                 ts = gidx + (bs.row - (bs.band << 3));
                 qs = (rend_reg << 3) - 1 - bs.col;
             } else if (best.v > 0) {
-                /* reverse region narrower than G words (the ring's reader
+                bool done = false;
+                if constexpr (G > 32) {
+                    /* a two-warp group with a reverse region of 32-63 words:
+                     * warp 0 sweeps it alone on 32 lanes */
+                    if (rend_reg >= 32) {
+                        done = true;
+                        if (threadIdx.x < 32) {
+                            WcRec b2, s2;
+                            int g4 = 0;
+                            wc_sweep<32, 1, false, false>(qr, rend_reg, tr, gend_reg, 0, 0, a.sc, S, ring, nullptr,
+                                                          best.v, bandmax, false, b2, s2, g4);
+                            b2 = rec_reduce<32>(b2);
+                            const int gidx = (gend_reg << 3) - 1 - (b2.band << 3);
+                            ts = gidx + (b2.row - (b2.band << 3));
+                            qs = (rend_reg << 3) - 1 - b2.col;
+                        }
+                    }
+                }
+                /* reverse region narrower than 32 words (the ring's reader
                  * must trail its writer): the group's first lane runs the
                  * one-thread start pass with the group's ring as row buffer.
                  * It stops at the first cell reaching the score -- for the
                  * short local hits that end this early, a few bands -- where
-                 * the group would finish a G-band round. */
-                if (gl == 0) {
+                 * the group would finish a 32-band round. */
+                if (!done && gl == 0) {
                     RowBuf rb{ring, 1u};
                     Res rr = {best.v, best.col, best.row, 0, 0, 0, 0, 0};
                     if (S.fast) {
@@ -712,7 +869,8 @@ __global__ void __launch_bounds__(128) dp_wc_kernel(DpArgs a, const uint32_t *li
                     qs = rr.q_start, ts = rr.t_start;
                 }
             }
-            __syncwarp();
+            if constexpr (G > 32) __syncthreads();
+            else __syncwarp();
         }
         if (gl == 0 && has) {
             if (a.score) a.score[i] = best.v;
@@ -738,7 +896,7 @@ __global__ void __launch_bounds__(128) dp_wc_kernel(DpArgs a, const uint32_t *li
 size_t wc_smem_bytes(int algo, int group, int warps, int max_q8, int max_t8)
 {
     const size_t per = (size_t)max_q8 + (algo == SEMI_GLOBAL_ ? 0 : (size_t)max_t8 / 8 + 1);
-    return (size_t)warps * (32 / group) * per * 4;
+    return (size_t)warps * 32 / group * per * 4; /* groups per block x per group */
 }
 
 /* one kernel instantiation per (group, algo, start, second best) */
@@ -764,6 +922,7 @@ template <int G, class F> static cudaError_t with_wc_kernel(int algo, int start,
 }
 template <class F> static cudaError_t with_wc_kernel(int group, int algo, int start, bool second, F &&f)
 {
+    if (group == 64) return with_wc_kernel<64>(algo, start, second, f);
     if (group == 8) return with_wc_kernel<8>(algo, start, second, f);
     if (group == 16) return with_wc_kernel<16>(algo, start, second, f);
     if (group == 32) return with_wc_kernel<32>(algo, start, second, f);
@@ -794,6 +953,7 @@ static WcLaunch wc_shape(int algo, int start, bool second, int group, int max_q8
     WcLaunch best;
     int best_res = 0;
     for (int warps : {4, 2, 1}) {
+        if (group == 64 && warps != 2) continue; /* one two-warp group per block */
         const size_t smem = wc_smem_bytes(algo, group, warps, max_q8, max_t8);
         const int res = wc_blocks_per_sm(algo, start, second, group, warps, smem) * warps;
         if (res > best_res) {
@@ -811,6 +971,12 @@ WcLaunch wc_plan(int algo, int start, bool second, int nlist, int max_q8, int ma
     if (nlist <= 0) return l;
     if (forced_group > 0) {
         l = wc_shape(algo, start, second, forced_group, max_q8, max_t8);
+    } else if (max_group >= 64) {
+        /* queries of 64+ words (the launch of the longest pairs): a few
+         * hundred pairs of very unequal length, so the launch lasts as long
+         * as its longest pair's sweep; two-warp groups halve that */
+        l = wc_shape(algo, start, second, 64, max_q8, max_t8);
+        if (l.group == 0) l = wc_shape(algo, start, second, 32, max_q8, max_t8);
     } else {
         /* the narrowest group that keeps 3/4 of the 32-lane kernel's
          * resident warps: narrower groups waste fewer lanes on each pair's
@@ -834,7 +1000,7 @@ WcLaunch wc_plan(int algo, int start, bool second, int nlist, int max_q8, int ma
     int dev = 0, sms = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    const int per_block = l.warps * (32 / l.group);
+    const int per_block = l.warps * 32 / l.group;
     l.blocks = (nlist + per_block - 1) / per_block;
     const int cap = sms * 64 / l.warps; /* at most 64 warps per SM's worth of blocks; warps loop over pairs */
     if (l.blocks > cap) l.blocks = cap;
@@ -844,7 +1010,7 @@ WcLaunch wc_plan(int algo, int start, bool second, int nlist, int max_q8, int ma
 size_t wc_scratch_words(int algo, const WcLaunch &l, int max_t8)
 {
     if (algo != SEMI_GLOBAL_ || l.group == 0) return 0;
-    return (size_t)l.blocks * l.warps * (32 / l.group) * ((size_t)max_t8 + 8);
+    return (size_t)l.blocks * l.warps * 32 / l.group * ((size_t)max_t8 + 8);
 }
 
 cudaError_t launch_dp_wc(int algo, int start, bool second, const DpArgs &a, const uint32_t *list, int nlist,

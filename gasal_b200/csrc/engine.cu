@@ -220,15 +220,16 @@ int plan_batch(const RunCfg &cfg, const DevBatch &b, const DevOut &o, Workspace 
         const int wstart = (cfg.algo == SEMI_GLOBAL_ && cfg.start == WITH_TB_) ? WITHOUT_START_ : cfg.start;
         const bool wsecond = cfg.second && (cfg.algo == LOCAL_ || cfg.algo == SEMI_GLOBAL_);
         const int max_group = min_words >= 32 ? 32 : min_words >= 16 ? 16 : 8;
-        auto shape_for = [&](int n, uint32_t mq, uint32_t mt) {
+        auto shape_for = [&](int n, uint32_t mq, uint32_t mt, int mg) {
             const int mq8 = (int)((mq + 7) & ~7u), mt8 = (int)((mt + 7) & ~7u);
             if (n <= 0 || mq8 > st.wc_max_q8) return WcLaunch{};
-            return wc_plan(cfg.algo, wstart, wsecond, n, mq8, mt8, st.wc_group, max_group);
+            return wc_plan(cfg.algo, wstart, wsecond, n, mq8, mt8, st.wc_group, mg);
         };
         const int nsmall = nlong - nbig;
         if (nlong > 0 && b.n >= st.min_order_pairs) {
-            p.wc = shape_for(nsmall, max_q_long, max_t_long);
-            p.wc_big = shape_for(nbig, max_q_big, max_t_big);
+            p.wc = shape_for(nsmall, max_q_long, max_t_long, max_group);
+            /* the long launch's pairs all have 127+ query words: two-warp groups fit */
+            p.wc_big = shape_for(nbig, max_q_big, max_t_big, 64);
         }
         p.use_wc = nlong > 0 && b.n >= st.min_order_pairs && (nsmall == 0 || p.wc.group > 0) &&
                    (nbig == 0 || p.wc_big.group > 0);

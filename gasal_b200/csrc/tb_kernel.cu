@@ -81,6 +81,11 @@ __global__ void __launch_bounds__(128) traceback_kernel(TbArgs a)
             if (a.t_start) a.t_start[p] = i;
             if (a.q_start) a.q_start[p] = j;
         }
+    } else if (a.algo == LOCAL_) {
+        /* an empty query or target: no operations and start 0, like every
+         * other result of such a pair (nothing else writes the starts) */
+        if (a.t_start) a.t_start[p] = 0;
+        if (a.q_start) a.q_start[p] = 0;
     }
     if (a.n_cigar) a.n_cigar[p] = n_ops;
 }

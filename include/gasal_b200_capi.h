@@ -240,9 +240,10 @@ typedef struct {
                               device counter (default); 0: one thread per pair on a grid over the batch.
                               With min_order_pairs above the batch size, ksw_warp 0 and split_start 0
                               this is the plain full-DP form: every pair one per thread, in input order */
-    int32_t wc_group;      /* lanes per pair in the warp-cooperative kernels: 32, 16 or 8 (a warp sweeps
-                              32/wc_group pairs side by side), or 0 (default) to pick per launch the
-                              narrowest group that keeps 3/4 of the 32-lane kernel's resident blocks.
+    int32_t wc_group;      /* lanes per pair in the warp-cooperative kernels: 64 (two warps per pair),
+                              32, 16 or 8 (a warp sweeps 32/wc_group pairs side by side), or 0 (default):
+                              per launch the narrowest group that keeps 3/4 of the 32-lane kernel's
+                              resident warps, and two-warp groups for the launch of 127+ word queries.
                               Pairs go warp-cooperative from max(wc_min_qregs, wc_group) query words */
 } gb_tuning_t;
 int gb_set_tuning(const gb_tuning_t *t);

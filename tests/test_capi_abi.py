@@ -112,7 +112,7 @@ def test_tuning_and_graph_settings_validate(so):
     cur = GbTuning()
     assert so.gb_get_tuning(C.byref(cur)) == 0
     for bad in (GbTuning(256, 32, 0, 1, 1, 1, 16), GbTuning(64, 4, 0, 1, 1, 1, 16), GbTuning(64, 32, -1, 1, 1, 1, 16),
-                GbTuning(64, 32, 0, 1, 1, 1, 4), GbTuning(64, 32, 0, 1, 1, 1, 24)):
+                GbTuning(64, 32, 0, 1, 1, 1, 4), GbTuning(64, 32, 0, 1, 1, 1, 24), GbTuning(64, 32, 0, 1, 1, 1, 128)):
         assert so.gb_set_tuning(C.byref(bad)) == -1
     ok = GbTuning(128, 48, 4096, 0, 0, 0, 8)
     assert so.gb_set_tuning(C.byref(ok)) == 0

@@ -119,7 +119,7 @@ def test_plain_form_matches_oracle():
         gl.set_tuning(**saved)
 
 
-@pytest.mark.parametrize("group", [0, 8, 16, 32])
+@pytest.mark.parametrize("group", [0, 8, 16, 32, 64])
 def test_wc_lane_groups_match_oracle(group):
     """Warp-cooperative kernels with 32/group pairs per warp: every mode on
     mixed 50-1000 bp pairs with the cut at `group` words (so the shortest
@@ -181,7 +181,7 @@ def test_long_prefix_runs_its_own_wc_launch():
         gl.set_tuning(**saved)
 
 
-@pytest.mark.parametrize("group", [0, 8, 16, 32])
+@pytest.mark.parametrize("group", [0, 8, 16, 32, 64])
 def test_wc_boundary_shapes(group):
     """Shapes at the edges of the warp-cooperative split, per lane group:
     queries of exactly 249/256 bases (the 32-word cut) and 1009/1016 bases
