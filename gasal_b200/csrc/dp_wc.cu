@@ -298,10 +298,13 @@ __device__ void wc_sweep(QW qword, int qregs, TW tword, int tregs, int qlen, int
     int hit_round = 0x7fffffff;
     const long gsteps = rounds > 0 && qregs > 0 ? (long)rounds * qregs + G - 1 : 0;
     const long steps = G >= 32 ? gsteps : (long)__reduce_max_sync(0xFFFFFFFFu, (unsigned)gsteps);
+    /* this lane's position: word cw of round cr (cw < 0 before its first
+     * step); step s puts the lane at s - gl words into its sweep */
+    int cw = -gl, cr = 0;
     for (long s = 0; s < steps; s++) {
-        const long rel = s - gl;
-        const int r = rel >= 0 && qregs > 0 ? (int)(rel / qregs) : -1;
-        const int w = rel >= 0 ? (int)(rel - (long)r * qregs) : 0;
+        const bool started = cw >= 0;
+        const int r = started ? cr : -1;
+        const int w = started ? cw : 0;
         const int band = r * G + gl;
         /* a group is done once its lanes are past the first round with a
          * hit (MODE 1) or its sweep has ended; the warp (block for G = 64)
@@ -309,7 +312,7 @@ __device__ void wc_sweep(QW qword, int qregs, TW tword, int tregs, int qlen, int
         const bool gdone = s >= gsteps || (MODE == 1 && hit_round != 0x7fffffff &&
                                            s >= (long)(hit_round + 1) * qregs + G - 1);
         if (MODE == 1 && (G >= 32 ? gdone : __all_sync(0xFFFFFFFFu, gdone))) break;
-        const bool active = !gdone && rel >= 0 && r < rounds && band < tregs;
+        const bool active = !gdone && started && r < rounds && band < tregs;
         /* inputs: bottom H/E of the band above at the 8 columns of word w */
         uint32_t in[8];
 #pragma unroll
@@ -443,6 +446,7 @@ __device__ void wc_sweep(QW qword, int qregs, TW tword, int tregs, int qlen, int
             const int hr = __shfl_sync(0xFFFFFFFFu, r, m ? __ffs(m) - 1 : lane);
             if (m && hr < hit_round) hit_round = hr;
         }
+        if (++cw == qregs) cw = 0, ++cr;
     }
     best_out = best;
     sec_out = sec;
@@ -481,15 +485,16 @@ __device__ void wc_semi_sweep(QW qword, int qregs, TW tword, int tregs, int T0, 
     const int lastw = (qlen - 1) >> 3, lastb = (qlen - 1) & 7;
     const long gsteps = rounds > 0 && qregs > 0 ? (long)rounds * qregs + G - 1 : 0;
     const long steps = G >= 32 ? gsteps : (long)__reduce_max_sync(0xFFFFFFFFu, (unsigned)gsteps);
+    int cw = -gl, cr = 0; /* word and round of this lane's step (cw < 0: not started) */
     for (long st = 0; st < steps; st++) {
-        const long rel = st - gl;
-        const int r = rel >= 0 && qregs > 0 ? (int)(rel / qregs) : -1;
-        const int w = rel >= 0 ? (int)(rel - (long)r * qregs) : 0;
+        const bool started = cw >= 0;
+        const int r = started ? cr : -1;
+        const int w = started ? cw : 0;
         const int brel = r * G + gl;
         const bool gdone = st >= gsteps || (START_PASS && hit_round != 0x7fffffff &&
                                             st >= (long)(hit_round + 1) * qregs + G - 1);
         if (START_PASS && (G >= 32 ? gdone : __all_sync(0xFFFFFFFFu, gdone))) break;
-        const bool active = !gdone && rel >= 0 && r < rounds && brel < nb;
+        const bool active = !gdone && started && r < rounds && brel < nb;
         uint32_t in[8];
 #pragma unroll
         for (int k = 0; k < 8; k++) in[k] = __shfl_up_sync(0xFFFFFFFFu, out[k], 1, SW);
@@ -601,6 +606,7 @@ __device__ void wc_semi_sweep(QW qword, int qregs, TW tword, int tregs, int T0, 
             const int hr = __shfl_sync(0xFFFFFFFFu, r, m ? __ffs(m) - 1 : lane);
             if (m && hr < hit_round) hit_round = hr;
         }
+        if (++cw == qregs) cw = 0, ++cr;
     }
     if constexpr (G > 32) __syncthreads();
     else __syncwarp();
