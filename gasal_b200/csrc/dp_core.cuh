@@ -382,6 +382,97 @@ __device__ void global_fwd(const uint32_t *q, int qregs, int qlen, const uint32_
     r.score = score;
 }
 
+/* GLOBAL score without traceback, two 8-row bands per sweep of the query:
+ * the same cells, in the same order per band, with the same values as
+ * global_fwd.  H and E crossing from the first band to the second are
+ * narrowed to int16 exactly as the row buffer narrows them between bands;
+ * they just stay in registers, so each column carries 16 rows of
+ * independent work (the single-band loop is latency-bound) and the row
+ * buffer is read and written once per two bands. */
+template <class SC>
+__device__ void global_fwd2(const uint32_t *q, int qregs, int qlen, const uint32_t *t, int tregs, int tlen,
+                            const Scores &sc, RowBuf rb, SC scr, Res &r)
+{
+    const int q8 = qregs << 3;
+    rb.st(0, pack_he(0, NEG16));
+    for (int c = 1; c < q8; c++) rb.st(c, pack_he(-(sc.o + sc.e * c), NEG16));
+    const int last_row = tlen - 1 - ((tregs - 1) << 3);
+    int score = 0;
+    SC scb = scr;
+    for (int T = 0; T < tregs; T += 2) {
+        const bool two = T + 1 < tregs;
+        scr.band(t[T], sc, false);
+        if (two) scb.band(t[T + 1], sc, false);
+        int F[8], D[8], FB[8], DB[8];
+#pragma unroll
+        for (int k = 0; k < 8; k++) {
+            const int R = (T << 3) + k, RB = R + 8;
+            F[k] = NEG16, FB[k] = NEG16;
+            D[k] = R == 0 ? 0 : -(sc.o + sc.e * R);
+            DB[k] = -(sc.o + sc.e * RB);
+        }
+        const bool last_a = T == tregs - 1, last_b = T + 1 == tregs - 1;
+        for (int j = 0; j < qregs; j++) {
+            const uint32_t qw = q[j];
+#pragma unroll
+            for (int b = 0; b < 8; b++) {
+                const int c = (j << 3) + b;
+                const int cq = code(qw, b);
+                scr.column(cq);
+                const uint32_t v = rb.ld(c);
+                const int up0 = sext16(v);
+                int e = hi16(v);
+                int Hn[8];
+#pragma unroll
+                for (int k = 0; k < 8; k++) {
+                    const int M = D[k] + scr.s(k);
+                    const int H = __vimax3_s32(M, F[k], e);
+                    const int t0 = M - sc.oe;
+                    F[k] = __viaddmax_s32(F[k], -sc.e, t0);
+                    e = __viaddmax_s32(e, -sc.e, t0);
+                    Hn[k] = H;
+                }
+                D[0] = up0;
+#pragma unroll
+                for (int k = 1; k < 8; k++) D[k] = Hn[k - 1];
+                if (last_a && c == qlen - 1) {
+#pragma unroll
+                    for (int k = 0; k < 8; k++)
+                        if (k == last_row) score = Hn[k];
+                }
+                if (two) {
+                    /* the second band sees the first through the int16 row buffer */
+                    const int upB = (int)(int16_t)Hn[7];
+                    int eB = (int)(int16_t)e;
+                    scb.column(cq);
+                    int HB[8];
+#pragma unroll
+                    for (int k = 0; k < 8; k++) {
+                        const int M = DB[k] + scb.s(k);
+                        const int H = __vimax3_s32(M, FB[k], eB);
+                        const int t0 = M - sc.oe;
+                        FB[k] = __viaddmax_s32(FB[k], -sc.e, t0);
+                        eB = __viaddmax_s32(eB, -sc.e, t0);
+                        HB[k] = H;
+                    }
+                    rb.st(c, pack_he(HB[7], eB));
+                    DB[0] = upB;
+#pragma unroll
+                    for (int k = 1; k < 8; k++) DB[k] = HB[k - 1];
+                    if (last_b && c == qlen - 1) {
+#pragma unroll
+                        for (int k = 0; k < 8; k++)
+                            if (k == last_row) score = HB[k];
+                    }
+                } else {
+                    rb.st(c, pack_he(Hn[7], e));
+                }
+            }
+        }
+    }
+    r.score = score;
+}
+
 /* ========================= SEMI_GLOBAL ================================== */
 /* Reference src/kernels/semiglobal_kernel_template.h.  Standard Gotoh (gaps
  * opened from H), N scores 0.  head/tail select the free end gaps. */

@@ -47,7 +47,8 @@ __device__ __forceinline__ void run_pair(const DpArgs &a, const uint32_t *q, int
         local_fwd<SECOND, START == WITH_TB_>(q, qregs, t, tregs, a.sc, rb, tb, scr, r);
         if (START == WITH_START_) local_start(q, qregs, t, tregs, a.sc, rb, scr, r);
     } else if (ALGO == GLOBAL_) {
-        global_fwd<START == WITH_TB_>(q, qregs, qlen, t, tregs, tlen, a.sc, rb, tb, scr, r);
+        if (START == WITH_TB_) global_fwd<true>(q, qregs, qlen, t, tregs, tlen, a.sc, rb, tb, scr, r);
+        else global_fwd2(q, qregs, qlen, t, tregs, tlen, a.sc, rb, scr, r);
     } else if (ALGO == SEMI_GLOBAL_) {
         semi_global<SECOND, START == WITH_START_>(q, qregs, qlen, t, tregs, tlen, a.sc, a.head, a.tail, a.mql, rb,
                                                  scr, r);
