@@ -70,19 +70,6 @@ template <int G> __device__ __forceinline__ int glane_of() { return G > 32 ? (in
 
 /* Block-wide pieces of the 64-lane (two-warp) groups; each ends with the
  * block barrier so its shared slots can be reused at once. */
-template <int G> __device__ __forceinline__ int grp_max(int v)
-{
-#pragma unroll
-    for (int off = (G > 32 ? 32 : G) / 2; off > 0; off >>= 1) v = max(v, __shfl_xor_sync(0xFFFFFFFFu, v, off));
-    if constexpr (G > 32) {
-        __shared__ int x[2];
-        if ((threadIdx.x & 31) == 0) x[threadIdx.x >> 5] = v;
-        __syncthreads();
-        v = max(x[0], x[1]);
-        __syncthreads();
-    }
-    return v;
-}
 /* inclusive prefix maximum over the group's lanes in lane order */
 template <int G> __device__ __forceinline__ int grp_prefix_max(int v)
 {
