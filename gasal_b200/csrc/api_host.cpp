@@ -54,115 +54,110 @@ Parameters::~Parameters()
     target_batch_fasta.close();
 }
 
+/* The CLI members exist so that callers such as the reference's test program
+ * link unchanged; the option grammar is the one that program relies on (flags
+ * before the two FASTA names, -x taking a head and a tail keyword). */
+
 void Parameters::print()
 {
-    std::cerr << "sa=" << sa << " , sb=" << sb << " , gapo=" << gapo << " , gape=" << gape << std::endl;
-    std::cerr << "start_pos=" << start_pos << " , print_out=" << print_out << " , n_threads=" << n_threads << std::endl;
-    std::cerr << "semiglobal_skipping_head=" << semiglobal_skipping_head
-              << " , semiglobal_skipping_tail=" << semiglobal_skipping_tail << " , algo=" << algo << std::endl;
-    std::cerr << std::boolalpha << "isPacked = " << isPacked << " , secondBest = " << secondBest << std::endl;
-    std::cerr << "query_batch_fasta_filename=" << query_batch_fasta_filename
-              << " , target_batch_fasta_filename=" << target_batch_fasta_filename << std::endl;
+    std::cerr << "[gasal_b200] algo " << algo << ", start " << start_pos << ", scores " << sa << '/' << sb << '/'
+              << gapo << '/' << gape << ", second-best " << secondBest << ", semi-global skip " << semiglobal_skipping_head
+              << '/' << semiglobal_skipping_tail << ", threads " << n_threads << ", band " << k_band << ", files "
+              << query_batch_fasta_filename << ' ' << target_batch_fasta_filename << std::endl;
 }
 
 void Parameters::failure(fail_type f)
 {
-    switch (f) {
-    case NOT_ENOUGH_ARGS:
-        std::cerr << "Not enough Parameters. Required: -y AL_TYPE file1.fasta file2.fasta. See help (--help, -h) for usage. "
-                  << std::endl;
-        break;
-    case WRONG_ARG:
-        std::cerr << "Wrong argument. See help (--help, -h) for usage. " << std::endl;
-        break;
-    case WRONG_FILES:
-        std::cerr << "File error: either a file doesn't exist, or cannot be opened." << std::endl;
-        break;
-    default:
-        break;
-    }
+    static const char *const why[] = {"too few arguments", "too many arguments", "unknown or malformed option",
+                                      "cannot open an input file", "unknown alignment type"};
+    const int k = (int)f;
+    std::cerr << "[gasal_b200] " << (k >= 0 && k < 5 ? why[k] : "bad arguments") << "; -h lists the options"
+              << std::endl;
     exit(1);
 }
 
 void Parameters::help()
 {
-    std::cerr << "Usage: ./test_prog.out [-a] [-b] [-q] [-r] [-s] [-t] [-p] [-n] [-y] <query_batch.fasta> <target_batch.fasta>" << std::endl;
-    std::cerr << "Options: -a INT    match score [" << sa << "]" << std::endl;
-    std::cerr << "         -b INT    mismatch penalty [" << sb << "]" << std::endl;
-    std::cerr << "         -q INT    gap open penalty [" << gapo << "]" << std::endl;
-    std::cerr << "         -r INT    gap extension penalty [" << gape << "]" << std::endl;
-    std::cerr << "         -s        find the start position" << std::endl;
-    std::cerr << "         -t        compute traceback (implies the start position)" << std::endl;
-    std::cerr << "         -p        print the alignment results" << std::endl;
-    std::cerr << "         -n INT    Number of threads [" << n_threads << "]" << std::endl;
-    std::cerr << "         -y AL_TYPE       Alignment type . Must be \"local\", \"semi_global\", \"global\", \"ksw\" " << std::endl;
-    std::cerr << "         -x HEAD TAIL     semi-global: what to skip at heads and tails (NONE, QUERY, TARGET, BOTH)" << std::endl;
-    std::cerr << "         -k INT    Band width in case \"banded\" is selected." << std::endl;
-    std::cerr << "         --help, -h : displays this message." << std::endl;
-    std::cerr << "         --second-best   displays second best score (WITHOUT_START only)." << std::endl;
+    std::cerr << "usage: <program> [options] <query.fasta> <target.fasta>\n"
+                 "  -y local|global|semi_global|ksw   alignment type\n"
+                 "  -a/-b/-q/-r N                     match, mismatch, gap open, gap extend ("
+              << sa << '/' << sb << '/' << gapo << '/' << gape
+              << ")\n"
+                 "  -s | -t                           start positions | traceback\n"
+                 "  -x HEAD TAIL                      semi-global skipped ends: NONE QUERY TARGET BOTH\n"
+                 "  -k N  -n N  -p  --second-best     band width, threads, print results, second best\n";
 }
 
-static data_source parse_src(const std::string &s, bool *ok)
+namespace {
+
+bool skip_keyword(const char *s, data_source *out)
 {
-    *ok = true;
-    if (s == "NONE") return NONE;
-    if (s == "TARGET") return TARGET;
-    if (s == "QUERY") return QUERY;
-    if (s == "BOTH") return BOTH;
-    *ok = false;
-    return NONE;
+    static const struct { const char *name; data_source v; } kw[] = {
+        {"NONE", NONE}, {"QUERY", QUERY}, {"TARGET", TARGET}, {"BOTH", BOTH}};
+    for (const auto &k : kw)
+        if (std::strcmp(s, k.name) == 0) {
+            *out = k.v;
+            return true;
+        }
+    return false;
 }
+
+} // namespace
 
 void Parameters::parse()
 {
-    for (int c = 1; c < argc; c++) {
-        std::string a(argv[c]);
-        if (a == "--help" || a == "-h") {
+    for (int k = 1; k < argc; k++)
+        if (!std::strcmp(argv[k], "-h") || !std::strcmp(argv[k], "--help")) {
             help();
             exit(0);
         }
-    }
     if (argc < 4) failure(NOT_ENOUGH_ARGS);
-    int c;
-    for (c = 1; c < argc - 2; c++) {
-        std::string cur(argv[c]);
-        if (cur.size() >= 2 && cur[0] == '-' && cur[1] == '-') {
-            if (cur == "--second-best") secondBest = TRUE;
-        } else if (!cur.empty() && cur[0] == '-') {
-            if (cur.size() > 2) failure(WRONG_ARG);
-            bool ok = true;
-            switch (cur[1]) {
-            case 'y': {
-                std::string v(argv[++c]);
-                if (v == "local") algo = LOCAL;
-                else if (v == "semi_global") algo = SEMI_GLOBAL;
-                else if (v == "global") algo = GLOBAL;
-                else if (v == "ksw") algo = KSW;
-                break;
+
+    /* integer-valued flags and where they land */
+    struct IntFlag { char flag; int32_t Parameters::*field; };
+    static const IntFlag ints[] = {{'a', &Parameters::sa},   {'b', &Parameters::sb},
+                                   {'q', &Parameters::gapo}, {'r', &Parameters::gape},
+                                   {'n', &Parameters::n_threads}, {'k', &Parameters::k_band}};
+    const int last_opt = argc - 2; /* the final two words are the FASTA files */
+    int k = 1;
+    auto value = [&]() -> const char * { return argv[++k]; };
+    for (; k < last_opt; k++) {
+        const char *w = argv[k];
+        if (w[0] != '-') failure(WRONG_ARG);
+        if (w[1] == '-') { /* long options: only --second-best means anything */
+            if (!std::strcmp(w, "--second-best")) secondBest = TRUE;
+            continue;
+        }
+        if (w[1] == '\0' || w[2] != '\0') failure(WRONG_ARG);
+        const char f = w[1];
+        bool done = false;
+        for (const IntFlag &x : ints)
+            if (x.flag == f) {
+                this->*(x.field) = std::stoi(value());
+                done = true;
             }
-            case 'a': sa = std::stoi(argv[++c]); break;
-            case 'b': sb = std::stoi(argv[++c]); break;
-            case 'q': gapo = std::stoi(argv[++c]); break;
-            case 'r': gape = std::stoi(argv[++c]); break;
-            case 's': start_pos = WITH_START; break;
-            case 't': start_pos = WITH_TB; break;
-            case 'p': print_out = 1; break;
-            case 'n': n_threads = std::stoi(argv[++c]); break;
-            case 'k': k_band = std::stoi(argv[++c]); break;
-            case 'x':
-                semiglobal_skipping_head = parse_src(argv[++c], &ok);
-                if (!ok) failure(WRONG_ARG);
-                semiglobal_skipping_tail = parse_src(argv[++c], &ok);
-                if (!ok) failure(WRONG_ARG);
-                break;
-            default: break;
-            }
-        } else {
-            failure(WRONG_ARG);
+        if (done) continue;
+        switch (f) {
+        case 'y': {
+            static const struct { const char *name; algo_type a; } algos[] = {
+                {"local", LOCAL}, {"global", GLOBAL}, {"semi_global", SEMI_GLOBAL}, {"ksw", KSW}};
+            const char *v = value();
+            for (const auto &x : algos)
+                if (!std::strcmp(v, x.name)) algo = x.a;
+            break;
+        }
+        case 's': start_pos = WITH_START; break;
+        case 't': start_pos = WITH_TB; break;
+        case 'p': print_out = 1; break;
+        case 'x':
+            if (!skip_keyword(value(), &semiglobal_skipping_head)) failure(WRONG_ARG);
+            if (!skip_keyword(value(), &semiglobal_skipping_tail)) failure(WRONG_ARG);
+            break;
+        default: break; /* other single-letter flags are ignored */
         }
     }
-    query_batch_fasta_filename = std::string(argv[c]);
-    target_batch_fasta_filename = std::string(argv[c + 1]);
+    query_batch_fasta_filename = argv[k];
+    target_batch_fasta_filename = argv[k + 1];
     fileopen();
 }
 
@@ -406,40 +401,61 @@ void gasal_host_batch_reset(gasal_gpu_storage_t *gpu_storage)
     }
 }
 
+namespace {
+
+/* One side's page chain and the storage's running total of its host bytes. */
+struct PageChain {
+    host_batch_t *head;
+    uint32_t *total;
+    const char *side;
+};
+
+PageChain chain_of(gasal_gpu_storage_t *s, data_source src)
+{
+    if (src == QUERY) return {s->extensible_host_unpacked_query_batch, &s->host_max_query_batch_bytes, "query"};
+    return {s->extensible_host_unpacked_target_batch, &s->host_max_target_batch_bytes, "target"};
+}
+
+uint32_t page_room(const host_batch_t *p) { return p->page_size - p->data_size; }
+
+} // namespace
+
+/* Appends one sequence, N-padded to a multiple of 8, to the chain's open page:
+ * the first page not yet locked.  When that page lacks room, it is locked and
+ * the write moves to its successor -- re-based to start where the locked
+ * page's data ends -- or, past the last page, to a new page of twice the size
+ * (which also grows the storage's host byte total).  The move happens once per
+ * call; if the page reached still lacks room, nothing is written.  Returns the
+ * byte index after the written sequence (or `idx` unchanged). */
 uint32_t gasal_host_batch_fill(gasal_gpu_storage_t *gpu_storage, uint32_t idx, const char *data, uint32_t size,
                                data_source SRC)
 {
-    host_batch_t *cur = (SRC == QUERY) ? gpu_storage->extensible_host_unpacked_query_batch
-                                       : gpu_storage->extensible_host_unpacked_target_batch;
-    uint32_t *p_batch_bytes = (SRC == QUERY) ? &gpu_storage->host_max_query_batch_bytes
-                                             : &gpu_storage->host_max_target_batch_bytes;
-    const uint32_t pad = (8u - (size & 7u)) & 7u;
-    const uint32_t need = size + pad;
-    while (cur->is_locked) cur = cur->next;
-    if (cur->next == NULL && cur->page_size - cur->data_size < need) {
-        fprintf(stderr,
-                "[GASAL WARNING:] Trying to write %d bytes while only %d remain (%s) (block size %d, filled %d bytes).\n"
-                "                 Allocating a new block of size %d, total size available reaches %d. Doing this repeadtedly slows down the execution.\n",
-                need, cur->page_size - cur->data_size, (SRC == QUERY ? "query" : "target"), cur->page_size,
-                cur->data_size, cur->page_size * 2, *p_batch_bytes + cur->page_size * 2);
-        host_batch_t *res = gasal_host_batch_new(cur->page_size * 2, cur->offset + cur->data_size);
-        cur->next = res;
-        cur->is_locked = 1;
-        *p_batch_bytes = *p_batch_bytes + cur->page_size * 2;
-        cur = cur->next;
+    const PageChain ch = chain_of(gpu_storage, SRC);
+    const uint32_t need = round8(size);
+    host_batch_t *pg = ch.head;
+    while (pg->is_locked) pg = pg->next;
+    if (page_room(pg) < need) {
+        const uint32_t data_end = pg->offset + pg->data_size;
+        if (pg->next == NULL) {
+            const uint32_t grown = pg->page_size * 2;
+            fprintf(stderr,
+                    "[GASAL WARNING:] %s pages: %u bytes needed, %u free on the last page; chaining a new page of %u "
+                    "bytes (host total %u). Size the storage for the batch to avoid this.\n",
+                    ch.side, need, page_room(pg), grown, *ch.total + grown);
+            pg->next = gasal_host_batch_new(grown, data_end);
+            *ch.total += grown;
+        } else {
+            pg->next->offset = data_end;
+        }
+        pg->is_locked = 1;
+        pg = pg->next;
     }
-    if (cur->next != NULL && cur->page_size - cur->data_size < need) {
-        cur->next->offset = cur->offset + cur->data_size;
-        cur->is_locked = 1;
-        cur = cur->next;
-    }
-    if (cur->page_size - cur->data_size >= need) {
-        memcpy(&(cur->data[idx - cur->offset]), data, size);
-        memset(&(cur->data[idx + size - cur->offset]), N_CODE, pad);
-        idx += need;
-        cur->data_size += need;
-    }
-    return idx;
+    if (page_room(pg) < need) return idx;
+    uint8_t *dst = pg->data + (idx - pg->offset);
+    memcpy(dst, data, size);
+    memset(dst + size, N_CODE, need - size);
+    pg->data_size += need;
+    return idx + need;
 }
 
 uint32_t gasal_host_batch_addbase(gasal_gpu_storage_t *gpu_storage, uint32_t idx, const char base, data_source SRC)
@@ -447,31 +463,36 @@ uint32_t gasal_host_batch_addbase(gasal_gpu_storage_t *gpu_storage, uint32_t idx
     return gasal_host_batch_add(gpu_storage, idx, &base, 1, SRC);
 }
 
+/* Writes raw bytes (no padding) at batch index idx into the page that covers
+ * [idx, idx + size): walking from the head, the first page with no successor
+ * or whose successor starts at or after idx + size.  When the storage's host
+ * byte total is below idx + size, the total doubles (until it holds `size`)
+ * and a new page of the new total, starting at idx, is hung after the page the
+ * walk stands on (in place of any successor). */
 uint32_t gasal_host_batch_add(gasal_gpu_storage_t *gpu_storage, uint32_t idx, const char *data, uint32_t size,
                               data_source SRC)
 {
-    host_batch_t *cur = (SRC == QUERY) ? gpu_storage->extensible_host_unpacked_query_batch
-                                       : gpu_storage->extensible_host_unpacked_target_batch;
-    uint32_t *p_batch_bytes = (SRC == QUERY) ? &gpu_storage->host_max_query_batch_bytes
-                                             : &gpu_storage->host_max_target_batch_bytes;
-    for (;;) {
-        if (*p_batch_bytes >= idx + size && (cur->next == NULL || cur->next->offset >= idx + size)) {
-            memcpy(&(cur->data[idx - cur->offset]), data, size);
-            return idx + size;
-        }
-        if (*p_batch_bytes >= idx + size && cur->next != NULL && cur->next->offset < idx + size) {
-            cur = cur->next;
+    const PageChain ch = chain_of(gpu_storage, SRC);
+    const uint32_t stop = idx + size;
+    host_batch_t *pg = ch.head;
+    while (*ch.total < stop || (pg->next != NULL && pg->next->offset < stop)) {
+        if (*ch.total >= stop) {
+            pg = pg->next;
             continue;
         }
+        const uint32_t before = *ch.total;
+        do {
+            *ch.total *= 2;
+        } while (*ch.total < size);
         fprintf(stderr,
-                "[GASAL WARNING:] Trying to write %d bytes at position %d on host memory (%s) while only  %d bytes are available. Therefore, allocating %d bytes more on CPU. Repeating this many times can provoke a degradation of performance.\n",
-                size, idx, (SRC == QUERY ? "query" : "target"), *p_batch_bytes, *p_batch_bytes * 2);
-        *p_batch_bytes += *p_batch_bytes;
-        while (*p_batch_bytes < size) *p_batch_bytes += *p_batch_bytes;
-        host_batch_t *res = gasal_host_batch_new(*p_batch_bytes, idx);
-        cur->next = res;
-        cur = cur->next;
+                "[GASAL WARNING:] %s pages: %u bytes at index %u exceed the %u host bytes; chaining a page of %u "
+                "bytes. Size the storage for the batch to avoid this.\n",
+                ch.side, size, idx, before, *ch.total);
+        pg->next = gasal_host_batch_new(*ch.total, idx);
+        pg = pg->next;
     }
+    memcpy(pg->data + (idx - pg->offset), data, size);
+    return stop;
 }
 
 void gasal_host_batch_print(host_batch_t *res)

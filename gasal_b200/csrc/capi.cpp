@@ -322,7 +322,9 @@ void dev_args(const gb_params_t *p, const gb_dev_batch_t *b, const gb_dev_out_t 
 
 extern "C" int gb_align_dev(const gb_params_t *p, const gb_dev_batch_t *b, const gb_dev_out_t *o, void *stream)
 {
-    if (!p || !b || !o || b->n <= 0 || !b->h_q_len || !b->h_t_len) return GB_ERR_ARG;
+    if (!p || !b || !o || b->n < 0) return GB_ERR_ARG;
+    if (b->n == 0) return GB_OK; /* an empty batch: nothing to launch */
+    if (!b->h_q_len || !b->h_t_len) return GB_ERR_ARG;
     DevWs *w = dev_ws(stream);
     if (!w) return GB_ERR_CUDA;
     gb::RunCfg cfg;

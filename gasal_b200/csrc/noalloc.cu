@@ -21,12 +21,15 @@
  * clearing between calls.  Calls whose work overlaps on the GPU (two streams,
  * or two host threads) race on the array: serialise them.
  *
- * The first call on a device resolves the array's device address with
- * cudaGetSymbolAddress while that device is current; make that first call
- * before any stream capture.
+ * The first call in a device's context resolves the array's device address
+ * with cudaGetSymbolAddress while that device is current (again after a
+ * cudaDeviceReset, which gives the device a new context); make that first call
+ * before any stream capture.  An empty batch (n == 0) returns GB_OK and
+ * launches nothing.
  */
 #include "engine.h"
 
+#include <cuda.h>
 #include <mutex>
 #include <unordered_map>
 
@@ -37,11 +40,44 @@ constexpr size_t NOALLOC_SCRATCH_WORDS = (size_t)8 << 20;
 static __device__ __align__(256) uint32_t g_noalloc_scratch[NOALLOC_SCRATCH_WORDS];
 
 namespace {
-std::mutex g_addr_mu;
-std::unordered_map<int, uint32_t *> g_addr;
 
-/* Device address of g_noalloc_scratch for the current device (the host-side
- * symbol is only a stand-in; kernels must be given this address). */
+/* The array's device address belongs to the context the library's module
+ * was loaded into: a cudaDeviceReset (or any teardown of the primary context)
+ * loads the module again, possibly at another address.  The cache is
+ * therefore keyed on the driver's context id, which is unique for the life of
+ * the process, and an address is never reused across contexts. */
+typedef CUresult (*CtxGetCurrentFn)(CUcontext *);
+typedef CUresult (*CtxGetIdFn)(CUcontext, unsigned long long *);
+
+std::mutex g_addr_mu;
+std::unordered_map<unsigned long long, uint32_t *> g_addr;
+
+bool current_context_id(unsigned long long *id)
+{
+    static CtxGetCurrentFn get_current = nullptr;
+    static CtxGetIdFn get_id = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void *f = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            get_current = reinterpret_cast<CtxGetCurrentFn>(f);
+        f = nullptr;
+        if (cudaGetDriverEntryPoint("cuCtxGetId", &f, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            get_id = reinterpret_cast<CtxGetIdFn>(f);
+        cudaGetLastError();
+    });
+    CUcontext ctx = nullptr;
+    if (!get_current || !get_id || get_current(&ctx) != CUDA_SUCCESS || ctx == nullptr) return false;
+    return get_id(ctx, id) == CUDA_SUCCESS;
+}
+
+/* Device address of g_noalloc_scratch in the current device's context (the
+ * host-side symbol is only a stand-in; kernels must be given this address).
+ * Resolved with cudaGetSymbolAddress once per context; when the context id
+ * cannot be read the address is resolved on every call. */
 int scratch_address(uint32_t **out)
 {
     int dev = 0;
@@ -49,11 +85,15 @@ int scratch_address(uint32_t **out)
         cudaGetLastError();
         return GB_ERR_CUDA;
     }
-    std::lock_guard<std::mutex> lk(g_addr_mu);
-    auto it = g_addr.find(dev);
-    if (it != g_addr.end()) {
-        *out = it->second;
-        return GB_OK;
+    unsigned long long id = 0;
+    bool keyed = current_context_id(&id);
+    if (keyed) {
+        std::lock_guard<std::mutex> lk(g_addr_mu);
+        auto it = g_addr.find(id);
+        if (it != g_addr.end()) {
+            *out = it->second;
+            return GB_OK;
+        }
     }
     void *p = nullptr;
     const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
@@ -61,7 +101,11 @@ int scratch_address(uint32_t **out)
         cudaGetLastError();
         return GB_ERR_CUDA;
     }
-    g_addr[dev] = static_cast<uint32_t *>(p);
+    if (!keyed) keyed = current_context_id(&id); /* the lookup above made the context current */
+    if (keyed) {
+        std::lock_guard<std::mutex> lk(g_addr_mu);
+        g_addr[id] = static_cast<uint32_t *>(p);
+    }
     *out = static_cast<uint32_t *>(p);
     return GB_OK;
 }
@@ -73,7 +117,9 @@ extern "C" int gb_align_dev_noalloc(const gb_params_t *p, const gb_dev_batch_t *
                                     void *stream)
 {
     using namespace gb;
-    if (!p || !b || !o || b->n <= 0 || !b->h_q_len || !b->h_t_len || !b->pq || !b->pt) return GB_ERR_ARG;
+    if (!p || !b || !o || b->n < 0) return GB_ERR_ARG;
+    if (b->n == 0) return GB_OK; /* an empty batch: nothing to launch */
+    if (!b->h_q_len || !b->h_t_len || !b->pq || !b->pt) return GB_ERR_ARG;
     if (p->algo != LOCAL_ && p->algo != GLOBAL_ && p->algo != SEMI_GLOBAL_ && p->algo != BANDED_ && p->algo != KSW_)
         return GB_ERR_ARG;
     if (p->start_pos == WITH_TB_ && (p->algo == LOCAL_ || p->algo == GLOBAL_)) return GB_ERR_ARG;

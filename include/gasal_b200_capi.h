@@ -174,7 +174,7 @@ int gb_align(const gb_params_t *p, const gb_batch_t *b, gb_out_t *o);
  * (a cudaStream_t, NULL = legacy default stream).  Uses a workspace per
  * (device, stream) that the library grows on demand; calls on one stream must
  * come from one host thread at a time.  The device half of gasal_aln_async
- * (src/gasal_align.cu:180-264). */
+ * (src/gasal_align.cu:180-264).  n == 0 returns GB_OK and launches nothing. */
 int gb_align_dev(const gb_params_t *p, const gb_dev_batch_t *b, const gb_dev_out_t *o, void *stream);
 
 /* Allocation-free variant of gb_align_dev, for callers that cannot call
@@ -184,8 +184,10 @@ int gb_align_dev(const gb_params_t *p, const gb_dev_batch_t *b, const gb_dev_out
  * 32 MiB static device array that each GPU loading the library holds until
  * exit.  Rejects WITH_TB (GB_ERR_ARG) and batches whose longest query leaves
  * the array room for fewer than 32 threads (GB_ERR_LIMIT).  Calls share the
- * array, so calls that overlap on the GPU race.  The first call on a device
- * resolves the array's address and should precede any stream capture. */
+ * array, so calls that overlap on the GPU race.  The first call in a device's
+ * context (again after a cudaDeviceReset) resolves the array's address and
+ * should precede any stream capture.  n == 0 returns GB_OK and launches
+ * nothing, as gb_align_dev does. */
 int gb_align_dev_noalloc(const gb_params_t *p, const gb_dev_batch_t *b, const gb_dev_out_t *o, void *stream);
 
 /* Forward CIGAR text on the device (no counterpart in the reference

@@ -43,24 +43,59 @@ def _run(torch, gl, p, m, b, dev, noalloc):
     return {k: v.cpu().numpy() for k, v in outs.items()}
 
 
-def test_noalloc_matches_allocating_entry_point_twice():
+def _cases(W, capi):
+    """(Params, Batch) for every algorithm family the entry point serves."""
+    from gasal_b200.capi import (Params, LOCAL, GLOBAL, SEMI_GLOBAL, BANDED, KSW, WITH_START, WITHOUT_START,
+                                 TARGET, TRUE)
+    w1 = W.workload1(6000, seed=31)
+    ksw = W.workload3(400, seed=33)
+    return [
+        ("local_start_second_rc", Params(algo=LOCAL, start_pos=WITH_START, second_best=TRUE, reverse_complement=1),
+         w1[0][1]),
+        ("global_long", Params(algo=GLOBAL), W.workload3(300, seed=32)),  # queries up to 2000 bp: a small grid
+        ("semi_global_target_target_start", Params(algo=SEMI_GLOBAL, start_pos=WITH_START, head=TARGET, tail=TARGET,
+                                                   second_best=TRUE), w1[2][1]),
+        ("banded_k32", Params(algo=BANDED, k_band=32), W.workload0(3000, seed=34)),
+        ("ksw_zdrop100", Params(algo=KSW, zdrop=100), ksw),
+        ("ksw_zdrop0", Params(algo=KSW), ksw),
+    ]
+
+
+@pytest.mark.parametrize("case", ["local_start_second_rc", "global_long", "semi_global_target_target_start",
+                                  "banded_k32", "ksw_zdrop100", "ksw_zdrop0"])
+def test_noalloc_matches_allocating_entry_point_and_oracle(case):
+    """Two calls in a row through gb_align_dev_noalloc must each equal
+    gb_align_dev's output and the scalar oracle's, field for field."""
     torch = pytest.importorskip("torch")
-    from gasal_b200 import lib as gl, workloads as W
-    from gasal_b200.capi import Params, LOCAL, GLOBAL, WITH_START, TRUE
+    from gasal_b200 import lib as gl, workloads as W, capi
+    from oracle.bindings import oracle_align
     dev = torch.device("cuda", 0)
     gl.set_reference_reverse(True)
-    calls = [
-        (Params(algo=LOCAL, start_pos=WITH_START, second_best=TRUE, reverse_complement=1),
-         W.workload1(6000, seed=31)[0][1]),
-        (Params(algo=GLOBAL), W.workload3(300, seed=32)),  # queries up to 2000 bp: a small grid
-    ]
-    for p, b in calls:
-        m, keep = _device_batch(torch, b, dev)
+    name, p, b = next(c for c in _cases(W, capi) if c[0] == case)
+    m, keep = _device_batch(torch, b, dev)
+    want = _run(torch, gl, p, m, b, dev, noalloc=False)
+    exp = oracle_align(p, b).as_dict(p)
+    for call in range(2):
         got = _run(torch, gl, p, m, b, dev, noalloc=True)
-        want = _run(torch, gl, p, m, b, dev, noalloc=False)
-        for k in FIELDS:
-            assert np.array_equal(got[k], want[k]), f"{p.key()} {k}: {np.nonzero(got[k] != want[k])[0][:5]}"
-        del keep
+        for k in (f for f in FIELDS if f in exp):  # the arrays the reference defines for these options
+            assert np.array_equal(got[k], want[k]), f"call {call} {p.key()} {k}: {np.nonzero(got[k] != want[k])[0][:5]}"
+        for k, v in exp.items():
+            if k in got:
+                assert np.array_equal(got[k], v), f"call {call} {p.key()} {k} vs oracle: {np.nonzero(got[k] != v)[0][:5]}"
+    del keep
+
+
+def test_noalloc_empty_batch_is_a_no_op():
+    torch = pytest.importorskip("torch")
+    from gasal_b200 import lib as gl
+    from gasal_b200.capi import Params, LOCAL
+    import ctypes as C
+    b = gl.GbDevBatch()
+    b.n = 0
+    o = gl.GbDevOut()
+    cp = Params(algo=LOCAL).to_c()
+    assert gl.lib().gb_align_dev_noalloc(C.byref(cp), C.byref(b), C.byref(o), C.c_void_p(0)) == 0
+    torch.cuda.synchronize()
 
 
 def test_noalloc_rejects_traceback_and_oversized_queries():
