@@ -1,28 +1,40 @@
 #!/usr/bin/env python
 """Throughput of GASAL2's batched alignment path on B200 (aligned pairs/s).
 
-Workload (default): 1,000,000 pairs in three launches -- one third each
-LOCAL (second best) / GLOBAL / SEMI_GLOBAL (head = tail = TARGET), all
-WITH_START, 150 bp queries, 150-300 bp targets (3% substitutions, 1% indels),
-half of the queries REVERSE_COMPLEMENT, scores 1/4/6/1.  Seeded synthetic data
-(numpy PCG64, seed 20261203+1); inputs (~384 MB) exceed the 126 MB L2, so no
-flush is needed between steps.
+Default workload (w4, the full mixed production batch): 10,000,000 pairs,
+query lengths log-normal (median 250 bp, sigma 0.8, clipped to 50-5000),
+60% short-read-like, 30% long-read-like (5-12% errors, indel-dominated), 10%
+unrelated; four launches on four streams -- LOCAL WITH_START 30%, LOCAL
+WITH_TB 20%, SEMI_GLOBAL (TARGET, TARGET) WITH_START 25%, ksw z-drop 100 25%
+-- scores 1/4/6/1.  Seeded synthetic data (per-pair xoshiro256** streams,
+seed 20261203+4); the inputs (~7 GB) exceed the 126 MB L2, so no flush is
+needed between steps.  Other workloads: --workload w0..w3.
 
-One step = the three launches.  Reported:
-  value   pairs/s with the batch already in HBM: pack -> reverse/complement ->
-          DP (+ start pass) per launch, timed with CUDA events on the launch
-          stream, max over ranks
-  e2e     pairs/s through the GASAL2 storage API (gasal_aln_async +
-          gasal_is_aln_async_done on three streams): host->device copy of the
-          pinned batch, kernels, device->host copy of every result array
-  roofline  DP kernels' algorithmic integer ops / their CUDA-event time,
-          against this GPU's measured integer-add issue rate
-  cpu_baseline  the scalar C oracle with OpenMP on all host cores, on a
-          bounded sample of the same workload
+One step = every launch of the workload, each on its own stream.  Reported:
+  value      pairs/s with the batch already in HBM (pack -> reverse/complement
+             -> length-binned order -> DP -> start pass / traceback), CUDA
+             events on the timing stream, max over ranks
+  e2e        pairs/s through the GASAL2 storage API (gasal_c_aln_async +
+             gasal_c_is_aln_async_done, one storage per launch): host->device
+             copy of the pinned batch, kernels, device->host copy of every
+             result array
+  plain      the plain full-DP form (every pair one per thread, in input
+             order, no band) against the batched form on the same stratified
+             sample, outputs compared bit for bit
+  band       the learned ksw band: certificate acceptance, recomputations,
+             computed cells (with --band learned)
+  roofline   algorithmic integer ops of every alignment kernel of a step /
+             the step's wall clock, against this GPU's measured integer-add
+             issue rate; pack and reverse/complement in GB/s against the
+             measured HBM copy bandwidth
+  cpu_baseline  the scalar C oracle, OpenMP on all host cores, on a
+             stratified subsample; its outputs are also compared with the GPU
+             run's outputs for those pairs (oracle_check)
 
 --impl reference times the reference GASAL2 kernels compiled for the host
-(OpenMP over pairs) on a bounded sample per step; the reference has no CPU
-aligner of its own.
+(OpenMP over pairs) on a bounded stratified sample per step; the reference
+has no CPU aligner of its own and cannot run on this GPU's box as a library
+install (it has no packaging).
 """
 from __future__ import annotations
 
@@ -40,38 +52,38 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 from gasal_b200 import workloads as W  # noqa: E402
-from gasal_b200.capi import LOCAL, GLOBAL, SEMI_GLOBAL, KSW, Params  # noqa: E402
+from gasal_b200.capi import LOCAL, GLOBAL, SEMI_GLOBAL, KSW, WITH_TB, Params  # noqa: E402
 
 UNIT = "pairs/s"
-# integer ops per cell, per algorithm (LOCAL 11, GLOBAL 9, SEMI_GLOBAL 10; +4 with traceback)
+# integer ops per computed cell, per algorithm (+4 with traceback)
 OPS_PER_CELL = {LOCAL: 11, GLOBAL: 9, SEMI_GLOBAL: 10, KSW: 13}
 TB_OPS = 4
+HEADLINE_METRIC = "aligned pairs/s + GCUPS, 1 B200: learned-band vs plain full DP, bit-exact"
 
+# name -> (metric, config description, default pairs, generator id, launch params, launch shares)
 WORKLOADS = {
+    "w4": (HEADLINE_METRIC,
+           "w4 full mixed production batch: 10M pairs/GPU, query lengths log-normal (median 250, sigma 0.8, "
+           "clipped 50-5000), 60% short-read-like (1-2% subs, 0.2% indels), 30% long-read-like (5-12% errors, "
+           "75% indels of 1-5 bp), 10% unrelated; LOCAL WITH_START 30%, LOCAL WITH_TB 20%, "
+           "SEMI_GLOBAL(TARGET,TARGET) WITH_START 25%, ksw (h0 20-60, z-drop 100) 25%; four launches on four "
+           "streams; scores 1/4/6/1", 10_000_000, 4, W.WORKLOAD4_PARAMS, W.WORKLOAD4_SHARES),
     "w1": ("aligned pairs/s (1M-pair mixed LOCAL/GLOBAL/SEMI_GLOBAL WITH_START batch, RC on 50%)",
            "w1: 1M pairs/GPU, thirds LOCAL(second best)/GLOBAL/SEMI_GLOBAL(TARGET,TARGET), WITH_START, q=150, "
-           "t=150-300 (3% subs, 1% indels), RC 50% of queries, scores 1/4/6/1", 1_000_000),
+           "t=150-300 (3% subs, 1% indels), RC 50% of queries, scores 1/4/6/1", 1_000_000, 1,
+           W.WORKLOAD1_PARAMS, (1 / 3, 1 / 3, 1 / 3)),
     "w2": ("aligned pairs/s (2M-pair uneven-length GLOBAL WITH_TB batch, CIGAR out)",
            "w2: 2M pairs/GPU, GLOBAL WITH_TB, query log-uniform 50-1000, target = query with 1-8% subs and "
-           "0.5-3% indels (len 1-10) per pair, scores 1/4/6/1", 2_000_000),
+           "0.5-3% indels (len 1-10) per pair, scores 1/4/6/1", 2_000_000, 2,
+           [Params(algo=GLOBAL, start_pos=WITH_TB)], (1.0,)),
     "w3": ("aligned pairs/s (ksw seed extension, z-drop 100, query 250-2000 bp)",
-           "w3: ksw extension, query U[250,2000], target = query with indel rate {0.5,2,5,10}% (len 1-3) + "
-           "1-5% subs per pair, h0 U[20,60], zdrop 100, scores 1/4/6/1", 400_000),
-    "w4": ("aligned pairs/s (mixed-length LOCAL / LOCAL+traceback / SEMI_GLOBAL / ksw on four streams)",
-           "w4: query lengths log-normal (median 250, clipped 50-5000), 60% short-read-like, 30% long-read-like "
-           "(5-12% errors, indel-dominated), 10% unrelated; LOCAL WITH_START 30%, LOCAL WITH_TB 20%, "
-           "SEMI_GLOBAL(TARGET,TARGET) WITH_START 25%, ksw z-drop 100 25%; one storage/stream per launch, graphs on",
-           1_000_000),
+           "w3: 4M pairs/GPU, ksw extension, query U[250,2000], target = query with indel rate {0.5,2,5,10}% "
+           "(len 1-3) + 1-5% subs per pair, h0 U[20,60], zdrop 100, scores 1/4/6/1", 4_000_000, 3,
+           [Params(algo=KSW, zdrop=100)], (1.0,)),
     "w0": ("aligned pairs/s (20k-pair LOCAL WITHOUT_START batch)",
            "w0: 20k pairs, LOCAL WITHOUT_START, q 100-150 with 0.1% N, t = q + 0-20 flanks, 2% subs, 0.5% "
-           "indels", 20_000),
+           "indels", 20_000, 0, [Params(algo=LOCAL)], (1.0,)),
 }
-METRIC = WORKLOADS["w1"][0]
-# DRAM bytes (read + write) of one w1 launch of the dominant kernel
-# (dp_kernel, LOCAL third): 28.1 MB measured by ncu on the 133,334-pair launch
-# of a 400k-pair run (profiles/dp_kernel_w1_ncu_full.md), scaled by pairs to
-# the 333,334-pair launch of the full 1M-pair workload.
-DP_TRAFFIC_BYTES = 28.14e6 * 333334 / 133334
 
 
 def log(*a):
@@ -136,42 +148,44 @@ class ClockSampler:
                 "power_w_max": max(pw) if pw else None, "reasons": reasons, "samples": len(rows)}
 
 
-def build_workload(n: int, seed: int, name: str = "w1"):
-    t = time.time()
-    if name == "w1":
-        parts = W.workload1(n, seed=seed)
-    elif name == "w2":
-        from gasal_b200.capi import WITH_TB
-        parts = [(Params(algo=GLOBAL, start_pos=WITH_TB), W.workload2(n, seed=seed + 1))]
-    elif name == "w3":
-        parts = [(Params(algo=KSW, zdrop=100), W.workload3(n, seed=seed + 2))]
-    elif name == "w4":
-        parts = W.workload4(n, seed=seed + 3)
+def build_parts(name: str, n: int, seed: int, idx=None):
+    """[(Params, Batch)] of workload `name` -- pairs [0, n), or the pairs
+    listed in idx (ascending workload indexes) -- one entry per launch."""
+    _, _, _, gen, params, shares = WORKLOADS[name]
+    cuts = W._cuts(n, shares)
+    if idx is None:
+        batches = W.generate(gen, n, seed, cuts)
     else:
-        parts = [(Params(algo=LOCAL), W.workload0(n, seed=seed - 1))]
-    log(f"workload {name}: {n} pairs generated in {time.time() - t:.1f}s")
-    return parts
+        idx = np.asarray(idx, dtype=np.int64)
+        sub_cuts = [int(np.searchsorted(idx, c)) for c in cuts]
+        batches = W.generate(gen, 0, seed, sub_cuts, idx=idx)
+    return [(p, b) for p, b in zip(params, batches)]
 
 
-def cpu_baseline(parts, budget_s: float = 12.0) -> dict:
-    """Scalar C oracle, OpenMP on every host core, on a bounded sample."""
-    from oracle.bindings import oracle_align
-    cores = os.cpu_count() or 1
-    probe = 3000
-    t0 = time.time()
-    k = len(parts)
-    probe = min(probe, min(b.n for _, b in parts))
-    for p, b in parts:
-        oracle_align(p, b.subset(np.arange(probe)), threads=cores)
-    per_pair = (time.time() - t0) / (k * probe)
-    m = int(max(probe, min(min(b.n for _, b in parts), budget_s / per_pair / k)))
-    t0 = time.time()
-    for p, b in parts:
-        oracle_align(p, b.subset(np.arange(min(m, b.n))), threads=cores)
-    dt = time.time() - t0
-    return {"value": k * m / dt, "unit": UNIT, "cores": cores, "kind": "port",
-            "sample": f"first {m} pairs of each of the {k} launch(es) ({k * m} pairs), {dt:.1f}s"}
+def stratified(n: int, every: int) -> np.ndarray:
+    """Every `every`-th pair of [0, n): the workload's pairs are i.i.d. in
+    index order, so this is a uniform sample of each launch's pairs."""
+    return np.arange(0, n, max(1, int(every)), dtype=np.int64)
 
+
+def local_index(name: str, n: int, idx: np.ndarray):
+    """For each launch: positions of workload indexes idx inside that launch."""
+    cuts = W._cuts(n, WORKLOADS[name][5])
+    out = []
+    for lo, hi in zip(cuts[:-1], cuts[1:]):
+        sel = idx[(idx >= lo) & (idx < hi)]
+        out.append(sel - lo)
+    return out
+
+
+def alg_ops(parts) -> float:
+    return float(sum(b.cells() * (OPS_PER_CELL[p.algo] + (TB_OPS if p.start_pos == WITH_TB else 0))
+                     for p, b in parts))
+
+
+# ------------------------------------------------------------------------------------------------------------
+# reference arm
+# ------------------------------------------------------------------------------------------------------------
 
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
@@ -179,195 +193,252 @@ def run_reference(args):
         return
     from oracle.bindings import ref_host_align
     cores = os.cpu_count() or 1
-    parts = build_workload(args.pairs or WORKLOADS[args.workload][2], W.SEED_BASE + 1, args.workload)
-    m = args.ref_sample
-    sample = [(p, b.subset(np.arange(min(m, b.n)))) for p, b in parts]
+    n = args.pairs or WORKLOADS[args.workload][2]
+    every = max(1, n // args.ref_sample)
+    idx = stratified(n, every)
+    sample = build_parts(args.workload, n, W.SEED_BASE + WORKLOADS[args.workload][3], idx)
+    chunk = 256  # bounds the reference's traceback tile buffer (longest pair's tiles x pairs per batch)
+
+    chunks = [(p, [b.subset(np.arange(lo, min(b.n, lo + chunk))) for lo in range(0, b.n, chunk)]
+               if p.start_pos == WITH_TB and b.n > chunk else [b]) for p, b in sample]
+
+    def step():
+        for p, cs in chunks:
+            for c in cs:
+                ref_host_align(p, c, threads=cores)
+
     for _ in range(args.warmup):
-        for p, b in sample:
-            ref_host_align(p, b, threads=cores)
+        step()
     times = []
     for _ in range(args.steps):
         t0 = time.time()
-        for p, b in sample:
-            ref_host_align(p, b, threads=cores)
+        step()
         times.append(time.time() - t0)
     npairs = sum(b.n for _, b in sample)
     v = npairs / float(np.mean(times))
-    line = {"impl": "reference", "metric": WORKLOADS[args.workload][0], "value": v, "unit": UNIT, "n_gpus": args.gpus,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * float(np.mean(times)),
+    line = {"impl": "reference", "metric": WORKLOADS[args.workload][0], "value": v, "unit": UNIT,
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * float(np.mean(times)),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int32",
-            "data": "synthetic",
+            "data": "synthetic (per-pair xoshiro256** streams)",
             "config": {"workload": WORKLOADS[args.workload][1], "pairs_per_step": npairs},
             "cpu_baseline": {"value": v, "unit": UNIT, "cores": cores, "kind": "reference",
-                             "sample": f"first {m} pairs of each launch per step ({npairs} pairs); reference "
-                                       f"kernel headers compiled for the host, OpenMP over pairs"},
+                             "sample": f"every {every}th pair of the {n}-pair workload ({npairs} pairs per step, "
+                                       f"traceback launches in chunks of {chunk}); the reference kernel headers compiled for the host "
+                                       f"(MAX_QUERY_LEN 8192), OpenMP over pairs; ksw at the reference's "
+                                       f"hard-coded z-drop 0"},
             "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
 
-def main():
-    ap = argparse.ArgumentParser()
-    ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
-    ap.add_argument("--warmup", type=int, default=3)
-    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="w1", choices=sorted(WORKLOADS))
-    ap.add_argument("--pairs", type=int, default=0, help="pairs per GPU (default: the workload's size)")
-    ap.add_argument("--ref-sample", type=int, default=4000)
-    ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--band", default="off", choices=["off", "learned"],
-                    help="ksw launches (w3, w4): learned band with certificate; the model is trained first on a "
-                         "separate sample")
-    ap.add_argument("--no-plain", action="store_true",
-                    help="skip timing the plain full-DP form (one pair per thread, input order) on the same batch")
-    ap.add_argument("--plain-budget-s", type=float, default=15.0,
-                    help="device time the plain form's timed steps may take (at least one step)")
-    ap.add_argument("--band-train-pairs", type=int, default=100_000)
-    args = ap.parse_args()
-    if args.warmup < 3:
-        args.warmup = 3
-    if args.impl == "reference":
-        run_reference(args)
-        return
+# ------------------------------------------------------------------------------------------------------------
+# device-resident batches
+# ------------------------------------------------------------------------------------------------------------
 
-    import torch
-    import ctypes as C
-    from gasal_b200 import lib as gl
+OUTS = ("score", "q_end", "t_end", "q_start", "t_start", "score2", "q_end2", "t_end2")
 
-    from gasal_b200 import shard
-    rank, world, local_rank = shard.rank_info()
-    torch.cuda.set_device(local_rank)
-    dist = None
-    if world > 1:
-        import torch.distributed as dist
-        from datetime import timedelta
-        dist.init_process_group("nccl", timeout=timedelta(seconds=120))
 
-    gl.lib()
-    gl.set_reference_reverse(True)
-    peak = gl.probe_int_peak()
-    n_pairs = args.pairs or WORKLOADS[args.workload][2]
-    parts = build_workload(n_pairs, shard.shard_seed(W.SEED_BASE + 1, rank), args.workload)
-    npairs = sum(b.n for _, b in parts)
-    dev = torch.device("cuda", local_rank)
+class DevPart:
+    """One launch's batch in device memory plus its output buffers, with the
+    gb_dev_batch_t / gb_dev_out_t address map."""
 
-    # ---------------- kernel level: inputs resident in HBM -----------------
-    def t_(a, dtype=None):
-        return torch.from_numpy(np.ascontiguousarray(a).view(dtype or a.dtype)).to(dev)
-
-    dparts = []
-    for p, b in parts:
-        d = {"q_t": t_(b.q), "t_t": t_(b.t), "qo": t_(b.q_off, np.int32), "to": t_(b.t_off, np.int32),
-             "ql": t_(b.q_len, np.int32), "tl": t_(b.t_len, np.int32),
-             "qop": t_(b.q_op) if b.q_op is not None else None, "top": t_(b.t_op) if b.t_op is not None else None,
-             "seed": t_(b.seed, np.int32) if b.seed is not None else None}
-        d["pq"] = torch.empty(b.q.shape[0] // 8, dtype=torch.int32, device=dev)
-        d["pt"] = torch.empty(b.t.shape[0] // 8, dtype=torch.int32, device=dev)
-        outs = {k: torch.empty(b.n, dtype=torch.int32, device=dev) for k in
-                ("score", "q_end", "t_end", "q_start", "t_start", "score2", "q_end2", "t_end2")}
-        d["outs"] = outs
-        d["cigar"] = torch.empty(b.q.shape[0], dtype=torch.uint8, device=dev)
-        d["ncig"] = torch.empty(b.n, dtype=torch.int32, device=dev)
-        m = {"q_bytes": b.q.shape[0], "t_bytes": b.t.shape[0], "q": d["q_t"].data_ptr(), "t": d["t_t"].data_ptr(),
-             "pq": d["pq"].data_ptr(), "pt": d["pt"].data_ptr(), "q_off": d["qo"].data_ptr(),
-             "t_off": d["to"].data_ptr(), "q_len": d["ql"].data_ptr(), "t_len": d["tl"].data_ptr(),
-             "q_op": d["qop"].data_ptr() if d["qop"] is not None else None,
-             "t_op": d["top"].data_ptr() if d["top"] is not None else None,
-             "seed": d["seed"].data_ptr() if d["seed"] is not None else None}
-        for k, v in outs.items():
+    def __init__(self, torch, p: Params, b, dev):
+        def t_(a, dtype=None):
+            return torch.from_numpy(np.ascontiguousarray(a).view(dtype or a.dtype)).to(dev)
+        self.p, self.b = p, b
+        self.t = {"q": t_(b.q), "t": t_(b.t), "qo": t_(b.q_off, np.int32), "to": t_(b.t_off, np.int32),
+                  "ql": t_(b.q_len, np.int32), "tl": t_(b.t_len, np.int32)}
+        if b.q_op is not None:
+            self.t["qop"], self.t["top"] = t_(b.q_op), t_(b.t_op)
+        if b.seed is not None:
+            self.t["seed"] = t_(b.seed, np.int32)
+        self.t["pq"] = torch.empty(b.q.shape[0] // 8, dtype=torch.int32, device=dev)
+        self.t["pt"] = torch.empty(b.t.shape[0] // 8, dtype=torch.int32, device=dev)
+        self.outs = {k: torch.empty(b.n, dtype=torch.int32, device=dev) for k in OUTS}
+        self.cigar = torch.empty(b.q.shape[0], dtype=torch.uint8, device=dev)
+        self.ncig = torch.empty(b.n, dtype=torch.int32, device=dev)
+        m = {"q_bytes": b.q.shape[0], "t_bytes": b.t.shape[0]}
+        for k, src in (("q", "q"), ("t", "t"), ("pq", "pq"), ("pt", "pt"), ("q_off", "qo"), ("t_off", "to"),
+                       ("q_len", "ql"), ("t_len", "tl"), ("q_op", "qop"), ("t_op", "top"), ("seed", "seed")):
+            m[k] = self.t[src].data_ptr() if src in self.t else None
+        for k, v in self.outs.items():
             m["out_" + k] = v.data_ptr()
-        m["out_cigar"] = d["cigar"].data_ptr()
-        m["out_n_cigar"] = d["ncig"].data_ptr()
         if not p.second_best:
             m["out_score2"] = m["out_q_end2"] = m["out_t_end2"] = None
-        d["map"] = m
-        dparts.append((p, b, d))
+        m["out_cigar"] = self.cigar.data_ptr()
+        m["out_n_cigar"] = self.ncig.data_ptr()
+        self.map = m
 
-    stream = torch.cuda.Stream(device=dev)
+    def fields(self):
+        """Output arrays defined for this launch's options (name -> tensor)."""
+        from gasal_b200.capi import Outputs
+        names = Outputs.fields_for(None, self.p)
+        d = {k: self.outs[k] for k in names}
+        if self.p.start_pos == WITH_TB and self.p.algo in (LOCAL, GLOBAL):
+            d["n_cigar"] = self.ncig
+        return d
 
-    band_info = None
-    model = None
-    if args.band == "learned":
-        if args.workload not in ("w3", "w4"):
-            raise SystemExit("--band learned applies to the workloads with ksw launches (w3, w4)")
-        from gasal_b200 import band_train as BT
-        t0 = time.time()
-        # a separate sample of the same workload; w4's ksw launch is a quarter of it
-        n_train = args.band_train_pairs * (4 if args.workload == "w4" else 1)
-        tparts = build_workload(n_train, shard.shard_seed(W.SEED_BASE + 101, rank), args.workload)
-        tp, tb = next((p, b) for p, b in tparts if p.algo == KSW)
-        tdb = BT.DeviceBatch(torch, tb, dev)
-        feat = BT.features(torch, tdb)
-        lab = BT.labels(torch, tp, tdb)
-        model = gl.BandModel(seed=11)
-        trace = BT.train(torch, model, feat, lab, steps=600, batch=8192, tau=0.8, lr=3e-3)
-        model.install(16, 1024)
-        band_info = {"train_pairs": tb.n, "train_s": round(time.time() - t0, 1),
-                     "label_hist_log2": {str(k): int(v) for k, v in zip(*np.unique(lab, return_counts=True))},
-                     "loss_first": trace[0], "loss_last": trace[-1]}
-        del tdb, feat
-        log(f"band model trained in {band_info['train_s']} s; loss {trace[0]:.3f} -> {trace[-1]:.3f}")
+    def cigar_of(self, i: int):
+        o, n = int(self.b.q_off[i]), int(self.ncig[i].item())
+        return self.cigar[o:o + n]
 
-    def step():
-        for p, b, d in dparts:
-            gl.align_dev(p, d["map"], b.q_len, b.t_len, stream.cuda_stream)
 
-    clk = ClockSampler(local_rank).__enter__()
-    with torch.cuda.stream(stream):
-        for _ in range(args.warmup):
-            step()
-    torch.cuda.synchronize()
-    if dist:
-        dist.barrier()
-    torch.cuda.synchronize()
-    gl.kernel_timing(True)
-    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    clk.mark_start()
-    ev0.record(stream)
-    for _ in range(args.steps):
-        step()
-    ev1.record(stream)
-    torch.cuda.synchronize()
-    clk.mark_end()
-    clk.__exit__()
-    kt = gl.kernel_timing_read()
-    gl.kernel_timing(False)
-    ms = shard.max_over_ranks(ev0.elapsed_time(ev1), dist, dev)
-    if dist:
-        dist.barrier()
-    ms_step = ms / args.steps
-    value = shard.job_throughput(npairs, world, args.steps, ms)
-    cells = sum(b.cells() for _, b in parts)
-    dp_ms, dp_n = kt["dp"]
-    from gasal_b200.capi import WITH_TB as _TB
-    alg_ops = sum(b.cells() * (OPS_PER_CELL[p.algo] + (TB_OPS if p.start_pos == _TB else 0))
-                  for p, b in parts) * args.steps
-    achieved = alg_ops / (dp_ms * 1e-3) / 1e12
-    launches = sum(n * gl.KERNELS_PER_MARK[k] for k, (_, n) in kt.items())
+class Runner:
+    """Launches every part on its own stream, joined into one timing stream."""
 
-    # ---------------- end to end through the storage API ----------------
-    e2e = None
+    def __init__(self, torch, gl, parts, dev):
+        self.torch, self.gl, self.parts, self.dev = torch, gl, parts, dev
+        self.main = torch.cuda.Stream(device=dev)
+        self.streams = [torch.cuda.Stream(device=dev) for _ in parts]
+
+    def step(self):
+        torch = self.torch
+        fork = torch.cuda.Event()
+        fork.record(self.main)
+        for d, s in zip(self.parts, self.streams):
+            s.wait_event(fork)
+            self.gl.align_dev(d.p, d.map, d.b.q_len, d.b.t_len, s.cuda_stream)
+            done = torch.cuda.Event()
+            done.record(s)
+            self.main.wait_event(done)
+
+    def time(self, steps: int, warmup: int, dist=None, before_timed=None):
+        torch = self.torch
+        for _ in range(warmup):
+            self.step()
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+        if before_timed:
+            before_timed()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(self.main)
+        for _ in range(steps):
+            self.step()
+        e1.record(self.main)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1)
+
+
+def outputs_equal(torch, a_parts, b_parts, a_idx=None):
+    """Every defined output of b_parts equals a_parts' (at rows a_idx[k] of
+    a_parts[k] when given); returns (equal, mismatched pair count)."""
+    bad = 0
+    for k, (a, b) in enumerate(zip(a_parts, b_parts)):
+        sel = None if a_idx is None else torch.from_numpy(a_idx[k]).to(a.outs["score"].device)
+        for name, tb_ in b.fields().items():
+            ta = a.fields()[name]
+            if sel is not None:
+                ta = ta.index_select(0, sel)
+            bad += int((ta != tb_).sum().item())
+        if b.p.start_pos == WITH_TB and b.p.algo in (LOCAL, GLOBAL):
+            ia = None if a_idx is None else a_idx[k]
+            nb = b.ncig.cpu().numpy()
+            na = a.ncig.cpu().numpy() if ia is None else a.ncig.cpu().numpy()[ia]
+            ca, cb = a.cigar.cpu().numpy(), b.cigar.cpu().numpy()
+            for j in range(b.b.n):
+                i = j if ia is None else int(ia[j])
+                oa, ob = int(a.b.q_off[i]), int(b.b.q_off[j])
+                if na[j] != nb[j] or not np.array_equal(ca[oa:oa + int(na[j])], cb[ob:ob + int(nb[j])]):
+                    bad += 1
+    return bad == 0, bad
+
+
+# ------------------------------------------------------------------------------------------------------------
+# the measured arm
+# ------------------------------------------------------------------------------------------------------------
+
+def train_band(torch, gl, args, rank, dev):
+    """Train the ksw band model on a separate sample of the same workload
+    (its ksw launch) and install it for every ksw call."""
+    from gasal_b200 import band_train as BT
+    t0 = time.time()
+    name = args.workload
+    shares = WORKLOADS[name][5]
+    ksw_k = [p.algo for p in WORKLOADS[name][4]].index(KSW)
+    n_train = int(args.band_train_pairs / shares[ksw_k])
+    tparts = build_parts(name, n_train, W.SEED_BASE + 101 + 1000 * rank)
+    tp, tb = tparts[ksw_k]
+    tdb = BT.DeviceBatch(torch, tb, dev)
+    feat = BT.features(torch, tdb)
+    lab = BT.labels(torch, tp, tdb)
+    model = gl.BandModel(seed=11)
+    trace = BT.train(torch, model, feat, lab, steps=600, batch=8192, tau=0.8, lr=3e-3)
+    model.install(16, 1024)
+    info = {"train_pairs": tb.n, "train_s": round(time.time() - t0, 1),
+            "label_hist_log2": {str(k): int(v) for k, v in zip(*np.unique(lab, return_counts=True))},
+            "loss_first": trace[0], "loss_last": trace[-1]}
+    log(f"band model trained in {info['train_s']} s; loss {trace[0]:.3f} -> {trace[-1]:.3f}")
+    return model, info
+
+
+def prep_bandwidth(torch, gl, dparts, hbm_gbs, reps=5):
+    """Pack and reverse/complement kernels alone on the resident batch
+    (CUDA events on their stream; every step re-packs, so running them here
+    changes nothing later).  Algorithmic bytes: pack 1.5 B per base (1 read,
+    0.5 written), reverse/complement 1 B per base of sequences with an
+    operation (0.5 read, 0.5 written)."""
+    s = torch.cuda.Stream(device=dparts[0].outs["score"].device)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    out = {}
+    pack_bytes = sum(1.5 * (d.b.q.shape[0] + d.b.t.shape[0]) for d in dparts)
+    with torch.cuda.stream(s):
+        for _ in range(2):
+            for d in dparts:
+                gl.pack_dev(d.map["q"], d.b.q.shape[0], d.map["pq"], s.cuda_stream)
+                gl.pack_dev(d.map["t"], d.b.t.shape[0], d.map["pt"], s.cuda_stream)
+        e0.record(s)
+        for _ in range(reps):
+            for d in dparts:
+                gl.pack_dev(d.map["q"], d.b.q.shape[0], d.map["pq"], s.cuda_stream)
+                gl.pack_dev(d.map["t"], d.b.t.shape[0], d.map["pt"], s.cuda_stream)
+        e1.record(s)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / reps
+        gbs = pack_bytes / (ms * 1e-3) / 1e9
+        out["pack"] = {"gbs": gbs, "frac_of_hbm": gbs / hbm_gbs, "ms_per_step": ms, "bytes_per_step": pack_bytes,
+                       "launches_per_step": 2 * len(dparts)}
+        rc = [d for d in dparts if d.b.q_op is not None and (d.b.q_op != 0).any()]
+        if rc:
+            rc_bytes = 0.0
+            for d in rc:
+                rc_bytes += float(np.sum(d.b.q_len[d.b.q_op != 0])) + float(np.sum(d.b.t_len[d.b.t_op != 0]))
+            for _ in range(2):
+                for d in rc:
+                    gl.revcomp_dev(d.map, d.b.n, s.cuda_stream)
+            e0.record(s)
+            for _ in range(reps):
+                for d in rc:
+                    gl.revcomp_dev(d.map, d.b.n, s.cuda_stream)
+            e1.record(s)
+            torch.cuda.synchronize()
+            ms = e0.elapsed_time(e1) / reps
+            gbs = rc_bytes / (ms * 1e-3) / 1e9
+            out["revcomp"] = {"gbs": gbs, "frac_of_hbm": gbs / hbm_gbs, "ms_per_step": ms,
+                              "bytes_per_step": rc_bytes, "launches_per_step": len(rc)}
+    return out
+
+
+def e2e_leg(torch, gl, parts, args, dev, dist):
+    """The storage API with host buffers: per step, every launch's pinned batch
+    goes host->device, aligns, and every result array comes back."""
+    from gasal_b200 import shard
     streams = []
     for p, b in parts:
-        # host pages sized to the batch's own bytes (one bulk gasal_host_batch_fill per side)
         s = gl.Streams(1, -(-int(b.q.shape[0]) // b.n) + 8, -(-int(b.t.shape[0]) // b.n) + 8, b.n, p)
         streams.append((p, b, s))
-    h2d = sum(int(b.q.shape[0] + b.t.shape[0]) + b.n * (4 * 4 + 2) for _, b, _ in streams)
-    d2h = 0
-    for p, b, s in streams:
-        nf = 5 + (3 if p.second_best else 0)
-        if p.algo == GLOBAL:
-            nf = 1
-        if p.algo == KSW:
-            nf = 3
-            h2d += 4 * b.n
+    h2d = d2h = 0
+    for p, b, _ in streams:
+        h2d += int(b.q.shape[0] + b.t.shape[0]) + b.n * (4 * 4 + 2) + (4 * b.n if p.algo == KSW else 0)
+        nf = 1 if p.algo == GLOBAL else (3 if p.algo == KSW else 5 + (3 if p.second_best else 0))
         d2h += 4 * b.n * nf
-        if p.start_pos == _TB:
+        if p.start_pos == WITH_TB:
             d2h += int(b.q.shape[0]) + 4 * b.n
-    e2e_times = []
+    times = []
     ext = [torch.cuda.ExternalStream(s.view(0).stream, device=dev) for _, _, s in streams]
-    for it in range(args.warmup + min(args.steps, 5)):
-        sizes = [s.fill_fast(0, b) for _, b, s in streams]
+    sizes = [s.fill_fast(0, b) for _, b, s in streams]
+    n_timed = min(args.steps, args.e2e_steps)
+    for it in range(args.warmup + n_timed):
         torch.cuda.synchronize()
         starts = [torch.cuda.Event(enable_timing=True) for _ in streams]
         ends = [torch.cuda.Event(enable_timing=True) for _ in streams]
@@ -379,89 +450,163 @@ def main():
             s.wait(0)
         torch.cuda.synchronize()
         if it >= args.warmup:
-            span = max(starts[0].elapsed_time(e) for e in ends)
-            e2e_times.append(span)
+            times.append(max(starts[0].elapsed_time(e) for e in ends))
     for _, _, s in streams:
         s.close()
-    e2e_ms = shard.max_over_ranks(float(np.mean(e2e_times)), dist, dev)
-    e2e = {"value": npairs * world / (e2e_ms * 1e-3), "unit": UNIT, "h2d_bytes_per_step": h2d,
-           "d2h_bytes_per_step": d2h, "ms_per_step": e2e_ms,
-           "path": "gasal_c_aln_async + gasal_c_is_aln_async_done (3 streams), pinned host batches"}
+    npairs = sum(b.n for _, b in parts)
+    ms = shard.max_over_ranks(float(np.mean(times)), dist, dev)
+    world = dist.get_world_size() if dist else 1
+    return {"value": npairs * world / (ms * 1e-3), "unit": UNIT, "h2d_bytes_per_step": h2d,
+            "d2h_bytes_per_step": d2h, "ms_per_step": ms, "steps": n_timed,
+            "path": f"gasal_c_aln_async + gasal_c_is_aln_async_done, one storage per launch ({len(parts)} streams), "
+                    f"pinned host batches filled (gasal_host_batch_fill) before the timed region"}
 
-    kparts = [x for x in dparts if x[0].algo == KSW]
-    if kparts:
-        # band statistics of one more (untimed) pass over the ksw launch:
-        # computed cells, and with a band how many results the certificate kept
-        p3, b3, d3 = kparts[0]
-        wide = None if args.band == "learned" else torch.full((b3.n,), 1 << 20, dtype=torch.int32, device=dev)
-        with torch.cuda.stream(stream):
-            st = gl.ksw_band_align(p3, d3["map"], b3.q_len, b3.t_len, wide.data_ptr() if wide is not None else None,
-                                   None, stream.cuda_stream)
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="w4", choices=sorted(WORKLOADS))
+    ap.add_argument("--pairs", type=int, default=0, help="pairs per GPU (default: the workload's size)")
+    ap.add_argument("--ref-sample", type=int, default=4000, help="pairs per step of the reference arm")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-budget-s", type=float, default=12.0)
+    ap.add_argument("--band", default="learned", choices=["off", "learned"],
+                    help="ksw launches: learned band with certificate (the model is trained first on a separate "
+                         "sample of the workload)")
+    ap.add_argument("--band-train-pairs", type=int, default=60_000)
+    ap.add_argument("--no-plain", action="store_true",
+                    help="skip the plain full-DP form (one pair per thread, input order, no band)")
+    ap.add_argument("--plain-budget-s", type=float, default=20.0,
+                    help="device time the plain form's timed step may take; beyond it a stratified sample is used")
+    ap.add_argument("--e2e-steps", type=int, default=3)
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        run_reference(args)
+        return
+
+    import torch
+    from gasal_b200 import lib as gl
+    from gasal_b200 import shard
+    rank, world, local_rank = shard.rank_info()
+    torch.cuda.set_device(local_rank)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300))
+
+    gl.lib()
+    gl.set_reference_reverse(True)
+    peak = gl.probe_int_peak()
+    hbm = None
+    try:
+        hbm = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))["hbm_gbs"]
+        hbm_src = "MEASURED_PEAKS.json hbm_gbs (STREAM-style copy on this pool's B200s)"
+    except (OSError, KeyError, ValueError):
+        hbm, hbm_src = 6650.0, "fallback 6.65 TB/s (earlier measurement on this pool)"
+    name = args.workload
+    n_pairs = args.pairs or WORKLOADS[name][2]
+    seed = shard.shard_seed(W.SEED_BASE + WORKLOADS[name][3], rank)
+    t0 = time.time()
+    parts = build_parts(name, n_pairs, seed)
+    log(f"workload {name}: {n_pairs} pairs generated in {time.time() - t0:.1f}s "
+        f"({W.generator_threads()} threads)")
+    npairs = sum(b.n for _, b in parts)
+    cells = sum(b.cells() for _, b in parts)
+    dev = torch.device("cuda", local_rank)
+    dparts = [DevPart(torch, p, b, dev) for p, b in parts]
+
+    model, band_info = None, None
+    has_ksw = any(p.algo == KSW for p, _ in parts)
+    if args.band == "learned" and has_ksw:
+        model, band_info = train_band(torch, gl, args, rank, dev)
+
+    # ---------------- kernel level: inputs resident in HBM -----------------
+    runner = Runner(torch, gl, dparts, dev)
+    clk = ClockSampler(local_rank).__enter__()
+
+    def arm():
+        gl.kernel_timing(True)
+        clk.mark_start()
+
+    ms = runner.time(args.steps, args.warmup, dist, before_timed=arm)
+    clk.mark_end()
+    clk.__exit__()
+    kt = gl.kernel_timing_read()
+    gl.kernel_timing(False)
+    ms = shard.max_over_ranks(ms, dist, dev)
+    ms_step = ms / args.steps
+    value = shard.job_throughput(npairs, world, args.steps, ms)
+    ops = alg_ops(parts)
+    achieved = ops / (ms_step * 1e-3) / 1e12
+    launches = sum(n * gl.KERNELS_PER_MARK[k] for k, (_, n) in kt.items())
+
+    prep = prep_bandwidth(torch, gl, dparts, hbm)
+
+    kpart = next((d for d in dparts if d.p.algo == KSW), None)
+    if kpart is not None:
+        # band statistics of one more (untimed) pass over the ksw launch: with the installed model, or,
+        # without one, a band wider than every matrix (the unbanded computation's cells)
+        wide = None
+        if model is None:
+            wide = torch.full((kpart.b.n,), 1 << 20, dtype=torch.int32, device=dev)
+        with torch.cuda.stream(runner.main):
+            st = gl.ksw_band_align(kpart.p, kpart.map, kpart.b.q_len, kpart.b.t_len,
+                                   None if wide is None else wide.data_ptr(), None, runner.main.cuda_stream)
         band_info = dict(band_info or {}, mode=args.band, **st,
-                         computed_cells_fraction=st["cells"] / max(1, b3.cells()))
-    # ---------------- the plain full-DP form on the same batch ----------------
+                         acceptance_rate=st["accepted"] / max(1, st["pairs"]),
+                         computed_cells_fraction=st["cells"] / max(1, kpart.b.cells()))
+        del wide
+
+    # ---------------- end to end through the storage API ----------------
+    e2e = e2e_leg(torch, gl, parts, args, dev, dist)
+
+    # ---------------- the plain full-DP form on a stratified sample ----------------
     plain = None
     if not args.no_plain:
-        want = [[v.clone() for v in list(d["outs"].values()) + [d["cigar"], d["ncig"]]] for _, _, d in dparts]
-        saved = gl.get_tuning()
-        if model is not None:
-            gl.BandModel.uninstall()
-        gl.set_tuning(**gl.PLAIN_FORM)
-        try:
-            p0, p1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            p0.record(stream)
-            step()  # warm-up; its time sizes the timed leg
-            p1.record(stream)
-            torch.cuda.synchronize()
-            t1 = shard.max_over_ranks(p0.elapsed_time(p1), dist, dev)
-            k_plain = int(max(1, min(args.steps, args.plain_budget_s * 1e3 // max(t1, 1e-3))))
-            if dist:
-                dist.barrier()
-            torch.cuda.synchronize()
-            p0.record(stream)
-            for _ in range(k_plain):
-                step()
-            p1.record(stream)
-            torch.cuda.synchronize()
-            pms = shard.max_over_ranks(p0.elapsed_time(p1), dist, dev)
-        finally:
-            gl.set_tuning(**saved)
-            if model is not None:
-                model.install(16, 1024)
-        got = [list(d["outs"].values()) + [d["cigar"], d["ncig"]] for _, _, d in dparts]
-        same = all(torch.equal(g, w) for gs, ws in zip(got, want) for g, w in zip(gs, ws))
-        pval = shard.job_throughput(npairs, world, k_plain, pms)
-        plain = {"value": pval, "unit": UNIT, "ms_per_step": pms / k_plain, "steps": k_plain, "warmup": 1,
-                 "gcups": cells * world / (pms / k_plain * 1e-3) / 1e9,
-                 "form": "every pair one per thread in input order on a grid over the batch: no device work "
-                         "counter, no length ordering, no warp-cooperative or warp-per-pair kernels, no band, "
-                         "start passes in the forward launch",
-                 "value_over_plain": value / pval, "bit_exact_vs_plain": bool(same)}
+        plain = plain_leg(torch, gl, args, name, n_pairs, seed, dparts, model, dev, dist, value, world)
+
     in_mb = sum(int(b.q.shape[0] + b.t.shape[0]) + 16 * b.n for _, b in parts) / 1e6
     l2_note = (f"inputs {in_mb:.0f} MB > 126 MB L2, no flush" if in_mb > 126 else
                f"inputs {in_mb:.0f} MB fit the 126 MB L2 (no flush: each step re-reads them, as a caller "
                f"re-aligning resident batches would)")
     if rank == 0:
-        cpu = None if args.no_cpu_baseline else cpu_baseline(parts)
+        cpu = None if args.no_cpu_baseline else cpu_baseline(name, n_pairs, seed, dparts, args.cpu_budget_s)
+        computed = None
+        if band_info is not None and kpart is not None:
+            computed = cells - kpart.b.cells() + band_info["cells"]
         line = {
-            "metric": WORKLOADS[args.workload][0], "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "metric": WORKLOADS[name][0], "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "int32", "data": "synthetic (seeded numpy PCG64)",
-            "config": {"workload": WORKLOADS[args.workload][1],
+            "vs_baseline": None, "dtype": "int32",
+            "data": "synthetic (seeded per-pair xoshiro256** streams, splitmix64-seeded)",
+            "config": {"workload": WORKLOADS[name][1],
                        "pairs_per_step_per_gpu": npairs, "cells_per_step_per_gpu": cells,
+                       "launches": [p.key() for p, _ in parts],
+                       "band": args.band if has_ksw else None,
                        "parallelism": f"pair shards x{world}, no collective in the data path",
                        "l2": l2_note},
             "gcups": cells * world / (ms_step * 1e-3) / 1e9,
+            "gcups_computed": None if computed is None else computed * world / (ms_step * 1e-3) / 1e9,
             "roofline": {"bound": "int32", "achieved": achieved, "peak": peak["iadd_tops"], "unit": "Tops/s",
-                         "frac": achieved / peak["iadd_tops"],
-                         "traffic": DP_TRAFFIC_BYTES if args.workload == "w1" else None,
-                         "kernel": "dp_kernel / dp_wc_kernel (one DP launch per algorithm per step)",
-                         "dp_ms_per_step": dp_ms / args.steps,
+                         "frac": achieved / peak["iadd_tops"], "traffic": None,
+                         "traffic_note": "no per-run DRAM counter; see the ncu summaries of the alignment kernels",
+                         "kernel": "every alignment kernel of the step (DP, start passes, traceback; four launches "
+                                   "on four streams): algorithmic integer ops / the step's wall clock",
+                         "ops_per_step": ops,
                          "ops_per_cell": {"local": 11, "global": 9, "semi_global": 10, "ksw": 13,
                                           "traceback_extra": 4},
                          "peak_source": "measured live: 2-input int32 add issue rate (gb_probe_int_peak)",
-                         "imnmx_tops": peak["imnmx_tops"], "dpx_tops": peak["dpx_tops"]},
+                         "imnmx_tops": peak["imnmx_tops"], "dpx_tops": peak["dpx_tops"],
+                         "align_span_ms_per_step": kt["span"][0] / args.steps},
+            "prep_bandwidth": dict(prep, peak_gbs=hbm, peak_source=hbm_src),
             "kernel_ms_per_step": {k: v[0] / args.steps for k, v in kt.items()},
+            "kernel_ms_note": "summed per-kind CUDA-event times; kinds overlap across the four streams",
             "gpu_launches": launches,
             "cpu_baseline": cpu,
             "e2e": e2e,
@@ -470,9 +615,129 @@ def main():
             "plain": plain,
         }
         print(json.dumps(line), flush=True)
+    if model is not None:
+        gl.BandModel.uninstall()
     if dist:
         dist.barrier()
         dist.destroy_process_group()
+
+
+def plain_leg(torch, gl, args, name, n_pairs, seed, dparts, model, dev, dist, value, world):
+    """Batched vs plain full-DP form on one stratified sample of the
+    workload, each timed over one step after a warm-up step, outputs compared
+    with each other and with the full run's outputs for the same pairs."""
+    from gasal_b200 import shard
+    # size the sample from the plain form's rate on a 0.5% probe sample
+    probe_every = 200
+    pidx = stratified(n_pairs, probe_every)
+    probe = [DevPart(torch, p, b, dev) for p, b in build_parts(name, n_pairs, seed, pidx)]
+    saved = gl.get_tuning()
+    if model is not None:
+        gl.BandModel.uninstall()
+    gl.set_tuning(**gl.PLAIN_FORM)
+    try:
+        r = Runner(torch, gl, probe, dev)
+        probe_ms = r.time(1, 1)
+    finally:
+        gl.set_tuning(**saved)
+        if model is not None:
+            model.install(16, 1024)
+    est_full_s = probe_ms * 1e-3 * probe_every
+    every = 1 if est_full_s <= args.plain_budget_s else int(np.ceil(est_full_s / args.plain_budget_s))
+    if every == 1:
+        sample = dparts
+        sidx = None
+    else:
+        sidx = stratified(n_pairs, every)
+        sample = [DevPart(torch, p, b, dev) for p, b in build_parts(name, n_pairs, seed, sidx)]
+    npairs = sum(d.b.n for d in sample)
+    cells = sum(d.b.cells() for d in sample)
+    rb = Runner(torch, gl, sample, dev)
+    bms = shard.max_over_ranks(rb.time(1, 1), dist, dev)
+    batched_out = [{k: v.clone() for k, v in d.fields().items()} for d in sample]
+    batched_cig = [(d.cigar.clone(), d.ncig.clone()) for d in sample]
+    if model is not None:
+        gl.BandModel.uninstall()
+    gl.set_tuning(**gl.PLAIN_FORM)
+    try:
+        rp = Runner(torch, gl, sample, dev)
+        pms = shard.max_over_ranks(rp.time(1, 1), dist, dev)
+    finally:
+        gl.set_tuning(**saved)
+        if model is not None:
+            model.install(16, 1024)
+    same = True
+    for d, bo, (bc, bn) in zip(sample, batched_out, batched_cig):
+        for k, v in d.fields().items():
+            same &= bool(torch.equal(v, bo[k]))
+        if d.p.start_pos == WITH_TB:
+            same &= bool(torch.equal(d.cigar, bc)) and bool(torch.equal(d.ncig, bn))
+    # the full run's outputs for the sampled pairs
+    full_same = None
+    if sidx is not None:
+        lidx = local_index(name, n_pairs, sidx)
+        # outputs of the sample currently hold the plain run's, equal to the batched sample run's when `same`
+        full_same, bad = outputs_equal(torch, dparts, sample, lidx)
+    pval = shard.job_throughput(npairs, world, 1, pms)
+    bval = shard.job_throughput(npairs, world, 1, bms)
+    return {"value": pval, "unit": UNIT, "ms_per_step": pms, "steps": 1, "warmup": 1,
+            "sample": "full batch" if sidx is None else
+                      f"stratified: every {every}th pair of the {n_pairs}-pair workload ({npairs} pairs, all "
+                      f"launches); the plain form on the full batch would take ~{est_full_s:.0f} s",
+            "gcups": cells * world / (pms * 1e-3) / 1e9,
+            "form": "every pair one per thread in input order on a grid over the batch: no device work counter, "
+                    "no length ordering, no warp-cooperative or warp-per-pair kernels, no band, start passes in "
+                    "the forward launch",
+            "batched_same_sample": {"value": bval, "ms_per_step": bms},
+            "value_over_plain": bval / pval,
+            "full_value_over_plain_sample_rate": value / pval,
+            "bit_exact_vs_plain": bool(same),
+            "full_run_equals_sample_run": full_same}
+
+
+def cpu_baseline(name, n_pairs, seed, dparts, budget_s: float) -> dict:
+    """Scalar C oracle, OpenMP on every host core, on a stratified subsample
+    sized to about budget_s of CPU time; its outputs are compared with the GPU
+    run's outputs for the same pairs."""
+    from oracle.bindings import oracle_align
+    cores = os.cpu_count() or 1
+    probe_every = max(1, n_pairs // 3000)
+    pidx = stratified(n_pairs, probe_every)
+    probe = build_parts(name, n_pairs, seed, pidx)
+    t0 = time.time()
+    for p, b in probe:
+        oracle_align(p, b, threads=cores)
+    per_pair = (time.time() - t0) / max(1, len(pidx))
+    m = int(min(n_pairs, max(len(pidx), budget_s / max(per_pair, 1e-9))))
+    every = max(1, n_pairs // m)
+    sidx = stratified(n_pairs, every)
+    sample = build_parts(name, n_pairs, seed, sidx)
+    t0 = time.time()
+    outs = [oracle_align(p, b, threads=cores) for p, b in sample]
+    dt = time.time() - t0
+    # parity of the full GPU run on these pairs
+    lidx = local_index(name, n_pairs, sidx)
+    bad = 0
+    for (p, b), o, d, li in zip(sample, outs, dparts, lidx):
+        exp = o.as_dict(p)
+        for k, v in exp.items():
+            if k == "cigar":
+                cg = d.cigar.cpu().numpy()
+                for j, i in enumerate(li):
+                    oe, og = int(b.q_off[j]), int(d.b.q_off[i])
+                    nc = int(exp["n_cigar"][j])
+                    if not np.array_equal(v[oe:oe + nc], cg[og:og + nc]):
+                        bad += 1
+                continue
+            got = (d.ncig if k == "n_cigar" else d.outs[k]).cpu().numpy()[li]
+            bad += int((got.astype(np.int64) != v.astype(np.int64)).sum())
+    n = len(sidx)
+    return {"value": n / dt, "unit": UNIT, "cores": cores, "kind": "port",
+            "sample": f"stratified: every {every}th pair of the {n_pairs}-pair workload ({n} pairs, "
+                      f"{100.0 * n / n_pairs:.2f}%), {dt:.1f} s",
+            "oracle_check": {"pairs": n, "mismatched_values": bad,
+                             "what": "every defined output (and CIGAR bytes) of the full GPU run at these pairs "
+                                     "vs the oracle's"}}
 
 
 if __name__ == "__main__":

@@ -348,6 +348,26 @@ void set_last_error(const char *where, cudaError_t e)
 }
 } // namespace
 
+/* The pack kernel alone (reference gasal_pack_kernel, src/kernels/pack_rc_seqs.h:13-53). */
+extern "C" int gb_pack_dev(const uint8_t *ascii, uint32_t nbytes, uint32_t *packed, void *stream)
+{
+    if ((nbytes & 7) || (nbytes && (!ascii || !packed))) return GB_ERR_ARG;
+    return gb::launch_pack(ascii, nbytes, packed, (cudaStream_t)stream) == cudaSuccess ? GB_OK : GB_ERR_CUDA;
+}
+
+/* The reverse/complement kernel alone on packed words (reference
+ * gasal_reversecomplement_kernel, src/kernels/pack_rc_seqs.h:56-212). */
+extern "C" int gb_revcomp_dev(uint32_t *pq, uint32_t *pt, const uint32_t *q_off, const uint32_t *t_off,
+                              const uint32_t *q_len, const uint32_t *t_len, const uint8_t *q_op, const uint8_t *t_op,
+                              int32_t n, void *stream)
+{
+    if (n < 0 || (n && (!pq || !pt || !q_off || !t_off || !q_len || !t_len))) return GB_ERR_ARG;
+    return gb::launch_revcomp(pq, pt, q_off, t_off, q_len, t_len, q_op, t_op, n, gb::settings().ref_reverse,
+                              (cudaStream_t)stream) == cudaSuccess
+               ? GB_OK
+               : GB_ERR_CUDA;
+}
+
 extern "C" const char *gb_last_error(void) { return g_last_error; }
 
 extern "C" int gb_autotune(const gb_params_t *p, const gb_dev_batch_t *b, const gb_dev_out_t *o, void *stream,

@@ -543,6 +543,9 @@ static int enqueue_order(const uint32_t *q_len, const uint32_t *t_len, int n, Wo
     return e == cudaSuccess ? GB_OK : GB_ERR_CUDA;
 }
 
+static int enqueue_align(const RunCfg &cfg, const DevBatch &b, const DevOut &o, Workspace &ws, const Plan &p,
+                         cudaStream_t s);
+
 int enqueue_batch(const RunCfg &cfg, const DevBatch &b, const DevOut &o, Workspace &ws, const Plan &p,
                   cudaStream_t s)
 {
@@ -561,6 +564,16 @@ int enqueue_batch(const RunCfg &cfg, const DevBatch &b, const DevOut &o, Workspa
                                cfg.ref_reverse, s));
         timing_mark(K_RC, false, s);
     }
+    timing_mark(K_SPAN, true, s);
+    const int rc = enqueue_align(cfg, b, o, ws, p, s);
+    timing_mark(K_SPAN, false, s);
+    return rc;
+}
+
+/* ordering, DP and traceback of a packed batch */
+static int enqueue_align(const RunCfg &cfg, const DevBatch &b, const DevOut &o, Workspace &ws, const Plan &p,
+                         cudaStream_t s)
+{
     if (!p.tb) {
         const uint32_t *ord = nullptr;
         if (p.order_on) {

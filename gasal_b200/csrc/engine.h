@@ -147,7 +147,10 @@ struct Settings {
 Settings &settings();
 
 /* Optional per-kernel CUDA-event timing (off by default).  Kinds: */
-enum KernelKind { K_PACK = 0, K_RC = 1, K_DP = 2, K_TB = 3, K_ORDER = 4, K_KINDS = 5 };
+/* K_SPAN is not a kernel: one mark per batch on the launch stream, from the
+ * first alignment-phase operation (ordering or DP) to the last (DP joined back
+ * from the auxiliary stream, traceback included) -- the phase's wall clock. */
+enum KernelKind { K_PACK = 0, K_RC = 1, K_DP = 2, K_TB = 3, K_ORDER = 4, K_SPAN = 5, K_KINDS = 6 };
 void timing_enable(bool on);
 void timing_mark(int kind, bool start, cudaStream_t s);
 int timing_read(double ms[K_KINDS], int64_t launches[K_KINDS]);

@@ -89,6 +89,8 @@ SIGNATURES = {
     "gasal_c_is_aln_async_done": (C.c_int, [C.c_void_p]),
     "gb_align": (C.c_int, [C.POINTER(GbParams), C.POINTER(GbBatch), C.POINTER(GbOut)]),
     "gb_align_dev": (C.c_int, [C.POINTER(GbParams), C.POINTER(GbDevBatch), C.POINTER(GbDevOut), C.c_void_p]),
+    "gb_pack_dev": (C.c_int, [C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p]),
+    "gb_revcomp_dev": (C.c_int, [C.c_void_p] * 8 + [C.c_int32, C.c_void_p]),
     "gb_align_dev_noalloc": (C.c_int, [C.POINTER(GbParams), C.POINTER(GbDevBatch), C.POINTER(GbDevOut),
                                        C.c_void_p]),
     "gb_set_reference_reverse": (C.c_int, [C.c_int]),
@@ -197,8 +199,9 @@ def set_tuning(**kw):
     _check(lib().gb_set_tuning(C.byref(t)), "gb_set_tuning")
 
 
-KERNEL_KINDS = ("pack", "revcomp", "dp", "traceback", "order")
-KERNELS_PER_MARK = {"pack": 1, "revcomp": 1, "dp": 1, "traceback": 1, "order": 3}
+KERNEL_KINDS = ("pack", "revcomp", "dp", "traceback", "order", "span")
+# kernels behind one mark of each kind; "span" marks the alignment phase's wall clock, no kernel of its own
+KERNELS_PER_MARK = {"pack": 1, "revcomp": 1, "dp": 1, "traceback": 1, "order": 3, "span": 0}
 
 
 def kernel_timing(on: bool):
@@ -206,8 +209,8 @@ def kernel_timing(on: bool):
 
 
 def kernel_timing_read() -> dict:
-    ms = (C.c_double * 5)()
-    n = (C.c_int64 * 5)()
+    ms = (C.c_double * len(KERNEL_KINDS))()
+    n = (C.c_int64 * len(KERNEL_KINDS))()
     _check(lib().gb_kernel_timing_read(ms, n), "gb_kernel_timing_read")
     return {k: (ms[i], n[i]) for i, k in enumerate(KERNEL_KINDS)}
 
@@ -331,6 +334,19 @@ def cigar_text_dev(cigar_ptr: int, q_off_ptr: int, n_cigar_ptr: int, n: int, tex
     _check(lib().gb_cigar_text(C.c_void_p(cigar_ptr), C.c_void_p(q_off_ptr), C.c_void_p(n_cigar_ptr), int(n),
                                C.c_void_p(text_ptr), int(stride), C.c_void_p(text_len_ptr), C.c_void_p(stream_handle)),
            "gb_cigar_text")
+
+
+def pack_dev(ascii_ptr: int, nbytes: int, packed_ptr: int, stream_handle: int = 0):
+    """The pack kernel alone on device buffers (gb_pack_dev)."""
+    _check(lib().gb_pack_dev(C.c_void_p(ascii_ptr), nbytes, C.c_void_p(packed_ptr), C.c_void_p(stream_handle)),
+           "gb_pack_dev")
+
+
+def revcomp_dev(dev: dict, n: int, stream_handle: int = 0):
+    """The reverse/complement kernel alone on a device batch's packed words
+    (gb_revcomp_dev); dev holds pq, pt, q_off, t_off, q_len, t_len, q_op, t_op."""
+    args = [C.c_void_p(dev.get(k)) for k in ("pq", "pt", "q_off", "t_off", "q_len", "t_len", "q_op", "t_op")]
+    _check(lib().gb_revcomp_dev(*args, n, C.c_void_p(stream_handle)), "gb_revcomp_dev")
 
 
 def align_dev(p: Params, dev: dict, h_q_len: np.ndarray, h_t_len: np.ndarray, stream_handle: int = 0,

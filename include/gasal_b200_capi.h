@@ -177,6 +177,18 @@ int gb_align(const gb_params_t *p, const gb_batch_t *b, gb_out_t *o);
  * (src/gasal_align.cu:180-264).  n == 0 returns GB_OK and launches nothing. */
 int gb_align_dev(const gb_params_t *p, const gb_dev_batch_t *b, const gb_dev_out_t *o, void *stream);
 
+/* The two preparation kernels alone, on device buffers, queued on `stream`:
+ * gb_pack_dev packs nbytes (a multiple of 8) of N-padded ASCII bases into
+ * nbytes / 8 words of 4-bit codes (reference gasal_pack_kernel,
+ * src/kernels/pack_rc_seqs.h:13-53); gb_revcomp_dev applies each sequence's
+ * operation_on_seq (q_op / t_op may be NULL) to the packed words in place
+ * (reference gasal_reversecomplement_kernel, src/kernels/pack_rc_seqs.h:
+ * 56-212; gb_set_reference_reverse selects the reversal form).  Both are the
+ * first steps of gb_align_dev. */
+int gb_pack_dev(const uint8_t *ascii, uint32_t nbytes, uint32_t *packed, void *stream);
+int gb_revcomp_dev(uint32_t *pq, uint32_t *pt, const uint32_t *q_off, const uint32_t *t_off, const uint32_t *q_len,
+                   const uint32_t *t_len, const uint8_t *q_op, const uint8_t *t_op, int32_t n, void *stream);
+
 /* Allocation-free variant of gb_align_dev, for callers that cannot call
  * cudaMalloc (inside stream capture, under a device-memory arena, or as a
  * plugin that must not allocate).  No counterpart in the reference.  The
@@ -268,8 +280,10 @@ const char *gb_last_error(void);
  * and starts recording a CUDA event pair around every kernel the library
  * launches; gb_kernel_timing_read() waits for them and returns, per kind
  * (0 pack, 1 reverse/complement, 2 alignment DP, 3 traceback, 4 length-binned
- * ordering = 3 kernels per mark), the summed milliseconds and the number of
- * marks, in arrays of 5.  gb_probe_int_peak() times the
+ * ordering = 3 kernels per mark, 5 the alignment phase's wall clock on the
+ * launch stream: ordering through DP -- auxiliary-stream kernels joined back --
+ * and traceback, one mark per batch), the summed milliseconds and the number
+ * of marks, in arrays of 6.  gb_probe_int_peak() times the
  * integer instructions the DP is bound by on the current GPU (tera-ops/s). */
 /* ---- Learned ksw band (no reference counterpart) ----
  * A small MLP (67 pair features -> 64 -> 64 -> 1, ReLU, BF16 inference,

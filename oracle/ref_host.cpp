@@ -16,6 +16,7 @@
 
 #include <cstring>
 #include <cmath>
+#include <algorithm>
 #include <vector>
 #include <omp.h>
 
@@ -152,12 +153,18 @@ extern "C" int ref_host_align(const gb_params_t *p, const gb_batch_t *b, gb_out_
     /* 16 spare target rows, as the GPU driver allocates (the GLOBAL traceback
      * reads one tile row past the matrix when a length is a multiple of 8) */
     const uint32_t maxt8 = ((uint32_t)(*std::max_element(tl.begin(), tl.end()) + 7) & ~7u) + 16;
-    std::vector<uint4> tb;
+    /* The reference allocates its tile buffer once, at gasal_init_streams
+     * (src/ctors.cpp:60-66), not per batch: keep one buffer across calls and
+     * grow it.  GLOBAL traceback reads a tile row past the matrix, which a
+     * fresh device allocation holds as zeros, so those tiles are cleared. */
+    static std::vector<uint4> tb_keep;
+    uint4 *tbp = NULL;
     if (p->start_pos == WITH_TB && (p->algo == LOCAL || p->algo == GLOBAL)) {
-        size_t tiles = (size_t)ceil((double)((uint64_t)maxq8 * maxt8) / 32.0);
-        tb.assign(tiles * (size_t)n, make_uint4(0, 0, 0, 0));
+        const size_t tiles = (size_t)ceil((double)((uint64_t)maxq8 * maxt8) / 32.0) * (size_t)n;
+        if (tb_keep.size() < tiles) tb_keep.resize(tiles);
+        if (p->algo == GLOBAL) std::fill(tb_keep.begin(), tb_keep.begin() + tiles, make_uint4(0, 0, 0, 0));
+        tbp = tb_keep.data();
     }
-    uint4 *tbp = tb.empty() ? NULL : tb.data();
     uint32_t *PQ = pq.data(), *PT = pt.data(), *QL = ql.data(), *TL = tl.data(), *QO = qo.data(), *TO = to.data();
     const bool sb = p->second_best != 0;
 

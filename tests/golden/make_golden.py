@@ -24,7 +24,7 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
 
-from gasal_b200 import workloads as W  # noqa: E402
+import np_workloads as W  # noqa: E402  (the generator these fixtures were made with)
 from gasal_b200.capi import (Batch, Params, LOCAL, GLOBAL, SEMI_GLOBAL, BANDED, KSW,  # noqa: E402
                              WITHOUT_START, WITH_START, WITH_TB, NONE, QUERY, TARGET, BOTH)
 

@@ -42,3 +42,36 @@ def test_workload4_mix_and_split():
         _check_layout(b)
     again = W.workload4(20000, seed=7)
     assert all(np.array_equal(a.q, c.q) and np.array_equal(a.t, c.t) for (_, a), (_, c) in zip(parts, again))
+
+
+def test_pairs_do_not_depend_on_threads_or_batch_size():
+    """Each pair has its own xoshiro256** stream keyed by (seed, pair index)."""
+    a = W.generate(4, 3000, seed=11, threads=1)[0]
+    b = W.generate(4, 3000, seed=11, threads=4)[0]
+    assert np.array_equal(a.q, b.q) and np.array_equal(a.t, b.t) and np.array_equal(a.seed, b.seed)
+    big = W.generate(4, 5000, seed=11)[0]
+    for i in (0, 1, 1234, 2999):
+        assert a.seq(i, "q") == big.seq(i, "q") and a.seq(i, "t") == big.seq(i, "t")
+    other = W.generate(4, 3000, seed=12)[0]
+    assert not np.array_equal(a.q_len, other.q_len)
+
+
+def test_workload_shapes_and_padding():
+    b0 = W.workload0(4000, seed=3)
+    _check_layout(b0)
+    assert b0.q_len.min() >= 100 and b0.q_len.max() <= 150
+    assert (b0.t_len >= b0.q_len - 10).all()
+    for b in (b0, W.workload2(2000, seed=4)):
+        for i in (0, 17, b.n - 1):
+            o, n = int(b.q_off[i]), int(b.q_len[i])
+            assert (b.q[o + n:o + ((n + 7) // 8) * 8] == ord("N")).all()
+    b2 = W.workload2(4000, seed=4)
+    assert b2.q_len.min() >= 50 and b2.q_len.max() <= 1000 and b2.t_len.min() >= 1
+    # unrelated pairs exist in workload 4: identity near 1/4 for some pairs
+    p, b4 = W.workload4(4000, seed=9)[0]
+    ident = []
+    for i in range(200):
+        q, t = b4.seq(i, "q"), b4.seq(i, "t")
+        m = min(len(q), len(t))
+        ident.append(np.mean(np.frombuffer(q[:m], np.uint8) == np.frombuffer(t[:m], np.uint8)))
+    assert min(ident) < 0.4 and max(ident) > 0.9
