@@ -124,39 +124,93 @@ __device__ void revcomp_one(uint32_t *w, uint32_t len, int op, int ref_reverse)
     }
 }
 
-/* Reference-identical reversal, word-parallel: blockDim = (32, 8), one row of
- * 32 threads per pair, thread x handling word pairs (x, regs-1-x) for
- * x < ceil(regs/2) in steps of 32.  Each word is read by at most one thread
- * (its own index, below ceil(regs/2)) and written only after that read, so
- * the in-place update is race-free; the complement of the untouched words
- * runs after a row barrier. */
-__device__ __forceinline__ void revcomp_ref_row(uint32_t *w, uint32_t len, int op)
+/* Complement of every A/C/G/T nibble (codes 1, 3, 7, 4: A<->T, C<->G), other
+ * codes unchanged, without branches: per code an exact zero-nibble test of
+ * x ^ code marks its nibbles, and the swap is one XOR per class (A and T differ
+ * by 0x5, C and G by 0x4). */
+__device__ __forceinline__ uint32_t nib_eq(uint32_t x, uint32_t rep)
 {
-    const uint32_t regs = (len + 7) >> 3;
-    if (op & 1) {
-        const uint32_t half = (regs + 1) >> 1;
-        for (uint32_t i = threadIdx.x; i < half; i += 32) {
-            const uint32_t head = w[i];
-            uint32_t rev = nib_reverse(head);
-            if (op & 2) rev = complement_word(rev);
-            if (i != regs - 1 - i) w[i] = 0u;
-            w[regs - 1 - i] = rev;
-        }
-    } else if (op & 2) {
-        for (uint32_t i = threadIdx.x; i < regs; i += 32) w[i] = complement_word(w[i]);
-    }
+    uint32_t t = x ^ rep;
+    t |= t >> 1;
+    t |= t >> 2;
+    return (~t & 0x11111111u) * 0xFu; /* 0xF in every nibble equal to the code */
 }
 
-__global__ void __launch_bounds__(256) revcomp_ref_kernel(uint32_t *pq, uint32_t *pt, const uint32_t *q_off,
-                                                          const uint32_t *t_off, const uint32_t *q_len,
-                                                          const uint32_t *t_len, const uint8_t *q_op,
-                                                          const uint8_t *t_op, int32_t n)
+__device__ __forceinline__ uint32_t complement_flat(uint32_t x)
 {
-    const int i = blockIdx.x * blockDim.y + threadIdx.y;
-    if (i >= n) return;
-    const int qo = q_op ? q_op[i] : 0, to = t_op ? t_op[i] : 0;
-    if (qo & 3) revcomp_ref_row(pq + (q_off[i] >> 3), q_len[i], qo);
-    if (to & 3) revcomp_ref_row(pt + (t_off[i] >> 3), t_len[i], to);
+    const uint32_t at = nib_eq(x, 0x11111111u) | nib_eq(x, 0x44444444u);
+    const uint32_t cg = nib_eq(x, 0x33333333u) | nib_eq(x, 0x77777777u);
+    return x ^ (at & 0x55555555u) ^ (cg & 0x44444444u);
+}
+
+/* Reference-identical reversal, flat over the batch.  A warp takes 32
+ * sequences (queries, then targets, in groups of 32), prefix-sums their word
+ * tasks across lanes -- ceil(regs/2) word pairs when reversing, regs words when
+ * only complementing, none otherwise -- and sweeps the concatenated task list
+ * 32 tasks at a time: consecutive lanes take consecutive words of a sequence,
+ * so loads and stores stream through the batch instead of one short sequence
+ * per 32-thread row.  Task i of a reversed sequence reads word i, writes its
+ * nibble-reversed (and, for op 3, complemented) value to word regs-1-i and
+ * zeroes word i (the sm_100a build's result); no other task touches those
+ * words, so the update in place is race-free. */
+__global__ void __launch_bounds__(256) revcomp_flat_kernel(uint32_t *pq, uint32_t *pt, const uint32_t *q_off,
+                                                           const uint32_t *t_off, const uint32_t *q_len,
+                                                           const uint32_t *t_len, const uint8_t *q_op,
+                                                           const uint8_t *t_op, int32_t n)
+{
+    const int lane = threadIdx.x & 31;
+    const int groups_q = q_op ? (n + 31) >> 5 : 0;
+    const int groups = groups_q + (t_op ? (n + 31) >> 5 : 0);
+    const int warp0 = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int nwarps = (gridDim.x * blockDim.x) >> 5;
+    for (int g = warp0; g < groups; g += nwarps) {
+        const bool tside = g >= groups_q;
+        const int p = ((tside ? g - groups_q : g) << 5) + lane;
+        const uint8_t *ops = tside ? t_op : q_op;
+        uint32_t *words = tside ? pt : pq;
+        int op = p < n ? (ops[p] & 3) : 0;
+        uint32_t base = 0, regs = 0;
+        if (op) {
+            base = (tside ? t_off[p] : q_off[p]) >> 3;
+            regs = ((tside ? t_len[p] : q_len[p]) + 7) >> 3;
+        }
+        const uint32_t tasks = (op & 1) ? (regs + 1) >> 1 : (op == 2 ? regs : 0u);
+        uint32_t incl = tasks;
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, incl, d);
+            if (lane >= d) incl += y;
+        }
+        const uint32_t total = __shfl_sync(0xFFFFFFFFu, incl, 31);
+        for (uint32_t k0 = 0; k0 < total; k0 += 32) {
+            const uint32_t k = k0 + lane;
+            /* owner: the first lane whose inclusive count exceeds k */
+            int owner = 0;
+#pragma unroll
+            for (int step = 16; step > 0; step >>= 1) {
+                const uint32_t c = __shfl_sync(0xFFFFFFFFu, incl, owner + step - 1);
+                if (c <= k) owner += step;
+            }
+            const uint32_t o_incl = __shfl_sync(0xFFFFFFFFu, incl, owner & 31);
+            const uint32_t o_tasks = __shfl_sync(0xFFFFFFFFu, tasks, owner & 31);
+            const uint32_t o_base = __shfl_sync(0xFFFFFFFFu, base, owner & 31);
+            const uint32_t o_regs = __shfl_sync(0xFFFFFFFFu, regs, owner & 31);
+            const int o_op = __shfl_sync(0xFFFFFFFFu, op, owner & 31);
+            if (k >= total) continue;
+            const uint32_t i = k - (o_incl - o_tasks);
+            uint32_t *w = words + o_base;
+            if (o_op & 1) {
+                const uint32_t head = w[i];
+                uint32_t rev = nib_reverse(head);
+                if (o_op & 2) rev = complement_flat(rev);
+                const uint32_t mirror = o_regs - 1 - i;
+                if (i != mirror) w[i] = 0u;
+                w[mirror] = rev;
+            } else {
+                w[i] = complement_flat(w[i]);
+            }
+        }
+    }
 }
 
 __global__ void revcomp_kernel(uint32_t *pq, uint32_t *pt, const uint32_t *q_off, const uint32_t *t_off,
@@ -176,8 +230,14 @@ cudaError_t launch_revcomp(uint32_t *pq, uint32_t *pt, const uint32_t *q_off, co
 {
     if (n <= 0) return cudaSuccess;
     if (ref_reverse) {
-        const dim3 blk(32, 8);
-        revcomp_ref_kernel<<<(n + 7) / 8, blk, 0, s>>>(pq, pt, q_off, t_off, q_len, t_len, q_op, t_op, n);
+        int dev = 0, sms = 148;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        const int groups = ((q_op ? (n + 31) / 32 : 0) + (t_op ? (n + 31) / 32 : 0));
+        if (groups == 0) return cudaSuccess;
+        int blocks = (groups + 7) / 8; /* 8 warps per block */
+        if (blocks > sms * 8) blocks = sms * 8;
+        revcomp_flat_kernel<<<blocks, 256, 0, s>>>(pq, pt, q_off, t_off, q_len, t_len, q_op, t_op, n);
     } else {
         revcomp_kernel<<<(n + 127) / 128, 128, 0, s>>>(pq, pt, q_off, t_off, q_len, t_len, q_op, t_op, n, 0);
     }
