@@ -419,7 +419,7 @@ def prep_bandwidth(torch, gl, dparts, hbm_gbs, reps=5):
     return out
 
 
-def e2e_leg(torch, gl, parts, args, dev, dist):
+def e2e_leg(torch, gl, parts, args, dev, dist, job_pairs):
     """The storage API with host buffers: per step, every launch's pinned batch
     goes host->device, aligns, and every result array comes back."""
     from gasal_b200 import shard
@@ -453,10 +453,8 @@ def e2e_leg(torch, gl, parts, args, dev, dist):
             times.append(max(starts[0].elapsed_time(e) for e in ends))
     for _, _, s in streams:
         s.close()
-    npairs = sum(b.n for _, b in parts)
     ms = shard.max_over_ranks(float(np.mean(times)), dist, dev)
-    world = dist.get_world_size() if dist else 1
-    return {"value": npairs * world / (ms * 1e-3), "unit": UNIT, "h2d_bytes_per_step": h2d,
+    return {"value": job_pairs / (ms * 1e-3), "unit": UNIT, "h2d_bytes_per_step": h2d,
             "d2h_bytes_per_step": d2h, "ms_per_step": ms, "steps": n_timed,
             "path": f"gasal_c_aln_async + gasal_c_is_aln_async_done, one storage per launch ({len(parts)} streams), "
                     f"pinned host batches filled (gasal_host_batch_fill) before the timed region"}
@@ -482,6 +480,9 @@ def main():
     ap.add_argument("--plain-budget-s", type=float, default=20.0,
                     help="device time the plain form's timed step may take; beyond it a stratified sample is used")
     ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--split", default="weak", choices=["weak", "cells"],
+                    help="N>1: weak = every rank aligns its own full-size seeded shard; cells = the ranks split one "
+                         "workload into contiguous slices of equal DP cells (strong scaling)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -511,13 +512,23 @@ def main():
         hbm, hbm_src = 6650.0, "fallback 6.65 TB/s (earlier measurement on this pool)"
     name = args.workload
     n_pairs = args.pairs or WORKLOADS[name][2]
-    seed = shard.shard_seed(W.SEED_BASE + WORKLOADS[name][3], rank)
+    strong = args.split == "cells" and world > 1
+    seed = W.SEED_BASE + WORKLOADS[name][3] if strong else shard.shard_seed(W.SEED_BASE + WORKLOADS[name][3], rank)
     t0 = time.time()
-    parts = build_parts(name, n_pairs, seed)
+    if strong:
+        all_cells = W.pair_cells(WORKLOADS[name][3], n_pairs, seed)
+        lo, hi = shard.cell_shard_range(all_cells, rank, world)
+        parts = build_parts(name, n_pairs, seed, np.arange(lo, hi, dtype=np.int64))
+    else:
+        parts = build_parts(name, n_pairs, seed)
     log(f"workload {name}: {n_pairs} pairs generated in {time.time() - t0:.1f}s "
         f"({W.generator_threads()} threads)")
     npairs = sum(b.n for _, b in parts)
     cells = sum(b.cells() for _, b in parts)
+    if strong:
+        args.no_plain = True  # the plain-form and oracle comparisons index the whole workload, not a slice
+    job_pairs = n_pairs if strong else npairs * world  # pairs the whole job aligns per step
+    job_cells = float(all_cells.sum()) if strong else float(cells) * world
     dev = torch.device("cuda", local_rank)
     dparts = [DevPart(torch, p, b, dev) for p, b in parts]
 
@@ -541,7 +552,7 @@ def main():
     gl.kernel_timing(False)
     ms = shard.max_over_ranks(ms, dist, dev)
     ms_step = ms / args.steps
-    value = shard.job_throughput(npairs, world, args.steps, ms)
+    value = job_pairs * args.steps / (ms * 1e-3)
     ops = alg_ops(parts)
     achieved = ops / (ms_step * 1e-3) / 1e12
     launches = sum(n * gl.KERNELS_PER_MARK[k] for k, (_, n) in kt.items())
@@ -564,7 +575,7 @@ def main():
         del wide
 
     # ---------------- end to end through the storage API ----------------
-    e2e = e2e_leg(torch, gl, parts, args, dev, dist)
+    e2e = e2e_leg(torch, gl, parts, args, dev, dist, job_pairs)
 
     # ---------------- the plain full-DP form on a stratified sample ----------------
     plain = None
@@ -576,23 +587,28 @@ def main():
                f"inputs {in_mb:.0f} MB fit the 126 MB L2 (no flush: each step re-reads them, as a caller "
                f"re-aligning resident batches would)")
     if rank == 0:
-        cpu = None if args.no_cpu_baseline else cpu_baseline(name, n_pairs, seed, dparts, args.cpu_budget_s)
+        cpu = None if args.no_cpu_baseline else cpu_baseline(name, n_pairs, seed, None if strong else dparts,
+                                                             args.cpu_budget_s)
         computed = None
         if band_info is not None and kpart is not None:
             computed = cells - kpart.b.cells() + band_info["cells"]
         line = {
             "metric": WORKLOADS[name][0], "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
+            "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True,
+            "scaling": "strong" if strong else "weak",
             "vs_baseline": None, "dtype": "int32",
             "data": "synthetic (seeded per-pair xoshiro256** streams, splitmix64-seeded)",
             "config": {"workload": WORKLOADS[name][1],
                        "pairs_per_step_per_gpu": npairs, "cells_per_step_per_gpu": cells,
                        "launches": [p.key() for p, _ in parts],
                        "band": args.band if has_ksw else None,
-                       "parallelism": f"pair shards x{world}, no collective in the data path",
+                       "parallelism": (f"one workload split into {world} contiguous slices of equal DP cells, no "
+                                       f"collective in the data path" if strong else
+                                       f"pair shards x{world} (a full-size seeded shard per rank), no collective "
+                                       f"in the data path"),
                        "l2": l2_note},
-            "gcups": cells * world / (ms_step * 1e-3) / 1e9,
-            "gcups_computed": None if computed is None else computed * world / (ms_step * 1e-3) / 1e9,
+            "gcups": job_cells / (ms_step * 1e-3) / 1e9,
+            "gcups_computed": None if computed is None else computed * (job_cells / cells) / (ms_step * 1e-3) / 1e9,
             "roofline": {"bound": "int32", "achieved": achieved, "peak": peak["iadd_tops"], "unit": "Tops/s",
                          "frac": achieved / peak["iadd_tops"], "traffic": None,
                          "traffic_note": "no per-run DRAM counter; see the ncu summaries of the alignment kernels",
@@ -715,6 +731,12 @@ def cpu_baseline(name, n_pairs, seed, dparts, budget_s: float) -> dict:
     t0 = time.time()
     outs = [oracle_align(p, b, threads=cores) for p, b in sample]
     dt = time.time() - t0
+    n = len(sidx)
+    line = {"value": n / dt, "unit": UNIT, "cores": cores, "kind": "port",
+            "sample": f"stratified: every {every}th pair of the {n_pairs}-pair workload ({n} pairs, "
+                      f"{100.0 * n / n_pairs:.2f}%), {dt:.1f} s"}
+    if dparts is None:
+        return line
     # parity of the full GPU run on these pairs
     lidx = local_index(name, n_pairs, sidx)
     bad = 0
@@ -731,13 +753,10 @@ def cpu_baseline(name, n_pairs, seed, dparts, budget_s: float) -> dict:
                 continue
             got = (d.ncig if k == "n_cigar" else d.outs[k]).cpu().numpy()[li]
             bad += int((got.astype(np.int64) != v.astype(np.int64)).sum())
-    n = len(sidx)
-    return {"value": n / dt, "unit": UNIT, "cores": cores, "kind": "port",
-            "sample": f"stratified: every {every}th pair of the {n_pairs}-pair workload ({n} pairs, "
-                      f"{100.0 * n / n_pairs:.2f}%), {dt:.1f} s",
-            "oracle_check": {"pairs": n, "mismatched_values": bad,
-                             "what": "every defined output (and CIGAR bytes) of the full GPU run at these pairs "
-                                     "vs the oracle's"}}
+    line["oracle_check"] = {"pairs": n, "mismatched_values": bad,
+                            "what": "every defined output (and CIGAR bytes) of the full GPU run at these pairs vs "
+                                    "the oracle's"}
+    return line
 
 
 if __name__ == "__main__":

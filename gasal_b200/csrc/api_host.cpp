@@ -852,7 +852,9 @@ static int grow_dev(void **p, uint32_t old_bytes, uint32_t new_bytes)
     (void)old_bytes;
     if (*p) cudaFree(*p);
     *p = NULL;
-    return cudaMalloc(p, new_bytes) == cudaSuccess ? GB_OK : GB_ERR_ALLOC;
+    if (gb::dev_malloc(p, new_bytes) == cudaSuccess) return GB_OK;
+    cudaGetLastError();
+    return GB_ERR_ALLOC;
 }
 
 /* zdrop: the ksw z-drop threshold.  GASAL2's kernel hard-codes 0

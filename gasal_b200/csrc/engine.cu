@@ -136,6 +136,30 @@ Workspace::~Workspace()
      * context is current; nothing to do at static destruction time */
 }
 
+/* Every device allocation of the engine's workspaces and of the storage API's
+ * regrowth goes through here.  GASAL_B200_FAIL_ALLOC_AFTER=k (read once) makes
+ * the allocation after the first k fail once, as an out-of-memory would, so
+ * the callers' GB_ERR_ALLOC paths can be exercised without exhausting a GPU;
+ * later allocations are served normally. */
+cudaError_t dev_malloc(void **p, size_t bytes)
+{
+    static std::mutex mu;
+    static long countdown = [] {
+        const char *e = getenv("GASAL_B200_FAIL_ALLOC_AFTER");
+        return e ? atol(e) : -1L;
+    }();
+    {
+        std::lock_guard<std::mutex> lk(mu);
+        if (countdown == 0) {
+            countdown = -1;
+            *p = nullptr;
+            return cudaErrorMemoryAllocation;
+        }
+        if (countdown > 0) countdown--;
+    }
+    return cudaMalloc(p, bytes);
+}
+
 static int grow(void **p, size_t *cap, size_t need, size_t elem)
 {
     if (*cap >= need) return GB_OK;
@@ -143,9 +167,9 @@ static int grow(void **p, size_t *cap, size_t need, size_t elem)
     *p = nullptr;
     *cap = 0;
     size_t want = need + need / 4 + 1024;
-    if (cudaMalloc(p, want * elem) != cudaSuccess) {
+    if (dev_malloc(p, want * elem) != cudaSuccess) {
         cudaGetLastError();
-        if (cudaMalloc(p, need * elem) != cudaSuccess) {
+        if (dev_malloc(p, need * elem) != cudaSuccess) {
             cudaGetLastError();
             *p = nullptr;
             return GB_ERR_ALLOC;
@@ -174,7 +198,7 @@ static int grow(void **p, size_t *cap, size_t need, size_t elem)
 static int ensure_order_buffers(Workspace &ws, size_t n)
 {
     if (grow((void **)&ws.order, &ws.order_cap, n, 4) != GB_OK) return GB_ERR_ALLOC;
-    if (!ws.bins && cudaMalloc((void **)&ws.bins, (size_t)order_bins() * 4) != cudaSuccess) {
+    if (!ws.bins && dev_malloc((void **)&ws.bins, (size_t)order_bins() * 4) != cudaSuccess) {
         cudaGetLastError();
         return GB_ERR_ALLOC;
     }
@@ -259,7 +283,7 @@ int plan_batch(const RunCfg &cfg, const DevBatch &b, const DevOut &o, Workspace 
     a.score = o.score, a.q_end = o.q_end, a.t_end = o.t_end, a.q_start = o.q_start, a.t_start = o.t_start;
     a.score2 = o.score2, a.q_end2 = o.q_end2, a.t_end2 = o.t_end2;
     a.sc = cfg.sc, a.head = cfg.head, a.tail = cfg.tail, a.k_band = cfg.k_band, a.zdrop = cfg.zdrop, a.mql = cfg.mql;
-    if (!ws.queue && cudaMalloc((void **)&ws.queue, 64) != cudaSuccess) {
+    if (!ws.queue && dev_malloc((void **)&ws.queue, 64) != cudaSuccess) {
         cudaGetLastError();
         return GB_ERR_ALLOC;
     }
@@ -344,7 +368,7 @@ int plan_batch(const RunCfg &cfg, const DevBatch &b, const DevOut &o, Workspace 
                     b.n >= st.min_order_pairs && o.score && o.q_end && o.t_end;
     if (p.split_start) {
         if (grow((void **)&ws.order2, &ws.order2_cap, (size_t)b.n, 4) != GB_OK) return GB_ERR_ALLOC;
-        if (!ws.bins && cudaMalloc((void **)&ws.bins, (size_t)order_bins() * 4) != cudaSuccess) {
+        if (!ws.bins && dev_malloc((void **)&ws.bins, (size_t)order_bins() * 4) != cudaSuccess) {
             cudaGetLastError();
             return GB_ERR_ALLOC;
         }
@@ -367,7 +391,7 @@ int plan_batch(const RunCfg &cfg, const DevBatch &b, const DevOut &o, Workspace 
         ws.h_tb_off = nullptr, ws.d_tb_off = nullptr, ws.tb_off_cap = 0;
         const size_t want = (size_t)b.n + b.n / 4 + 1024;
         if (cudaMallocHost((void **)&ws.h_tb_off, want * 8) != cudaSuccess ||
-            cudaMalloc((void **)&ws.d_tb_off, want * 8) != cudaSuccess) {
+            dev_malloc((void **)&ws.d_tb_off, want * 8) != cudaSuccess) {
             cudaGetLastError();
             return GB_ERR_ALLOC;
         }

@@ -146,6 +146,9 @@ struct Settings {
 };
 Settings &settings();
 
+/* cudaMalloc with an optional injected failure (GASAL_B200_FAIL_ALLOC_AFTER). */
+cudaError_t dev_malloc(void **p, size_t bytes);
+
 /* Optional per-kernel CUDA-event timing (off by default).  Kinds: */
 /* K_SPAN is not a kernel: one mark per batch on the launch stream, from the
  * first alignment-phase operation (ordering or DP) to the last (DP joined back

@@ -251,10 +251,43 @@ def autotune(p: Params, dev: dict, h_q_len: np.ndarray, h_t_len: np.ndarray, str
     return d
 
 
+BAND_BLOB_MAGIC = b"GBBAND01"
+
+
+def band_blob(params: np.ndarray, feature_stride: int) -> bytes:
+    """Serialised band-model weights: magic, parameter count and feature
+    stride (uint32 little endian), the float32 parameters in the
+    gb_band_model_params layout, then a CRC-32 of everything before it."""
+    import struct
+    import zlib
+    p = np.ascontiguousarray(params, dtype="<f4")
+    body = BAND_BLOB_MAGIC + struct.pack("<II", p.shape[0], int(feature_stride)) + p.tobytes()
+    return body + struct.pack("<I", zlib.crc32(body) & 0xFFFFFFFF)
+
+
+def band_unblob(blob: bytes, n_params: int, feature_stride: int) -> np.ndarray:
+    """Parameters from band_blob(); raises GasalError when the magic, the
+    sizes or the checksum do not match this library's model."""
+    import struct
+    import zlib
+    head = len(BAND_BLOB_MAGIC) + 8
+    if len(blob) < head + 4 or blob[:len(BAND_BLOB_MAGIC)] != BAND_BLOB_MAGIC:
+        raise GasalError("band model blob: bad magic or truncated")
+    n, stride = struct.unpack("<II", blob[len(BAND_BLOB_MAGIC):head])
+    if n != n_params or stride != feature_stride:
+        raise GasalError(f"band model blob: {n} parameters / stride {stride}, library has {n_params} / {feature_stride}")
+    if len(blob) != head + 4 * n + 4:
+        raise GasalError("band model blob: wrong length")
+    (crc,) = struct.unpack("<I", blob[-4:])
+    if zlib.crc32(blob[:-4]) & 0xFFFFFFFF != crc:
+        raise GasalError("band model blob: checksum mismatch")
+    return np.frombuffer(blob[head:head + 4 * n], dtype="<f4").astype(np.float32)
+
+
 class BandModel:
     """The learned ksw band MLP (gb_band_model_*): parameters live on the
     current device; train_step runs the hand-written gradient and Adam
-    kernels."""
+    kernels; save / load keep the weights in a checksummed file."""
 
     def __init__(self, seed: int = 1):
         self._m = lib().gb_band_model_new(int(seed))
@@ -288,6 +321,14 @@ class BandModel:
         _check(lib().gb_band_train_step(self._m, feat_ptr, label_ptr, int(n), float(tau), float(lr), stream,
                                         C.byref(loss)), "gb_band_train_step")
         return loss.value
+
+    def save(self, path: str):
+        with open(path, "wb") as f:
+            f.write(band_blob(self.params(), lib().gb_band_feature_stride()))
+
+    def load(self, path: str):
+        with open(path, "rb") as f:
+            self.set_params(band_unblob(f.read(), self.n_params, lib().gb_band_feature_stride()))
 
     def install(self, band_min: int = 16, band_max: int = 1024):
         _check(lib().gb_set_band_model(self._m, int(band_min), int(band_max)), "gb_set_band_model")

@@ -31,6 +31,33 @@ def shard_range(n_total: int, rank: int, world: int):
     return lo, lo + q + (1 if rank < r else 0)
 
 
+def cell_shard_range(cells, rank: int, world: int):
+    """Contiguous [lo, hi) slice of a batch for a rank, balanced by work: the
+    cut points are where the running sum of per-pair cells (qlen * tlen)
+    crosses k/world of the total, so every rank gets about the same number of
+    DP cells rather than of pairs (a strong-scaling split of one batch whose
+    lengths are uneven).  Every pair lands in exactly one slice."""
+    cells = np.asarray(cells, dtype=np.float64)
+    n = len(cells)
+    if n == 0:
+        return 0, 0
+    csum = np.cumsum(cells)
+    total = csum[-1]
+    if total <= 0:
+        return shard_range(n, rank, world)
+    def cut(k):
+        if k <= 0:
+            return 0
+        if k >= world:
+            return n
+        # slice k-1 ends after the pair whose running sum first reaches k/world of the total
+        return int(np.searchsorted(csum, total * k / world, side="left")) + 1
+    lo, hi = cut(rank), cut(rank + 1)
+    lo = min(lo, n)
+    hi = min(max(hi, lo), n)
+    return lo, hi
+
+
 def max_over_ranks(value: float, dist=None, device=None) -> float:
     """Job time = slowest rank's time (all_reduce MAX); identity without a
     process group."""

@@ -89,6 +89,17 @@ def generate(w: int, n: int, seed: int, cuts=None, threads: int = 0, idx=None) -
     return out
 
 
+def pair_cells(w: int, n: int, seed: int, threads: int = 0) -> np.ndarray:
+    """qlen * tlen of every pair of workload w (the generator's first pass
+    only: no bases are written)."""
+    L = _gen()
+    q_len = np.empty(n, np.uint32)
+    t_len = np.empty(n, np.uint32)
+    if L.gbw_lengths(w, seed, 0, None, n, _ptr(q_len), _ptr(t_len), None, None, threads) != 0:
+        raise MemoryError("workload generator failed")
+    return q_len.astype(np.int64) * t_len
+
+
 def _cuts(n: int, shares) -> list:
     return [int(x) for x in np.round(np.cumsum((0.0,) + tuple(shares)) * n).astype(np.int64)]
 

@@ -1,0 +1,84 @@
+"""Allocation failures are reported, and the library recovers from them.
+
+GASAL_B200_FAIL_ALLOC_AFTER=k makes the engine's (k+1)-th device allocation
+fail once, as an out-of-memory would, on the host side -- no GPU fault is
+involved.  Each case runs in a child process (the variable is read once):
+the first gb_align_dev call must return GB_ERR_ALLOC (or succeed when the
+batch needs fewer than k+1 allocations), and a second call on the same batch
+must succeed with results equal to the oracle's.
+"""
+import json
+import os
+import subprocess
+import sys
+
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+CHILD = r"""
+import json, sys
+import numpy as np
+import torch
+sys.path.insert(0, sys.argv[1])
+from gasal_b200 import lib as gl, workloads as W
+from gasal_b200.capi import Params, GLOBAL, KSW, WITH_TB
+from oracle.bindings import oracle_align
+dev = torch.device("cuda", 0)
+out = {}
+for name, p, b in [("global_tb", Params(algo=GLOBAL, start_pos=WITH_TB), W.workload2(3000, seed=61)),
+                   ("ksw", Params(algo=KSW, zdrop=100), W.workload3(600, seed=62))]:
+    def t_(a, dt=None):
+        return torch.from_numpy(np.ascontiguousarray(a).view(dt or a.dtype)).to(dev)
+    keep = {"q": t_(b.q), "t": t_(b.t), "qo": t_(b.q_off, np.int32), "to": t_(b.t_off, np.int32),
+            "ql": t_(b.q_len, np.int32), "tl": t_(b.t_len, np.int32),
+            "pq": torch.zeros(b.q.shape[0] // 8, dtype=torch.int32, device=dev),
+            "pt": torch.zeros(b.t.shape[0] // 8, dtype=torch.int32, device=dev)}
+    if b.seed is not None:
+        keep["seed"] = t_(b.seed, np.int32)
+    outs = {k: torch.zeros(b.n, dtype=torch.int32, device=dev) for k in ("score", "q_end", "t_end", "q_start", "t_start")}
+    cig = torch.zeros(b.q.shape[0], dtype=torch.uint8, device=dev)
+    ncig = torch.zeros(b.n, dtype=torch.int32, device=dev)
+    m = {"q_bytes": b.q.shape[0], "t_bytes": b.t.shape[0]}
+    for k, src in (("q", "q"), ("t", "t"), ("pq", "pq"), ("pt", "pt"), ("q_off", "qo"), ("t_off", "to"),
+                   ("q_len", "ql"), ("t_len", "tl"), ("seed", "seed")):
+        if src in keep:
+            m[k] = keep[src].data_ptr()
+    for k, v in outs.items():
+        m["out_" + k] = v.data_ptr()
+    m["out_cigar"], m["out_n_cigar"] = cig.data_ptr(), ncig.data_ptr()
+    first = "ok"
+    try:
+        gl.align_dev(p, m, b.q_len, b.t_len)
+        torch.cuda.synchronize()
+    except gl.GasalError as e:
+        first = str(e)
+    gl.align_dev(p, m, b.q_len, b.t_len)
+    torch.cuda.synchronize()
+    exp = oracle_align(p, b).as_dict(p)
+    got = {k: v.cpu().numpy() for k, v in outs.items()}
+    got["n_cigar"] = ncig.cpu().numpy().astype(np.uint32)
+    got["cigar"] = cig.cpu().numpy()
+    bad = [k for k in exp if not np.array_equal(got[k].astype(np.int64), exp[k].astype(np.int64))]
+    out[name] = {"first": first, "mismatched": bad}
+print(json.dumps(out))
+"""
+
+
+@pytest.mark.parametrize("k", [0, 1, 2, 3, 5, 8])
+def test_injected_allocation_failure_is_reported_and_recovered(k):
+    env = dict(os.environ, GASAL_B200_FAIL_ALLOC_AFTER=str(k))
+    r = subprocess.run([sys.executable, "-c", CHILD, ROOT], env=env, capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stderr[-3000:]
+    res = json.loads(r.stdout.strip().splitlines()[-1])
+    firsts = [v["first"] for v in res.values()]
+    # exactly one failure is injected per process: at most one launch reports it
+    assert sum(f != "ok" for f in firsts) <= 1, res
+    for f in firsts:
+        assert f == "ok" or "allocation failed" in f, res
+    if k <= 2:
+        assert firsts[0] != "ok", f"the first launch allocates more than {k} buffers: {res}"
+    for name, v in res.items():
+        assert not v["mismatched"], f"{name} after the injected failure: {v}"

@@ -173,3 +173,17 @@ def test_trained_band_beats_a_fixed_band_of_the_same_width():
     kept = {k: v["accepted"] / eb.n for k, v in stats.items()}
     assert kept["learned"] > kept["fixed"] + 0.03, (kept, mean_w)
     assert stats["learned"]["cells"] < stats["fixed"]["cells"], stats
+
+
+def test_band_model_save_load_gives_the_same_weights(tmp_path):
+    torch = pytest.importorskip("torch")
+    from gasal_b200 import lib as gl
+    a = gl.BandModel(seed=5)
+    b = gl.BandModel(seed=6)
+    assert not np.array_equal(a.params(), b.params())
+    path = str(tmp_path / "band.bin")
+    a.save(path)
+    b.load(path)
+    assert np.array_equal(a.params(), b.params())
+    a.close()
+    b.close()

@@ -40,3 +40,24 @@ def test_features_of_a_shifted_copy():
     nq = len(q) - 10
     assert round(float(f[0, 3 + 2]) * nq) == nq      # all in the d = +2 bin
     assert abs(f[0, 0] - len(q) / 1024) < 1e-7 and abs(f[0, 2] - 2 / 128) < 1e-7
+
+
+def test_band_model_blob_round_trip_and_checksum():
+    """The weights file: round trip, and every corruption is refused."""
+    import numpy as np
+    import pytest
+    from gasal_b200 import lib as gl
+    n, stride = gl.lib().gb_band_param_count(), gl.lib().gb_band_feature_stride()
+    p = np.random.default_rng(3).standard_normal(n).astype(np.float32)
+    blob = gl.band_blob(p, stride)
+    assert np.array_equal(gl.band_unblob(blob, n, stride), p)
+    flipped = bytearray(blob)
+    flipped[40] ^= 0x01
+    with pytest.raises(gl.GasalError, match="checksum"):
+        gl.band_unblob(bytes(flipped), n, stride)
+    with pytest.raises(gl.GasalError, match="magic"):
+        gl.band_unblob(b"XX" + blob[2:], n, stride)
+    with pytest.raises(gl.GasalError):
+        gl.band_unblob(blob[:-8], n, stride)
+    with pytest.raises(gl.GasalError, match="parameters"):
+        gl.band_unblob(gl.band_blob(p[:-1], stride), n, stride)

@@ -59,3 +59,56 @@ def test_shard_range_partitions():
             assert all(a[1] == b[0] for a, b in zip(spans, spans[1:]))
             sizes = [hi - lo for lo, hi in spans]
             assert max(sizes) - min(sizes) <= 1
+
+
+def test_cell_shard_range_balances_work():
+    from gasal_b200 import shard, workloads as W
+    parts = W.workload4(40000, seed=3)
+    cells = np.concatenate([b.q_len.astype(np.int64) * b.t_len for _, b in parts])
+    for w in (1, 2, 3, 4, 8):
+        spans = [shard.cell_shard_range(cells, r, w) for r in range(w)]
+        assert spans[0][0] == 0 and spans[-1][1] == len(cells)
+        assert all(a[1] == b[0] for a, b in zip(spans, spans[1:]))
+        work = [cells[lo:hi].sum() for lo, hi in spans]
+        # every slice within one pair's worth of the even share
+        assert max(work) - min(work) <= 2 * cells.max(), (w, work)
+    assert shard.cell_shard_range(np.zeros(0), 0, 2) == (0, 0)
+    assert [shard.cell_shard_range(np.zeros(5), r, 2) for r in range(2)] == [(0, 3), (3, 5)]
+
+
+def _strong_main(rank, world, port, out_dir):
+    import sys
+    sys.path.insert(0, os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+    import torch.distributed as dist
+    from datetime import timedelta
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port), RANK=str(rank), WORLD_SIZE=str(world),
+                      LOCAL_RANK=str(rank))
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=timedelta(seconds=60))
+    from gasal_b200 import shard, workloads as W
+    from oracle.bindings import oracle_align
+    b = W.workload2(900, seed=17)                      # one batch, the same on every rank
+    cells = b.q_len.astype(np.int64) * b.t_len
+    lo, hi = shard.cell_shard_range(cells, rank, world)
+    from gasal_b200.capi import Params, GLOBAL
+    mine = b.subset(np.arange(lo, hi))
+    scores = oracle_align(Params(algo=GLOBAL), mine, threads=1).score
+    np.savez(os.path.join(out_dir, f"s{rank}.npz"), lo=lo, hi=hi, scores=scores, work=cells[lo:hi].sum())
+    dist.barrier()
+    dist.destroy_process_group()
+
+
+def test_two_gloo_ranks_strong_split_of_one_batch(tmp_path):
+    """A strong split: two ranks take cell-balanced slices of one batch; the
+    concatenated results equal the whole batch aligned at once."""
+    import torch.multiprocessing as mp
+    port = _free_port()
+    mp.start_processes(_strong_main, args=(2, port, str(tmp_path)), nprocs=2, start_method="spawn", join=True)
+    s0, s1 = (np.load(tmp_path / f"s{k}.npz") for k in (0, 1))
+    assert int(s0["lo"]) == 0 and int(s0["hi"]) == int(s1["lo"]) and int(s1["hi"]) == 900
+    from gasal_b200 import workloads as W
+    from gasal_b200.capi import Params, GLOBAL
+    from oracle.bindings import oracle_align
+    whole = oracle_align(Params(algo=GLOBAL), W.workload2(900, seed=17), threads=1).score
+    assert np.array_equal(np.concatenate([s0["scores"], s1["scores"]]), whole)
+    w0, w1 = float(s0["work"]), float(s1["work"])
+    assert abs(w0 - w1) / (w0 + w1) < 0.05
