@@ -372,50 +372,55 @@ def train_band(torch, gl, args, rank, dev):
     return model, info
 
 
-def prep_bandwidth(torch, gl, dparts, hbm_gbs, reps=5):
-    """Pack and reverse/complement kernels alone on the resident batch
-    (CUDA events on their stream; every step re-packs, so running them here
-    changes nothing later).  Algorithmic bytes: pack 1.5 B per base (1 read,
-    0.5 written), reverse/complement 1 B per base of sequences with an
-    operation (0.5 read, 0.5 written)."""
+def prep_bandwidth(torch, gl, dparts, hbm_gbs, reps=20):
+    """Pack and reverse/complement kernels alone on the resident batch, each
+    leg captured once as a CUDA graph of every launch's calls and replayed
+    `reps` times between CUDA events on its stream (so host launch overhead is
+    not timed; every step re-packs, so running them here changes nothing
+    later).  Algorithmic bytes: pack 1.5 B per base (1 read, 0.5 written),
+    reverse/complement 1 B per base of sequences with an operation (0.5 read,
+    0.5 written)."""
     s = torch.cuda.Stream(device=dparts[0].outs["score"].device)
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     out = {}
-    pack_bytes = sum(1.5 * (d.b.q.shape[0] + d.b.t.shape[0]) for d in dparts)
-    with torch.cuda.stream(s):
-        for _ in range(2):
-            for d in dparts:
-                gl.pack_dev(d.map["q"], d.b.q.shape[0], d.map["pq"], s.cuda_stream)
-                gl.pack_dev(d.map["t"], d.b.t.shape[0], d.map["pt"], s.cuda_stream)
-        e0.record(s)
-        for _ in range(reps):
-            for d in dparts:
-                gl.pack_dev(d.map["q"], d.b.q.shape[0], d.map["pq"], s.cuda_stream)
-                gl.pack_dev(d.map["t"], d.b.t.shape[0], d.map["pt"], s.cuda_stream)
-        e1.record(s)
+
+    def timed(calls, nbytes, launches):
+        with torch.cuda.stream(s):
+            calls()  # warm-up outside the capture
         torch.cuda.synchronize()
-        ms = e0.elapsed_time(e1) / reps
-        gbs = pack_bytes / (ms * 1e-3) / 1e9
-        out["pack"] = {"gbs": gbs, "frac_of_hbm": gbs / hbm_gbs, "ms_per_step": ms, "bytes_per_step": pack_bytes,
-                       "launches_per_step": 2 * len(dparts)}
-        rc = [d for d in dparts if d.b.q_op is not None and (d.b.q_op != 0).any()]
-        if rc:
-            rc_bytes = 0.0
-            for d in rc:
-                rc_bytes += float(np.sum(d.b.q_len[d.b.q_op != 0])) + float(np.sum(d.b.t_len[d.b.t_op != 0]))
-            for _ in range(2):
-                for d in rc:
-                    gl.revcomp_dev(d.map, d.b.n, s.cuda_stream)
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(g, stream=s):
+            calls()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        with torch.cuda.stream(s):
+            g.replay()
             e0.record(s)
             for _ in range(reps):
-                for d in rc:
-                    gl.revcomp_dev(d.map, d.b.n, s.cuda_stream)
+                g.replay()
             e1.record(s)
-            torch.cuda.synchronize()
-            ms = e0.elapsed_time(e1) / reps
-            gbs = rc_bytes / (ms * 1e-3) / 1e9
-            out["revcomp"] = {"gbs": gbs, "frac_of_hbm": gbs / hbm_gbs, "ms_per_step": ms,
-                              "bytes_per_step": rc_bytes, "launches_per_step": len(rc)}
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / reps
+        gbs = nbytes / (ms * 1e-3) / 1e9
+        del g
+        return {"gbs": gbs, "frac_of_hbm": gbs / hbm_gbs, "ms_per_step": ms, "bytes_per_step": nbytes,
+                "launches_per_step": launches, "timing": f"CUDA graph of the step's launches, {reps} replays"}
+
+    def pack_all():
+        for d in dparts:
+            gl.pack_dev(d.map["q"], d.b.q.shape[0], d.map["pq"], torch.cuda.current_stream().cuda_stream)
+            gl.pack_dev(d.map["t"], d.b.t.shape[0], d.map["pt"], torch.cuda.current_stream().cuda_stream)
+
+    pack_bytes = sum(1.5 * (d.b.q.shape[0] + d.b.t.shape[0]) for d in dparts)
+    out["pack"] = timed(pack_all, pack_bytes, 2 * len(dparts))
+    rc = [d for d in dparts if d.b.q_op is not None and (d.b.q_op != 0).any()]
+    if rc:
+        rc_bytes = sum(float(np.sum(d.b.q_len[d.b.q_op != 0])) + float(np.sum(d.b.t_len[d.b.t_op != 0]))
+                       for d in rc)
+
+        def rc_all():
+            for d in rc:
+                gl.revcomp_dev(d.map, d.b.n, torch.cuda.current_stream().cuda_stream)
+
+        out["revcomp"] = timed(rc_all, rc_bytes, len(rc))
     return out
 
 
