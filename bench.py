@@ -21,8 +21,12 @@ One step = every launch of the workload, each on its own stream.  Reported:
   plain      the plain full-DP form (every pair one per thread, in input
              order, no band) against the batched form on the same stratified
              sample, outputs compared bit for bit
-  band       the learned ksw band: certificate acceptance, recomputations,
-             computed cells (with --band learned)
+  band       the ksw launch's computed cells; with --band compare (default)
+             the same step timed again with the learned band installed
+             (band.learned_leg: pairs/s, ratio to the unbanded step, ksw
+             outputs compared bit for bit, certificate acceptance,
+             recomputations, computed cells); --band learned makes the
+             banded step the headline
   roofline   algorithmic integer ops of every alignment kernel of a step /
              the step's wall clock, against this GPU's measured integer-add
              issue rate; pack and reverse/complement in GB/s against the
@@ -290,16 +294,26 @@ class Runner:
         self.main = torch.cuda.Stream(device=dev)
         self.streams = [torch.cuda.Stream(device=dev) for _ in parts]
 
-    def step(self):
+    def step(self, finish_times=False):
         torch = self.torch
-        fork = torch.cuda.Event()
+        fork = torch.cuda.Event(enable_timing=finish_times)
         fork.record(self.main)
+        dones = []
         for d, s in zip(self.parts, self.streams):
             s.wait_event(fork)
             self.gl.align_dev(d.p, d.map, d.b.q_len, d.b.t_len, s.cuda_stream)
-            done = torch.cuda.Event()
+            done = torch.cuda.Event(enable_timing=finish_times)
             done.record(s)
             self.main.wait_event(done)
+            dones.append(done)
+        if finish_times:
+            self.finish = (fork, dones)
+
+    def launch_finish_ms(self):
+        """Per launch, ms from the last timed step's start to that launch's
+        end (the launches of a step run concurrently on their streams)."""
+        fork, dones = self.finish
+        return [fork.elapsed_time(e) for e in dones]
 
     def time(self, steps: int, warmup: int, dist=None, before_timed=None):
         torch = self.torch
@@ -313,8 +327,8 @@ class Runner:
             before_timed()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(self.main)
-        for _ in range(steps):
-            self.step()
+        for k in range(steps):
+            self.step(finish_times=k == steps - 1)
         e1.record(self.main)
         torch.cuda.synchronize()
         return e0.elapsed_time(e1)
@@ -361,15 +375,42 @@ def train_band(torch, gl, args, rank, dev):
     tp, tb = tparts[ksw_k]
     tdb = BT.DeviceBatch(torch, tb, dev)
     feat = BT.features(torch, tdb)
-    lab = BT.labels(torch, tp, tdb)
+    if args.band_labels == "max_off":
+        lab, _ = BT.labels_max_off(torch, tp, tdb)
+    else:
+        lab = BT.labels(torch, tp, tdb)
     model = gl.BandModel(seed=11)
     trace = BT.train(torch, model, feat, lab, steps=600, batch=8192, tau=0.8, lr=3e-3)
     model.install(16, 1024)
-    info = {"train_pairs": tb.n, "train_s": round(time.time() - t0, 1),
+    info = {"train_pairs": tb.n, "train_s": round(time.time() - t0, 1), "labels": args.band_labels,
             "label_hist_log2": {str(k): int(v) for k, v in zip(*np.unique(lab, return_counts=True))},
             "loss_first": trace[0], "loss_last": trace[-1]}
     log(f"band model trained in {info['train_s']} s; loss {trace[0]:.3f} -> {trace[-1]:.3f}")
     return model, info
+
+
+def learned_band_leg(torch, gl, args, rank, dev, runner, kpart, dist, unbanded_value, job_pairs):
+    """The headline step again with the learned band installed for the ksw
+    launch (trained first, untimed): its throughput against the unbanded
+    headline, its ksw outputs against the unbanded run's (bit-exact), and the
+    certificate's statistics over the launch."""
+    from gasal_b200 import shard
+    ref = {k: v.clone() for k, v in kpart.fields().items()}
+    model, info = train_band(torch, gl, args, rank, dev)
+    try:
+        ms = shard.max_over_ranks(runner.time(args.steps, args.warmup, dist), dist, dev)
+        same = all(bool(torch.equal(v, ref[k])) for k, v in kpart.fields().items())
+        with torch.cuda.stream(runner.main):
+            st = gl.ksw_band_align(kpart.p, kpart.map, kpart.b.q_len, kpart.b.t_len, None, None,
+                                   runner.main.cuda_stream)
+    finally:
+        gl.BandModel.uninstall()
+        model.close()
+    value = job_pairs * args.steps / (ms * 1e-3)
+    return dict(info, value=value, unit=UNIT, ms_per_step=ms / args.steps, steps=args.steps,
+                value_over_unbanded=value / unbanded_value, bit_exact_vs_unbanded=same, **st,
+                acceptance_rate=st["accepted"] / max(1, st["pairs"]),
+                computed_cells_fraction=st["cells"] / max(1, kpart.b.cells()))
 
 
 def prep_bandwidth(torch, gl, dparts, hbm_gbs, reps=20):
@@ -456,13 +497,44 @@ def e2e_leg(torch, gl, parts, args, dev, dist, job_pairs):
         torch.cuda.synchronize()
         if it >= args.warmup:
             times.append(max(starts[0].elapsed_time(e) for e in ends))
+    # the same with the host staging inside the timed region: every step refills each storage's pinned
+    # pages from the caller's buffers (gasal_host_batch_fill_mt, all host threads) just before its
+    # gasal_aln_async, so the fills of later storages overlap the GPU work of earlier ones
+    ftimes, fill_s = [], []
+    seq_bytes = sum(int(b.q.shape[0] + b.t.shape[0]) for _, b, _ in streams)
+    for it in range(1 + n_timed):
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        ends = [torch.cuda.Event(enable_timing=True) for _ in streams]
+        e0.record(ext[0])
+        fs = 0.0
+        for k, (p, b, s) in enumerate(streams):
+            t0 = time.perf_counter()
+            qi, ti = s.fill_bulk(0, b)
+            fs += time.perf_counter() - t0
+            s.aln_async(0, qi, ti, b.n)
+            ends[k].record(ext[k])
+        for _, _, s in streams:
+            s.wait(0)
+        torch.cuda.synchronize()
+        if it >= 1:
+            ftimes.append(max(e0.elapsed_time(e) for e in ends))
+            fill_s.append(fs)
     for _, _, s in streams:
         s.close()
     ms = shard.max_over_ranks(float(np.mean(times)), dist, dev)
+    fms = shard.max_over_ranks(float(np.mean(ftimes)), dist, dev)
+    fill_ms = float(np.mean(fill_s)) * 1e3
     return {"value": job_pairs / (ms * 1e-3), "unit": UNIT, "h2d_bytes_per_step": h2d,
             "d2h_bytes_per_step": d2h, "ms_per_step": ms, "steps": n_timed,
             "path": f"gasal_c_aln_async + gasal_c_is_aln_async_done, one storage per launch ({len(parts)} streams), "
-                    f"pinned host batches filled (gasal_host_batch_fill) before the timed region"}
+                    f"pinned host batches filled (gasal_host_batch_fill) before the timed region",
+            "with_fill": {"value": job_pairs / (fms * 1e-3), "unit": UNIT, "ms_per_step": fms, "steps": n_timed,
+                          "host_fill_ms_per_step": fill_ms, "host_fill_gbs": seq_bytes / (fill_ms * 1e-3) / 1e9,
+                          "sequence_bytes_per_step": seq_bytes,
+                          "path": "per step and storage: gasal_host_batch_fill_mt of the query and target blocks "
+                                  "(all host threads) + offsets/lengths/ops/seeds, then gasal_c_aln_async; later "
+                                  "storages' fills overlap earlier storages' GPU work"}}
 
 
 def main():
@@ -476,10 +548,15 @@ def main():
     ap.add_argument("--ref-sample", type=int, default=4000, help="pairs per step of the reference arm")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-budget-s", type=float, default=12.0)
-    ap.add_argument("--band", default="learned", choices=["off", "learned"],
-                    help="ksw launches: learned band with certificate (the model is trained first on a separate "
-                         "sample of the workload)")
+    ap.add_argument("--band", default="compare", choices=["off", "learned", "compare"],
+                    help="ksw launches: off (unbanded), learned (the headline step runs with the learned band and "
+                         "its certificate; the model is trained first on a separate sample of the workload), or "
+                         "compare (headline unbanded, then the same step timed again with the learned band "
+                         "installed, outputs compared)")
     ap.add_argument("--band-train-pairs", type=int, default=60_000)
+    ap.add_argument("--band-labels", default="ladder", choices=["ladder", "max_off"],
+                    help="band labels: the narrowest ladder band the certificate keeps, or log2(max_off + 16) "
+                         "from the plain ksw's own maximum diagonal offset")
     ap.add_argument("--no-plain", action="store_true",
                     help="skip the plain full-DP form (one pair per thread, input order, no band)")
     ap.add_argument("--plain-budget-s", type=float, default=20.0,
@@ -551,6 +628,7 @@ def main():
         clk.mark_start()
 
     ms = runner.time(args.steps, args.warmup, dist, before_timed=arm)
+    finish_ms = runner.launch_finish_ms()
     clk.mark_end()
     clk.__exit__()
     kt = gl.kernel_timing_read()
@@ -579,6 +657,10 @@ def main():
                          computed_cells_fraction=st["cells"] / max(1, kpart.b.cells()))
         del wide
 
+    if args.band == "compare" and kpart is not None:
+        band_info["learned_leg"] = learned_band_leg(torch, gl, args, rank, dev, runner, kpart, dist, value,
+                                                    job_pairs)
+
     # ---------------- end to end through the storage API ----------------
     e2e = e2e_leg(torch, gl, parts, args, dev, dist, job_pairs)
 
@@ -606,7 +688,8 @@ def main():
             "config": {"workload": WORKLOADS[name][1],
                        "pairs_per_step_per_gpu": npairs, "cells_per_step_per_gpu": cells,
                        "launches": [p.key() for p, _ in parts],
-                       "band": args.band if has_ksw else None,
+                       "band": ({"compare": "off (the learned band timed as a second leg, band.learned_leg)"}
+                                .get(args.band, args.band) if has_ksw else None),
                        "parallelism": (f"one workload split into {world} contiguous slices of equal DP cells, no "
                                        f"collective in the data path" if strong else
                                        f"pair shards x{world} (a full-size seeded shard per rank), no collective "
@@ -627,6 +710,9 @@ def main():
                          "align_span_ms_per_step": kt["span"][0] / args.steps},
             "prep_bandwidth": dict(prep, peak_gbs=hbm, peak_source=hbm_src),
             "kernel_ms_per_step": {k: v[0] / args.steps for k, v in kt.items()},
+            "launch_finish_ms": {p.key(): round(t, 2) for (p, _), t in zip(parts, finish_ms)},
+            "launch_finish_note": "last timed step: ms from its start until each launch (own stream) finished; "
+                                  "the gap between the last two is the time one launch ran alone",
             "kernel_ms_note": "summed per-kind CUDA-event times; kinds overlap across the four streams",
             "gpu_launches": launches,
             "cpu_baseline": cpu,

@@ -1,8 +1,10 @@
 """Training the learned ksw band (no reference counterpart).
 
-Labels come from the banded kernel itself: a pair's label is log2 of the
-narrowest band in a ladder whose result the certificate keeps (log2(2048)
-when none does).  The model is trained with the pinball loss at quantile tau
+Labels: labels_max_off() takes them from the plain (unbanded) ksw's own
+max_off -- the largest |column - row| where its running maximum rose, as
+ksw_extend2 tracks it -- plus a margin; labels() from the banded kernel
+itself: log2 of the narrowest band in a ladder whose result the certificate
+keeps (log2(2048) when none does).  The model is trained with the pinball loss at quantile tau
 (tau > 0.5 prefers bands a little wider than needed: a refused band costs a
 full recomputation, a wider one only a few more columns).
 
@@ -71,6 +73,22 @@ def labels(torch, p: Params, db: DeviceBatch, ladder=LADDER, stream: int = 0) ->
         lab[new] = np.log2(w)
         done |= kept
     return lab
+
+
+MAX_OFF_MARGIN = 16  # diagonals added to max_off: the certificate needs room beside the path
+
+
+def labels_max_off(torch, p: Params, db: DeviceBatch, margin: int = MAX_OFF_MARGIN, stream: int = 0):
+    """log2(max_off + margin) per pair, max_off from the plain (unbanded) ksw
+    itself: the largest |column - row| over the cells where its running
+    maximum rose -- how far from the main diagonal the alignment reached.
+    Returns (labels, max_off)."""
+    dev = db.keep["q"].device
+    mo = torch.zeros(db.b.n, dtype=torch.int32, device=dev)
+    gl.ksw_align_max_off(p, db.map, db.b.q_len, db.b.t_len, mo.data_ptr(), stream)
+    torch.cuda.synchronize()
+    m = mo.cpu().numpy()
+    return np.log2(m.astype(np.float64) + margin).astype(np.float32), m
 
 
 def train(torch, model: "gl.BandModel", feat, lab: np.ndarray, steps: int = 400, batch: int = 8192,

@@ -22,6 +22,8 @@
 #include <atomic>
 #include <mutex>
 #include <string>
+#include <thread>
+#include <vector>
 #include <unordered_map>
 
 /* ========================= Parameters =================================== */
@@ -420,18 +422,16 @@ uint32_t page_room(const host_batch_t *p) { return p->page_size - p->data_size; 
 
 } // namespace
 
-/* Appends one sequence, N-padded to a multiple of 8, to the chain's open page:
- * the first page not yet locked.  When that page lacks room, it is locked and
- * the write moves to its successor -- re-based to start where the locked
- * page's data ends -- or, past the last page, to a new page of twice the size
- * (which also grows the storage's host byte total).  The move happens once per
- * call; if the page reached still lacks room, nothing is written.  Returns the
- * byte index after the written sequence (or `idx` unchanged). */
-uint32_t gasal_host_batch_fill(gasal_gpu_storage_t *gpu_storage, uint32_t idx, const char *data, uint32_t size,
-                               data_source SRC)
+namespace {
+
+/* The page a fill of `need` bytes writes to: the chain's open page (the first
+ * one not yet locked).  When that page lacks room, it is locked and the write
+ * moves to its successor -- re-based to start where the locked page's data
+ * ends -- or, past the last page, to a new page of twice the size (which also
+ * grows the storage's host byte total).  The move happens once per call;
+ * nullptr when the page reached still lacks room. */
+host_batch_t *fill_page(const PageChain &ch, uint32_t need)
 {
-    const PageChain ch = chain_of(gpu_storage, SRC);
-    const uint32_t need = round8(size);
     host_batch_t *pg = ch.head;
     while (pg->is_locked) pg = pg->next;
     if (page_room(pg) < need) {
@@ -450,9 +450,62 @@ uint32_t gasal_host_batch_fill(gasal_gpu_storage_t *gpu_storage, uint32_t idx, c
         pg->is_locked = 1;
         pg = pg->next;
     }
-    if (page_room(pg) < need) return idx;
+    return page_room(pg) < need ? nullptr : pg;
+}
+
+/* memcpy split into `threads` contiguous slices of at least 1 MiB, one
+ * std::thread each (the calling thread takes the first) */
+void copy_parallel(uint8_t *dst, const char *src, size_t n, int threads)
+{
+    const size_t min_slice = (size_t)1 << 20;
+    if (threads <= 0) threads = (int)std::max(1u, std::thread::hardware_concurrency());
+    size_t parts = std::min<size_t>((size_t)threads, std::max<size_t>(1, n / min_slice));
+    if (parts <= 1) {
+        memcpy(dst, src, n);
+        return;
+    }
+    const size_t slice = (n + parts - 1) / parts;
+    std::vector<std::thread> pool;
+    pool.reserve(parts - 1);
+    for (size_t k = 1; k < parts; k++) {
+        const size_t lo = k * slice, hi = std::min(n, lo + slice);
+        if (lo < hi) pool.emplace_back([=] { memcpy(dst + lo, src + lo, hi - lo); });
+    }
+    memcpy(dst, src, std::min(n, slice));
+    for (auto &t : pool) t.join();
+}
+
+} // namespace
+
+/* Appends one sequence, N-padded to a multiple of 8, to the chain's open page
+ * (fill_page).  Returns the byte index after the written sequence, or `idx`
+ * unchanged when even the page moved to lacks room. */
+uint32_t gasal_host_batch_fill(gasal_gpu_storage_t *gpu_storage, uint32_t idx, const char *data, uint32_t size,
+                               data_source SRC)
+{
+    const uint32_t need = round8(size);
+    host_batch_t *pg = fill_page(chain_of(gpu_storage, SRC), need);
+    if (!pg) return idx;
     uint8_t *dst = pg->data + (idx - pg->offset);
     memcpy(dst, data, size);
+    memset(dst + size, N_CODE, need - size);
+    pg->data_size += need;
+    return idx + need;
+}
+
+/* gasal_host_batch_fill with the copy split over `threads` host threads (0:
+ * every hardware thread): the same page, padding and return value.  Meant
+ * for a whole batch staged as one block (sequences already padded to 8 at
+ * ascending offsets), where one thread's memcpy bandwidth would otherwise
+ * bound the host side of a multi-gigabyte step. */
+uint32_t gasal_host_batch_fill_mt(gasal_gpu_storage_t *gpu_storage, uint32_t idx, const char *data, uint32_t size,
+                                  data_source SRC, int threads)
+{
+    const uint32_t need = round8(size);
+    host_batch_t *pg = fill_page(chain_of(gpu_storage, SRC), need);
+    if (!pg) return idx;
+    uint8_t *dst = pg->data + (idx - pg->offset);
+    copy_parallel(dst, data, size, threads);
     memset(dst + size, N_CODE, need - size);
     pg->data_size += need;
     return idx + need;

@@ -210,4 +210,33 @@ int gb_ksw_band_align(const gb_params_t *p, const gb_dev_batch_t *b, const gb_de
     return GB_OK;
 }
 
+/* Unbanded ksw (the plain computation every banded result must equal) with
+ * one more output per pair: max_off, the largest |column - row| over the cells
+ * where the running maximum rose (ksw_extend2's max_off), the diagonal reach
+ * the alignment needed -- the band labels' source. */
+int gb_ksw_align_max_off(const gb_params_t *p, const gb_dev_batch_t *b, const gb_dev_out_t *o, int32_t *max_off,
+                         void *stream)
+{
+    if (!p || !b || !o || !max_off || b->n <= 0 || !b->h_q_len || !b->h_t_len || p->algo != KSW) return GB_ERR_ARG;
+    DevWs *w = band_ws(stream);
+    if (!w) return GB_ERR_CUDA;
+    const gb::Settings &set = gb::settings();
+    gb::RunCfg cfg{};
+    cfg.algo = p->algo, cfg.start = p->start_pos, cfg.second = 0, cfg.head = p->head, cfg.tail = p->tail;
+    cfg.k_band = p->k_band, cfg.zdrop = p->zdrop;
+    cfg.sc = {p->match, p->mismatch, p->gap_open, p->gap_extend, p->gap_open + p->gap_extend};
+    cfg.ref_reverse = set.ref_reverse, cfg.mql = set.mql, cfg.is_packed = 0;
+    cfg.reverse_complement = p->reverse_complement;
+    cfg.band_w = nullptr, cfg.band_model = nullptr; /* unbanded, whatever model is installed */
+    gb::DevBatch db{};
+    db.n = b->n, db.q_bytes = b->q_bytes, db.t_bytes = b->t_bytes, db.q = b->q, db.t = b->t;
+    db.pq = b->pq, db.pt = b->pt, db.q_off = b->q_off, db.t_off = b->t_off, db.q_len = b->q_len;
+    db.t_len = b->t_len, db.q_op = b->q_op, db.t_op = b->t_op, db.seed = b->seed;
+    db.h_q_len = b->h_q_len, db.h_t_len = b->h_t_len;
+    gb::DevOut dout{};
+    dout.score = o->score, dout.q_end = o->q_end, dout.t_end = o->t_end;
+    dout.max_off = max_off;
+    return gb::run_batch(cfg, db, dout, w->ws, (cudaStream_t)stream);
+}
+
 } // extern "C"

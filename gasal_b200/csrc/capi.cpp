@@ -154,6 +154,12 @@ uint32_t gasal_c_host_batch_fill(void *storage, uint32_t idx, const char *data, 
     return gasal_host_batch_fill(S(storage), idx, data, size, (data_source)src);
 }
 
+uint32_t gasal_c_host_batch_fill_mt(void *storage, uint32_t idx, const char *data, uint32_t size, int src,
+                                    int threads)
+{
+    return gasal_host_batch_fill_mt(S(storage), idx, data, size, (data_source)src, threads);
+}
+
 uint32_t gasal_c_host_batch_add(void *storage, uint32_t idx, const char *data, uint32_t size, int src)
 {
     return gasal_host_batch_add(S(storage), idx, data, size, (data_source)src);

@@ -30,6 +30,18 @@ __device__ __forceinline__ uint32_t pack_he(int h, int e) { return (uint32_t)(ui
 
 __device__ __forceinline__ int code(uint32_t w, int k) { return (int)((w >> (28 - 4 * k)) & 15u); }
 
+/* a * b + c (low 32 bits) as one integer multiply-add.  The cell loops are
+ * bound by the ALU pipe (min/max, permutes, logic); position keys and 16-bit
+ * merges written this way issue on the FMA pipe instead. */
+__device__ __forceinline__ uint32_t mad_lo_u32(uint32_t a, uint32_t b, uint32_t c)
+{
+    uint32_t d;
+    asm("mad.lo.u32 %0, %1, %2, %3;" : "=r"(d) : "r"(a), "r"(b), "r"(c));
+    return d;
+}
+/* the column key 8*H + r (r = 7 - row in the band) */
+__device__ __forceinline__ int key8(int H, int r) { return (int)mad_lo_u32((uint32_t)H, 8u, (uint32_t)r); }
+
 __device__ __forceinline__ uint32_t nib_rev(uint32_t x)
 {
     const uint32_t r = __byte_perm(x, 0, 0x0123);
@@ -229,7 +241,7 @@ __device__ void local_fwd(const uint32_t *q, int qregs, const uint32_t *t, int t
                     const int t0 = M - sc.oe;
                     F[k] = __viaddmax_s32(F[k], -sc.e, t0);
                     e = __viaddmax_s32(e, -sc.e, t0);
-                    key[k] = (H << 3) + (7 - k);
+                    key[k] = key8(H, 7 - k);
                     if (SECOND) {
                         bool ge;
                         run = __vibmax_s32(H, run, &ge);
@@ -301,7 +313,7 @@ __device__ void local_start(const uint32_t *q, int qregs, const uint32_t *t, int
                     const int t0 = M - sc.oe;
                     F[k] = __viaddmax_s32(F[k], -sc.e, t0);
                     e = __viaddmax_s32(e, -sc.e, t0);
-                    key[k] = (H << 3) + (7 - k);
+                    key[k] = key8(H, 7 - k);
                     Hn[k] = H;
                 }
                 rb.st(c, pack_he(Hn[7], e));
@@ -665,7 +677,7 @@ __device__ void banded(const uint32_t *q, int qregs, const uint32_t *t, int treg
                     int H = __vimax3_s32_relu(D[k] + scr.s(k), F[k], 0);
                     e = __viaddmax_s32(e, -sc.e, up - sc.oe);
                     H = max(H, e);
-                    key[k] = (H << 3) + (7 - k);
+                    key[k] = key8(H, 7 - k);
                     Hn[k] = H;
                     up = H;
                 }
@@ -704,7 +716,7 @@ __device__ void ksw(const uint32_t *q, int qlen, const uint32_t *t, int tlen, ui
         prevh -= e_ins;
         rb.st(2 * j, (uint32_t)prevh);
     }
-    int mx = h0, max_i = -1, max_j = -1, max_ie = -1, gscore = -1;
+    int mx = h0, max_i = -1, max_j = -1, max_ie = -1, gscore = -1, mo = 0;
     int beg = 0, end = qlen;
     for (int i = 0; i < tlen;) {
         int f = 0, h1, m = 0, mj = -1;
@@ -744,6 +756,7 @@ __device__ void ksw(const uint32_t *q, int qlen, const uint32_t *t, int tlen, ui
             leave = true;
         } else if (m > mx) {
             mx = m, max_i = i, max_j = mj;
+            mo = max(mo, abs(mj - i));
         } else if (zdrop > 0) {
             if (i - max_i > mj - max_j) {
                 if (mx - m - ((i - max_i) - (mj - max_j)) * e_del > zdrop) leave = true;
@@ -769,6 +782,7 @@ __device__ void ksw(const uint32_t *q, int qlen, const uint32_t *t, int tlen, ui
     } else {
         r.score = gscore, r.q_end = qlen, r.t_end = max_ie + 1;
     }
+    r.score2 = mo; /* ksw has no second best: the slot carries max_off */
 }
 
 

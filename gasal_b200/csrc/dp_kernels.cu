@@ -101,6 +101,7 @@ __device__ __forceinline__ void dp_one(const DpArgs &a, uint32_t w, RowBuf rb, c
         return;
     }
     if (a.score) a.score[i] = r.score;
+    if (ALGO == KSW_ && a.max_off) a.max_off[i] = r.score2;
     if (ALGO != GLOBAL_) {
         if (a.q_end) a.q_end[i] = r.q_end;
         if (a.t_end) a.t_end[i] = r.t_end;

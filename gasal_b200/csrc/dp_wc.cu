@@ -362,7 +362,7 @@ __device__ void wc_sweep(QW qword, int qregs, TW tword, int tregs, int qlen, int
                     const int t0 = M - sc.oe;
                     F[k] = __viaddmax_s32(F[k], -sc.e, t0);
                     e = __viaddmax_s32(e, -sc.e, t0);
-                    key[k] = (H << 3) + (7 - k);
+                    key[k] = key8(H, 7 - k);
                     if (SECOND_PASS2) {
                         bool ge;
                         run = __vibmax_s32(H, run, &ge);

@@ -282,6 +282,7 @@ int plan_batch(const RunCfg &cfg, const DevBatch &b, const DevOut &o, Workspace 
     a.seed = b.seed, a.order = nullptr, a.n = b.n;
     a.score = o.score, a.q_end = o.q_end, a.t_end = o.t_end, a.q_start = o.q_start, a.t_start = o.t_start;
     a.score2 = o.score2, a.q_end2 = o.q_end2, a.t_end2 = o.t_end2;
+    a.max_off = cfg.algo == KSW_ ? o.max_off : nullptr;
     a.sc = cfg.sc, a.head = cfg.head, a.tail = cfg.tail, a.k_band = cfg.k_band, a.zdrop = cfg.zdrop, a.mql = cfg.mql;
     if (!ws.queue && dev_malloc((void **)&ws.queue, 64) != cudaSuccess) {
         cudaGetLastError();

@@ -50,6 +50,7 @@ struct DevOut {
     int32_t *score, *q_end, *t_end, *q_start, *t_start, *score2, *q_end2, *t_end2;
     uint8_t *cigar;             /* device buffer of q_bytes (the query batch) */
     uint32_t *n_cigar;
+    int32_t *max_off;           /* ksw: largest diagonal offset of a rise of the maximum (optional) */
 };
 
 /* Device scratch owned by one stream (grown on demand, never shrunk). */

@@ -55,6 +55,8 @@ struct DpArgs {
                                            (q_max 0: no upper limit) */
     int32_t *lastcol;                   /* warp-cooperative SEMI_GLOBAL: last-column H of every row,
                                            one slot of scratch_cols words per lane group of the grid */
+    int32_t *max_off;                   /* unbanded ksw: largest |column - row| of the cells where the
+                                           running maximum rose (ksw_extend2's max_off), or null */
 };
 
 /* Shape of one warp-cooperative launch: lanes per pair (0: it cannot run),

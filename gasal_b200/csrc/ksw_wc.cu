@@ -52,6 +52,139 @@ __device__ __forceinline__ int kslot(int j) { return (j & ~255) | ((j & 7) << 5)
 /* 16-bit prmt selector that sign-extends byte c (class c < 8) */
 __device__ __forceinline__ uint32_t sel16(uint32_t c) { return c * 0x1111u | 0x8880u; }
 
+/* The row loop is bound by the ALU pipe (min/max, permutes, logic): the
+ * 16-bit split and merge of the eh words and the row-maximum keys are
+ * written as integer multiply-adds so they issue on the FMA pipe. */
+__device__ __forceinline__ uint32_t high16(uint32_t x)
+{
+    uint32_t d;
+    asm("mul.hi.u32 %0, %1, %2;" : "=r"(d) : "r"(x), "r"(65536u));
+    return d;
+}
+
+/* Per-row values shared by the tiles of one row, and the state they carry. */
+struct TileConst {
+    uint32_t *eh;
+    const uint4 *selw;
+    int slots;
+    uint2 tab;
+    int sm, sx, g, lane, end, Cmul, oe, e_del;
+};
+struct TileState {
+    int fcarry, hcarry, kmax, hlast, flast; /* F and H entering the next tile, row-maximum key, H/F at end-1 */
+    int fcol, fcnt;                         /* columns of the first lane holding a non-zero eh entry */
+    int lcol, lcnt;                         /* ... and of the last one */
+};
+
+/* One tile of a row starting at column pos (a multiple of 8): lane L owns the
+ * CPL columns pos + CPL*L ..  (CPL = 8: 256 columns; 4 and 2: the narrower
+ * tiles that finish a row whose remaining range is at most 128 or 64
+ * columns, so a trimmed row does not run whole 256-column tiles).  The eh
+ * slots keep the 8-column layout of kslot(); with CPL = 4 / 2, two / four
+ * lanes share a bank, which costs no more shared-memory cycles than the
+ * 8-column tile's eight conflict-free accesses.  FULLT: every column lies
+ * before the row's end (no per-column checks; the row's last column, if in
+ * this tile, is lane 31's last). */
+template <bool FAST, bool BAND, bool FULLT, int CPL>
+__device__ __forceinline__ void ksw_tile(const TileConst &c, int pos, TileState &ts)
+{
+    static_assert(CPL == 8 || CPL == 4 || CPL == 2, "columns per lane");
+    const int lane = c.lane;
+    const int j0 = pos + lane * CPL;
+    const int nv = FULLT ? CPL : min(max(c.end - j0, 0), CPL);
+    /* lanes past the row (nv == 0) read slot group 0 and store nothing */
+    const int jr = (FULLT || j0 < c.slots) ? j0 : 0;
+    const int sub0 = jr & 7; /* first column of the lane within its 8-column word */
+    const int sb = (jr & ~255) | ((jr >> 3) & 31);
+    const uint4 sw = c.selw[jr >> 3];
+    uint32_t swk[CPL / 2];
+    if (CPL == 8) {
+        swk[0] = sw.x, swk[1] = sw.y, swk[2] = sw.z, swk[3] = sw.w;
+    } else if (CPL == 4) {
+        const bool hi = sub0 != 0;
+        swk[0] = hi ? sw.z : sw.x;
+        swk[1] = hi ? sw.w : sw.y;
+    } else {
+        const int q4 = sub0 >> 1;
+        swk[0] = q4 == 0 ? sw.x : q4 == 1 ? sw.y : q4 == 2 ? sw.z : sw.w;
+    }
+    int vh[CPL], ve[CPL];
+#pragma unroll
+    for (int k = 0; k < CPL; k++) {
+        const uint32_t pv = c.eh[sb + 32 * (sub0 + k)];
+        const uint32_t hi = high16(pv);
+        ve[k] = (int)hi;
+        vh[k] = (int)mad_lo_u32(hi, 0xFFFF0000u, pv); /* pv - (hi << 16) */
+    }
+    /* pass 1: M', t and the lane's F fold */
+    int Mp[CPL], tv[CPL];
+    int agg = 0;
+#pragma unroll
+    for (int k = 0; k < CPL; k++) {
+        int s;
+        if (FAST) {
+            s = (int)prmt(c.tab.x, c.tab.y, (k & 1) ? (swk[k >> 1] >> 16) : swk[k >> 1]);
+        } else {
+            const int cd = (int)((sw.x >> (28 - 4 * (sub0 + k))) & 15u);
+            s = cd == N_CODE4 ? 0 : (cd == c.g ? c.sm : c.sx);
+        }
+        Mp[k] = __viaddmin_s32(vh[k], s, vh[k] * c.Cmul);
+        tv[k] = __viaddmax_s32(Mp[k], -c.oe, 0);
+        agg = k == 0 ? tv[0] : __viaddmax_s32(agg, -c.e_del, tv[k]);
+    }
+    /* F entering each lane: max-plus scan over lanes, decay e per column */
+    const int eK = c.e_del * CPL;
+    int x = agg;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+        const int y = __shfl_up_sync(FULL, x, d);
+        if (lane >= d) x = max(x, y - eK * d);
+    }
+    const int ex = __shfl_up_sync(FULL, x, 1);
+    int f = lane == 0 ? ts.fcarry : max(ex, ts.fcarry - eK * lane);
+    ts.fcarry = __shfl_sync(FULL, max(x, ts.fcarry - eK * (lane + 1)), 31);
+    /* pass 2: H, E, F, row maximum key */
+    int H[CPL];
+    int lkey = -1; /* FULLT: this lane's best H * 8 + k (the last column on ties) */
+#pragma unroll
+    for (int k = 0; k < CPL; k++) {
+        H[k] = __vimax3_s32(Mp[k], ve[k], f);
+        ve[k] = __viaddmax_s32(ve[k], -c.e_del, tv[k]);
+        f = __viaddmax_s32(f, -c.e_del, tv[k]);
+        if (FULLT) {
+            if (k & 1) lkey = __vimax3_s32(lkey, (int)mad_lo_u32((uint32_t)H[k - 1], 8u, (uint32_t)(k - 1)),
+                                           (int)mad_lo_u32((uint32_t)H[k], 8u, (uint32_t)k));
+        } else if (k < nv) {
+            ts.kmax = max(ts.kmax, (int)mad_lo_u32((uint32_t)H[k], 1u << KEY_BITS, (uint32_t)(j0 + k)));
+            ts.hlast = H[k];
+            if (BAND) ts.flast = f;
+        }
+    }
+    if (FULLT) {
+        ts.kmax = max(ts.kmax, (int)mad_lo_u32((uint32_t)(lkey >> 3), 1u << KEY_BITS, (uint32_t)(j0 + (lkey & 7))));
+        ts.hlast = H[CPL - 1];
+        if (BAND) ts.flast = f;
+    }
+    int hp = __shfl_up_sync(FULL, H[CPL - 1], 1);
+    if (lane == 0) hp = ts.hcarry;
+    ts.hcarry = __shfl_sync(FULL, H[CPL - 1], 31);
+    uint32_t nz = 0;
+#pragma unroll
+    for (int k = 0; k < CPL; k++) {
+        const int hs = k == 0 ? hp : H[k - 1];
+        if (FULLT || k < nv) {
+            const uint32_t pv = mad_lo_u32((uint32_t)ve[k], 65536u, (uint32_t)hs);
+            c.eh[sb + 32 * (sub0 + k)] = pv;
+            nz |= pv;
+        }
+    }
+    const unsigned bm = __ballot_sync(FULL, nz != 0);
+    if (bm) {
+        if (ts.fcol < 0) ts.fcol = pos + (__ffs(bm) - 1) * CPL, ts.fcnt = CPL;
+        ts.lcol = pos + (31 - __clz(bm)) * CPL, ts.lcnt = CPL;
+    }
+}
+
 /* Band certificate state (BAND mode).  C bounds every value of the
  * unbanded computation that the banded one does not have: cells outside the
  * band and band cells whose unbanded value was raised from outside.  Paths
@@ -81,7 +214,6 @@ __device__ bool ksw_pair(const DpArgs &a, uint32_t pid, uint32_t *eh, const uint
                          unsigned long long &ncells)
 {
     const int e_del = a.sc.e, oe = a.sc.oe, o_del = a.sc.o;
-    const int eK = e_del * 8;
     const int mpos = max(a.sc.match, 0);
     /* C bounds every substitution score so that min(M + s, M*C) is M + s for
      * M >= 1 and <= 0 for M = 0 (0 and a negative value act alike below:
@@ -108,7 +240,7 @@ __device__ bool ksw_pair(const DpArgs &a, uint32_t pid, uint32_t *eh, const uint
     if (BAND) ct.C = (int)init_h(w + 1); /* the seed-derived entries right of the first row's band */
 
     const int L8 = (qlen >> 3) << 3;
-    int mx = h0, max_i = -1, max_j = -1, max_ie = -1, gscore = -1;
+    int mx = h0, max_i = -1, max_j = -1, max_ie = -1, gscore = -1, mo = 0;
     int beg = 0, end = qlen;
     ncells = 0;
     for (int i = 0; i < tlen;) {
@@ -129,8 +261,7 @@ __device__ bool ksw_pair(const DpArgs &a, uint32_t pid, uint32_t *eh, const uint
             if (h1 < 0) h1 = 0;
         }
         int m = 0, mj = -1, fout = 0;
-        int tf = -1, tl = -1;
-        unsigned mf = 0, ml = 0;
+        int fcol = -1, fcnt = 0, lcol = -1, lcnt = 0;
         if (beg < end) {
             ncells += (unsigned long long)(end - beg);
             uint2 tab = make_uint2(0, 0);
@@ -141,85 +272,39 @@ __device__ bool ksw_pair(const DpArgs &a, uint32_t pid, uint32_t *eh, const uint
                 sm = g == N_CODE4 ? 0 : a.sc.match;
                 sx = g == N_CODE4 ? 0 : -a.sc.mismatch;
             }
-            int fcarry = 0, hcarry = h1, kmax = -1, hlast = 0, flast = 0;
-            const int c0 = beg & ~7;
-            const int ntiles = (end - c0 + KT - 1) / KT;
-            for (int tt = 0; tt < ntiles; tt++) {
-                const int j0 = c0 + tt * KT + lane * 8;
-                const int nv = min(max(end - j0, 0), 8);
-                /* lanes past the row (nv == 0) read slot group 0 and store nothing */
-                const int jr = j0 < slots ? j0 : 0;
-                const int sb = (jr & ~255) | ((jr >> 3) & 31);
-                const uint4 sw = selw[jr >> 3];
-                const uint32_t swk[4] = {sw.x, sw.y, sw.z, sw.w};
-                int2 v[8];
-                int Mp[8], tv[8];
-#pragma unroll
-                for (int k = 0; k < 8; k++) {
-                    const uint32_t pv = eh[sb + 32 * k];
-                    v[k] = make_int2((int)(pv & 0xFFFFu), (int)(pv >> 16));
-                }
-                /* pass 1: M', t and the lane's F fold */
-                int agg = 0;
-#pragma unroll
-                for (int k = 0; k < 8; k++) {
-                    int s;
-                    if (FAST) {
-                        s = (int)prmt(tab.x, tab.y, (k & 1) ? (swk[k >> 1] >> 16) : swk[k >> 1]);
-                    } else {
-                        const int c = (int)((sw.x >> (28 - 4 * k)) & 15u);
-                        s = c == N_CODE4 ? 0 : (c == g ? sm : sx);
-                    }
-                    Mp[k] = __viaddmin_s32(v[k].x, s, v[k].x * Cmul);
-                    tv[k] = __viaddmax_s32(Mp[k], -oe, 0);
-                    agg = k == 0 ? tv[0] : __viaddmax_s32(agg, -e_del, tv[k]);
-                }
-                /* F entering each lane: max-plus scan over lanes, decay e per column */
-                int x = agg;
-#pragma unroll
-                for (int d = 1; d < 32; d <<= 1) {
-                    const int y = __shfl_up_sync(FULL, x, d);
-                    if (lane >= d) x = max(x, y - eK * d);
-                }
-                const int ex = __shfl_up_sync(FULL, x, 1);
-                int f = lane == 0 ? fcarry : max(ex, fcarry - eK * lane);
-                fcarry = __shfl_sync(FULL, max(x, fcarry - eK * (lane + 1)), 31);
-                /* pass 2: H, E, F, row maximum key */
-                int H[8];
-#pragma unroll
-                for (int k = 0; k < 8; k++) {
-                    H[k] = __vimax3_s32(Mp[k], v[k].y, f);
-                    v[k].y = __viaddmax_s32(v[k].y, -e_del, tv[k]);
-                    f = __viaddmax_s32(f, -e_del, tv[k]);
-                    if (k < nv) {
-                        kmax = max(kmax, H[k] * (1 << KEY_BITS) + (j0 + k));
-                        hlast = H[k];
-                        if (BAND) flast = f;
-                    }
-                }
-                int hp = __shfl_up_sync(FULL, H[7], 1);
-                if (lane == 0) hp = hcarry;
-                hcarry = __shfl_sync(FULL, H[7], 31);
-                uint32_t nz = 0;
-#pragma unroll
-                for (int k = 0; k < 8; k++) {
-                    const int hs = k == 0 ? hp : H[k - 1];
-                    if (k < nv) {
-                        const uint32_t pv = (uint32_t)hs | ((uint32_t)v[k].y << 16);
-                        eh[sb + 32 * k] = pv;
-                        nz |= pv;
-                    }
-                }
-                const unsigned bm = __ballot_sync(FULL, nz != 0);
-                if (bm) {
-                    if (tf < 0) tf = tt, mf = bm;
-                    tl = tt, ml = bm;
+            TileState ts{0, h1, -1, 0, 0, -1, 0, -1, 0};
+            const TileConst tc{eh, selw, slots, tab, sm, sx, g, lane, end, Cmul, oe, e_del};
+            /* 256-column tiles while more than 128 columns remain, then one
+             * 128- or 64-column tile for the rest; FULLT when the whole tile
+             * lies inside the row */
+            int pos = beg & ~7, lpos = pos, lcpl = 8;
+            while (pos < end) {
+                const int rem = end - pos;
+                lpos = pos;
+                if (rem > 128) {
+                    lcpl = 8;
+                    if (rem >= 256) ksw_tile<FAST, BAND, true, 8>(tc, pos, ts);
+                    else ksw_tile<FAST, BAND, false, 8>(tc, pos, ts);
+                    pos += 256;
+                } else if (rem > 64) {
+                    lcpl = 4;
+                    if (rem == 128) ksw_tile<FAST, BAND, true, 4>(tc, pos, ts);
+                    else ksw_tile<FAST, BAND, false, 4>(tc, pos, ts);
+                    pos += 128;
+                } else {
+                    lcpl = 2;
+                    if (rem == 64) ksw_tile<FAST, BAND, true, 2>(tc, pos, ts);
+                    else ksw_tile<FAST, BAND, false, 2>(tc, pos, ts);
+                    pos += 64;
                 }
             }
+            int kmax = ts.kmax;
+            const int hlast = ts.hlast, flast = ts.flast;
+            fcol = ts.fcol, fcnt = ts.fcnt, lcol = ts.lcol, lcnt = ts.lcnt;
             kmax = __reduce_max_sync(FULL, kmax);
             m = kmax >> KEY_BITS;
             mj = kmax & ((1 << KEY_BITS) - 1);
-            const int owner = ((end - 1 - c0) >> 3) & 31;
+            const int owner = (end - 1 - lpos) / lcpl;
             h1 = __shfl_sync(FULL, hlast, owner);
             if (BAND) fout = __shfl_sync(FULL, flast, owner);
         }
@@ -269,6 +354,7 @@ __device__ bool ksw_pair(const DpArgs &a, uint32_t pid, uint32_t *eh, const uint
             leave = true;
         } else if (m > mx) {
             mx = m, max_i = i, max_j = mj;
+            mo = max(mo, abs(mj - i));
         } else if (a.zdrop > 0) {
             if (i - max_i > mj - max_j) {
                 if (mx - m - ((i - max_i) - (mj - max_j)) * e_del > a.zdrop) leave = true;
@@ -281,29 +367,23 @@ __device__ bool ksw_pair(const DpArgs &a, uint32_t pid, uint32_t *eh, const uint
             i = ((i >> 3) + 1) << 3;
             continue;
         }
-        /* trimming (ksw_kernel_template.h:188-196) */
-        int nbeg = end;
-        if (tf >= 0) {
-            const int base = (beg & ~7) + tf * KT + (__ffs(mf) - 1) * 8;
-            for (int k = 7; k >= 0; k--) {
-                const int j = base + k;
-                if (j < end) {
-                    if (eh[kslot(j)]) nbeg = j;
-                }
-            }
+        /* trimming (ksw_kernel_template.h:188-196): the first non-zero entry
+         * lies among the columns of the first lane (over the row's tiles)
+         * whose stores were non-zero, the last one (unless eh[end] = h1 is
+         * non-zero) among those of the last such lane; lanes 0-7 read the
+         * first group, lanes 8-15 the second, and one ballot gives both */
+        int jj = -1;
+        if (lane < 8) {
+            if (fcol >= 0 && lane < fcnt) jj = fcol + lane;
+        } else if (lane < 16) {
+            if (h1 == 0 && lcol >= 0 && lane - 8 < lcnt) jj = lcol + (lane - 8);
         }
+        const bool nzj = jj >= 0 && jj < end && eh[kslot(jj)] != 0u;
+        const unsigned bal = __ballot_sync(FULL, nzj);
+        const int nbeg = (bal & 0xFFu) ? fcol + __ffs(bal & 0xFFu) - 1 : end;
         int lastnz = nbeg - 1;
-        if (h1 != 0) {
-            lastnz = end;
-        } else if (tl >= 0) {
-            const int base = (beg & ~7) + tl * KT + (31 - __clz(ml)) * 8;
-            for (int k = 0; k < 8; k++) {
-                const int j = base + k;
-                if (j < end) {
-                    if (eh[kslot(j)]) lastnz = j;
-                }
-            }
-        }
+        if (h1 != 0) lastnz = end;
+        else if (bal & 0xFF00u) lastnz = lcol + (31 - __clz(bal & 0xFF00u)) - 8;
         beg = nbeg;
         end = lastnz + 2 < qlen ? lastnz + 2 : qlen;
         __syncwarp(); /* the scans above read slots their owners rewrite next row */
@@ -329,6 +409,7 @@ __device__ bool ksw_pair(const DpArgs &a, uint32_t pid, uint32_t *eh, const uint
         if (a.score) a.score[pid] = sc;
         if (a.q_end) a.q_end[pid] = qe;
         if (a.t_end) a.t_end[pid] = te;
+        if (!BAND && a.max_off) a.max_off[pid] = mo;
     }
     __syncwarp();
     return true;

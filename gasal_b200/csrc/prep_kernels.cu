@@ -146,13 +146,17 @@ __device__ __forceinline__ uint32_t complement_flat(uint32_t x)
 /* Reference-identical reversal, flat over the batch.  A warp takes 32
  * sequences (queries, then targets, in groups of 32), prefix-sums their word
  * tasks across lanes -- ceil(regs/2) word pairs when reversing, regs words when
- * only complementing, none otherwise -- and sweeps the concatenated task list
- * 32 tasks at a time: consecutive lanes take consecutive words of a sequence,
- * so loads and stores stream through the batch instead of one short sequence
- * per 32-thread row.  Task i of a reversed sequence reads word i, writes its
- * nibble-reversed (and, for op 3, complemented) value to word regs-1-i and
- * zeroes word i (the sm_100a build's result); no other task touches those
- * words, so the update in place is race-free. */
+ * only complementing, none otherwise -- cut into chunks of RC_CHUNK
+ * consecutive tasks of one sequence, and sweeps the concatenated chunk list 32
+ * chunks at a time: a lane finds its chunk's sequence with one 5-step search
+ * over the lanes' inclusive counts, then issues the chunk's loads together
+ * (RC_CHUNK independent loads in flight per lane) before its stores.  Task i
+ * of a reversed sequence reads word i, writes its nibble-reversed (and, for
+ * op 3, complemented) value to word regs-1-i and zeroes word i (the sm_100a
+ * build's result); no other task touches those words, so the update in place
+ * is race-free. */
+constexpr uint32_t RC_CHUNK = 4;
+
 __global__ void __launch_bounds__(256) revcomp_flat_kernel(uint32_t *pq, uint32_t *pt, const uint32_t *q_off,
                                                            const uint32_t *t_off, const uint32_t *q_len,
                                                            const uint32_t *t_len, const uint8_t *q_op,
@@ -175,7 +179,8 @@ __global__ void __launch_bounds__(256) revcomp_flat_kernel(uint32_t *pq, uint32_
             regs = ((tside ? t_len[p] : q_len[p]) + 7) >> 3;
         }
         const uint32_t tasks = (op & 1) ? (regs + 1) >> 1 : (op == 2 ? regs : 0u);
-        uint32_t incl = tasks;
+        const uint32_t chunks = (tasks + RC_CHUNK - 1) / RC_CHUNK;
+        uint32_t incl = chunks;
 #pragma unroll
         for (int d = 1; d < 32; d <<= 1) {
             const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, incl, d);
@@ -192,22 +197,33 @@ __global__ void __launch_bounds__(256) revcomp_flat_kernel(uint32_t *pq, uint32_
                 if (c <= k) owner += step;
             }
             const uint32_t o_incl = __shfl_sync(0xFFFFFFFFu, incl, owner & 31);
+            const uint32_t o_chunks = __shfl_sync(0xFFFFFFFFu, chunks, owner & 31);
             const uint32_t o_tasks = __shfl_sync(0xFFFFFFFFu, tasks, owner & 31);
             const uint32_t o_base = __shfl_sync(0xFFFFFFFFu, base, owner & 31);
             const uint32_t o_regs = __shfl_sync(0xFFFFFFFFu, regs, owner & 31);
             const int o_op = __shfl_sync(0xFFFFFFFFu, op, owner & 31);
             if (k >= total) continue;
-            const uint32_t i = k - (o_incl - o_tasks);
+            const uint32_t i0 = (k - (o_incl - o_chunks)) * RC_CHUNK;
+            const uint32_t nt = min(RC_CHUNK, o_tasks - i0);
             uint32_t *w = words + o_base;
+            uint32_t v[RC_CHUNK];
+#pragma unroll
+            for (uint32_t u = 0; u < RC_CHUNK; u++) v[u] = u < nt ? w[i0 + u] : 0u;
             if (o_op & 1) {
-                const uint32_t head = w[i];
-                uint32_t rev = nib_reverse(head);
-                if (o_op & 2) rev = complement_flat(rev);
-                const uint32_t mirror = o_regs - 1 - i;
-                if (i != mirror) w[i] = 0u;
-                w[mirror] = rev;
+#pragma unroll
+                for (uint32_t u = 0; u < RC_CHUNK; u++) {
+                    if (u < nt) {
+                        const uint32_t i = i0 + u, mirror = o_regs - 1 - i;
+                        uint32_t rev = nib_reverse(v[u]);
+                        if (o_op & 2) rev = complement_flat(rev);
+                        if (i != mirror) w[i] = 0u;
+                        w[mirror] = rev;
+                    }
+                }
             } else {
-                w[i] = complement_flat(w[i]);
+#pragma unroll
+                for (uint32_t u = 0; u < RC_CHUNK; u++)
+                    if (u < nt) w[i0 + u] = complement_flat(v[u]);
             }
         }
     }

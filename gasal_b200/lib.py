@@ -81,6 +81,7 @@ SIGNATURES = {
     "gasal_c_storage_view": (C.c_int, [C.c_void_p, C.POINTER(GbStorageView)]),
     "gasal_c_host_batch_fill": (C.c_uint32, [C.c_void_p, C.c_uint32, C.c_char_p, C.c_uint32, C.c_int]),
     "gasal_c_host_batch_add": (C.c_uint32, [C.c_void_p, C.c_uint32, C.c_void_p, C.c_uint32, C.c_int]),
+    "gasal_c_host_batch_fill_mt": (C.c_uint32, [C.c_void_p, C.c_uint32, C.c_void_p, C.c_uint32, C.c_int, C.c_int]),
     "gasal_c_host_batch_reset": (C.c_int, [C.c_void_p]),
     "gasal_c_op_fill": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_int]),
     "gasal_c_host_alns_resize": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p]),
@@ -113,6 +114,8 @@ SIGNATURES = {
     "gb_band_train_step": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_float, C.c_float, C.c_void_p,
                                      C.POINTER(C.c_float)]),
     "gb_set_band_model": (C.c_int, [C.c_void_p, C.c_int, C.c_int]),
+    "gb_ksw_align_max_off": (C.c_int, [C.POINTER(GbParams), C.POINTER(GbDevBatch), C.POINTER(GbDevOut), C.c_void_p,
+                                       C.c_void_p]),
     "gb_ksw_band_align": (C.c_int, [C.POINTER(GbParams), C.POINTER(GbDevBatch), C.POINTER(GbDevOut), C.c_void_p,
                                     C.c_void_p, C.c_void_p, C.POINTER(GbBandStats)]),
     "gb_last_error": (C.c_char_p, []),
@@ -368,6 +371,16 @@ def ksw_band_align(p: Params, dev: dict, h_q_len: np.ndarray, h_t_len: np.ndarra
     return {k: getattr(st, k) for k, _ in GbBandStats._fields_}
 
 
+def ksw_align_max_off(p: Params, dev: dict, h_q_len: np.ndarray, h_t_len: np.ndarray, max_off_ptr: int,
+                      stream: int = 0):
+    """gb_ksw_align_max_off: the unbanded ksw with each pair's max_off (the
+    largest |column - row| where the running maximum rose) in max_off_ptr."""
+    b, o = _dev_structs(dev, h_q_len, h_t_len)
+    cp = p.to_c()
+    _check(lib().gb_ksw_align_max_off(C.byref(cp), C.byref(b), C.byref(o), max_off_ptr, stream),
+           "gb_ksw_align_max_off")
+
+
 def cigar_text_dev(cigar_ptr: int, q_off_ptr: int, n_cigar_ptr: int, n: int, text_ptr: int, stride: int,
                    text_len_ptr: int, stream_handle: int = 0):
     """gb_cigar_text on device buffers: forward CIGAR strings in stride-byte
@@ -481,6 +494,32 @@ class Streams:
             raise GasalError("fill_fast needs 8-byte padded buffers")
         qi = L.gasal_c_host_batch_fill(s, 0, C.c_char_p(b.q.ctypes.data), nq, QUERY)
         ti = L.gasal_c_host_batch_fill(s, 0, C.c_char_p(b.t.ctypes.data), nt, TARGET)
+        if qi != nq or ti != nt:
+            raise GasalError("host page smaller than the batch; create the storage with larger maxima or use fill()")
+        self._arr(v.host_query_batch_offsets, C.c_uint32, n)[:] = b.q_off
+        self._arr(v.host_target_batch_offsets, C.c_uint32, n)[:] = b.t_off
+        self._arr(v.host_query_batch_lens, C.c_uint32, n)[:] = b.q_len
+        self._arr(v.host_target_batch_lens, C.c_uint32, n)[:] = b.t_len
+        zeros = np.zeros(n, dtype=np.uint8)
+        _check(L.gasal_c_op_fill(s, _ptr(b.q_op if b.q_op is not None else zeros), n, QUERY), "gasal_op_fill")
+        _check(L.gasal_c_op_fill(s, _ptr(b.t_op if b.t_op is not None else zeros), n, TARGET), "gasal_op_fill")
+        if self.params.algo == KSW:
+            self._arr(v.host_seed_scores, C.c_uint32, n)[:] = b.seed if b.seed is not None else 0
+        return qi, ti
+
+    def fill_bulk(self, i: int, b: Batch, threads: int = 0):
+        """fill_fast with the sequence copies split over host threads
+        (gasal_c_host_batch_fill_mt; 0 = every hardware thread)."""
+        L = lib()
+        s = self.storage(i)
+        v = self.view(i)
+        n = b.n
+        nq, nt = int(b.q.shape[0]), int(b.t.shape[0])
+        if nq % 8 or nt % 8:
+            raise GasalError("fill_bulk needs 8-byte padded buffers")
+        _check(L.gasal_c_host_batch_reset(s), "gasal_host_batch_reset")
+        qi = L.gasal_c_host_batch_fill_mt(s, 0, b.q.ctypes.data, nq, QUERY, threads)
+        ti = L.gasal_c_host_batch_fill_mt(s, 0, b.t.ctypes.data, nt, TARGET, threads)
         if qi != nq or ti != nt:
             raise GasalError("host page smaller than the batch; create the storage with larger maxima or use fill()")
         self._arr(v.host_query_batch_offsets, C.c_uint32, n)[:] = b.q_off

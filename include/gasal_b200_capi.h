@@ -150,6 +150,10 @@ int gasal_c_storage_view(void *storage, gb_storage_view_t *view);
 uint32_t gasal_c_host_batch_fill(void *storage, uint32_t idx, const char *data, uint32_t size, int src);
 uint32_t gasal_c_host_batch_add(void *storage, uint32_t idx, const char *data, uint32_t size, int src);
 int gasal_c_host_batch_reset(void *storage);
+/* Extension: gasal_host_batch_fill with the copy split over `threads` host
+ * threads (0 = every hardware thread); same page, padding and return value. */
+uint32_t gasal_c_host_batch_fill_mt(void *storage, uint32_t idx, const char *data, uint32_t size, int src,
+                                    int threads);
 
 /* gasal_op_fill / gasal_host_alns_resize / gasal_set_device, reference
  * src/interfaces.h:9-14. */
@@ -323,6 +327,12 @@ int gb_band_train_step(gb_band_model_t *m, const float *feat, const float *label
 /* install (or with NULL remove) the model for every ksw call; predicted
  * widths are clamped to [band_min, band_max] */
 int gb_set_band_model(gb_band_model_t *m, int band_min, int band_max);
+/* Unbanded ksw with max_off (device int32 per pair): the largest
+ * |column - row| over the cells where the running maximum rose, as
+ * ksw_extend2 tracks it -- the diagonal reach the alignment needed, from
+ * which band labels are made. */
+int gb_ksw_align_max_off(const gb_params_t *p, const gb_dev_batch_t *b, const gb_dev_out_t *o, int32_t *max_off,
+                         void *stream);
 /* ksw with a band: band_w (device int32 per pair, negative = none) or, when
  * NULL, the installed model's prediction.  band_ok (device, optional): 1 where
  * the banded result was kept.  stats (optional) syncs the stream. */

@@ -23,6 +23,11 @@ uint32_t gasal_host_batch_add(gasal_gpu_storage_t *gpu_storage, uint32_t idx, co
                               data_source SRC);
 uint32_t gasal_host_batch_addbase(gasal_gpu_storage_t *gpu_storage, uint32_t idx, const char base,
                                   data_source SRC);
+/* Extension (no reference counterpart): gasal_host_batch_fill with the copy
+ * split over `threads` host threads (0 = all), for a whole padded batch staged
+ * as one block. */
+uint32_t gasal_host_batch_fill_mt(gasal_gpu_storage_t *gpu_storage, uint32_t idx, const char *data, uint32_t size,
+                                  data_source SRC, int threads);
 void gasal_host_batch_print(host_batch_t *res);
 void gasal_host_batch_printall(host_batch_t *res);
 

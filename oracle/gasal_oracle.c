@@ -540,7 +540,7 @@ static void ksw(const uint8_t *qc, int qlen, const uint8_t *tc, int tlen, uint32
         end = j + 2 < qlen ? j + 2 : qlen;
         i++;
     }
-    (void)max_off;
+    r->score2 = max_off; /* ksw has no second best: the slot carries max_off (checker of the band labels) */
     if (gscore <= 0 || gscore <= max - 5) { /* PEN_CLIP5, :20,188-197 */
         r->score = max, r->q_end = max_j + 1, r->t_end = max_i + 1;
     } else {
@@ -709,6 +709,7 @@ int oracle_align_ex(const gb_params_t *p, const gb_batch_t *b, gb_out_t *o, int 
                         if (o->q_start) o->q_start[i] = r.q_start;
                         if (o->t_start) o->t_start[i] = r.t_start;
                     }
+                    if (algo == A_KSW && o->score2) o->score2[i] = r.score2; /* max_off */
                     if (p->second_best && (algo == A_LOCAL || algo == A_SEMI_GLOBAL)) {
                         if (o->score2) o->score2[i] = r.score2;
                         if (o->q_end2) o->q_end2[i] = r.q_end2;

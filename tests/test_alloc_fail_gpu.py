@@ -3,9 +3,11 @@
 GASAL_B200_FAIL_ALLOC_AFTER=k makes the engine's (k+1)-th device allocation
 fail once, as an out-of-memory would, on the host side -- no GPU fault is
 involved.  Each case runs in a child process (the variable is read once):
-the first gb_align_dev call must return GB_ERR_ALLOC (or succeed when the
-batch needs fewer than k+1 allocations), and a second call on the same batch
-must succeed with results equal to the oracle's.
+the first gb_align_dev call must return GB_ERR_ALLOC, or succeed when the
+batch needs fewer than k+1 allocations or the failed one was a workspace
+buffer that the engine retries at its exact size, and a second call on the same batch
+must succeed with results equal to the oracle's (CIGAR bytes compared over
+each pair's n_cigar operations).
 """
 import json
 import os
@@ -61,6 +63,13 @@ for name, p, b in [("global_tb", Params(algo=GLOBAL, start_pos=WITH_TB), W.workl
     got = {k: v.cpu().numpy() for k, v in outs.items()}
     got["n_cigar"] = ncig.cpu().numpy().astype(np.uint32)
     got["cigar"] = cig.cpu().numpy()
+    if "cigar" in exp:
+        # only each pair's n_cigar bytes at its query offset are results; past them
+        # the oracle's buffer holds leftovers, as the reference's does
+        keep = np.zeros(len(exp["cigar"]), dtype=bool)
+        for o, k in zip(b.q_off.astype(np.int64), exp["n_cigar"].astype(np.int64)):
+            keep[o:o + k] = True
+        got["cigar"], exp["cigar"] = got["cigar"][keep], exp["cigar"][keep]
     bad = [k for k in exp if not np.array_equal(got[k].astype(np.int64), exp[k].astype(np.int64))]
     out[name] = {"first": first, "mismatched": bad}
 print(json.dumps(out))
@@ -78,7 +87,8 @@ def test_injected_allocation_failure_is_reported_and_recovered(k):
     assert sum(f != "ok" for f in firsts) <= 1, res
     for f in firsts:
         assert f == "ok" or "allocation failed" in f, res
-    if k <= 2:
-        assert firsts[0] != "ok", f"the first launch allocates more than {k} buffers: {res}"
+    if k == 0:
+        # the first allocation of the first launch (its work-queue word) has no smaller retry
+        assert firsts[0] != "ok", f"the first launch's first allocation failure went unreported: {res}"
     for name, v in res.items():
         assert not v["mismatched"], f"{name} after the injected failure: {v}"

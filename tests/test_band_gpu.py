@@ -119,6 +119,30 @@ def test_band_certificate_never_changes_a_result(zdrop):
     assert kept[0] < kept[512]        # and narrow bands are refused more often
 
 
+@pytest.mark.parametrize("zdrop", [0, 100])
+def test_max_off_matches_oracle(zdrop):
+    """gb_ksw_align_max_off: the unbanded results and each pair's max_off
+    (largest |column - row| where the running maximum rose) equal the
+    oracle's, on the warp kernel and on pairs it hands to the one-thread
+    kernel (seed scores of 2^15 and more)."""
+    b = W.workload3(1200, seed=125 + zdrop)
+    b.seed = b.seed.copy()
+    b.seed[::97] = 40000  # seed + match*qlen >= 2^15: the one-thread kernel's pairs
+    p = Params(algo=KSW, zdrop=zdrop)
+    r = oracle_align(p, b)
+    exp = r.as_dict(p)
+    m, keep = _dev(b)
+    mo = torch.full((b.n,), -7, dtype=torch.int32, device=DEV)
+    gl.ksw_align_max_off(p, m, b.q_len, b.t_len, mo.data_ptr(), _stream())
+    torch.cuda.synchronize()
+    for k in OUTS:
+        assert np.array_equal(keep[k].cpu().numpy(), exp[k]), k
+    got = mo.cpu().numpy()
+    bad = np.nonzero(got != r.score2)[0]
+    assert len(bad) == 0, f"{len(bad)} max_off differ, first {bad[:5]}: {got[bad[:5]]} vs {r.score2[bad[:5]]}"
+    assert got.max() > 0
+
+
 def test_installed_model_path_matches_oracle():
     b = W.workload3(800, seed=124)
     p = Params(algo=KSW, zdrop=100)

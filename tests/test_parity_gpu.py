@@ -157,6 +157,25 @@ def test_streams_api_per_sequence_fill():
             assert st.is_done(i) == -2  # nothing in flight after completion
 
 
+def test_streams_api_bulk_fill_repeated():
+    """gasal_host_batch_fill_mt (the batch's padded blocks copied over host
+    threads, after gasal_host_batch_reset) staged twice into one storage:
+    both runs equal the oracle, the second after the first batch's pages
+    were reused."""
+    p = Params(algo=GLOBAL, start_pos=WITH_TB)
+    batches = [W.workload2(3000, seed=15), W.workload2(2500, seed=16)]
+    nq = max(int(b.q.shape[0]) for b in batches)
+    nt = max(int(b.t.shape[0]) for b in batches)
+    with gl.Streams(1, nq // 2500 + 8, nt // 2500 + 8, 3000, p) as st:
+        for k, b in enumerate(batches):
+            qi, ti = st.fill_bulk(0, b, threads=4)
+            assert (qi, ti) == (int(b.q.shape[0]), int(b.t.shape[0]))
+            st.aln_async(0, qi, ti, b.n)
+            st.wait(0)
+            got = st.results(0, b.n, b)
+            assert_same(got, oracle_align(p, b).as_dict(p), f"bulk fill {k}")
+
+
 def test_streams_api_grows_buffers():
     """A batch larger than the storage was created for is accepted after the
     host pages chain and device buffers regrow (reference behaviour)."""
