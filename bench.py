@@ -383,7 +383,8 @@ def train_band(torch, gl, args, rank, dev):
     trace = BT.train(torch, model, feat, lab, steps=600, batch=8192, tau=0.8, lr=3e-3)
     model.install(16, 1024)
     info = {"train_pairs": tb.n, "train_s": round(time.time() - t0, 1), "labels": args.band_labels,
-            "label_hist_log2": {str(k): int(v) for k, v in zip(*np.unique(lab, return_counts=True))},
+            "label_hist_log2": {f"{k:.2f}": int(v) for k, v in zip(*np.unique(np.round(lab * 4) / 4,
+                                                                                 return_counts=True))},
             "loss_first": trace[0], "loss_last": trace[-1]}
     log(f"band model trained in {info['train_s']} s; loss {trace[0]:.3f} -> {trace[-1]:.3f}")
     return model, info

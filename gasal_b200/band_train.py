@@ -18,8 +18,19 @@ import numpy as np
 from . import lib as gl
 from .capi import Batch, Params
 
-LADDER = (16, 32, 64, 128, 256, 512, 1024)
+# the widest band of each warp-kernel tile cost (a banded row spans at most
+# 2w + 8 columns: one 64- or 128-column tile, then whole 256-column tiles)
+LADDER = (28, 60, 124, 252, 380, 508, 636, 764, 892, 1020)
 NO_BAND = 11.0  # log2(2048): no ladder band was kept
+
+
+def ladder_label(k: int) -> float:
+    """Label of ladder rung k: the middle of the log2 interval of predictions
+    that widths_from_pred maps to that rung (from 16, the narrowest band, for
+    the first), so a prediction off by less than half an interval still
+    lands on the rung."""
+    lo = np.log2(16.0) if k == 0 else np.log2(LADDER[k - 1])
+    return float(0.5 * (lo + np.log2(LADDER[k])))
 
 
 class DeviceBatch:
@@ -59,18 +70,19 @@ def features(torch, db: DeviceBatch, stream: int = 0):
 
 
 def labels(torch, p: Params, db: DeviceBatch, ladder=LADDER, stream: int = 0) -> np.ndarray:
-    """log2 of the narrowest ladder band the certificate keeps, per pair."""
+    """The label (ladder_label) of the narrowest ladder band the certificate
+    keeps, per pair; NO_BAND when none does."""
     n = db.b.n
     dev = db.keep["q"].device
     lab = np.full(n, NO_BAND, dtype=np.float32)
     done = np.zeros(n, dtype=bool)
     ok = torch.zeros(n, dtype=torch.uint8, device=dev)
-    for w in ladder:
+    for k, w in enumerate(ladder):
         band = torch.full((n,), int(w), dtype=torch.int32, device=dev)
         gl.ksw_band_align(p, db.map, db.b.q_len, db.b.t_len, band.data_ptr(), ok.data_ptr(), stream)
         kept = ok.cpu().numpy().astype(bool)
         new = kept & ~done
-        lab[new] = np.log2(w)
+        lab[new] = ladder_label(k) if tuple(ladder) == LADDER else np.log2(w)
         done |= kept
     return lab
 
@@ -89,6 +101,23 @@ def labels_max_off(torch, p: Params, db: DeviceBatch, margin: int = MAX_OFF_MARG
     torch.cuda.synchronize()
     m = mo.cpu().numpy()
     return np.log2(m.astype(np.float64) + margin).astype(np.float32), m
+
+
+def widths_from_pred(pred: np.ndarray, q_len: np.ndarray, t_len: np.ndarray, bmin: int = 16,
+                     bmax: int = 1024) -> np.ndarray:
+    """The per-pair half-widths the library derives from predictions
+    (band_from_pred_kernel): ceil(2^y) clamped to [bmin, bmax], widened to
+    the widest band of the same warp-kernel tile cost (2w + 8 columns in one
+    64- or 128-column tile, or whole 256-column tiles), -1 (unbanded) where
+    the band covers the matrix."""
+    y = np.clip(np.asarray(pred, dtype=np.float32), 0, 20)
+    w = np.ceil(np.exp2(y)).astype(np.int64)
+    w = np.clip(w, bmin, bmax)
+    span = 2 * w + 8
+    w = np.where(span <= 64, 28, np.where(span <= 128, 60, 128 * ((span + 255) // 256) - 4))
+    w = np.minimum(w, bmax)
+    cover = np.maximum(q_len, t_len).astype(np.int64)
+    return np.where(w >= cover, -1, w).astype(np.int32)
 
 
 def train(torch, model: "gl.BandModel", feat, lab: np.ndarray, steps: int = 400, batch: int = 8192,

@@ -51,6 +51,7 @@ Settings &settings()
         if (const char *e = getenv("GASAL_B200_BLOCK")) v.block = atoi(e);
         if (const char *e = getenv("GASAL_B200_MIN_ORDER_PAIRS")) v.min_order_pairs = atoi(e);
         if (const char *e = getenv("GASAL_B200_WC_MIN_QREGS")) v.wc_min_qregs = atoi(e);
+        if (const char *e = getenv("GASAL_B200_WC_BIG_GROUP")) v.wc_big_group = atoi(e);
         return v;
     }();
     return s;
@@ -253,7 +254,13 @@ int plan_batch(const RunCfg &cfg, const DevBatch &b, const DevOut &o, Workspace 
         if (nlong > 0 && b.n >= st.min_order_pairs) {
             p.wc = shape_for(nsmall, max_q_long, max_t_long, max_group);
             /* the long launch's pairs all have 127+ query words: two-warp groups fit */
-            p.wc_big = shape_for(nbig, max_q_big, max_t_big, 64);
+            p.wc_big = st.wc_big_group > 0 && st.wc_group == 0
+                           ? [&] {
+                                 const int mq8 = (int)((max_q_big + 7) & ~7u), mt8 = (int)((max_t_big + 7) & ~7u);
+                                 if (nbig <= 0 || mq8 > st.wc_max_q8) return WcLaunch{};
+                                 return wc_plan(cfg.algo, wstart, wsecond, nbig, mq8, mt8, st.wc_big_group, 64);
+                             }()
+                           : shape_for(nbig, max_q_big, max_t_big, 64);
         }
         p.use_wc = nlong > 0 && b.n >= st.min_order_pairs && (nsmall == 0 || p.wc.group > 0) &&
                    (nbig == 0 || p.wc_big.group > 0);

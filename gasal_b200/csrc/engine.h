@@ -144,6 +144,7 @@ struct Settings {
                                    pair on a grid over the batch */
     const void *band_model = nullptr; /* installed band MLP (BF16 parameters on the device) */
     int band_min = 16, band_max = 1024;
+    int wc_big_group = 0;       /* lane group of the 127+ word launch: 0 = automatic (64 when it fits), 32 or 64 */
 };
 Settings &settings();
 

@@ -300,8 +300,14 @@ __global__ void band_from_pred_kernel(const float *pred, const uint32_t *q_len, 
     if (i >= n) return;
     const float y = fminf(fmaxf(pred[i], 0.f), 20.f);
     int w = (int)ceilf(exp2f(y));
-    w = (w + 7) & ~7;
     w = max(bmin, min(bmax, w));
+    /* a banded row spans at most 2w + 1 columns from a tile start up to 7
+     * columns left of it; the warp kernel runs it as one 64- or 128-column
+     * tile, or 256-column tiles: widen w to the widest band of the same tile
+     * cost (more results kept, no more work) */
+    const int span = 2 * w + 8;
+    w = span <= 64 ? 28 : span <= 128 ? 60 : 128 * ((span + 255) / 256) - 4;
+    w = min(bmax, w);
     const int cover = (int)max(q_len[i], t_len[i]);
     band[i] = w >= cover ? -1 : w;
 }

@@ -178,11 +178,9 @@ def test_trained_band_beats_a_fixed_band_of_the_same_width():
     model.predict(ef.data_ptr(), eb.n, pred.data_ptr(), _stream())
     torch.cuda.synchronize()
     model.close()
-    # the same transform as band_from_pred_kernel: ceil(2^y), multiple of 8, [16, 1024]
-    w = np.ceil(np.exp2(np.clip(pred.cpu().numpy(), 0, 20))).astype(np.int64)
-    w = np.clip((w + 7) & ~7, 16, 1024)
+    # the same transform as band_from_pred_kernel
+    learned = BT.widths_from_pred(pred.cpu().numpy(), eb.q_len, eb.t_len)
     cover = np.maximum(eb.q_len, eb.t_len).astype(np.int64)
-    learned = np.where(w >= cover, -1, w).astype(np.int32)
     mean_w = int(np.mean(np.where(learned < 0, cover, learned)))
     fixed = np.full(eb.n, (mean_w + 7) & ~7, np.int32)
     exp = oracle_align(p, eb).as_dict(p)
