@@ -407,7 +407,20 @@ int plan_batch(const RunCfg &cfg, const DevBatch &b, const DevOut &o, Workspace 
     }
     if (!ws.tb_off_free && cudaEventCreateWithFlags(&ws.tb_off_free, cudaEventDisableTiming) != cudaSuccess)
         return GB_ERR_CUDA;
-    const uint64_t budget = std::max<uint64_t>(st.tb_budget_bytes / 16, 1);
+    /* tile budget: the setting, but at most half of the device memory that is
+     * free or already held as this stream's tiles (fewer, longer chunks on a
+     * large device; room left for other streams) */
+    uint64_t budget_bytes = st.tb_budget_bytes;
+    {
+        size_t free_b = 0, total_b = 0;
+        if (cudaMemGetInfo(&free_b, &total_b) == cudaSuccess) {
+            const uint64_t avail = ((uint64_t)free_b + (uint64_t)ws.tb_cap * 16) / 2;
+            budget_bytes = std::min<uint64_t>(budget_bytes, std::max<uint64_t>(avail, (uint64_t)1 << 30));
+        } else {
+            cudaGetLastError();
+        }
+    }
+    const uint64_t budget = std::max<uint64_t>(budget_bytes / 16, 1);
     p.cut = {0};
     uint64_t run = 0, chunk_max = 0;
     for (int i = 0; i < b.n; i++) {

@@ -71,7 +71,7 @@ def test_workload2_traceback_chunked():
     try:
         _vs_oracle(Params(algo=GLOBAL, start_pos=WITH_TB), b)
     finally:
-        gl.set_tb_budget_mb(16384)
+        gl.set_tb_budget_mb(65536)
 
 
 def test_local_traceback_and_second_best():
