@@ -289,10 +289,14 @@ class DevPart:
 class Runner:
     """Launches every part on its own stream, joined into one timing stream."""
 
-    def __init__(self, torch, gl, parts, dev):
+    def __init__(self, torch, gl, parts, dev, tb_priority=True):
         self.torch, self.gl, self.parts, self.dev = torch, gl, parts, dev
         self.main = torch.cuda.Stream(device=dev)
-        self.streams = [torch.cuda.Stream(device=dev) for _ in parts]
+        # a WITH_TB launch runs its traceback chunks one after another and would finish last; its stream
+        # (and, through the library, its auxiliary stream) gets the highest priority so its blocks are
+        # scheduled first and the other launches fill the GPU around it
+        self.streams = [torch.cuda.Stream(device=dev, priority=-5 if tb_priority and d.p.start_pos == WITH_TB else 0)
+                        for d in parts]
 
     def step(self, finish_times=False):
         torch = self.torch
@@ -563,6 +567,8 @@ def main():
     ap.add_argument("--plain-budget-s", type=float, default=20.0,
                     help="device time the plain form's timed step may take; beyond it a stratified sample is used")
     ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--tb-priority", default="on", choices=["on", "off"],
+                    help="kernel-level step: run WITH_TB launches on the highest-priority stream")
     ap.add_argument("--split", default="weak", choices=["weak", "cells"],
                     help="N>1: weak = every rank aligns its own full-size seeded shard; cells = the ranks split one "
                          "workload into contiguous slices of equal DP cells (strong scaling)")
@@ -621,7 +627,7 @@ def main():
         model, band_info = train_band(torch, gl, args, rank, dev)
 
     # ---------------- kernel level: inputs resident in HBM -----------------
-    runner = Runner(torch, gl, dparts, dev)
+    runner = Runner(torch, gl, dparts, dev, tb_priority=args.tb_priority == "on")
     clk = ClockSampler(local_rank).__enter__()
 
     def arm():
@@ -695,7 +701,9 @@ def main():
                                        f"collective in the data path" if strong else
                                        f"pair shards x{world} (a full-size seeded shard per rank), no collective "
                                        f"in the data path"),
-                       "l2": l2_note},
+                       "l2": l2_note,
+                       "stream_priority": "WITH_TB launches on the highest-priority stream" if args.tb_priority == "on"
+                                          else "all launches on default-priority streams"},
             "gcups": job_cells / (ms_step * 1e-3) / 1e9,
             "gcups_computed": None if computed is None else computed * (job_cells / cells) / (ms_step * 1e-3) / 1e9,
             "roofline": {"bound": "int32", "achieved": achieved, "peak": peak["iadd_tops"], "unit": "Tops/s",

@@ -1044,7 +1044,7 @@ int aln_async(gasal_gpu_storage_t *s, uint32_t qbytes, uint32_t tbytes, uint32_t
 
     /* every host decision and allocation of the batch */
     gb::Plan plan;
-    int rc = gb::plan_batch(cfg, b, o, ss.ws, plan);
+    int rc = gb::plan_batch(cfg, b, o, ss.ws, plan, s->str);
     if (rc != GB_OK) return E.fail(rc, "[GASAL ERROR:] alignment launch failed\n");
 
     /* the stream operations of the batch: host pages -> device

@@ -206,7 +206,7 @@ static int ensure_order_buffers(Workspace &ws, size_t n)
     return GB_OK;
 }
 
-int plan_batch(const RunCfg &cfg, const DevBatch &b, const DevOut &o, Workspace &ws, Plan &p)
+int plan_batch(const RunCfg &cfg, const DevBatch &b, const DevOut &o, Workspace &ws, Plan &p, cudaStream_t s)
 {
     if (b.n <= 0) return GB_ERR_ARG;
     const Settings &st = settings();
@@ -361,7 +361,14 @@ int plan_batch(const RunCfg &cfg, const DevBatch &b, const DevOut &o, Workspace 
         }
     }
     if (p.use_wc && !ws.aux) {
-        if (cudaStreamCreateWithFlags(&ws.aux, cudaStreamNonBlocking) != cudaSuccess ||
+        /* the warp-cooperative kernels run on the auxiliary stream: with the
+         * launch stream's priority, so a caller's prioritised batch keeps it */
+        int prio = 0;
+        if (s && cudaStreamGetPriority(s, &prio) != cudaSuccess) {
+            cudaGetLastError();
+            prio = 0;
+        }
+        if (cudaStreamCreateWithPriority(&ws.aux, cudaStreamNonBlocking, prio) != cudaSuccess ||
             cudaEventCreateWithFlags(&ws.fork, cudaEventDisableTiming) != cudaSuccess ||
             cudaEventCreateWithFlags(&ws.join, cudaEventDisableTiming) != cudaSuccess) {
             cudaGetLastError();
@@ -668,7 +675,7 @@ static int enqueue_align(const RunCfg &cfg, const DevBatch &b, const DevOut &o, 
 int run_batch(const RunCfg &cfg, const DevBatch &b, const DevOut &o, Workspace &ws, cudaStream_t s)
 {
     Plan p;
-    int rc = plan_batch(cfg, b, o, ws, p);
+    int rc = plan_batch(cfg, b, o, ws, p, s);
     if (rc != GB_OK) return rc;
     rc = enqueue_batch(cfg, b, o, ws, p, s);
     if (rc == GB_OK && p.tb) GB_CUDA(cudaEventRecord(ws.tb_off_free, s));

@@ -112,7 +112,10 @@ struct Plan {
 };
 
 /* status codes of gasal_b200_capi.h */
-int plan_batch(const RunCfg &cfg, const DevBatch &b, const DevOut &o, Workspace &ws, Plan &p);
+/* s: the stream the batch will run on (its priority is given to the
+ * workspace's auxiliary stream when that is created) */
+int plan_batch(const RunCfg &cfg, const DevBatch &b, const DevOut &o, Workspace &ws, Plan &p,
+               cudaStream_t s = nullptr);
 int enqueue_batch(const RunCfg &cfg, const DevBatch &b, const DevOut &o, Workspace &ws, const Plan &p,
                   cudaStream_t s);
 int run_batch(const RunCfg &cfg, const DevBatch &b, const DevOut &o, Workspace &ws, cudaStream_t s);

@@ -172,11 +172,15 @@ __global__ void __launch_bounds__(256) revcomp_flat_kernel(uint32_t *pq, uint32_
         const int p = ((tside ? g - groups_q : g) << 5) + lane;
         const uint8_t *ops = tside ? t_op : q_op;
         uint32_t *words = tside ? pt : pq;
-        int op = p < n ? (ops[p] & 3) : 0;
+        /* the op, offset and length loads are independent: issue them together */
+        int op = 0;
         uint32_t base = 0, regs = 0;
-        if (op) {
-            base = (tside ? t_off[p] : q_off[p]) >> 3;
-            regs = ((tside ? t_len[p] : q_len[p]) + 7) >> 3;
+        if (p < n) {
+            const uint8_t o8 = __ldg(ops + p);
+            const uint32_t off = __ldg((tside ? t_off : q_off) + p), len = __ldg((tside ? t_len : q_len) + p);
+            op = o8 & 3;
+            base = op ? off >> 3 : 0u;
+            regs = op ? (len + 7) >> 3 : 0u;
         }
         const uint32_t tasks = (op & 1) ? (regs + 1) >> 1 : (op == 2 ? regs : 0u);
         const uint32_t chunks = (tasks + RC_CHUNK - 1) / RC_CHUNK;
