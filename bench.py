@@ -289,12 +289,11 @@ class DevPart:
 class Runner:
     """Launches every part on its own stream, joined into one timing stream."""
 
-    def __init__(self, torch, gl, parts, dev, tb_priority=True):
+    def __init__(self, torch, gl, parts, dev, tb_priority=False):
         self.torch, self.gl, self.parts, self.dev = torch, gl, parts, dev
         self.main = torch.cuda.Stream(device=dev)
-        # a WITH_TB launch runs its traceback chunks one after another and would finish last; its stream
-        # (and, through the library, its auxiliary stream) gets the highest priority so its blocks are
-        # scheduled first and the other launches fill the GPU around it
+        # optionally (tb_priority) a WITH_TB launch, which runs its traceback chunks one after another and
+        # finishes last, gets the highest stream priority (the library gives its auxiliary stream the same)
         self.streams = [torch.cuda.Stream(device=dev, priority=-5 if tb_priority and d.p.start_pos == WITH_TB else 0)
                         for d in parts]
 
@@ -567,8 +566,9 @@ def main():
     ap.add_argument("--plain-budget-s", type=float, default=20.0,
                     help="device time the plain form's timed step may take; beyond it a stratified sample is used")
     ap.add_argument("--e2e-steps", type=int, default=3)
-    ap.add_argument("--tb-priority", default="on", choices=["on", "off"],
-                    help="kernel-level step: run WITH_TB launches on the highest-priority stream")
+    ap.add_argument("--tb-priority", default="off", choices=["on", "off"],
+                    help="kernel-level step: run WITH_TB launches on the highest-priority stream (measured slower "
+                         "on w4: the prioritised launch finishes early and the others then run on alone)")
     ap.add_argument("--split", default="weak", choices=["weak", "cells"],
                     help="N>1: weak = every rank aligns its own full-size seeded shard; cells = the ranks split one "
                          "workload into contiguous slices of equal DP cells (strong scaling)")

@@ -290,7 +290,7 @@ void batch_signature(std::vector<uint8_t> &v, const gasal_gpu_storage_t *s, cons
     }
     put(v, plan.tb), put(v, plan.second), put(v, plan.use_wc), put(v, plan.order_on);
     put(v, plan.start), put(v, plan.block), put(v, plan.mq8), put(v, plan.mt8), put(v, plan.wc_min_q);
-    put(v, plan.ksw_slots), put(v, plan.fb_blocks), put(v, plan.band);
+    put(v, plan.ksw_slots), put(v, plan.fb_blocks), put(v, plan.band), put(v, plan.ksw_short);
     put(v, plan.tier2), put(v, plan.tier_q), put(v, plan.tier2_cols), put(v, plan.tier2_blocks);
     put(v, plan.split_start), put(v, plan.wc), put(v, plan.wc_big), put(v, plan.mq8_big);
     put(v, plan.mt8_big), put(v, (const void *)ss.ws.wc_rows);

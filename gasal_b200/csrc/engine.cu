@@ -52,6 +52,7 @@ Settings &settings()
         if (const char *e = getenv("GASAL_B200_MIN_ORDER_PAIRS")) v.min_order_pairs = atoi(e);
         if (const char *e = getenv("GASAL_B200_WC_MIN_QREGS")) v.wc_min_qregs = atoi(e);
         if (const char *e = getenv("GASAL_B200_WC_BIG_GROUP")) v.wc_big_group = atoi(e);
+        if (const char *e = getenv("GASAL_B200_KSW_GROUPS")) v.ksw_groups = atoi(e);
         return v;
     }();
     return s;
@@ -300,6 +301,7 @@ int plan_batch(const RunCfg &cfg, const DevBatch &b, const DevOut &o, Workspace 
      * back (queries beyond 2046 bases, huge seed scores) */
     if (cfg.algo == KSW_ && st.ksw_wc && ksw_wc_scores_ok(cfg.sc)) {
         ksw_wc_classes(b.h_q_len, b.n, p.ksw_slots);
+        p.ksw_short = st.ksw_groups ? ksw_grp_short(b.h_q_len, b.n) : 0;
         if (grow((void **)&ws.fb, &ws.fb_cap, (size_t)b.n, 4) != GB_OK) return GB_ERR_ALLOC;
         p.band = cfg.band_w != nullptr || cfg.band_model != nullptr;
         if (p.band) {
@@ -550,7 +552,8 @@ static int launch_dp_split(int algo, int start, bool second, const Plan &p, DpAr
  * whose counts it reads on the device.  queue words: [0..1] one-thread work
  * counters, [2] handed-back count, [3] refused count, [4..5] computed cells
  * (u64), [6..7] warp work counters of the two length classes, [8..9] the
- * same for the recomputation pass. */
+ * same for the recomputation pass, [10] and [11] the lane-group launches'
+ * counters of the two passes. */
 static int launch_ksw_split(const RunCfg &cfg, const DevBatch &b, const Plan &p, const uint32_t *order, int n,
                             Workspace &ws, cudaStream_t s)
 {
@@ -570,9 +573,13 @@ static int launch_ksw_split(const RunCfg &cfg, const DevBatch &b, const Plan &p,
         if (cfg.band_ok) GB_CUDA(launch_band_ok(cfg.band_ok, n, ws.retry, ws.queue + 3, s));
         DpArgs ra = p.a;
         ra.n_dev = ws.queue + 3;
-        GB_CUDA(launch_ksw_wc(ra, ws.retry, n, p.ksw_slots, ws.fb, ws.queue + 2, ws.queue + 8, cells, s));
+        GB_CUDA(launch_ksw_wc(ra, ws.retry, n, p.ksw_slots, ws.fb, ws.queue + 2, ws.queue + 8, cells, s,
+                              p.ksw_short > 0 ? -1 : -2, ws.queue + 11));
     } else {
-        GB_CUDA(launch_ksw_wc(p.a, order, n, p.ksw_slots, ws.fb, ws.queue + 2, ws.queue + 6, cells, s));
+        /* a length order lists the short pairs last */
+        const int split = p.ksw_short <= 0 ? -2 : (order ? n - p.ksw_short : -1);
+        GB_CUDA(launch_ksw_wc(p.a, order, n, p.ksw_slots, ws.fb, ws.queue + 2, ws.queue + 6, cells, s, split,
+                              ws.queue + 10));
     }
     timing_mark(K_DP, false, s);
     DpArgs fa = p.a;

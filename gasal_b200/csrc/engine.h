@@ -98,6 +98,7 @@ struct Plan {
     WcLaunch wc_big;
     int mq8_big = 0, mt8_big = 0;
     int ksw_slots[2] = {0, 0}; /* [0] > 0: ksw runs warp-per-pair; eh columns per warp of the two length classes */
+    int ksw_short = 0;         /* unbanded ksw pairs of at most 31 query words, run on lane groups (0: none) */
     bool tier2 = false;     /* one-thread pairs split: short ones with shared-memory rows (a), long ones
                                with global rows on a small grid (tier2_* overrides of a) */
     uint32_t tier_q = 0;    /* queries up to tier_q: shared-memory tier */
@@ -148,6 +149,7 @@ struct Settings {
     const void *band_model = nullptr; /* installed band MLP (BF16 parameters on the device) */
     int band_min = 16, band_max = 1024;
     int wc_big_group = 0;       /* lane group of the 127+ word launch: 0 = automatic (64 when it fits), 32 or 64 */
+    int ksw_groups = 1;         /* unbanded ksw pairs of at most 31 query words run 4 to a warp (lane groups) */
 };
 Settings &settings();
 

@@ -150,8 +150,16 @@ bool ksw_wc_scores_ok(const Scores &sc);
  * these query lengths: class 0 takes queries up to 2046 bases, class 1 up to
  * 8190 (0 = no such pairs). */
 void ksw_wc_classes(const uint32_t *h_q_len, int n, int slots[2]);
+/* split: -2 no lane-group launch; -1 a lane-group launch over the whole list
+ * for queries of at most 248 bases (31 words), the class launches skipping
+ * them; >= 0 the list is length-ordered and its short pairs are exactly
+ * list[split, nlist): lane groups take those, the class launches the prefix.
+ * gq: the lane-group launch's zeroed work counter. */
 cudaError_t launch_ksw_wc(const DpArgs &a, const uint32_t *list, int nlist, const int slots[2], uint32_t *fb,
-                          uint32_t *fbn, uint32_t *wq, unsigned long long *cells, cudaStream_t s);
+                          uint32_t *fbn, uint32_t *wq, unsigned long long *cells, cudaStream_t s, int split = -2,
+                          uint32_t *gq = nullptr);
+/* pairs with at most 31 query words (the lane-group launch's) */
+int ksw_grp_short(const uint32_t *h_q_len, int n);
 /* The same with a band: pair p is computed within half-width band_w[p]
  * (negative: unbanded) and kept only if the band certificate proves it equal
  * to the unbanded result; otherwise nothing is written and p goes to retry

@@ -501,6 +501,341 @@ __global__ void __launch_bounds__(32) ksw_wc_kernel(DpArgs a, const uint32_t *li
     }
 }
 
+/* ---- lane groups: 32/G short pairs per warp ----------------------------
+ *
+ * A pair whose query fits one 256-column slot row runs on a group of G lanes
+ * (8 columns per lane, 8G-column tiles), 32/G pairs side by side in a warp.
+ * The groups step their pairs' rows in lockstep: every pass of the kernel's
+ * loop runs one row of every group that holds a pair (a group whose pair
+ * ended fetches the next one first), so the per-row work -- row maximum,
+ * trimming, z-drop -- is shared by 32/G pairs instead of paid by a whole warp
+ * for one, and a short trimmed row no longer spans a 256-column tile.  The
+ * collectives are the warp kernel's at width G with the group's lane mask.
+ * Group g's eh row starts 8g words past a multiple of 32 so that the groups'
+ * accesses of one tile step fall in different banks. */
+constexpr int GRP_SLOTS = 256;  /* eh columns per group: queries up to GRP_QMAX bases */
+constexpr int GRP_QMAX = 248;   /* 31 query words: the suffix of the length order */
+constexpr int GRP_PAD = 8;
+
+template <int G> __device__ __forceinline__ int kslot_g(int j)
+{
+    return (j & ~(8 * G - 1)) | ((j & 7) * G) | ((j >> 3) & (G - 1));
+}
+
+struct GrpConst {
+    uint32_t *eh;
+    const uint4 *selw;
+    uint2 tab;
+    int sm, sx, g, gl, end, Cmul, oe, e_del;
+    unsigned gmask;
+    int gbase;
+};
+
+/* one 8G-column tile of a group's row starting at column pos (a multiple of
+ * 8); lane gl owns pos + 8gl .. +7.  FULLT: the whole tile lies before end. */
+template <int G, bool FAST, bool FULLT>
+__device__ __forceinline__ void grp_tile(const GrpConst &c, int pos, TileState &ts)
+{
+    const int gl = c.gl;
+    const int j0 = pos + gl * 8;
+    const int nv = FULLT ? 8 : min(max(c.end - j0, 0), 8);
+    const int jr = (FULLT || j0 < GRP_SLOTS) ? j0 : 0;
+    const int sb = (jr & ~(8 * G - 1)) | ((jr >> 3) & (G - 1));
+    const uint4 sw = c.selw[jr >> 3];
+    const uint32_t swk[4] = {sw.x, sw.y, sw.z, sw.w};
+    int vh[8], ve[8], Mp[8], tv[8];
+#pragma unroll
+    for (int k = 0; k < 8; k++) {
+        const uint32_t pv = c.eh[sb + G * k];
+        const uint32_t hi = high16(pv);
+        ve[k] = (int)hi;
+        vh[k] = (int)mad_lo_u32(hi, 0xFFFF0000u, pv);
+    }
+    int agg = 0;
+#pragma unroll
+    for (int k = 0; k < 8; k++) {
+        int s;
+        if (FAST) {
+            s = (int)prmt(c.tab.x, c.tab.y, (k & 1) ? (swk[k >> 1] >> 16) : swk[k >> 1]);
+        } else {
+            const int cd = (int)((sw.x >> (28 - 4 * k)) & 15u);
+            s = cd == N_CODE4 ? 0 : (cd == c.g ? c.sm : c.sx);
+        }
+        Mp[k] = __viaddmin_s32(vh[k], s, vh[k] * c.Cmul);
+        tv[k] = __viaddmax_s32(Mp[k], -c.oe, 0);
+        agg = k == 0 ? tv[0] : __viaddmax_s32(agg, -c.e_del, tv[k]);
+    }
+    const int eK = c.e_del * 8;
+    int x = agg;
+#pragma unroll
+    for (int d = 1; d < G; d <<= 1) {
+        const int y = __shfl_up_sync(c.gmask, x, d, G);
+        if (gl >= d) x = max(x, y - eK * d);
+    }
+    const int ex = __shfl_up_sync(c.gmask, x, 1, G);
+    int f = gl == 0 ? ts.fcarry : max(ex, ts.fcarry - eK * gl);
+    ts.fcarry = __shfl_sync(c.gmask, max(x, ts.fcarry - eK * (gl + 1)), G - 1, G);
+    int H[8];
+    int lkey = -1;
+#pragma unroll
+    for (int k = 0; k < 8; k++) {
+        H[k] = __vimax3_s32(Mp[k], ve[k], f);
+        ve[k] = __viaddmax_s32(ve[k], -c.e_del, tv[k]);
+        f = __viaddmax_s32(f, -c.e_del, tv[k]);
+        if (FULLT) {
+            if (k & 1) lkey = __vimax3_s32(lkey, (int)mad_lo_u32((uint32_t)H[k - 1], 8u, (uint32_t)(k - 1)),
+                                           (int)mad_lo_u32((uint32_t)H[k], 8u, (uint32_t)k));
+        } else if (k < nv) {
+            ts.kmax = max(ts.kmax, (int)mad_lo_u32((uint32_t)H[k], 1u << KEY_BITS, (uint32_t)(j0 + k)));
+            ts.hlast = H[k];
+        }
+    }
+    if (FULLT) {
+        ts.kmax = max(ts.kmax, (int)mad_lo_u32((uint32_t)(lkey >> 3), 1u << KEY_BITS, (uint32_t)(j0 + (lkey & 7))));
+        ts.hlast = H[7];
+    }
+    int hp = __shfl_up_sync(c.gmask, H[7], 1, G);
+    if (gl == 0) hp = ts.hcarry;
+    ts.hcarry = __shfl_sync(c.gmask, H[7], G - 1, G);
+    uint32_t nz = 0;
+#pragma unroll
+    for (int k = 0; k < 8; k++) {
+        const int hs = k == 0 ? hp : H[k - 1];
+        if (FULLT || k < nv) {
+            const uint32_t pv = mad_lo_u32((uint32_t)ve[k], 65536u, (uint32_t)hs);
+            c.eh[sb + G * k] = pv;
+            nz |= pv;
+        }
+    }
+    const unsigned bm = (__ballot_sync(c.gmask, nz != 0) >> c.gbase) & ((G >= 32) ? 0xFFFFFFFFu : ((1u << G) - 1u));
+    if (bm) {
+        if (ts.fcol < 0) ts.fcol = pos + (__ffs(bm) - 1) * 8, ts.fcnt = 8;
+        ts.lcol = pos + (31 - __clz(bm)) * 8, ts.lcnt = 8;
+    }
+}
+
+/* The unbanded ksw on lane groups, for pairs of at most GRP_QMAX query bases.
+ * Pairs with longer queries are skipped (the 32-lane class launches take
+ * them); pairs whose seed + match * qlen reaches 2^15 go to fb.  With `split`
+ * >= 0 the list is length-ordered and its short pairs are exactly
+ * list[split, n): the launch visits only those. */
+template <int G>
+__global__ void __launch_bounds__(32) ksw_grp_kernel(DpArgs a, const uint32_t *list, int nlist, int split,
+                                                      uint32_t *fb, uint32_t *fbn, uint32_t *wq,
+                                                      unsigned long long *cells)
+{
+    static_assert(G == 8 || G == 16, "lane group");
+    constexpr int NG = 32 / G;
+    extern __shared__ __align__(16) uint32_t kg_smem[];
+    __shared__ uint2 stab[16];
+    build_score_table(stab, a.sc, true);
+    __syncthreads();
+    const int lane = threadIdx.x & 31, grp = lane / G, gl = lane & (G - 1), gbase = grp * G;
+    const unsigned gmask = (G >= 32) ? FULL : (((1u << G) - 1u) << gbase);
+    /* one warp per block: group grp's eh row, then the groups' selector rows */
+    uint32_t *eh = kg_smem + grp * (GRP_SLOTS + GRP_PAD);
+    uint4 *selw = reinterpret_cast<uint4 *>(kg_smem + NG * (GRP_SLOTS + GRP_PAD)) + grp * (GRP_SLOTS / 8);
+    const bool fast_scores = a.sc.match >= -128 && a.sc.match <= 127 && a.sc.mismatch >= -127 && a.sc.mismatch <= 128;
+    const long long mpos_ll = a.sc.match > 0 ? a.sc.match : 0;
+    const uint32_t n = a.n_dev ? min(*a.n_dev, (uint32_t)nlist) : (uint32_t)nlist;
+    const uint32_t first = split > 0 ? (uint32_t)split : 0u;
+    const int e_del = a.sc.e, oe = a.sc.oe, o_del = a.sc.o;
+    const int Cmul = max(max(a.sc.match, -a.sc.mismatch), 0) + 1;
+
+    bool have = false, done = false, plain = false;
+    uint32_t pid = 0;
+    int qlen = 0, tlen = 0, h0 = 0, i = 0, beg = 0, end = 0, L8 = 0;
+    int mx = 0, max_i = -1, max_j = -1, max_ie = -1, gscore = -1, mo = 0;
+    const uint32_t *t = nullptr;
+    unsigned long long nc = 0;
+    for (;;) {
+        if (!have && !done) {
+            /* this group fetches its next pair */
+            uint32_t idx = 0;
+            if (gl == 0) idx = first + atomicAdd(wq, 1u);
+            idx = __shfl_sync(gmask, idx, 0, G);
+            if (idx >= n) {
+                done = true;
+            } else {
+                pid = list ? list[idx] : idx;
+                qlen = (int)a.q_len[pid];
+                tlen = (int)a.t_len[pid];
+                const uint32_t h0u = a.seed ? a.seed[pid] : 0u;
+                if (qlen <= GRP_QMAX) {
+                    if ((long long)h0u + mpos_ll * qlen >= EH_LIMIT) {
+                        if (gl == 0) fb[atomicAdd(fbn, 1u)] = pid;
+                    } else {
+                        const uint32_t *q = a.pq + (a.q_off[pid] >> 3);
+                        t = a.pt + (a.t_off[pid] >> 3);
+                        h0 = (int)h0u;
+                        const int qregs = (qlen + 7) >> 3, tregs = (tlen + 7) >> 3;
+                        uint32_t bad = fast_scores ? 0u : 1u;
+                        for (int x = gl; x < qregs + tregs; x += G) {
+                            const uint32_t y = x < qregs ? q[x] : t[x - qregs];
+#pragma unroll
+                            for (int k = 0; k < 8; k++) bad |= ~(PLAIN_CODES >> ((y >> (4 * k)) & 15u)) & 1u;
+                        }
+                        plain = __all_sync(gmask, bad == 0);
+                        for (int gi = gl; gi < GRP_SLOTS / 8; gi += G) {
+                            const uint32_t y = gi < qregs ? q[gi] : 0u;
+                            uint4 sw;
+                            if (plain) {
+                                uint32_t cc[8];
+#pragma unroll
+                                for (int k = 0; k < 8; k++) cc[k] = sel16(class_of((y >> (28 - 4 * k)) & 15u));
+                                sw = make_uint4(cc[0] | (cc[1] << 16), cc[2] | (cc[3] << 16), cc[4] | (cc[5] << 16),
+                                                cc[6] | (cc[7] << 16));
+                            } else {
+                                sw = make_uint4(y, 0u, 0u, 0u);
+                            }
+                            selw[gi] = sw;
+                        }
+                        /* the reference's first row (ksw_kernel_template.h:75-79) */
+                        for (int s2 = gl; s2 < GRP_SLOTS; s2 += G) eh[s2] = 0u;
+                        __syncwarp(gmask);
+                        const int v1 = h0u > (uint32_t)oe ? h0 - oe : 0;
+                        for (int j = gl; j <= qlen + 1; j += G) {
+                            int h = 0;
+                            if (j == 0) h = h0;
+                            else if (j == 1) h = v1;
+                            else if (j <= qlen && v1 - (j - 2) * e_del > e_del) h = v1 - (j - 1) * e_del;
+                            if (h) eh[kslot_g<G>(j)] = (uint32_t)h;
+                        }
+                        __syncwarp(gmask);
+                        have = true;
+                        i = 0, beg = 0, end = qlen, L8 = (qlen >> 3) << 3;
+                        mx = h0, max_i = -1, max_j = -1, max_ie = -1, gscore = -1, mo = 0;
+                        nc = 0;
+                    }
+                }
+            }
+        }
+        if (__all_sync(FULL, done)) break;
+        if (have && i < tlen) {
+            /* one row of this group's pair */
+            const int g = code(__ldg(t + (i >> 3)), i & 7);
+            int h1 = 0;
+            if (beg == 0) {
+                h1 = (int)((uint32_t)h0 - (uint32_t)(o_del + e_del * (i + 1)));
+                if (h1 < 0) h1 = 0;
+            }
+            int m = 0, mj = -1;
+            int fcol = -1, lcol = -1;
+            if (beg < end) {
+                nc += (unsigned long long)(end - beg);
+                uint2 tab = make_uint2(0, 0);
+                int sm = 0, sx = 0;
+                if (plain) {
+                    tab = stab[g];
+                } else {
+                    sm = g == N_CODE4 ? 0 : a.sc.match;
+                    sx = g == N_CODE4 ? 0 : -a.sc.mismatch;
+                }
+                TileState ts{0, h1, -1, 0, 0, -1, 0, -1, 0};
+                const GrpConst gc{eh, selw, tab, sm, sx, g, gl, end, Cmul, oe, e_del, gmask, gbase};
+                int pos = beg & ~7, lpos = pos;
+                while (pos < end) {
+                    lpos = pos;
+                    const bool full = end - pos >= 8 * G;
+                    if (plain) {
+                        if (full) grp_tile<G, true, true>(gc, pos, ts);
+                        else grp_tile<G, true, false>(gc, pos, ts);
+                    } else {
+                        if (full) grp_tile<G, false, true>(gc, pos, ts);
+                        else grp_tile<G, false, false>(gc, pos, ts);
+                    }
+                    pos += 8 * G;
+                }
+                int kmax = ts.kmax;
+#pragma unroll
+                for (int o = G / 2; o > 0; o >>= 1) kmax = max(kmax, __shfl_xor_sync(gmask, kmax, o, G));
+                m = kmax >> KEY_BITS;
+                mj = kmax & ((1 << KEY_BITS) - 1);
+                h1 = __shfl_sync(gmask, ts.hlast, (end - 1 - lpos) >> 3, G);
+                fcol = ts.fcol, lcol = ts.lcol;
+            }
+            if (gl == 0) eh[kslot_g<G>(end)] = (uint32_t)h1;
+            __syncwarp(gmask);
+            if (max(L8, end) == qlen) {
+                max_ie = gscore > h1 ? max_ie : i;
+                gscore = max(gscore, h1);
+            }
+            bool leave = false;
+            if (m == 0) {
+                leave = true;
+            } else if (m > mx) {
+                mx = m, max_i = i, max_j = mj;
+                mo = max(mo, abs(mj - i));
+            } else if (a.zdrop > 0) {
+                if (i - max_i > mj - max_j) {
+                    if (mx - m - ((i - max_i) - (mj - max_j)) * e_del > a.zdrop) leave = true;
+                } else {
+                    if (mx - m - ((mj - max_j) - (i - max_i)) * e_del > a.zdrop) leave = true;
+                }
+            }
+            if (leave) {
+                i = ((i >> 3) + 1) << 3;
+            } else {
+                /* trimming (ksw_kernel_template.h:188-196): the first and last
+                 * non-zero entries lie among the 8 columns of the first and the
+                 * last group lane whose stores were non-zero */
+                const int jf = fcol >= 0 ? fcol + gl : -1;
+                const int jl = (h1 == 0 && lcol >= 0) ? lcol + gl : -1;
+                const bool nzf = gl < 8 && jf >= 0 && jf < end && eh[kslot_g<G>(jf)] != 0u;
+                const bool nzl = gl < 8 && jl >= 0 && jl < end && eh[kslot_g<G>(jl)] != 0u;
+                const unsigned bf = (__ballot_sync(gmask, nzf) >> gbase) & 0xFFu;
+                const unsigned bl = (__ballot_sync(gmask, nzl) >> gbase) & 0xFFu;
+                const int nbeg = bf ? fcol + __ffs(bf) - 1 : end;
+                int lastnz = nbeg - 1;
+                if (h1 != 0) lastnz = end;
+                else if (bl) lastnz = lcol + (31 - __clz(bl));
+                beg = nbeg;
+                end = lastnz + 2 < qlen ? lastnz + 2 : qlen;
+                i++;
+            }
+            __syncwarp(gmask); /* the scans above read slots their owners rewrite next row */
+        }
+        if (have && i >= tlen) {
+            if (gl == 0) {
+                int sc, qe, te;
+                if (gscore <= 0 || gscore <= mx - 5) {
+                    sc = mx, qe = max_j + 1, te = max_i + 1;
+                } else {
+                    sc = gscore, qe = qlen, te = max_ie + 1;
+                }
+                if (a.score) a.score[pid] = sc;
+                if (a.q_end) a.q_end[pid] = qe;
+                if (a.t_end) a.t_end[pid] = te;
+                if (a.max_off) a.max_off[pid] = mo;
+                if (cells) atomicAdd(cells, nc);
+            }
+            have = false;
+            __syncwarp(gmask);
+        }
+    }
+}
+
+template <int G> size_t grp_smem() { return (size_t)(32 / G) * ((GRP_SLOTS + GRP_PAD) * 4 + (GRP_SLOTS / 8) * 16); }
+
+cudaError_t launch_grp(const DpArgs &a, const uint32_t *list, int nlist, int split, uint32_t *fb, uint32_t *fbn,
+                       uint32_t *wq, unsigned long long *cells, cudaStream_t s)
+{
+    constexpr int G = 8;
+    const int nshort = split >= 0 ? nlist - split : nlist;
+    if (nshort <= 0) return cudaSuccess;
+    const size_t smem = grp_smem<G>();
+    int dev = 0, sms = 148, per_sm = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, ksw_grp_kernel<G>, 32, smem);
+    if (e != cudaSuccess) return e;
+    if (per_sm < 1) per_sm = 1;
+    int blocks = (nshort + 32 / G - 1) / (32 / G);
+    if (blocks > per_sm * sms) blocks = per_sm * sms;
+    ksw_grp_kernel<G><<<blocks, 32, smem, s>>>(a, list, nlist, split, fb, fbn, wq, cells);
+    return cudaGetLastError();
+}
+
 /* shared-memory slots per warp for queries up to max_qlen (whole tiles) */
 int slots_for(int max_qlen) { return ((max_qlen + 2 + KT - 1) / KT) * KT; }
 
@@ -545,12 +880,13 @@ void ksw_wc_classes(const uint32_t *h_q_len, int n, int slots[2])
     slots[1] = m1 >= 0 ? slots_for(m1) : 0;
 }
 
-/* the class launches over one list; wq[c] is class c's zeroed work counter */
+/* the class launches over one list; wq[c] is class c's zeroed work counter;
+ * class 0 skips queries shorter than q_lo0 (the lane-group launch's) */
 static cudaError_t launch_classes(const DpArgs &a, const uint32_t *list, int nlist, const int slots[2], uint32_t *fb,
-                                  uint32_t *fbn, uint32_t *wq, BandArgs ba, bool band, cudaStream_t s)
+                                  uint32_t *fbn, uint32_t *wq, BandArgs ba, bool band, cudaStream_t s, int q_lo0 = 0)
 {
     if (nlist <= 0) return cudaSuccess;
-    ba.q_lo = 0;
+    ba.q_lo = q_lo0;
     ba.handback = slots[1] == 0;
     cudaError_t e = launch_slots(a, list, nlist, slots[0], fb, fbn, wq, ba, band, s);
     if (e != cudaSuccess || slots[1] == 0) return e;
@@ -560,10 +896,24 @@ static cudaError_t launch_classes(const DpArgs &a, const uint32_t *list, int nli
 }
 
 cudaError_t launch_ksw_wc(const DpArgs &a, const uint32_t *list, int nlist, const int slots[2], uint32_t *fb,
-                          uint32_t *fbn, uint32_t *wq, unsigned long long *cells, cudaStream_t s)
+                          uint32_t *fbn, uint32_t *wq, unsigned long long *cells, cudaStream_t s, int split,
+                          uint32_t *gq)
 {
     BandArgs ba{nullptr, nullptr, nullptr, cells, 0, 1};
-    return launch_classes(a, list, nlist, slots, fb, fbn, wq, ba, false, s);
+    if (split < -1) return launch_classes(a, list, nlist, slots, fb, fbn, wq, ba, false, s);
+    /* short queries on lane groups: the order's suffix [split, nlist), or
+     * every pair of an unordered list skipping the longer ones */
+    const cudaError_t e = launch_grp(a, list, nlist, split, fb, fbn, gq, cells, s);
+    if (e != cudaSuccess) return e;
+    if (split >= 0) return launch_classes(a, list, split, slots, fb, fbn, wq, ba, false, s);
+    return launch_classes(a, list, nlist, slots, fb, fbn, wq, ba, false, s, GRP_QMAX + 1);
+}
+
+int ksw_grp_short(const uint32_t *h_q_len, int n)
+{
+    int c = 0;
+    for (int i = 0; i < n; i++) c += ((h_q_len[i] + 7) >> 3) <= (uint32_t)(GRP_QMAX / 8) ? 1 : 0;
+    return c;
 }
 
 cudaError_t launch_ksw_band(const DpArgs &a, const uint32_t *list, int nlist, const int slots[2],

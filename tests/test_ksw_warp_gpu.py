@@ -138,3 +138,72 @@ def test_long_class_columns_past_4095():
     got = _check(Params(algo=KSW, zdrop=100), b)
     assert int((got["q_end"] > 4096).sum()) > 45  # the maxima sit past column 4096
     _check(Params(algo=KSW), b)
+
+
+def _short_mixed(n, seed):
+    """Queries of 1-300 bases (most of them on lane groups, 31 words or fewer,
+    the rest on the 32-lane kernel), related and unrelated targets of 0-400
+    bases, N runs and IUPAC codes in some pairs, seeds 0-60 and a few of
+    40000 (handed back to the one-thread kernel)."""
+    rng = np.random.default_rng(seed)
+    qs, ts, h0 = [], [], []
+    for k in range(n):
+        ql = int(rng.integers(1, 300)) if k % 11 else 0
+        q = bytearray(rng.choice(list(b"ACGT"), size=ql).tolist())
+        if k % 3 == 0:
+            t = bytearray(rng.choice(list(b"ACGT"), size=int(rng.integers(0, 400))).tolist())
+        else:
+            t = bytearray(q)
+            for _ in range(int(rng.integers(0, 8))):
+                if not t:
+                    break
+                a = int(rng.integers(0, len(t)))
+                if rng.random() < 0.5:
+                    del t[a:a + int(rng.integers(1, 5))]
+                else:
+                    t[a:a] = bytes(rng.choice(list(b"ACGT"), size=int(rng.integers(1, 5))).tolist())
+            t += bytes(rng.choice(list(b"ACGT"), size=int(rng.integers(0, 60))).tolist())
+        if k % 7 == 1 and len(q) > 10:
+            q[3:6] = b"NNN"
+        if k % 13 == 2 and len(t) > 10:
+            t[4] = ord("R")
+        qs.append(bytes(q))
+        ts.append(bytes(t))
+        h0.append(40000 if k % 97 == 5 else int(rng.integers(0, 61)))
+    return Batch.from_seqs(qs, ts, seed=np.array(h0, dtype=np.uint32))
+
+
+@pytest.mark.parametrize("n", [1500, 6000])
+@pytest.mark.parametrize("zdrop", [0, 100, 8])
+def test_lane_groups_short_pairs(n, zdrop):
+    """Short pairs four to a warp (lane groups of 8): below the ordering
+    threshold (every pair visited, longer ones skipped) and above it (the
+    length order's suffix); empty sequences, N runs, IUPAC codes, seeds that
+    hand pairs back, all against the oracle."""
+    b = _short_mixed(n, 700 + zdrop + n)
+    _check(Params(algo=KSW, zdrop=zdrop), b, f"n={n}")
+
+
+def test_lane_groups_off_gives_the_same():
+    """GASAL_B200_KSW_GROUPS=0 (every pair on 32-lane warps) and the default
+    give identical outputs (checked in a child process: the setting is read
+    once)."""
+    import json, os, subprocess, sys
+    child = r"""
+import json, sys
+import numpy as np
+sys.path.insert(0, sys.argv[1])
+from gasal_b200 import lib as gl, workloads as W
+from gasal_b200.capi import Params, KSW
+p, b = W.workload4(20000, seed=731)[3]
+o = gl.align(Params(algo=KSW, zdrop=100), b).as_dict(Params(algo=KSW, zdrop=100))
+print(json.dumps({k: v.tolist() for k, v in o.items()}))
+"""
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    outs = []
+    for on in ("1", "0"):
+        env = dict(os.environ, GASAL_B200_KSW_GROUPS=on)
+        r = subprocess.run([sys.executable, "-c", child, root], env=env, capture_output=True, text=True, timeout=600)
+        assert r.returncode == 0, r.stderr[-2000:]
+        outs.append(json.loads(r.stdout.strip().splitlines()[-1]))
+    assert outs[0] == outs[1]
