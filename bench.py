@@ -289,8 +289,9 @@ class DevPart:
 class Runner:
     """Launches every part on its own stream, joined into one timing stream."""
 
-    def __init__(self, torch, gl, parts, dev, tb_priority=False):
+    def __init__(self, torch, gl, parts, dev, tb_priority=False, serial=False):
         self.torch, self.gl, self.parts, self.dev = torch, gl, parts, dev
+        self.serial = serial  # every launch on the timing stream, one after another
         self.main = torch.cuda.Stream(device=dev)
         # optionally (tb_priority) a WITH_TB launch, which runs its traceback chunks one after another and
         # finishes last, gets the highest stream priority (the library gives its auxiliary stream the same)
@@ -303,7 +304,10 @@ class Runner:
         fork.record(self.main)
         dones = []
         for d, s in zip(self.parts, self.streams):
-            s.wait_event(fork)
+            if self.serial:
+                s = self.main
+            else:
+                s.wait_event(fork)
             self.gl.align_dev(d.p, d.map, d.b.q_len, d.b.t_len, s.cuda_stream)
             done = torch.cuda.Event(enable_timing=finish_times)
             done.record(s)
@@ -566,6 +570,8 @@ def main():
     ap.add_argument("--plain-budget-s", type=float, default=20.0,
                     help="device time the plain form's timed step may take; beyond it a stratified sample is used")
     ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--serial", action="store_true",
+                    help="kernel-level step: the launches one after another on one stream instead of concurrently")
     ap.add_argument("--tb-priority", default="off", choices=["on", "off"],
                     help="kernel-level step: run WITH_TB launches on the highest-priority stream (measured slower "
                          "on w4: the prioritised launch finishes early and the others then run on alone)")
@@ -627,7 +633,7 @@ def main():
         model, band_info = train_band(torch, gl, args, rank, dev)
 
     # ---------------- kernel level: inputs resident in HBM -----------------
-    runner = Runner(torch, gl, dparts, dev, tb_priority=args.tb_priority == "on")
+    runner = Runner(torch, gl, dparts, dev, tb_priority=args.tb_priority == "on", serial=args.serial)
     clk = ClockSampler(local_rank).__enter__()
 
     def arm():
@@ -703,7 +709,9 @@ def main():
                                        f"in the data path"),
                        "l2": l2_note,
                        "stream_priority": "WITH_TB launches on the highest-priority stream" if args.tb_priority == "on"
-                                          else "all launches on default-priority streams"},
+                                          else "all launches on default-priority streams",
+                       "launch_streams": "one stream, launches in sequence" if args.serial else
+                                         "one stream per launch, concurrent"},
             "gcups": job_cells / (ms_step * 1e-3) / 1e9,
             "gcups_computed": None if computed is None else computed * (job_cells / cells) / (ms_step * 1e-3) / 1e9,
             "roofline": {"bound": "int32", "achieved": achieved, "peak": peak["iadd_tops"], "unit": "Tops/s",

@@ -167,21 +167,27 @@ __global__ void __launch_bounds__(256) revcomp_flat_kernel(uint32_t *pq, uint32_
     const int groups = groups_q + (t_op ? (n + 31) >> 5 : 0);
     const int warp0 = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int nwarps = (gridDim.x * blockDim.x) >> 5;
+    /* the op, offset and length of a group's 32 sequences: independent loads,
+     * issued together, and for the warp's next group before this one's words */
+    auto meta = [&](int g, uint32_t &o8, uint32_t &off, uint32_t &len) {
+        o8 = 0, off = 0, len = 0;
+        if (g >= groups) return;
+        const bool ts = g >= groups_q;
+        const int p = ((ts ? g - groups_q : g) << 5) + lane;
+        if (p < n) {
+            o8 = __ldg((ts ? t_op : q_op) + p);
+            off = __ldg((ts ? t_off : q_off) + p);
+            len = __ldg((ts ? t_len : q_len) + p);
+        }
+    };
+    uint32_t n_o8, n_off, n_len;
+    meta(warp0, n_o8, n_off, n_len);
     for (int g = warp0; g < groups; g += nwarps) {
         const bool tside = g >= groups_q;
-        const int p = ((tside ? g - groups_q : g) << 5) + lane;
-        const uint8_t *ops = tside ? t_op : q_op;
         uint32_t *words = tside ? pt : pq;
-        /* the op, offset and length loads are independent: issue them together */
-        int op = 0;
-        uint32_t base = 0, regs = 0;
-        if (p < n) {
-            const uint8_t o8 = __ldg(ops + p);
-            const uint32_t off = __ldg((tside ? t_off : q_off) + p), len = __ldg((tside ? t_len : q_len) + p);
-            op = o8 & 3;
-            base = op ? off >> 3 : 0u;
-            regs = op ? (len + 7) >> 3 : 0u;
-        }
+        const int op = (int)(n_o8 & 3u);
+        const uint32_t base = op ? n_off >> 3 : 0u, regs = op ? (n_len + 7) >> 3 : 0u;
+        meta(g + nwarps, n_o8, n_off, n_len);
         const uint32_t tasks = (op & 1) ? (regs + 1) >> 1 : (op == 2 ? regs : 0u);
         const uint32_t chunks = (tasks + RC_CHUNK - 1) / RC_CHUNK;
         uint32_t incl = chunks;
