@@ -223,6 +223,7 @@ void release_state(const gasal_gpu_storage_t *s)
     if (w.order) cudaFree(w.order);
     if (w.order2) cudaFree(w.order2);
     if (w.wc_rows) cudaFree(w.wc_rows);
+    if (w.wc_defer) cudaFree(w.wc_defer);
     if (w.aux) cudaStreamDestroy(w.aux);
     if (w.queue) cudaFree(w.queue);
     if (w.fork) cudaEventDestroy(w.fork);
@@ -276,7 +277,7 @@ void batch_signature(std::vector<uint8_t> &v, const gasal_gpu_storage_t *s, cons
                           s->host_query_batch_lens, s->host_target_batch_lens, s->host_query_batch_offsets,
                           s->host_target_batch_offsets, s->host_query_op, s->host_target_op, s->host_seed_scores,
                           ss.d_n_cigar, ss.ws.tb, ss.ws.d_tb_off, ss.ws.h_tb_off, ss.ws.order, ss.ws.bins,
-                          ss.ws.queue, ss.ws.aux, ss.ws.fork, ss.ws.join, ss.ws.fb, ss.ws.retry, ss.ws.feat, ss.ws.order2,
+                          ss.ws.queue, ss.ws.aux, ss.ws.fork, ss.ws.join, ss.ws.fb, ss.ws.retry, ss.ws.wc_defer, ss.ws.feat, ss.ws.order2,
                           ss.ws.pred, ss.ws.bandw, (const void *)s->str};
     for (const void *q : ptrs) put(v, q);
     const gasal_res_t *rs[] = {s->host_res, s->device_cpy, s->host_res_second, s->device_cpy_second};

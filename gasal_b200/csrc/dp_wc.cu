@@ -257,7 +257,7 @@ __device__ __forceinline__ uint32_t dnib(int M, int diag, int H, int F, int E, c
  * qword(j), tword(T): the words the sweep reads (reversed for MODE 1).
  * bandmax: per-band maxima (written when SECOND pass 1, read in pass 2).
  */
-template <int G, int MODE, bool TB, bool SECOND_PASS2, class QW, class TW>
+template <int G, int MODE, bool TB, bool SECOND_PASS2, bool FAST, class QW, class TW>
 __device__ void wc_sweep(QW qword, int qregs, TW tword, int tregs, int qlen, int tlen, const Scores &sc,
                          WcScore &S, uint32_t *ring, uint4 *tb, int stop, int *bandmax, bool write_bandmax,
                          WcRec &best_out, WcRec &sec_out, int &gscore)
@@ -342,7 +342,7 @@ __device__ void wc_sweep(QW qword, int qregs, TW tword, int tregs, int qlen, int
                 const int c = (w << 3) + b;
                 const int rbase = cd(qw, b);
                 uint2 tcol = make_uint2(0, 0);
-                if (S.fast) tcol = S.tab[rbase];
+                if (FAST) tcol = S.tab[rbase];
                 const bool rz = local && rbase == 14;
                 const uint32_t v = in[b];
                 const int up0 = sx16(v);
@@ -354,7 +354,7 @@ __device__ void wc_sweep(QW qword, int qregs, TW tword, int tregs, int qlen, int
 #pragma unroll
                 for (int k = 0; k < 8; k++) {
                     int s_;
-                    if (S.fast) s_ = (int)wprmt(tcol.x, tcol.y, S.sel[k]);
+                    if (FAST) s_ = (int)wprmt(tcol.x, tcol.y, S.sel[k]);
                     else s_ = rz ? 0 : ((rbase == S.g[k]) ? S.ma[k] : S.mm[k]);
                     const int M = D[k] + s_;
                     const int H = local ? __vimax3_s32_relu(M, F[k], e) : __vimax3_s32(M, F[k], e);
@@ -447,7 +447,7 @@ __device__ void wc_sweep(QW qword, int qregs, TW tword, int tregs, int qlen, int
  * reversed words, bands counted from T0 for the left boundary, leaving after
  * the first round whose bands reach `stop` at the last column.
  */
-template <int G, bool START_PASS, bool OPEN_NN, class QW, class TW>
+template <int G, bool START_PASS, bool OPEN_NN, bool FAST, class QW, class TW>
 __device__ void wc_semi_sweep(QW qword, int qregs, TW tword, int tregs, int T0, int qlen, const Scores &sc,
                               int head, WcScore &S, uint32_t *ring, int *lastcol, int stop)
 {
@@ -525,7 +525,7 @@ __device__ void wc_semi_sweep(QW qword, int qregs, TW tword, int tregs, int T0, 
             for (int b = 0; b < 8; b++) {
                 const int rbase = cd(qw, b);
                 uint2 tcol = make_uint2(0, 0);
-                if (S.fast) tcol = S.tab[rbase];
+                if (FAST) tcol = S.tab[rbase];
                 const bool rz = rbase == 14;
                 const uint32_t v = in[b];
                 const int up0 = sx16(v);
@@ -536,7 +536,7 @@ __device__ void wc_semi_sweep(QW qword, int qregs, TW tword, int tregs, int T0, 
 #pragma unroll
                 for (int k = 0; k < 8; k++) {
                     int s_;
-                    if (S.fast) s_ = (int)wprmt(tcol.x, tcol.y, S.sel[k]);
+                    if (FAST) s_ = (int)wprmt(tcol.x, tcol.y, S.sel[k]);
                     else s_ = rz ? 0 : ((rbase == S.g[k]) ? S.ma[k] : S.mm[k]);
                     F[k] = __viaddmax_s32(F[k], -sc.e, Hc[k] - sc.oe);
                     const int M = D[k] + s_;
@@ -631,7 +631,7 @@ __device__ void wc_lastcol_scan(const int *lastcol, int r0, int r1, int row0, in
     }
 }
 
-template <int G, bool SECOND, bool START>
+template <int G, bool SECOND, bool START, bool FAST>
 __global__ void __launch_bounds__(128) dp_wc_semi_kernel(DpArgs a, const uint32_t *list, int nlist, int ring_cols)
 {
     extern __shared__ uint32_t wc_smem[];
@@ -646,27 +646,35 @@ __global__ void __launch_bounds__(128) dp_wc_semi_kernel(DpArgs a, const uint32_
     int *lastcol = a.lastcol + ((size_t)blockIdx.x * gpb + slot) * a.scratch_cols;
     const bool fast_scores = a.sc.match >= -128 && a.sc.match <= 127 && a.sc.mismatch >= -127 && a.sc.mismatch <= 128;
     const bool open_nn = a.sc.o >= 0;
-    for (int item0 = blockIdx.x * gpb; item0 < nlist; item0 += gridDim.x * gpb) {
+    const int nl = a.n_dev ? min((int)*a.n_dev, nlist) : nlist;
+    for (int item0 = blockIdx.x * gpb; item0 < nl; item0 += gridDim.x * gpb) {
         if constexpr (G > 32) __syncthreads(); /* both warps are done with the previous pair */
         const int item = item0 + slot;
-        const bool has = item < nlist; /* the last warp may have groups without a pair */
-        const int i = has ? (int)list[item] : 0;
-        const int qlen = has ? (int)a.q_len[i] : 0, tlen = has ? (int)a.t_len[i] : 0;
-        const uint32_t *q = a.pq + (has ? (a.q_off[i] >> 3) : 0);
-        const uint32_t *t = a.pt + (has ? (a.t_off[i] >> 3) : 0);
+        const bool listed = item < nl; /* the last warp may have groups without a pair */
+        const int i = listed ? (int)list[item] : 0;
+        const int qlen0 = listed ? (int)a.q_len[i] : 0, tlen0 = listed ? (int)a.t_len[i] : 0;
+        const uint32_t *q = a.pq + (listed ? (a.q_off[i] >> 3) : 0);
+        const uint32_t *t = a.pt + (listed ? (a.t_off[i] >> 3) : 0);
+        /* FAST: this launch scores with the prmt table; a pair with another
+         * code or scores beyond a byte goes to the compare-scoring launch
+         * that follows (a.defer), and this launch skips it */
+        const bool plain_q = wc_plain<G>(q, (qlen0 + 7) >> 3); /* warp collectives: every lane calls both */
+        const bool plain_t = wc_plain<G>(t, (tlen0 + 7) >> 3);
+        const bool fast_pair = fast_scores && plain_q && plain_t;
+        const bool has = listed && (!FAST || fast_pair);
+        if (FAST && listed && !fast_pair && gl == 0) a.defer[atomicAdd(a.ndefer, 1u)] = (uint32_t)i;
+        const int qlen = has ? qlen0 : 0, tlen = has ? tlen0 : 0;
         const int qregs = (qlen + 7) >> 3, tregs = (tlen + 7) >> 3;
         WcScore S;
         S.local = true;
         S.tab = tab;
-        S.fast = fast_scores;
-        S.fast = wc_plain<G>(q, qregs) && S.fast;
-        S.fast = wc_plain<G>(t, tregs) && S.fast;
+        S.fast = fast_pair;
         auto qf = [&](int j) { return q[j]; };
         auto tf = [&](int T) { return t[T]; };
         if (open_nn)
-            wc_semi_sweep<G, false, true>(qf, qregs, tf, tregs, 0, qlen, a.sc, a.head, S, ring, lastcol, 0);
+            wc_semi_sweep<G, false, true, FAST>(qf, qregs, tf, tregs, 0, qlen, a.sc, a.head, S, ring, lastcol, 0);
         else
-            wc_semi_sweep<G, false, false>(qf, qregs, tf, tregs, 0, qlen, a.sc, a.head, S, ring, lastcol, 0);
+            wc_semi_sweep<G, false, false, FAST>(qf, qregs, tf, tregs, 0, qlen, a.sc, a.head, S, ring, lastcol, 0);
         int best, brow, sec, srow;
         wc_lastcol_scan<G, SECOND>(lastcol, 0, tlen, qlen, best, brow, sec, srow);
         int t_start = 0, q_start = 0;
@@ -679,11 +687,11 @@ __global__ void __launch_bounds__(128) dp_wc_semi_kernel(DpArgs a, const uint32_
             if constexpr (G > 32) __syncthreads();
             else __syncwarp();
             if (open_nn)
-                wc_semi_sweep<G, true, true>(rq, qregs, rt, tregs, gend_reg, qlen, a.sc, a.head, S, ring, lastcol,
+                wc_semi_sweep<G, true, true, FAST>(rq, qregs, rt, tregs, gend_reg, qlen, a.sc, a.head, S, ring, lastcol,
                                              best);
             else
-                wc_semi_sweep<G, true, false>(rq, qregs, rt, tregs, gend_reg, qlen, a.sc, a.head, S, ring, lastcol,
-                                              best);
+                wc_semi_sweep<G, true, false, FAST>(rq, qregs, rt, tregs, gend_reg, qlen, a.sc, a.head, S, ring,
+                                                    lastcol, best);
             /* rows up to the end of the first band that reached the forward score */
             const int r0 = gend_reg << 3;
             int r1 = min(tregs << 3, tlen);
@@ -730,7 +738,7 @@ __global__ void __launch_bounds__(128) dp_wc_semi_kernel(DpArgs a, const uint32_
 
 /* ---------------------------------------------------------------------- */
 
-template <int G, int ALGO, int START, bool SECOND>
+template <int G, int ALGO, int START, bool SECOND, bool FAST>
 __global__ void __launch_bounds__(128) dp_wc_kernel(DpArgs a, const uint32_t *list, int nlist, int ring_cols)
 {
     extern __shared__ uint32_t wc_smem[];
@@ -744,21 +752,29 @@ __global__ void __launch_bounds__(128) dp_wc_kernel(DpArgs a, const uint32_t *li
     uint32_t *ring = wc_smem + (size_t)slot * ring_cols;
     int *bandmax = (int *)(wc_smem + (size_t)gpb * ring_cols) + (size_t)slot * a.scratch_cols;
     const bool fast_scores = a.sc.match >= -128 && a.sc.match <= 127 && a.sc.mismatch >= -127 && a.sc.mismatch <= 128;
-    for (int item0 = blockIdx.x * gpb; item0 < nlist; item0 += gridDim.x * gpb) {
+    const int nl = a.n_dev ? min((int)*a.n_dev, nlist) : nlist;
+    for (int item0 = blockIdx.x * gpb; item0 < nl; item0 += gridDim.x * gpb) {
         if constexpr (G > 32) __syncthreads(); /* both warps are done with the previous pair */
         const int item = item0 + slot;
-        const bool has = item < nlist; /* the last warp may have groups without a pair */
-        const int i = has ? (int)list[item] : 0;
-        const int qlen = has ? (int)a.q_len[i] : 0, tlen = has ? (int)a.t_len[i] : 0;
-        const uint32_t *q = a.pq + (has ? (a.q_off[i] >> 3) : 0);
-        const uint32_t *t = a.pt + (has ? (a.t_off[i] >> 3) : 0);
+        const bool listed = item < nl; /* the last warp may have groups without a pair */
+        const int i = listed ? (int)list[item] : 0;
+        const int qlen0 = listed ? (int)a.q_len[i] : 0, tlen0 = listed ? (int)a.t_len[i] : 0;
+        const uint32_t *q = a.pq + (listed ? (a.q_off[i] >> 3) : 0);
+        const uint32_t *t = a.pt + (listed ? (a.t_off[i] >> 3) : 0);
+        /* FAST: this launch scores with the prmt table; a pair with another
+         * code or scores beyond a byte goes to the compare-scoring launch
+         * that follows (a.defer), and this launch skips it */
+        const bool plain_q = wc_plain<G>(q, (qlen0 + 7) >> 3); /* warp collectives: every lane calls both */
+        const bool plain_t = wc_plain<G>(t, (tlen0 + 7) >> 3);
+        const bool fast_pair = fast_scores && plain_q && plain_t;
+        const bool has = listed && (!FAST || fast_pair);
+        if (FAST && listed && !fast_pair && gl == 0) a.defer[atomicAdd(a.ndefer, 1u)] = (uint32_t)i;
+        const int qlen = has ? qlen0 : 0, tlen = has ? tlen0 : 0;
         const int qregs = (qlen + 7) >> 3, tregs = (tlen + 7) >> 3;
         WcScore S;
         S.local = ALGO == LOCAL_;
         S.tab = tab;
-        S.fast = fast_scores;
-        S.fast = wc_plain<G>(q, qregs) && S.fast;
-        S.fast = wc_plain<G>(t, tregs) && S.fast;
+        S.fast = fast_pair;
         uint4 *tb = nullptr;
         if (START == WITH_TB_ && has) {
             tb = a.tb + a.tb_off[i];
@@ -770,7 +786,7 @@ __global__ void __launch_bounds__(128) dp_wc_kernel(DpArgs a, const uint32_t *li
         WcRec best, sec;
         int gscore = 0;
         if (ALGO == GLOBAL_) {
-            wc_sweep<G, 2, START == WITH_TB_, false>(qf, qregs, tf, tregs, qlen, tlen, a.sc, S, ring, tb, 0,
+            wc_sweep<G, 2, START == WITH_TB_, false, FAST>(qf, qregs, tf, tregs, qlen, tlen, a.sc, S, ring, tb, 0,
                                                      bandmax, false, best, sec, gscore);
             /* the owner lane of the last band holds the score */
             gscore = grp_bcast<G>(gscore, (tregs - 1) & (G - 1));
@@ -778,7 +794,7 @@ __global__ void __launch_bounds__(128) dp_wc_kernel(DpArgs a, const uint32_t *li
             continue;
         }
         /* LOCAL forward (pass 1 also records per-band maxima for second best) */
-        wc_sweep<G, 0, START == WITH_TB_, false>(qf, qregs, tf, tregs, qlen, tlen, a.sc, S, ring, tb, 0, bandmax,
+        wc_sweep<G, 0, START == WITH_TB_, false, FAST>(qf, qregs, tf, tregs, qlen, tlen, a.sc, S, ring, tb, 0, bandmax,
                                                  SECOND, best, sec, gscore);
         best = rec_reduce<G>(best);
         WcRec secr = {0, 0x7fffffff, 0, 0};
@@ -800,8 +816,8 @@ __global__ void __launch_bounds__(128) dp_wc_kernel(DpArgs a, const uint32_t *li
             else __syncwarp();
             WcRec b2, s2;
             int g2 = 0;
-            wc_sweep<G, 0, false, true>(qf, qregs, tf, tregs, qlen, tlen, a.sc, S, ring, nullptr, 0, bandmax, false,
-                                        b2, s2, g2);
+            wc_sweep<G, 0, false, true, FAST>(qf, qregs, tf, tregs, qlen, tlen, a.sc, S, ring, nullptr, 0, bandmax,
+                                              false, b2, s2, g2);
             secr = rec_reduce<G>(s2);
         }
         int qs = 0, ts = 0;
@@ -815,7 +831,7 @@ __global__ void __launch_bounds__(128) dp_wc_kernel(DpArgs a, const uint32_t *li
             auto tr = [&](int T) { return nrev(t[gend_reg - 1 - T]); };
             WcRec bs, ss;
             int g3 = 0;
-            wc_sweep<G, 1, false, false>(qr, sweep ? rend_reg : 0, tr, sweep ? gend_reg : 0, 0, 0, a.sc, S, ring,
+            wc_sweep<G, 1, false, false, FAST>(qr, sweep ? rend_reg : 0, tr, sweep ? gend_reg : 0, 0, 0, a.sc, S, ring,
                                          nullptr, best.v, bandmax, false, bs, ss, g3);
             bs = rec_reduce<G>(bs);
             if (sweep) {
@@ -833,8 +849,8 @@ __global__ void __launch_bounds__(128) dp_wc_kernel(DpArgs a, const uint32_t *li
                         if (threadIdx.x < 32) {
                             WcRec b2, s2;
                             int g4 = 0;
-                            wc_sweep<32, 1, false, false>(qr, rend_reg, tr, gend_reg, 0, 0, a.sc, S, ring, nullptr,
-                                                          best.v, bandmax, false, b2, s2, g4);
+                            wc_sweep<32, 1, false, false, FAST>(qr, rend_reg, tr, gend_reg, 0, 0, a.sc, S, ring,
+                                                                nullptr, best.v, bandmax, false, b2, s2, g4);
                             b2 = rec_reduce<32>(b2);
                             const int gidx = (gend_reg << 3) - 1 - (b2.band << 3);
                             ts = gidx + (b2.row - (b2.band << 3));
@@ -893,32 +909,43 @@ size_t wc_smem_bytes(int algo, int group, int warps, int max_q8, int max_t8)
 }
 
 /* one kernel instantiation per (group, algo, start, second best) */
-template <int G, class F> static cudaError_t with_wc_kernel(int algo, int start, bool second, F &&f)
+template <int G, bool FAST, class F> static cudaError_t with_wc_kernel(int algo, int start, bool second, F &&f)
 {
     if (algo == SEMI_GLOBAL_) {
         if (start == WITH_START_)
-            return second ? f(dp_wc_semi_kernel<G, true, true>) : f(dp_wc_semi_kernel<G, false, true>);
-        return second ? f(dp_wc_semi_kernel<G, true, false>) : f(dp_wc_semi_kernel<G, false, false>);
+            return second ? f(dp_wc_semi_kernel<G, true, true, FAST>) : f(dp_wc_semi_kernel<G, false, true, FAST>);
+        return second ? f(dp_wc_semi_kernel<G, true, false, FAST>) : f(dp_wc_semi_kernel<G, false, false, FAST>);
     }
     if (algo == GLOBAL_)
-        return start == WITH_TB_ ? f(dp_wc_kernel<G, GLOBAL_, WITH_TB_, false>)
-                                 : f(dp_wc_kernel<G, GLOBAL_, WITHOUT_START_, false>);
+        return start == WITH_TB_ ? f(dp_wc_kernel<G, GLOBAL_, WITH_TB_, false, FAST>)
+                                 : f(dp_wc_kernel<G, GLOBAL_, WITHOUT_START_, false, FAST>);
     if (algo == LOCAL_) {
         if (start == WITH_START_)
-            return second ? f(dp_wc_kernel<G, LOCAL_, WITH_START_, true>) : f(dp_wc_kernel<G, LOCAL_, WITH_START_, false>);
+            return second ? f(dp_wc_kernel<G, LOCAL_, WITH_START_, true, FAST>)
+                          : f(dp_wc_kernel<G, LOCAL_, WITH_START_, false, FAST>);
         if (start == WITH_TB_)
-            return second ? f(dp_wc_kernel<G, LOCAL_, WITH_TB_, true>) : f(dp_wc_kernel<G, LOCAL_, WITH_TB_, false>);
-        return second ? f(dp_wc_kernel<G, LOCAL_, WITHOUT_START_, true>)
-                      : f(dp_wc_kernel<G, LOCAL_, WITHOUT_START_, false>);
+            return second ? f(dp_wc_kernel<G, LOCAL_, WITH_TB_, true, FAST>)
+                          : f(dp_wc_kernel<G, LOCAL_, WITH_TB_, false, FAST>);
+        return second ? f(dp_wc_kernel<G, LOCAL_, WITHOUT_START_, true, FAST>)
+                      : f(dp_wc_kernel<G, LOCAL_, WITHOUT_START_, false, FAST>);
     }
     return cudaErrorInvalidValue;
 }
-template <class F> static cudaError_t with_wc_kernel(int group, int algo, int start, bool second, F &&f)
+/* fast: the table-scoring kernels (the ones that run nearly every pair) */
+template <class F>
+static cudaError_t with_wc_kernel(int group, int algo, int start, bool second, F &&f, bool fast = true)
 {
-    if (group == 64) return with_wc_kernel<64>(algo, start, second, f);
-    if (group == 8) return with_wc_kernel<8>(algo, start, second, f);
-    if (group == 16) return with_wc_kernel<16>(algo, start, second, f);
-    if (group == 32) return with_wc_kernel<32>(algo, start, second, f);
+    if (fast) {
+        if (group == 64) return with_wc_kernel<64, true>(algo, start, second, f);
+        if (group == 8) return with_wc_kernel<8, true>(algo, start, second, f);
+        if (group == 16) return with_wc_kernel<16, true>(algo, start, second, f);
+        if (group == 32) return with_wc_kernel<32, true>(algo, start, second, f);
+    } else {
+        if (group == 64) return with_wc_kernel<64, false>(algo, start, second, f);
+        if (group == 8) return with_wc_kernel<8, false>(algo, start, second, f);
+        if (group == 16) return with_wc_kernel<16, false>(algo, start, second, f);
+        if (group == 32) return with_wc_kernel<32, false>(algo, start, second, f);
+    }
     return cudaErrorInvalidValue;
 }
 
@@ -1007,7 +1034,8 @@ size_t wc_scratch_words(int algo, const WcLaunch &l, int max_t8)
 }
 
 cudaError_t launch_dp_wc(int algo, int start, bool second, const DpArgs &a, const uint32_t *list, int nlist,
-                         int max_q8, int max_t8, const WcLaunch &l, int32_t *rows, cudaStream_t s)
+                         int max_q8, int max_t8, const WcLaunch &l, int32_t *rows, uint32_t *defer, uint32_t *ndefer,
+                         cudaStream_t s)
 {
     if (nlist <= 0) return cudaSuccess;
     if (l.group == 0) return cudaErrorInvalidValue;
@@ -1019,12 +1047,29 @@ cudaError_t launch_dp_wc(int algo, int start, bool second, const DpArgs &a, cons
         b.scratch_cols = (uint32_t)(max_t8 / 8 + 1); /* band maxima per group */
     }
     const int ring_cols = max_q8;
-    return with_wc_kernel(l.group, algo, start, second, [&](auto k) {
-        cudaError_t e = allow_dyn_smem(k);
-        if (e != cudaSuccess) return e;
-        k<<<l.blocks, 32 * l.warps, l.smem, s>>>(b, list, nlist, ring_cols);
-        return cudaGetLastError();
-    });
+    auto launch = [&](const DpArgs &args, const uint32_t *lst, int blocks, bool fast) {
+        return with_wc_kernel(l.group, algo, start, second, [&](auto k) {
+            cudaError_t e = allow_dyn_smem(k);
+            if (e != cudaSuccess) return e;
+            k<<<blocks, 32 * l.warps, l.smem, s>>>(args, lst, nlist, ring_cols);
+            return cudaGetLastError();
+        }, fast);
+    };
+    const bool byte_scores = a.sc.match >= -128 && a.sc.match <= 127 && a.sc.mismatch >= -127 && a.sc.mismatch <= 128;
+    if (!byte_scores || !defer || !ndefer) return launch(b, list, l.blocks, false);
+    /* the table-scoring launch, then the compare-scoring one over the pairs
+     * it left (usually none: its grid only checks an empty count) */
+    cudaError_t e = cudaMemsetAsync(ndefer, 0, sizeof(uint32_t), s);
+    if (e != cudaSuccess) return e;
+    b.defer = defer, b.ndefer = ndefer, b.n_dev = nullptr;
+    e = launch(b, list, l.blocks, true);
+    if (e != cudaSuccess) return e;
+    DpArgs c = b;
+    c.defer = nullptr, c.ndefer = nullptr, c.n_dev = ndefer;
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    return launch(c, defer, l.blocks < sms ? l.blocks : sms, false);
 }
 
 } // namespace gb

@@ -271,6 +271,7 @@ int plan_batch(const RunCfg &cfg, const DevBatch &b, const DevOut &o, Workspace 
             const size_t rows = std::max(wc_scratch_words(cfg.algo, p.wc, (int)((max_t_long + 7) & ~7u)),
                                          wc_scratch_words(cfg.algo, p.wc_big, (int)((max_t_big + 7) & ~7u)));
             if (rows > 0 && grow((void **)&ws.wc_rows, &ws.wc_rows_cap, rows, 4) != GB_OK) return GB_ERR_ALLOC;
+            if (grow((void **)&ws.wc_defer, &ws.wc_defer_cap, (size_t)nlong, 4) != GB_OK) return GB_ERR_ALLOC;
         }
     }
     if (!p.use_wc) {
@@ -524,12 +525,13 @@ static int launch_dp_split(int algo, int start, bool second, const Plan &p, DpAr
         GB_CUDA(cudaEventRecord(ws.fork, s));
         GB_CUDA(cudaStreamWaitEvent(ws.aux, ws.fork, 0));
         timing_mark(K_DP, true, ws.aux);
+        /* queue words 12 and 13: the two launches' counts of pairs left to compare scoring */
         if (nbig > 0)
             GB_CUDA(launch_dp_wc(algo, start, second, a, order, nbig, p.mq8_big, p.mt8_big, p.wc_big, ws.wc_rows,
-                                 ws.aux));
+                                 ws.wc_defer, ws.queue + 12, ws.aux));
         if (nlong > nbig)
             GB_CUDA(launch_dp_wc(algo, start, second, a, order + nbig, nlong - nbig, p.mq8, p.mt8, p.wc, ws.wc_rows,
-                                 ws.aux));
+                                 ws.wc_defer, ws.queue + 13, ws.aux));
         timing_mark(K_DP, false, ws.aux);
         GB_CUDA(cudaEventRecord(ws.join, ws.aux));
         DpArgs rest = a;

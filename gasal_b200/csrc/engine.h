@@ -67,6 +67,8 @@ struct Workspace {
     size_t order_cap = 0;
     int32_t *wc_rows = nullptr;  /* warp-cooperative SEMI_GLOBAL last-column rows */
     size_t wc_rows_cap = 0;
+    uint32_t *wc_defer = nullptr; /* pairs the table-scoring warp-cooperative launch leaves to compare scoring */
+    size_t wc_defer_cap = 0;
     uint32_t *order2 = nullptr;  /* visiting order of the separate start passes */
     size_t order2_cap = 0;
     uint32_t *bins = nullptr;    /* order_bins() class counters */

@@ -57,6 +57,8 @@ struct DpArgs {
                                            one slot of scratch_cols words per lane group of the grid */
     int32_t *max_off;                   /* unbanded ksw: largest |column - row| of the cells where the
                                            running maximum rose (ksw_extend2's max_off), or null */
+    uint32_t *defer, *ndefer;           /* warp-cooperative table-scoring launch: pairs it leaves to the
+                                           compare-scoring launch, and their count */
 };
 
 /* Shape of one warp-cooperative launch: lanes per pair (0: it cannot run),
@@ -120,9 +122,13 @@ cudaError_t launch_start_order(const uint32_t *q_len, const int32_t *q_end, cons
 /* warp-cooperative DP (dp_wc.cu) for the pairs listed in `list`: LOCAL,
  * GLOBAL and target-tail SEMI_GLOBAL, each pair on `l.group` lanes (32, 16
  * or 8; queries of at least that many words); `rows`: SEMI_GLOBAL's
- * last-column scratch of wc_scratch_words(...) words */
+ * last-column scratch of wc_scratch_words(...) words.  With `defer` (nlist
+ * words) and `ndefer` (one word) the pairs run on the kernels that score with
+ * the prmt table, and the few they cannot (codes outside A/C/G/T/N, scores
+ * beyond a byte) on the compare-scoring kernels after them. */
 cudaError_t launch_dp_wc(int algo, int start, bool second, const DpArgs &a, const uint32_t *list, int nlist,
-                         int max_q8, int max_t8, const WcLaunch &l, int32_t *rows, cudaStream_t s);
+                         int max_q8, int max_t8, const WcLaunch &l, int32_t *rows, uint32_t *defer, uint32_t *ndefer,
+                         cudaStream_t s);
 /* dynamic shared memory of one warp-cooperative block */
 size_t wc_smem_bytes(int algo, int group, int warps, int max_q8, int max_t8);
 /* launch shape for nlist pairs: the forced group, or (forced_group 0) the

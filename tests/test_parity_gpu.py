@@ -247,3 +247,33 @@ def test_wc_semi_global_scores_and_open_forms():
     for sc in (dict(match=2, mismatch=3, gap_open=5, gap_extend=2), dict(gap_open=0, gap_extend=2),
                dict(gap_open=-1, gap_extend=3)):
         _vs_oracle(Params(algo=SEMI_GLOBAL, head=TARGET, tail=TARGET, start_pos=WITH_START, second_best=1, **sc), b)
+
+
+def test_wc_table_and_compare_scoring_split():
+    """Long pairs on the warp-cooperative kernels, a fifth of them with IUPAC
+    codes outside A/C/G/T/N: those leave the table-scoring launch for the
+    compare-scoring one that follows it, in the same warps as plain pairs.
+    LOCAL (start and traceback), GLOBAL traceback and target-tail
+    SEMI_GLOBAL against the oracle; then scores beyond a byte, where every
+    pair takes the compare path."""
+    rng = np.random.default_rng(47)
+    from gasal_b200.capi import Batch
+    qs, ts = [], []
+    for k in range(2600):
+        q = bytearray(rng.choice(list(b"ACGT"), size=int(rng.integers(260, 900))).tolist())
+        t = bytearray(q)
+        for _ in range(int(rng.integers(0, 10))):
+            a = int(rng.integers(0, len(t)))
+            t[a] = int(rng.choice(list(b"ACGT")))
+        if k % 5 == 3:
+            q[int(rng.integers(0, len(q)))] = ord("R")
+        if k % 7 == 4:
+            t[int(rng.integers(0, len(t)))] = ord("Y")
+        qs.append(bytes(q))
+        ts.append(bytes(t) + bytes(rng.choice(list(b"ACGT"), size=int(rng.integers(0, 40))).tolist()))
+    b = Batch.from_seqs(qs, ts)
+    for p in (Params(algo=LOCAL, start_pos=WITH_START), Params(algo=LOCAL, start_pos=WITH_TB),
+              Params(algo=GLOBAL, start_pos=WITH_TB),
+              Params(algo=SEMI_GLOBAL, start_pos=WITH_START, head=TARGET, tail=TARGET)):
+        _vs_oracle(p, b)
+    _vs_oracle(Params(algo=LOCAL, start_pos=WITH_START, match=200, mismatch=150, gap_open=300, gap_extend=20), b)
