@@ -76,19 +76,25 @@ print(json.dumps(out))
 """
 
 
-@pytest.mark.parametrize("k", [0, 1, 2, 3, 5, 8])
-def test_injected_allocation_failure_is_reported_and_recovered(k):
-    env = dict(os.environ, GASAL_B200_FAIL_ALLOC_AFTER=str(k))
-    r = subprocess.run([sys.executable, "-c", CHILD, ROOT], env=env, capture_output=True, text=True, timeout=600)
-    assert r.returncode == 0, r.stderr[-3000:]
-    res = json.loads(r.stdout.strip().splitlines()[-1])
-    firsts = [v["first"] for v in res.values()]
-    # exactly one failure is injected per process: at most one launch reports it
-    assert sum(f != "ok" for f in firsts) <= 1, res
-    for f in firsts:
-        assert f == "ok" or "allocation failed" in f, res
-    if k == 0:
-        # the first allocation of the first launch (its work-queue word) has no smaller retry
-        assert firsts[0] != "ok", f"the first launch's first allocation failure went unreported: {res}"
-    for name, v in res.items():
-        assert not v["mismatched"], f"{name} after the injected failure: {v}"
+def test_injected_allocation_failure_is_reported_and_recovered():
+    """For k in 0, 1, 2, 3, 5, 8: the (k+1)-th device allocation fails once.
+    Whatever k hits -- a buffer the engine retries at its exact size, or one
+    it cannot do without -- the call either succeeds or reports the
+    allocation failure, and the retried call gives the oracle's results.  At
+    least one k must hit an allocation whose failure is reported."""
+    reported = 0
+    for k in (0, 1, 2, 3, 5, 8):
+        env = dict(os.environ, GASAL_B200_FAIL_ALLOC_AFTER=str(k))
+        r = subprocess.run([sys.executable, "-c", CHILD, ROOT], env=env, capture_output=True, text=True,
+                           timeout=600)
+        assert r.returncode == 0, r.stderr[-3000:]
+        res = json.loads(r.stdout.strip().splitlines()[-1])
+        firsts = [v["first"] for v in res.values()]
+        # exactly one failure is injected per process: at most one launch reports it
+        assert sum(f != "ok" for f in firsts) <= 1, (k, res)
+        for f in firsts:
+            assert f == "ok" or "allocation failed" in f, (k, res)
+        reported += sum(f != "ok" for f in firsts)
+        for name, v in res.items():
+            assert not v["mismatched"], f"k={k} {name} after the injected failure: {v}"
+    assert reported >= 1, "no injected failure was reported"

@@ -254,8 +254,8 @@ def test_wc_table_and_compare_scoring_split():
     codes outside A/C/G/T/N: those leave the table-scoring launch for the
     compare-scoring one that follows it, in the same warps as plain pairs.
     LOCAL (start and traceback), GLOBAL traceback and target-tail
-    SEMI_GLOBAL against the oracle; then scores beyond a byte, where every
-    pair takes the compare path."""
+    SEMI_GLOBAL against the oracle; then a mismatch penalty beyond a byte,
+    where every pair takes the compare path."""
     rng = np.random.default_rng(47)
     from gasal_b200.capi import Batch
     qs, ts = [], []
@@ -276,4 +276,7 @@ def test_wc_table_and_compare_scoring_split():
               Params(algo=GLOBAL, start_pos=WITH_TB),
               Params(algo=SEMI_GLOBAL, start_pos=WITH_START, head=TARGET, tail=TARGET)):
         _vs_oracle(p, b)
-    _vs_oracle(Params(algo=LOCAL, start_pos=WITH_START, match=200, mismatch=150, gap_open=300, gap_extend=20), b)
+    # a mismatch penalty beyond a byte (scores stay far inside the 16-bit row buffer)
+    _vs_oracle(Params(algo=LOCAL, start_pos=WITH_START, match=1, mismatch=200, gap_open=6, gap_extend=1), b)
+    _vs_oracle(Params(algo=SEMI_GLOBAL, start_pos=WITH_START, head=TARGET, tail=TARGET, match=1, mismatch=200,
+                      gap_open=6, gap_extend=1), b)
