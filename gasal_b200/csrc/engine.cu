@@ -215,7 +215,16 @@ int plan_batch(const RunCfg &cfg, const DevBatch &b, const DevOut &o, Workspace 
     p.block = st.block;
 
     /* split: long LOCAL/GLOBAL (and target-tail SEMI_GLOBAL) pairs go warp-cooperative */
-    const bool wc_algo = cfg.algo == LOCAL_ || cfg.algo == GLOBAL_ || (cfg.algo == SEMI_GLOBAL_ && cfg.tail == TARGET_);
+    bool wc_algo = cfg.algo == LOCAL_ || cfg.algo == GLOBAL_ || (cfg.algo == SEMI_GLOBAL_ && cfg.tail == TARGET_);
+    if (wc_algo && cfg.start != WITHOUT_START_ && cfg.sc.match > 0) {
+        /* start passes and tracebacks of pairs whose scores can leave the
+         * 16-bit row buffer (match * min(qlen, tlen) >= 2^15) stay on the
+         * one-pair-per-thread kernel: the warp-cooperative start sweep's stop
+         * test does not follow the reference once values wrap */
+        uint32_t longest = 0;
+        for (int i = 0; i < b.n; i++) longest = std::max(longest, std::min(b.h_q_len[i], b.h_t_len[i]));
+        if ((uint64_t)cfg.sc.match * longest >= (1u << 15)) wc_algo = false;
+    }
     uint32_t max_q_short = 0, max_q_long = 0, max_t_long = 0, max_q_big = 0, max_t_big = 0;
     int nlong = 0, nbig = 0;
     const uint32_t big_q = ORDER_CAP_WORDS * 8 - 7;

@@ -276,6 +276,10 @@ def test_wc_table_and_compare_scoring_split():
               Params(algo=GLOBAL, start_pos=WITH_TB),
               Params(algo=SEMI_GLOBAL, start_pos=WITH_START, head=TARGET, tail=TARGET)):
         _vs_oracle(p, b)
+    # scores that leave the 16-bit row buffer (match 200 on 260-900 bp): the start passes and
+    # tracebacks of such a batch run on the one-pair-per-thread kernel
+    big = Params(algo=LOCAL, start_pos=WITH_START, match=200, mismatch=150, gap_open=300, gap_extend=20)
+    _vs_oracle(big, b)
     # a mismatch penalty beyond a byte (scores stay far inside the 16-bit row buffer)
     _vs_oracle(Params(algo=LOCAL, start_pos=WITH_START, match=1, mismatch=200, gap_open=6, gap_extend=1), b)
     _vs_oracle(Params(algo=SEMI_GLOBAL, start_pos=WITH_START, head=TARGET, tail=TARGET, match=1, mismatch=200,
