@@ -474,6 +474,66 @@ def prep_bandwidth(torch, gl, dparts, hbm_gbs, reps=20):
     return out
 
 
+def mixed_leg(torch, gl, parts, dparts, dev, args, dist, job_pairs, value):
+    """The same step through the per-pair mixed dispatch: the workload's
+    launches as ONE batch whose pairs each name their kind (interleaved at
+    random), one gb_align_dev_mixed call per step, inputs resident; every
+    output compared with the per-launch step's."""
+    from gasal_b200 import shard
+    kinds, b, kind, idx = W.concat_parts(parts, shuffle_seed=11)
+    qb = np.cumsum([0] + [int(pb.q.shape[0]) for _, pb in parts])
+    d = DevPart(torch, kinds[0], b, dev)
+    for k in ("score2", "q_end2", "t_end2"):
+        d.map["out_" + k] = d.outs[k].data_ptr()
+    stream = torch.cuda.Stream(device=dev)
+    host_ms = []
+
+    def step():
+        h0 = time.perf_counter()
+        gl.align_dev_mixed(kinds, kind, d.map, b.q_len, b.t_len, stream.cuda_stream)
+        host_ms.append((time.perf_counter() - h0) * 1e3)
+
+    warm, steps = 2, max(1, min(args.steps, 3))
+    for _ in range(warm):
+        step()
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(steps):
+        step()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = shard.max_over_ranks(e0.elapsed_time(e1), dist, dev)
+    same = True
+    for k, kp in enumerate(dparts):
+        rows = torch.from_numpy(np.nonzero(kind == k)[0]).to(dev)
+        src = torch.from_numpy(idx[kind == k]).to(dev)
+        for f, t in kp.fields().items():
+            mine = d.ncig if f == "n_cigar" else d.outs[f]
+            same &= bool(torch.equal(mine[rows], t[src]))
+        if kp.p.start_pos == WITH_TB and kp.p.algo in (LOCAL, GLOBAL):
+            lens = kp.ncig.cpu().numpy().astype(np.int64)
+            starts = kp.b.q_off.astype(np.int64)
+            pos = np.repeat(starts, lens) + (np.arange(int(lens.sum())) - np.repeat(np.cumsum(lens) - lens, lens))
+            pos_t = torch.from_numpy(pos).to(dev)
+            same &= bool(torch.equal(kp.cigar[pos_t], d.cigar[pos_t + int(qb[k])]))
+    del d
+    torch.cuda.empty_cache()
+    v = job_pairs * steps / (ms * 1e-3)
+    return {"value": v, "unit": UNIT, "ms_per_step": ms / steps, "steps": steps, "warmup": warm,
+            "value_over_per_launch": v / value, "bit_exact_vs_per_launch": same,
+            "host_ms_per_call": float(np.median(host_ms)),
+            "host_ms_note": "wall time of the call on the host, including its waits for buffers the previous "
+                            "call's work still reads (the per-launch calls wait the same way)",
+            "kinds": [p.key() for p in kinds],
+            "path": "gb_align_dev_mixed: one call per step over one batch of every launch's pairs, kind per pair "
+                    "(seeded random interleave); packed once, each kind on a forked stream, results scattered "
+                    "back per pair"}
+
+
 def e2e_leg(torch, gl, parts, args, dev, dist, job_pairs):
     """The storage API with host buffers: per step, every launch's pinned batch
     goes host->device, aligns, and every result array comes back."""
@@ -585,6 +645,9 @@ def main():
     ap.add_argument("--tb-priority", default="off", choices=["on", "off"],
                     help="kernel-level step: run WITH_TB launches on the highest-priority stream (measured slower "
                          "on w4: the prioritised launch finishes early and the others then run on alone)")
+    ap.add_argument("--mixed", default="on", choices=["on", "off"],
+                    help="workloads of several launches: time the same step again as one per-pair mixed-dispatch "
+                         "call (gb_align_dev_mixed) and compare its outputs with the per-launch step's")
     ap.add_argument("--split", default="weak", choices=["weak", "cells"],
                     help="N>1: weak = every rank aligns its own full-size seeded shard; cells = the ranks split one "
                          "workload into contiguous slices of equal DP cells (strong scaling)")
@@ -664,6 +727,11 @@ def main():
     launches = sum(n * gl.KERNELS_PER_MARK[k] for k, (_, n) in kt.items())
 
     prep = prep_bandwidth(torch, gl, dparts, hbm)
+
+    # ---------------- the same step through the per-pair mixed dispatch ----------------
+    mixed = None
+    if len(parts) > 1 and args.mixed == "on":
+        mixed = mixed_leg(torch, gl, parts, dparts, dev, args, dist, job_pairs, value)
 
     kpart = next((d for d in dparts if d.p.algo == KSW), None)
     if kpart is not None:
@@ -747,6 +815,7 @@ def main():
             "clocks": clk.summary(),
             "band": band_info,
             "plain": plain,
+            "mixed": mixed,
         }
         print(json.dumps(line), flush=True)
     if model is not None:

@@ -94,6 +94,9 @@ SIGNATURES = {
     "gb_revcomp_dev": (C.c_int, [C.c_void_p] * 8 + [C.c_int32, C.c_void_p]),
     "gb_align_dev_noalloc": (C.c_int, [C.POINTER(GbParams), C.POINTER(GbDevBatch), C.POINTER(GbDevOut),
                                        C.c_void_p]),
+    "gb_align_dev_mixed": (C.c_int, [C.POINTER(GbParams), C.c_int, C.c_void_p, C.POINTER(GbDevBatch),
+                                     C.POINTER(GbDevOut), C.c_void_p]),
+    "gb_mixed_check": (C.c_int, [C.POINTER(GbParams), C.c_int, C.c_void_p, C.c_int32, C.c_int, C.c_void_p]),
     "gb_set_reference_reverse": (C.c_int, [C.c_int]),
     "gb_set_reference_max_query_len": (C.c_int, [C.c_int]),
     "gb_set_tb_budget_mb": (C.c_int, [C.c_int64]),
@@ -416,6 +419,40 @@ def align_dev(p: Params, dev: dict, h_q_len: np.ndarray, h_t_len: np.ndarray, st
     else:
         _check(lib().gb_align_dev(C.byref(cp), C.byref(b), C.byref(o), C.c_void_p(stream_handle)),
                "gb_align_dev")
+
+
+MIXED_MAX_KINDS = 8
+
+
+def _kinds_c(kinds):
+    if not 1 <= len(kinds) <= MIXED_MAX_KINDS:
+        raise GasalError(f"mixed dispatch takes 1..{MIXED_MAX_KINDS} kinds, got {len(kinds)}")
+    arr = (GbParams * len(kinds))()
+    for j, k in enumerate(kinds):
+        arr[j] = k.to_c()
+    return arr
+
+
+def mixed_check(kinds, h_kind: np.ndarray, has_seed: bool = True) -> np.ndarray:
+    """gb_mixed_check: the argument check of align_dev_mixed (no GPU needed);
+    returns the pairs of each kind."""
+    h_kind = np.ascontiguousarray(h_kind, dtype=np.uint8)
+    arr = _kinds_c(kinds)
+    counts = np.zeros(len(kinds), dtype=np.uint32)
+    _check(lib().gb_mixed_check(arr, len(kinds), _ptr(h_kind), int(h_kind.shape[0]), int(bool(has_seed)),
+                                _ptr(counts)), "gb_mixed_check")
+    return counts
+
+
+def align_dev_mixed(kinds, h_kind: np.ndarray, dev: dict, h_q_len: np.ndarray, h_t_len: np.ndarray,
+                    stream_handle: int = 0):
+    """gb_align_dev_mixed: pair i of the device batch (same ``dev`` map as
+    align_dev) aligned under kinds[h_kind[i]]; the kinds run concurrently."""
+    h_kind = np.ascontiguousarray(h_kind, dtype=np.uint8)
+    b, o = _dev_structs(dev, h_q_len, h_t_len)
+    arr = _kinds_c(kinds)
+    _check(lib().gb_align_dev_mixed(arr, len(kinds), _ptr(h_kind), C.byref(b), C.byref(o),
+                                    C.c_void_p(stream_handle)), "gb_align_dev_mixed")
 
 
 class Streams:

@@ -160,3 +160,38 @@ def workload4(n=10_000_000, seed=SEED_BASE + 4) -> List[Tuple[Params, Batch]]:
 
 def generator_threads() -> int:
     return int(_gen().gbw_threads())
+
+
+def concat_parts(parts, shuffle_seed=None):
+    """One batch holding every pair of [(Params, Batch)] parts, for the mixed
+    dispatch (gb_align_dev_mixed): returns (kinds, batch, kind, index_in_part),
+    kind[j] being the part pair j comes from.  Sequence bytes are laid out part after part; the pair
+    entries (offsets, lengths, ops, seeds, kind) are in part order, or in a
+    seeded random order when shuffle_seed is given -- GASAL2's offsets may
+    point anywhere in the batch, so the pairs of different kinds interleave
+    without moving bytes.  Seeds are 0 for parts without them."""
+    kinds = [p for p, _ in parts]
+    qb = np.cumsum([0] + [int(b.q.shape[0]) for _, b in parts])
+    tb = np.cumsum([0] + [int(b.t.shape[0]) for _, b in parts])
+    part_of = np.concatenate([np.full(b.n, k, dtype=np.uint8) for k, (_, b) in enumerate(parts)])
+    index_in = np.concatenate([np.arange(b.n, dtype=np.int64) for _, b in parts])
+    q_off = np.concatenate([b.q_off.astype(np.uint64) + qb[k] for k, (_, b) in enumerate(parts)])
+    t_off = np.concatenate([b.t_off.astype(np.uint64) + tb[k] for k, (_, b) in enumerate(parts)])
+    if q_off.size and (q_off.max() >= 2**32 or t_off.max() >= 2**32):
+        raise ValueError("the combined batch exceeds 32-bit byte offsets")
+    q_len = np.concatenate([b.q_len for _, b in parts])
+    t_len = np.concatenate([b.t_len for _, b in parts])
+    has_ops = any(b.q_op is not None for _, b in parts)
+    q_op = np.concatenate([b.q_op if b.q_op is not None else np.zeros(b.n, np.uint8) for _, b in parts]) \
+        if has_ops else None
+    t_op = np.concatenate([b.t_op if b.t_op is not None else np.zeros(b.n, np.uint8) for _, b in parts]) \
+        if has_ops else None
+    seed = np.concatenate([b.seed if b.seed is not None else np.zeros(b.n, np.uint32) for _, b in parts])
+    order = np.arange(part_of.shape[0])
+    if shuffle_seed is not None:
+        order = np.random.default_rng(shuffle_seed).permutation(part_of.shape[0])
+    pick = lambda a: None if a is None else np.ascontiguousarray(a[order])
+    batch = Batch(q=np.concatenate([b.q for _, b in parts]), t=np.concatenate([b.t for _, b in parts]),
+                  q_off=pick(q_off).astype(np.uint32), t_off=pick(t_off).astype(np.uint32),
+                  q_len=pick(q_len), t_len=pick(t_len), q_op=pick(q_op), t_op=pick(t_op), seed=pick(seed))
+    return kinds, batch, pick(part_of), pick(index_in)

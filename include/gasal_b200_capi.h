@@ -206,6 +206,27 @@ int gb_revcomp_dev(uint32_t *pq, uint32_t *pt, const uint32_t *q_off, const uint
  * nothing, as gb_align_dev does. */
 int gb_align_dev_noalloc(const gb_params_t *p, const gb_dev_batch_t *b, const gb_dev_out_t *o, void *stream);
 
+/* Per-pair mixed-algorithm dispatch (an extension: GASAL2 takes one algorithm
+ * per launch, Parameters::algo, reference src/gasal_align.cu:249 and
+ * src/gasal_align.h:89-107).  Pair i of the device batch is aligned under
+ * kinds[h_kind[i]] (h_kind: host array of b->n bytes, each < n_kinds <=
+ * GB_MIXED_MAX_KINDS), with the same results gb_align_dev gives that pair
+ * under those options.  The batch is packed once; each kind then runs on its
+ * own stream, forked from `stream` and joined back before the call's last
+ * operation, so the kinds overlap.  Result arrays a pair's kind does not
+ * produce keep their values; CIGAR bytes land at each pair's query offset.
+ * KSW kinds need b->seed.  n == 0 returns GB_OK and launches nothing.  Calls
+ * on one stream must come from one host thread at a time. */
+#define GB_MIXED_MAX_KINDS 8
+int gb_align_dev_mixed(const gb_params_t *kinds, int n_kinds, const uint8_t *h_kind, const gb_dev_batch_t *b,
+                       const gb_dev_out_t *o, void *stream);
+/* The argument check of gb_align_dev_mixed alone (no CUDA call): GB_OK, with
+ * the pairs of each kind in counts[0..n_kinds) when counts is not NULL, or
+ * GB_ERR_ARG (kind index out of range, too many kinds, unknown algorithm, a
+ * KSW kind with pairs but has_seed 0). */
+int gb_mixed_check(const gb_params_t *kinds, int n_kinds, const uint8_t *h_kind, int32_t n, int has_seed,
+                   uint32_t *counts);
+
 /* Forward CIGAR text on the device (no counterpart in the reference
  * library; its test program decodes on the host, test_prog/test_prog.cpp:
  * 382-428).  Input: the traceback's run-length bytes (count << 2 | op, last
