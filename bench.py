@@ -56,7 +56,7 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 from gasal_b200 import workloads as W  # noqa: E402
-from gasal_b200.capi import LOCAL, GLOBAL, SEMI_GLOBAL, KSW, WITH_TB, Params  # noqa: E402
+from gasal_b200.capi import LOCAL, GLOBAL, SEMI_GLOBAL, KSW, WITH_TB, Params, has_cigar  # noqa: E402
 
 UNIT = "pairs/s"
 # integer ops per computed cell, per algorithm (+4 with traceback)
@@ -278,7 +278,7 @@ class DevPart:
         from gasal_b200.capi import Outputs
         names = Outputs.fields_for(None, self.p)
         d = {k: self.outs[k] for k in names}
-        if self.p.start_pos == WITH_TB and self.p.algo in (LOCAL, GLOBAL):
+        if has_cigar(self.p):
             d["n_cigar"] = self.ncig
         return d
 
@@ -353,7 +353,7 @@ def outputs_equal(torch, a_parts, b_parts, a_idx=None):
             if sel is not None:
                 ta = ta.index_select(0, sel)
             bad += int((ta != tb_).sum().item())
-        if b.p.start_pos == WITH_TB and b.p.algo in (LOCAL, GLOBAL):
+        if has_cigar(b.p):
             ia = None if a_idx is None else a_idx[k]
             nb = b.ncig.cpu().numpy()
             na = a.ncig.cpu().numpy() if ia is None else a.ncig.cpu().numpy()[ia]
@@ -514,7 +514,7 @@ def mixed_leg(torch, gl, parts, dparts, dev, args, dist, job_pairs, value):
         for f, t in kp.fields().items():
             mine = d.ncig if f == "n_cigar" else d.outs[f]
             same &= bool(torch.equal(mine[rows], t[src]))
-        if kp.p.start_pos == WITH_TB and kp.p.algo in (LOCAL, GLOBAL):
+        if has_cigar(kp.p):
             lens = kp.ncig.cpu().numpy().astype(np.int64)
             starts = kp.b.q_off.astype(np.int64)
             pos = np.repeat(starts, lens) + (np.arange(int(lens.sum())) - np.repeat(np.cumsum(lens) - lens, lens))

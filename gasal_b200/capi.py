@@ -168,6 +168,12 @@ class Batch:
 OUT_FIELDS = ("score", "q_end", "t_end", "q_start", "t_start", "score2", "q_end2", "t_end2")
 
 
+def has_cigar(p: Params) -> bool:
+    """Whether a launch with these options writes CIGARs: LOCAL and GLOBAL
+    WITH_TB, and (an extension) target-tail SEMI_GLOBAL WITH_TB."""
+    return p.start_pos == WITH_TB and (p.algo in (LOCAL, GLOBAL) or (p.algo == SEMI_GLOBAL and p.tail == TARGET))
+
+
 class Outputs:
     """Host arrays for every result a launch can produce."""
 
@@ -189,19 +195,24 @@ class Outputs:
         f = ["score"]
         if p.algo == GLOBAL:
             pass
-        elif p.algo == KSW or p.algo == BANDED:
+        elif p.algo == KSW:
             f += ["q_end", "t_end"]
+        elif p.algo == BANDED:
+            f += ["q_end", "t_end"]
+            if p.start_pos == WITH_START:  # an extension: the reference's banded kernel has no start
+                f += ["q_start", "t_start"]
         else:
             f += ["q_end", "t_end"]
-            if p.start_pos in (WITH_START, WITH_TB) and not (p.algo == SEMI_GLOBAL and p.start_pos == WITH_TB):
-                f += ["q_start", "t_start"]
+            if p.start_pos in (WITH_START, WITH_TB) and not (p.algo == SEMI_GLOBAL and p.start_pos == WITH_TB
+                                                             and p.tail != TARGET):
+                f += ["q_start", "t_start"]  # target-tail SEMI_GLOBAL WITH_TB: an extension
             if p.second_best and p.algo in (LOCAL, SEMI_GLOBAL):
                 f += ["score2", "q_end2", "t_end2"]
         return f
 
     def as_dict(self, p: Params, batch: Optional[Batch] = None) -> dict:
         d = {k: getattr(self, k).copy() for k in self.fields_for(p)}
-        if p.start_pos == WITH_TB and p.algo in (LOCAL, GLOBAL):
+        if has_cigar(p):
             d["n_cigar"] = self.n_cigar.copy()
             d["cigar"] = self.cigar.copy()
         return d

@@ -255,8 +255,9 @@ int gb_align(const gb_params_t *p, const gb_batch_t *b, gb_out_t *o)
         if (o->score && r->aln_score) memcpy(o->score, r->aln_score, n * 4);
         if (o->q_end && r->query_batch_end) memcpy(o->q_end, r->query_batch_end, n * 4);
         if (o->t_end && r->target_batch_end) memcpy(o->t_end, r->target_batch_end, n * 4);
-        const bool has_start = p->start_pos == WITH_START || (p->start_pos == WITH_TB && p->algo == LOCAL);
-        if (has_start && p->algo != GLOBAL && p->algo != KSW && p->algo != BANDED) {
+        const bool has_start = p->start_pos == WITH_START ||
+                               (p->start_pos == WITH_TB && (p->algo == LOCAL || (p->algo == SEMI_GLOBAL && p->tail == TARGET)));
+        if (has_start && p->algo != GLOBAL && p->algo != KSW && !(p->algo == BANDED && p->start_pos != WITH_START)) {
             if (o->q_start && r->query_batch_start) memcpy(o->q_start, r->query_batch_start, n * 4);
             if (o->t_start && r->target_batch_start) memcpy(o->t_start, r->target_batch_start, n * 4);
         }

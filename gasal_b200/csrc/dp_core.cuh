@@ -512,9 +512,26 @@ __device__ void semi_init_rows(int head, int q8, const Scores &sc, RowBuf rb)
  * row above, a chain of three dependent operations per row.  When o >= 0,
  * E_{k-1} - (o+e) <= E_{k-1} - e, so E_k = max(E_{k-1} - e, max(M, F)_{k-1} -
  * (o+e)) -- the same value with one operation per row on the chain (OPEN_NN). */
-template <bool SECOND, bool OPEN_NN, class SC, class QW, class TW>
+/* Direction nibble of SEMI_GLOBAL cell (r, c) for its traceback (an
+ * extension: the reference instantiates semi-global WITH_TB empty,
+ * semiglobal_kernel_template.h:227).  Bits 0-1: the source of H (0 diagonal
+ * with M >= its diagonal predecessor, 1 diagonal with a drop, 3 F, 2 E; ties
+ * in that order); bit 3: F(r,c) extends F(r,c-1) (F(r,c-1) - e >= H(r,c-1) -
+ * (o+e)); bit 2: E(r,c) extends E(r-1,c) the same way.  Unlike dir_nib, the
+ * gap bits describe the cell's own F and E: gaps open from H here. */
+__device__ __forceinline__ uint32_t semi_nib(int M, int diag, int H, int F, int Fin, int Hleft, int Ein, int Hup,
+                                             const Scores &sc)
+{
+    uint32_t d = (H == M) ? (M >= diag ? 0u : 1u) : (H == F ? 3u : 2u);
+    d |= (Fin - sc.e >= Hleft - sc.oe) ? 8u : 0u;
+    d |= (Ein - sc.e >= Hup - sc.oe) ? 4u : 0u;
+    return d;
+}
+
+template <bool SECOND, bool OPEN_NN, class SC, class QW, class TW, bool TB = false>
 __device__ void semi_sweep(QW qword, int qregs, int qlen, TW tword, int tregs, int tlen, const Scores &sc,
-                           int head, int tail, int T0, int stop_at, RowBuf rb, SC &scr, SemiAcc &a)
+                           int head, int tail, int T0, int stop_at, RowBuf rb, SC &scr, SemiAcc &a,
+                           uint4 *tb = nullptr)
 {
     const bool free_head_t = (head == TARGET_ || head == BOTH_);
     const bool free_tail_t = (tail == TARGET_ || tail == BOTH_);
@@ -534,6 +551,7 @@ __device__ void semi_sweep(QW qword, int qregs, int qlen, TW tword, int tregs, i
         }
         for (int j = 0; j < qregs && a.best < stop_at; j++) {
             const uint32_t qw = qword(j);
+            uint32_t dir[8];
 #pragma unroll
             for (int b = 0; b < 8; b++) {
                 const int c = (j << 3) + b;
@@ -554,15 +572,19 @@ __device__ void semi_sweep(QW qword, int qregs, int qlen, TW tword, int tregs, i
                         Hn[k] = max(mf, e);
                     }
                 } else {
+                    uint32_t dw = 0;
 #pragma unroll
                     for (int k = 0; k < 8; k++) {
+                        const int Fin = F[k], Ein = e;
                         F[k] = __viaddmax_s32(F[k], -sc.e, Hc[k] - sc.oe);
                         const int M = D[k] + scr.s(k);
                         e = __viaddmax_s32(e, -sc.e, up - sc.oe);
                         const int H = __vimax3_s32(M, F[k], e);
+                        if (TB) dw |= semi_nib(M, D[k], H, F[k], Fin, Hc[k], Ein, up, sc) << (28 - 4 * k);
                         Hn[k] = H;
                         up = H;
                     }
+                    if (TB) dir[b] = dw;
                 }
                 rb.st(c, pack_he(Hn[7], e));
                 D[0] = up0;
@@ -578,6 +600,11 @@ __device__ void semi_sweep(QW qword, int qregs, int qlen, TW tword, int tregs, i
                         if (SECOND && H > a.sec && H < a.best && row < tlen) a.sec = H, a.srow = row;
                     }
                 }
+            }
+            if (TB) {
+                uint4 *tp = tb + (size_t)T * (2 * qregs) + 2 * j;
+                tp[0] = make_uint4(dir[0], dir[1], dir[2], dir[3]);
+                tp[1] = make_uint4(dir[4], dir[5], dir[6], dir[7]);
             }
         }
     }
@@ -624,14 +651,20 @@ __device__ void semi_start(const uint32_t *q, int qregs, int qlen, const uint32_
     r.q_start = (qlen - 1) - b.bcol;
 }
 
-template <bool SECOND, bool START, class SC>
+template <bool SECOND, bool START, class SC, bool TB = false>
 __device__ void semi_global(const uint32_t *q, int qregs, int qlen, const uint32_t *t, int tregs, int tlen,
-                            const Scores &sc, int head, int tail, int mql, RowBuf rb, SC scr, Res &r)
+                            const Scores &sc, int head, int tail, int mql, RowBuf rb, SC scr, Res &r,
+                            uint4 *tb = nullptr)
 {
     const int q8 = qregs << 3;
     SemiAcc a = {NEG16, qlen, tlen, NEG16, qlen, tlen};
     semi_init_rows(head, q8, sc, rb);
-    if (sc.o >= 0)
+    auto qf = [&](int j) { return q[j]; };
+    auto tf = [&](int T) { return t[T]; };
+    if (TB) /* the traceback reads the H-open recurrence's own gap bits: no OPEN_NN form */
+        semi_sweep<SECOND, false, SC, decltype(qf), decltype(tf), true>(qf, qregs, qlen, tf, tregs, tlen, sc, head,
+                                                                        tail, 0, 0x7fffffff, rb, scr, a, tb);
+    else if (sc.o >= 0)
         semi_sweep<SECOND, true>([&](int j) { return q[j]; }, qregs, qlen, [&](int T) { return t[T]; }, tregs, tlen,
                                  sc, head, tail, 0, 0x7fffffff, rb, scr, a);
     else
@@ -693,6 +726,68 @@ __device__ void banded(const uint32_t *q, int qregs, const uint32_t *t, int treg
         }
     }
     r.score = best, r.q_end = bcol, r.t_end = brow;
+}
+
+/* BANDED start position, an extension: the reference's banded kernel reports
+ * ends only (src/kernels/banded.h:10-139).  Defined as the LOCAL start pass
+ * (local_start): the banded recurrence run backwards from the 8-base words
+ * holding the end cell over the reversed words, on the forward pass's band
+ * tiles (band T's words [max(0, T-k_other+1), min(kw+T, qregs)), clipped to
+ * the end word, visited in reverse), leaving after the column in which the
+ * score reaches the forward score.  The start is reported as the forward row
+ * and column of the cell where that maximum was first reached. */
+template <class SC>
+__device__ void banded_start(const uint32_t *q, int qregs, const uint32_t *t, int tregs, int kw, const Scores &sc,
+                             RowBuf rb, SC scr, Res &r)
+{
+    const int rend_reg = min((r.q_end >> 3) + 1, qregs);
+    const int gend_reg = min((r.t_end >> 3) + 1, tregs);
+    const int k_other = tregs - (qregs - kw);
+    const int fwd = r.score;
+    const int qn = rend_reg << 3;
+    int best = 0, xs = 0, ys = 0;
+    for (int c = 0; c < qn; c++) rb.st(c, 0u);
+    for (int T = 0; T < gend_reg && best < fwd; T++) {
+        const int Tf = gend_reg - 1 - T;       /* the forward band */
+        const int gidx = (Tf << 3) + 7;        /* forward row of the reversed band's first row */
+        scr.band(nib_rev(t[Tf]), sc, true);
+        int F[8], D[8], Hc[8];
+#pragma unroll
+        for (int k = 0; k < 8; k++) F[k] = 0, D[k] = 0, Hc[k] = 0;
+        const int j_lo = max(0, Tf - k_other + 1), j_hi = min(min(kw + Tf, qregs), rend_reg);
+        for (int j = rend_reg - j_hi; j < rend_reg - j_lo && best < fwd; j++) {
+            const uint32_t qw = nib_rev(q[rend_reg - 1 - j]);
+#pragma unroll
+            for (int b = 0; b < 8; b++) {
+                if (best >= fwd) break;
+                const int c = (j << 3) + b;
+                scr.column(code(qw, b));
+                const uint32_t v = rb.ld(c);
+                const int up0 = sext16(v);
+                int e = hi16(v), up = up0;
+                int Hn[8], key[8];
+#pragma unroll
+                for (int k = 0; k < 8; k++) {
+                    F[k] = __viaddmax_s32(F[k], -sc.e, Hc[k] - sc.oe);
+                    int H = __vimax3_s32_relu(D[k] + scr.s(k), F[k], 0);
+                    e = __viaddmax_s32(e, -sc.e, up - sc.oe);
+                    H = max(H, e);
+                    key[k] = key8(H, 7 - k);
+                    Hn[k] = H;
+                    up = H;
+                }
+                rb.st(c, pack_he(Hn[7], e));
+                D[0] = up0;
+#pragma unroll
+                for (int k = 1; k < 8; k++) D[k] = Hn[k - 1];
+#pragma unroll
+                for (int k = 0; k < 8; k++) Hc[k] = Hn[k];
+                const int ck = col_key(key);
+                if ((ck >> 3) > best) best = ck >> 3, ys = gidx - (7 - (ck & 7)), xs = qn - 1 - c;
+            }
+        }
+    }
+    r.q_start = xs, r.t_start = ys;
 }
 
 /* ============================= KSW ====================================== */

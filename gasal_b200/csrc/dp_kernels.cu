@@ -50,10 +50,15 @@ __device__ __forceinline__ void run_pair(const DpArgs &a, const uint32_t *q, int
         if (START == WITH_TB_) global_fwd<true>(q, qregs, qlen, t, tregs, tlen, a.sc, rb, tb, scr, r);
         else global_fwd2(q, qregs, qlen, t, tregs, tlen, a.sc, rb, scr, r);
     } else if (ALGO == SEMI_GLOBAL_) {
-        semi_global<SECOND, START == WITH_START_>(q, qregs, qlen, t, tregs, tlen, a.sc, a.head, a.tail, a.mql, rb,
-                                                 scr, r);
+        if (START == WITH_TB_ && tb) /* target-tail SEMI_GLOBAL with a traceback (an extension) */
+            semi_global<SECOND, false, SC, true>(q, qregs, qlen, t, tregs, tlen, a.sc, a.head, a.tail, a.mql, rb, scr,
+                                                 r, tb);
+        else
+            semi_global<SECOND, START == WITH_START_>(q, qregs, qlen, t, tregs, tlen, a.sc, a.head, a.tail, a.mql,
+                                                     rb, scr, r);
     } else if (ALGO == BANDED_) {
         banded(q, qregs, t, tregs, a.k_band >> 3, a.sc, rb, scr, r);
+        if (START == WITH_START_) banded_start(q, qregs, t, tregs, a.k_band >> 3, a.sc, rb, scr, r);
     }
 }
 
@@ -79,7 +84,7 @@ __device__ __forceinline__ void dp_one(const DpArgs &a, uint32_t w, RowBuf rb, c
         const uint32_t *t = a.pt + (a.t_off[i] >> 3);
         const int qregs = (qlen + 7) >> 3, tregs = (tlen + 7) >> 3;
         uint4 *tb = nullptr;
-        if (START == WITH_TB_ && (ALGO == LOCAL_ || ALGO == GLOBAL_)) {
+        if (START == WITH_TB_ && (ALGO == LOCAL_ || ALGO == GLOBAL_ || ALGO == SEMI_GLOBAL_)) {
             tb = a.tb + a.tb_off[i];
             /* two zero tile rows past the matrix: the GLOBAL traceback
              * starts one past the last cell */
@@ -105,7 +110,7 @@ __device__ __forceinline__ void dp_one(const DpArgs &a, uint32_t w, RowBuf rb, c
     if (ALGO != GLOBAL_) {
         if (a.q_end) a.q_end[i] = r.q_end;
         if (a.t_end) a.t_end[i] = r.t_end;
-        if ((ALGO == LOCAL_ || ALGO == SEMI_GLOBAL_) && START == WITH_START_) {
+        if ((ALGO == LOCAL_ || ALGO == SEMI_GLOBAL_ || ALGO == BANDED_) && START == WITH_START_) {
             if (a.q_start) a.q_start[i] = r.q_start;
             if (a.t_start) a.t_start[i] = r.t_start;
         }
@@ -222,10 +227,12 @@ cudaError_t launch_dp_scratch_grid(int algo, int start, bool second, const DpArg
         return GB_SG(GLOBAL_, WITHOUT_START_, false);
     case SEMI_GLOBAL_:
         if (start == START_ONLY_) return GB_SG(SEMI_GLOBAL_, START_ONLY_, false);
+        if (start == WITH_TB_) return second ? GB_SG(SEMI_GLOBAL_, WITH_TB_, true) : GB_SG(SEMI_GLOBAL_, WITH_TB_, false);
         if (start == WITH_START_)
             return second ? GB_SG(SEMI_GLOBAL_, WITH_START_, true) : GB_SG(SEMI_GLOBAL_, WITH_START_, false);
         return second ? GB_SG(SEMI_GLOBAL_, WITHOUT_START_, true) : GB_SG(SEMI_GLOBAL_, WITHOUT_START_, false);
     case BANDED_:
+        if (start == WITH_START_) return GB_SG(BANDED_, WITH_START_, false);
         return GB_SG(BANDED_, WITHOUT_START_, false);
     case KSW_:
         return GB_SG(KSW_, WITHOUT_START_, false);
@@ -252,10 +259,13 @@ cudaError_t launch_dp(int algo, int start, bool second, const DpArgs &a, int blo
         return launch_one<GLOBAL_, WITHOUT_START_, false>(a, block, s);
     case SEMI_GLOBAL_:
         if (start == START_ONLY_) return launch_one<SEMI_GLOBAL_, START_ONLY_, false>(a, block, s);
+        if (start == WITH_TB_)
+            return second ? launch_one<SEMI_GLOBAL_, WITH_TB_, true>(a, block, s) : launch_one<SEMI_GLOBAL_, WITH_TB_, false>(a, block, s);
         if (start == WITH_START_)
             return second ? launch_one<SEMI_GLOBAL_, WITH_START_, true>(a, block, s) : launch_one<SEMI_GLOBAL_, WITH_START_, false>(a, block, s);
         return second ? launch_one<SEMI_GLOBAL_, WITHOUT_START_, true>(a, block, s) : launch_one<SEMI_GLOBAL_, WITHOUT_START_, false>(a, block, s);
     case BANDED_:
+        if (start == WITH_START_) return launch_one<BANDED_, WITH_START_, false>(a, block, s);
         return launch_one<BANDED_, WITHOUT_START_, false>(a, block, s);
     case KSW_:
         return launch_one<KSW_, WITHOUT_START_, false>(a, block, s);

@@ -216,6 +216,9 @@ int plan_batch(const RunCfg &cfg, const DevBatch &b, const DevOut &o, Workspace 
 
     /* split: long LOCAL/GLOBAL (and target-tail SEMI_GLOBAL) pairs go warp-cooperative */
     bool wc_algo = cfg.algo == LOCAL_ || cfg.algo == GLOBAL_ || (cfg.algo == SEMI_GLOBAL_ && cfg.tail == TARGET_);
+    /* target-tail SEMI_GLOBAL WITH_TB (the extension) runs one pair per thread */
+    const bool semi_tb = cfg.algo == SEMI_GLOBAL_ && cfg.start == WITH_TB_ && cfg.tail == TARGET_;
+    if (semi_tb) wc_algo = false;
     if (wc_algo && cfg.start != WITHOUT_START_ && cfg.sc.match > 0) {
         /* start passes and tracebacks of pairs whose scores can leave the
          * 16-bit row buffer (match * min(qlen, tlen) >= 2^15) stay on the
@@ -388,8 +391,9 @@ int plan_batch(const RunCfg &cfg, const DevBatch &b, const DevOut &o, Workspace 
         }
     }
 
-    p.tb = cfg.start == WITH_TB_ && (cfg.algo == LOCAL_ || cfg.algo == GLOBAL_);
-    p.start = (cfg.algo == SEMI_GLOBAL_ && cfg.start == WITH_TB_) ? WITHOUT_START_ : cfg.start;
+    p.tb = cfg.start == WITH_TB_ && (cfg.algo == LOCAL_ || cfg.algo == GLOBAL_ || semi_tb);
+    /* SEMI_GLOBAL WITH_TB with another tail returns the reference's outputs: the forward pass alone */
+    p.start = (cfg.algo == SEMI_GLOBAL_ && cfg.start == WITH_TB_ && !semi_tb) ? WITHOUT_START_ : cfg.start;
     p.second = cfg.second && (cfg.algo == LOCAL_ || cfg.algo == SEMI_GLOBAL_);
     p.split_start = st.split_start && p.start == WITH_START_ && (cfg.algo == LOCAL_ || cfg.algo == SEMI_GLOBAL_) &&
                     b.n >= st.min_order_pairs && o.score && o.q_end && o.t_end;
@@ -682,7 +686,7 @@ static int enqueue_align(const RunCfg &cfg, const DevBatch &b, const DevOut &o, 
         t.q_start = ca.q_start, t.t_start = ca.t_start;
         t.cigar = o.cigar, t.cigar_bytes = b.q_bytes;
         t.n_cigar = o.n_cigar ? o.n_cigar + p0 : nullptr;
-        t.n = ca.n, t.algo = cfg.algo, t.sc = cfg.sc;
+        t.n = ca.n, t.algo = cfg.algo, t.sc = cfg.sc, t.head = cfg.head;
         timing_mark(K_TB, true, s);
         GB_CUDA(launch_traceback(t, s));
         timing_mark(K_TB, false, s);

@@ -80,6 +80,7 @@ struct TbArgs {
     int32_t n;
     int32_t algo;
     Scores sc;
+    int32_t head;                       /* SEMI_GLOBAL: which leading bases are free */
 };
 
 /* ---- launchers (stream-ordered, no allocation) ---- */

@@ -12,10 +12,91 @@
  * cell, as the reference does -- and flushes leftover target / query bases as
  * 63-long runs.  The state machine (normal mode reads the 2 direction bits,
  * gap mode reads the extend bit of the gap's kind) is the reference's.
+ * Target-tail SEMI_GLOBAL (an extension) has its own walk, semi_walk.
  */
 #include "gb_internal.h"
 
 namespace gb {
+
+/* Run-length CIGAR writer: runs of one operation up to 63 long, last
+ * operation first, bytes past `room` counted but not written. */
+struct CigarOut {
+    uint8_t *out;
+    uint32_t room, n = 0, op = 0;
+    int count = 0;
+    __device__ __forceinline__ void put(uint32_t o)
+    {
+        if (count > 0 && count < 63 && o == op) {
+            count++;
+            return;
+        }
+        flush();
+        op = o, count = 1;
+    }
+    __device__ __forceinline__ void flush()
+    {
+        if (count > 0) {
+            if (n < room) out[n] = (uint8_t)(op | ((uint32_t)count << 2));
+            n++;
+        }
+        count = 0;
+    }
+};
+
+/* SEMI_GLOBAL traceback, an extension (the reference instantiates semi-global
+ * WITH_TB empty, semiglobal_kernel_template.h:227), for a free target tail:
+ * from the end cell (t_end, qlen - 1), an affine state machine over the
+ * nibbles of semi_nib -- in H the two low bits give the move (diagonal, or
+ * enter E / F at the same cell), in E (deletion) and F (insertion) the
+ * cell's own extend bit says whether the gap continues or was opened from H
+ * of the cell it came from.  At a free leading edge (target for head TARGET
+ * or BOTH, query for QUERY or BOTH) the walk stops; at a closed one the
+ * remaining bases become one gap.  Starts: the first aligned target row and
+ * query column. */
+__device__ uint32_t semi_walk(const uint4 *tb, int q8, int i, int j, int head, uint8_t *out, uint32_t room,
+                              int *si, int *sj)
+{
+    CigarOut c{out, room};
+    int state = 0; /* 0 H, 2 E (deletion), 3 F (insertion) */
+    while (i >= 0 && j >= 0) {
+        const int cell = (((i >> 3) * q8) << 3) + (j << 3) + (i & 7);
+        const uint4 tile = tb[cell >> 5];
+        const int in_tile = cell & 31, reg = in_tile >> 3;
+        const uint32_t word = reg == 0 ? tile.x : (reg == 1 ? tile.y : (reg == 2 ? tile.z : tile.w));
+        const uint32_t nib = (word >> (28 - ((in_tile & 7) << 2))) & 15u;
+        if (state == 0) {
+            const uint32_t src = nib & 3u;
+            if (src <= 1) {
+                c.put(src);
+                i--, j--;
+                continue;
+            }
+            state = (int)src;
+        }
+        if (state == 2) {
+            c.put(2);
+            state = (nib & 4u) ? 2 : 0;
+            i--;
+        } else {
+            c.put(3);
+            state = (nib & 8u) ? 3 : 0;
+            j--;
+        }
+    }
+    const bool free_t = head == TARGET_ || head == BOTH_, free_q = head == QUERY_ || head == BOTH_;
+    int ts = i + 1, qs = j + 1;
+    if (j < 0 && i >= 0 && !free_t) {
+        for (; i >= 0; i--) c.put(2);
+        ts = 0;
+    }
+    if (i < 0 && j >= 0 && !free_q) {
+        for (; j >= 0; j--) c.put(3);
+        qs = 0;
+    }
+    c.flush();
+    *si = ts, *sj = qs;
+    return c.n;
+}
 
 __global__ void __launch_bounds__(128) traceback_kernel(TbArgs a)
 {
@@ -23,6 +104,18 @@ __global__ void __launch_bounds__(128) traceback_kernel(TbArgs a)
     if (p >= a.n) return;
     const int qlen = (int)a.q_len[p], tlen = (int)a.t_len[p];
     uint32_t n_ops = 0;
+    if (a.algo == SEMI_GLOBAL_) {
+        int si = 0, sj = 0;
+        if (qlen > 0 && tlen > 0) {
+            const uint32_t room = a.q_off[p] < a.cigar_bytes ? a.cigar_bytes - a.q_off[p] : 0u;
+            n_ops = semi_walk(a.tb + a.tb_off[p], ((qlen + 7) >> 3) << 3, a.t_end[p], qlen - 1, a.head,
+                              a.cigar + a.q_off[p], room, &si, &sj);
+        }
+        if (a.t_start) a.t_start[p] = si;
+        if (a.q_start) a.q_start[p] = sj;
+        if (a.n_cigar) a.n_cigar[p] = n_ops;
+        return;
+    }
     if (qlen > 0 && tlen > 0) {
         const uint4 *tb = a.tb + a.tb_off[p];
         const int q8 = ((qlen + 7) >> 3) << 3;

@@ -312,9 +312,25 @@ static void semi_init_rows(int head, int n, int *Hb, int *Eb, const sc_t *s)
  * H(R,-1) = -(o+e*R) and diagonal 0 for R = 0 else -(o+e*R), R counting rows
  * from the start of this sweep.  The free-target-tail maximum is taken over
  * the last real query column, real rows only (:160-178). */
+/* Direction nibble of a SEMI_GLOBAL cell for the traceback extension (the
+ * reference instantiates semi-global WITH_TB empty,
+ * semiglobal_kernel_template.h:227): bits 0-1 the source of H (0 diagonal
+ * with M >= its diagonal predecessor, 1 diagonal with a drop, 3 F, 2 E; ties
+ * in that order); bit 3 set when F(r,c) extends F(r,c-1)
+ * (F(r,c-1) - e >= H(r,c-1) - (o+e)); bit 2 the same for E(r,c) from the row
+ * above.  The gap bits describe the cell's own F and E (gaps open from H). */
+static inline uint32_t semi_nibble(int M, int diag, int H, int F, int Fin, int Hleft, int Ein, int Hup,
+                                   const sc_t *s)
+{
+    uint32_t d = (H == M) ? (M >= diag ? 0u : 1u) : (H == F ? 3u : 2u);
+    if (Fin - s->e >= Hleft - s->oe) d |= 8u;
+    if (Ein - s->e >= Hup - s->oe) d |= 4u;
+    return d;
+}
+
 static void semi_sweep(const uint8_t *qc, int qregs, int qlen, const uint8_t *tc, int tregs, int tlen,
                        const sc_t *s, int head, int tail, int second, int T0, int stop_at, int *Hb, int *Eb,
-                       semi_acc_t *a)
+                       semi_acc_t *a, tile_t *tb)
 {
     const int free_head_t = (head == SRC_TARGET || head == SRC_BOTH);
     const int free_tail_t = (tail == SRC_TARGET || tail == SRC_BOTH);
@@ -337,10 +353,12 @@ static void semi_sweep(const uint8_t *qc, int qregs, int qlen, const uint8_t *tc
                 const int up0 = Hb[c];
                 int e = Eb[c], up = up0;
                 for (int k = 0; k < 8; k++) {
+                    const int Fin = F[k], Ein = e;
                     F[k] = imax(Hc[k] - s->oe, F[k] - s->e);
                     const int M = D[k] + sub_local(rb, g[k], s);
                     e = imax(up - s->oe, e - s->e);
                     const int H = imax(imax(M, F[k]), e);
+                    if (tb) tb_put(tb, qregs, T, c, k, semi_nibble(M, D[k], H, F[k], Fin, Hc[k], Ein, up, s));
                     Hn[k] = H;
                     up = H;
                 }
@@ -377,13 +395,13 @@ static void semi_tail_query(int qlen, int tlen, int mql, const int *Hb, int seco
 
 static void semi_global(const uint8_t *qc, int qregs, int qlen, const uint8_t *tc, int tregs, int tlen,
                         const sc_t *s, int head, int tail, int second, int with_start, int nrow,
-                        uint8_t *rq, uint8_t *rt, int *Hb, int *Eb, res_t *r)
+                        uint8_t *rq, uint8_t *rt, int *Hb, int *Eb, res_t *r, tile_t *tb)
 {
     /* end positions start as (row = query length, column = target length),
      * :63-64,73-74 */
     semi_acc_t a = {NEG16, qlen, tlen, NEG16, qlen, tlen};
     semi_init_rows(head, nrow, Hb, Eb, s);
-    semi_sweep(qc, qregs, qlen, tc, tregs, tlen, s, head, tail, second, 0, 0x7fffffff, Hb, Eb, &a);
+    semi_sweep(qc, qregs, qlen, tc, tregs, tlen, s, head, tail, second, 0, 0x7fffffff, Hb, Eb, &a, tb);
     if (tail == SRC_QUERY || tail == SRC_BOTH) semi_tail_query(qlen, tlen, s->mql, Hb, second, &a);
     r->score = a.best, r->t_end = a.brow, r->q_end = a.bcol;
     if (second) r->score2 = a.sec, r->t_end2 = a.srow, r->q_end2 = a.scol;
@@ -400,7 +418,7 @@ static void semi_global(const uint8_t *qc, int qregs, int qlen, const uint8_t *t
     const int fwd = a.best;
     semi_acc_t b = {NEG16, 0, a.bcol, NEG16, 0, 0};
     semi_init_rows(head, nrow, Hb, Eb, s);
-    semi_sweep(rq, qregs, qlen, rt, tregs, tlen, s, head, tail, 0, gend_reg, fwd, Hb, Eb, &b);
+    semi_sweep(rq, qregs, qlen, rt, tregs, tlen, s, head, tail, 0, gend_reg, fwd, Hb, Eb, &b, NULL);
     if (tail == SRC_QUERY || tail == SRC_BOTH) {
         for (int m = 0; m < s->mql; m++) {
             if (Hb[m] > b.best && m < qlen) b.bcol = m, b.best = Hb[m];
@@ -452,6 +470,55 @@ static void banded(const uint8_t *qc, int qregs, const uint8_t *tc, int tregs, i
         }
     }
     r->score = best, r->q_end = bcol, r->t_end = brow;
+}
+
+/* BANDED start position (an extension of this project: the reference's
+ * banded kernel reports ends only, src/kernels/banded.h:10-139).  Defined as
+ * the LOCAL start pass (local_start above): the banded recurrence run
+ * backwards from the 8-base words holding the end cell over the reversed
+ * padded sequences, on the forward pass's band tiles (forward band T's words
+ * clipped to the end word, visited in reverse), stopping after the column in
+ * which the score reaches the forward score.  The start is the forward row
+ * and column of the cell where that maximum was first reached. */
+static void banded_start(const uint8_t *qc, int qregs, const uint8_t *tc, int tregs, int kw, const sc_t *s,
+                         int *Hb, int *Eb, res_t *r)
+{
+    const int rend_reg = imin((r->q_end >> 3) + 1, qregs);
+    const int gend_reg = imin((r->t_end >> 3) + 1, tregs);
+    const int k_other = tregs - (qregs - kw);
+    const int fwd = r->score;
+    const int qn = 8 * rend_reg;
+    int best = 0, prev = 0, xs = 0, ys = 0;
+    for (int c = 0; c < qn; c++) Hb[c] = 0, Eb[c] = 0;
+    for (int T = 0; T < gend_reg && best < fwd; T++) {
+        const int Tf = gend_reg - 1 - T;   /* forward band */
+        const int gidx = 8 * Tf + 7;       /* forward row of the reversed band's first row */
+        int F[8] = {0}, D[8] = {0}, Hc[8] = {0}, Hn[8];
+        const int j_lo = imax(0, Tf - k_other + 1), j_hi = imin(imin(kw + Tf, qregs), rend_reg);
+        for (int c = 8 * (rend_reg - j_hi); c < 8 * (rend_reg - j_lo) && best < fwd; c++) {
+            const int qpos = qn - 1 - c;
+            const int rb = qc[qpos];
+            const int up0 = Hb[c];
+            int e = Eb[c], up = up0;
+            for (int k = 0; k < 8; k++) {
+                F[k] = imax(Hc[k] - s->oe, F[k] - s->e);
+                int H = imax(imax(D[k] + sub_local(rb, tc[gidx - k], s), F[k]), 0);
+                e = imax(up - s->oe, e - s->e);
+                H = imax(H, e);
+                if (best < H) best = H, ys = gidx - k;
+                Hn[k] = H;
+                up = H;
+            }
+            Hb[c] = row16(Hn[7], s);
+            Eb[c] = row16(e, s);
+            D[0] = up0;
+            for (int k = 1; k < 8; k++) D[k] = Hn[k - 1];
+            for (int k = 0; k < 8; k++) Hc[k] = Hn[k];
+            if (prev < best) xs = qpos;
+            prev = imax(best, prev);
+        }
+    }
+    r->q_start = xs, r->t_start = ys;
 }
 
 /* ------------------------------------------------------------------------ */
@@ -597,6 +664,70 @@ static uint32_t traceback(const tile_t *tb, int qregs, int algo, int i, int j, i
     return n_ops;
 }
 
+/* SEMI_GLOBAL traceback for a free target tail (the extension above): from
+ * the end cell (t_end, qlen - 1), in H the nibble's two low bits give a
+ * diagonal move or the gap (E / F) H came from at the same cell; in a gap the
+ * cell's own extend bit says whether the gap continues or was opened from H
+ * of the cell the move reaches.  At a free leading edge (target for head
+ * TARGET or BOTH, query for QUERY or BOTH) the walk stops; at a closed one
+ * the remaining bases become one gap.  Runs as in traceback(), at most 63
+ * long, last operation first.  si / sj: the first aligned target row and
+ * query column. */
+static uint32_t semi_traceback(const tile_t *tb, int qregs, int head, int i, int j, uint8_t *out, int *si,
+                               int *sj)
+{
+    const int q8 = 8 * qregs;
+    uint32_t n_ops = 0, run_op = 0;
+    int run = 0, state = 0; /* 0 H, 2 E (deletion), 3 F (insertion) */
+#define SEMI_PUT(o)                                                                                                \
+    do {                                                                                                           \
+        if (run > 0 && run < 63 && (uint32_t)(o) == run_op) {                                                      \
+            run++;                                                                                                 \
+        } else {                                                                                                   \
+            if (run > 0) out[n_ops++] = (uint8_t)(run_op | ((uint32_t)run << 2));                                  \
+            run_op = (uint32_t)(o), run = 1;                                                                       \
+        }                                                                                                          \
+    } while (0)
+    while (i >= 0 && j >= 0) {
+        const int cell = (((i >> 3) * q8) << 3) + (j << 3) + (i & 7);
+        const tile_t *t = &tb[cell >> 5];
+        const int in_tile = cell & 31;
+        const uint32_t nib = (t->w[in_tile >> 3] >> (28 - ((in_tile & 7) << 2))) & 15u;
+        if (state == 0) {
+            const uint32_t src = nib & 3u;
+            if (src <= 1) {
+                SEMI_PUT(src);
+                i--, j--;
+                continue;
+            }
+            state = (int)src;
+        }
+        if (state == 2) {
+            SEMI_PUT(2);
+            state = (nib & 4u) ? 2 : 0;
+            i--;
+        } else {
+            SEMI_PUT(3);
+            state = (nib & 8u) ? 3 : 0;
+            j--;
+        }
+    }
+    const int free_t = head == SRC_TARGET || head == SRC_BOTH, free_q = head == SRC_QUERY || head == SRC_BOTH;
+    int ts = i + 1, qs = j + 1;
+    if (j < 0 && i >= 0 && !free_t) {
+        for (; i >= 0; i--) SEMI_PUT(2);
+        ts = 0;
+    }
+    if (i < 0 && j >= 0 && !free_q) {
+        for (; j >= 0; j--) SEMI_PUT(3);
+        qs = 0;
+    }
+    if (run > 0) out[n_ops++] = (uint8_t)(run_op | ((uint32_t)run << 2));
+#undef SEMI_PUT
+    *si = ts, *sj = qs;
+    return n_ops;
+}
+
 /* ------------------------------------------------------------------------ */
 static void unpack_codes(const uint32_t *words, uint32_t word_off, int n, uint8_t *codes)
 {
@@ -640,7 +771,8 @@ int oracle_align_ex(const gb_params_t *p, const gb_batch_t *b, gb_out_t *o, int 
     }
     const int maxq8 = (int)((maxq + 7) & ~7u) + 8, maxt8 = (int)((maxt + 7) & ~7u) + 8;
     const int nrow = imax(maxq8, s.mql);
-    const int with_tb = (p->start_pos == S_WITH_TB) && (algo == A_LOCAL || algo == A_GLOBAL);
+    const int with_tb = (p->start_pos == S_WITH_TB) &&
+                        (algo == A_LOCAL || algo == A_GLOBAL || (algo == A_SEMI_GLOBAL && p->tail == SRC_TARGET));
     uint8_t **ops = with_tb ? (uint8_t **)calloc(n, sizeof(uint8_t *)) : NULL;
     uint32_t *nops = with_tb ? (uint32_t *)calloc(n, 4) : NULL;
     int err = 0;
@@ -680,10 +812,11 @@ int oracle_align_ex(const gb_params_t *p, const gb_batch_t *b, gb_out_t *o, int 
                         break;
                     case A_SEMI_GLOBAL:
                         semi_global(qc, qregs, qlen, tc, tregs, tlen, &s, p->head, p->tail, sb,
-                                    p->start_pos == S_WITH_START, nrow, rq, rt, Hb, Eb, &r);
+                                    p->start_pos == S_WITH_START, nrow, rq, rt, Hb, Eb, &r, tb);
                         break;
                     case A_BANDED:
                         banded(qc, qregs, tc, tregs, p->k_band >> 3, &s, Hb, Eb, &r);
+                        if (p->start_pos == S_WITH_START) banded_start(qc, qregs, tc, tregs, p->k_band >> 3, &s, Hb, Eb, &r);
                         break;
                     case A_KSW:
                         ksw(qc, qlen, tc, tlen, b->seed ? b->seed[i] : 0u, p->zdrop, &s, eh, &r);
@@ -694,9 +827,11 @@ int oracle_align_ex(const gb_params_t *p, const gb_batch_t *b, gb_out_t *o, int 
                         int si, sj;
                         if (algo == A_LOCAL)
                             nops[i] = traceback(tb, qregs, algo, r.t_end, r.q_end, r.score, &s, buf, &si, &sj);
+                        else if (algo == A_SEMI_GLOBAL)
+                            nops[i] = semi_traceback(tb, qregs, p->head, r.t_end, qlen - 1, buf, &si, &sj);
                         else
                             nops[i] = traceback(tb, qregs, algo, tlen, qlen, 0, &s, buf, &si, &sj);
-                        if (algo == A_LOCAL) r.t_start = si, r.q_start = sj;
+                        if (algo == A_LOCAL || algo == A_SEMI_GLOBAL) r.t_start = si, r.q_start = sj;
                         ops[i] = buf;
                         free(tb);
                     }
@@ -705,7 +840,7 @@ int oracle_align_ex(const gb_params_t *p, const gb_batch_t *b, gb_out_t *o, int 
                 if (algo != A_GLOBAL) {
                     if (o->q_end) o->q_end[i] = r.q_end;
                     if (o->t_end) o->t_end[i] = r.t_end;
-                    if (p->start_pos == S_WITH_START || (with_tb && algo == A_LOCAL)) {
+                    if (p->start_pos == S_WITH_START || (with_tb && algo != A_GLOBAL)) {
                         if (o->q_start) o->q_start[i] = r.q_start;
                         if (o->t_start) o->t_start[i] = r.t_start;
                     }

@@ -29,6 +29,8 @@ def _parts():
         (Params(algo=BANDED, k_band=32), W.workload0(800, seed=44)),
         (Params(algo=LOCAL, start_pos=WITH_TB, match=2, mismatch=3, gap_open=5, gap_extend=2),
          W.workload0(900, seed=45)),
+        (Params(algo=BANDED, k_band=24, start_pos=WITH_START), W.workload0(500, seed=46)),
+        (Params(algo=SEMI_GLOBAL, start_pos=WITH_TB, head=TARGET, tail=TARGET), w1[2][1]),
     ]
 
 

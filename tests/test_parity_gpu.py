@@ -7,7 +7,7 @@ import pytest
 
 from gasal_b200 import lib as gl
 from gasal_b200 import workloads as W
-from gasal_b200.capi import (Params, LOCAL, GLOBAL, SEMI_GLOBAL, BANDED, KSW, WITHOUT_START, WITH_START,
+from gasal_b200.capi import (Batch, Params, LOCAL, GLOBAL, SEMI_GLOBAL, BANDED, KSW, WITHOUT_START, WITH_START,
                              WITH_TB, NONE, QUERY, TARGET, BOTH)
 from golden_cases import cases, case_ids
 from oracle.bindings import oracle_align, ORC_ALL
@@ -122,6 +122,48 @@ def test_banded():
     b = W.workload0(1000, seed=10)
     for k in (8, 24, 64):
         _vs_oracle(Params(algo=BANDED, k_band=k), b)
+
+
+@pytest.mark.parametrize("head", [NONE, QUERY, TARGET, BOTH])
+def test_semi_global_traceback(head):
+    """Target-tail SEMI_GLOBAL WITH_TB, an extension (the reference
+    instantiates it empty): forward tiles on the one-pair-per-thread kernel,
+    the semi-global walk in the traceback kernel; CIGAR bytes, counts and
+    starts against the oracle, with second best and in several tile chunks."""
+    b = W.workload1(3000, seed=14)[2][1]
+    _vs_oracle(Params(algo=SEMI_GLOBAL, start_pos=WITH_TB, head=head, tail=TARGET), b)
+    gl.set_tb_budget_mb(4)
+    try:
+        _vs_oracle(Params(algo=SEMI_GLOBAL, start_pos=WITH_TB, head=head, tail=TARGET, second_best=1, match=2,
+                          mismatch=3, gap_open=5, gap_extend=2), W.workload2(400, seed=15))
+    finally:
+        gl.set_tb_budget_mb(65536)
+    # other tails keep the reference's outputs (no CIGAR)
+    _vs_oracle(Params(algo=SEMI_GLOBAL, start_pos=WITH_TB, head=head, tail=QUERY), b)
+
+
+def test_banded_with_start():
+    """BANDED WITH_START, an extension (the reference's banded kernel reports
+    ends only): the start pass runs the banded recurrence backwards over the
+    forward band's tiles.  Against the oracle on seeded pairs (long ones on
+    global row buffers too) and on hand-made pairs whose starts are known."""
+    b = W.workload0(1500, seed=12)
+    for k in (8, 24, 64, 512):
+        _vs_oracle(Params(algo=BANDED, k_band=k, start_pos=WITH_START), b)
+    _vs_oracle(Params(algo=BANDED, k_band=64, start_pos=WITH_START, match=2, mismatch=3, gap_open=5, gap_extend=2),
+               W.workload3(64, seed=13))
+    rng = np.random.default_rng(12)
+    acgt = np.frombuffer(b"ACGT", np.uint8)
+
+    def rs(n):
+        return bytes(acgt[rng.integers(0, 4, n)])
+    q = rs(100)
+    pairs = [(q, q), (q, rs(40) + q + rs(30)), (q, q[:30] + rs(10) + q[30:])]
+    hb = Batch.from_seqs([x for x, _ in pairs], [y for _, y in pairs])
+    o = gl.align(Params(algo=BANDED, k_band=64, start_pos=WITH_START), hb)
+    assert o.score.tolist() == [100, 100, 84]
+    assert list(zip(o.q_start.tolist(), o.t_start.tolist())) == [(0, 0), (0, 40), (0, 0)]
+    assert list(zip(o.q_end.tolist(), o.t_end.tolist())) == [(99, 99), (99, 139), (99, 109)]
 
 
 def test_correct_reverse_mode():
