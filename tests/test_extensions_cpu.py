@@ -115,3 +115,22 @@ def test_semi_global_traceback_walks_the_alignment():
                 exact += 1
         if head in (TARGET, BOTH):
             assert exact > b.n // 2
+
+
+def test_ksw_zdrop_hand_case():
+    """ksw z-drop on a pair whose answers follow from ksw_extend's rules by
+    hand (match 1, mismatch 4, gap 6+1, h0 20).  q = t = ACGT x4, then one
+    mismatch (A against C), then GATTACA on both.  The diagonal reaches
+    mx = 36 at row/column 15; row 16's best cell is the mismatch, 32, on the
+    same diagonal (di = dj = 1), a drop of 4.  z-drop 1: 4 > 1, the
+    extension leaves the 8-row tile, which is the last one (rows 16-23), so
+    the result is (36, q_end 16, t_end 16).  z-drop 0 (off) or 5: the
+    diagonal recovers to 39 at the last cell, which is also the end-to-end
+    score (gscore 39 > mx - 5), giving (39, 24, 24)."""
+    from gasal_b200.capi import KSW
+    q = b"ACGT" * 4 + b"A" + b"GATTACA"
+    t = b"ACGT" * 4 + b"C" + b"GATTACA"
+    b = Batch.from_seqs([q], [t], seed=np.array([20], dtype=np.uint32))
+    for zdrop, exp in ((1, (36, 16, 16)), (0, (39, 24, 24)), (5, (39, 24, 24))):
+        r = oracle_align(Params(algo=KSW, zdrop=zdrop), b)
+        assert (int(r.score[0]), int(r.q_end[0]), int(r.t_end[0])) == exp, zdrop

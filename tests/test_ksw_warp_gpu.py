@@ -207,3 +207,17 @@ print(json.dumps({k: v.tolist() for k, v in o.items()}))
         assert r.returncode == 0, r.stderr[-2000:]
         outs.append(json.loads(r.stdout.strip().splitlines()[-1]))
     assert outs[0] == outs[1]
+
+
+def test_zdrop_hand_case_on_the_warp_kernel():
+    """The hand-derived z-drop case (tests/test_extensions_cpu.py): 16
+    matches, one mismatch, 7 matches, h0 20.  z-drop 1 stops at the mismatch
+    row's tile: (36, 16, 16); z-drop 0 or 5 runs to (39, 24, 24).  Replicated
+    so the batch runs on the warp-per-pair kernel and its lane groups."""
+    q = b"ACGT" * 4 + b"A" + b"GATTACA"
+    t = b"ACGT" * 4 + b"C" + b"GATTACA"
+    n = 4096
+    b = Batch.from_seqs([q] * n, [t] * n, seed=np.full(n, 20, dtype=np.uint32))
+    for zdrop, exp in ((1, (36, 16, 16)), (0, (39, 24, 24)), (5, (39, 24, 24))):
+        o = gl.align(Params(algo=KSW, zdrop=zdrop), b)
+        assert (o.score == exp[0]).all() and (o.q_end == exp[1]).all() and (o.t_end == exp[2]).all(), zdrop
