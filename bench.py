@@ -731,7 +731,11 @@ def main():
     # ---------------- the same step through the per-pair mixed dispatch ----------------
     mixed = None
     if len(parts) > 1 and args.mixed == "on":
+        # each leg starts from the library's per-stream buffers released: the traceback tile budget is
+        # at most half the free device memory, so tiles still held by an earlier leg would shrink it
+        gl.release_workspaces()
         mixed = mixed_leg(torch, gl, parts, dparts, dev, args, dist, job_pairs, value)
+        gl.release_workspaces()
 
     kpart = next((d for d in dparts if d.p.algo == KSW), None)
     if kpart is not None:
@@ -753,6 +757,7 @@ def main():
                                                     job_pairs)
 
     # ---------------- end to end through the storage API ----------------
+    gl.release_workspaces()
     e2e = e2e_leg(torch, gl, parts, args, dev, dist, job_pairs)
 
     # ---------------- the plain full-DP form on a stratified sample ----------------

@@ -214,26 +214,7 @@ void release_state(const gasal_gpu_storage_t *s)
         p = std::move(it->second);
         g_state.erase(it);
     }
-    gb::Workspace &w = p->ws;
-    if (w.tb) cudaFree(w.tb);
-    if (w.d_tb_off) cudaFree(w.d_tb_off);
-    if (w.h_tb_off) cudaFreeHost(w.h_tb_off);
-    if (w.scratch) cudaFree(w.scratch);
-    if (w.tb_off_free) cudaEventDestroy(w.tb_off_free);
-    if (w.order) cudaFree(w.order);
-    if (w.order2) cudaFree(w.order2);
-    if (w.wc_rows) cudaFree(w.wc_rows);
-    if (w.wc_defer) cudaFree(w.wc_defer);
-    if (w.aux) cudaStreamDestroy(w.aux);
-    if (w.queue) cudaFree(w.queue);
-    if (w.fork) cudaEventDestroy(w.fork);
-    if (w.join) cudaEventDestroy(w.join);
-    if (w.bins) cudaFree(w.bins);
-    if (w.fb) cudaFree(w.fb);
-    if (w.retry) cudaFree(w.retry);
-    if (w.feat) cudaFree(w.feat);
-    if (w.pred) cudaFree(w.pred);
-    if (w.bandw) cudaFree(w.bandw);
+    gb::release_workspace(p->ws);
     if (p->d_n_cigar) cudaFree(p->d_n_cigar);
     if (p->exec) cudaGraphExecDestroy(p->exec);
 }

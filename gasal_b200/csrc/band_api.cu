@@ -61,6 +61,19 @@ DevWs *band_ws(void *stream)
 }
 } // namespace
 
+namespace gb {
+/* the band entry points' per-stream workspaces (gb_release_workspaces) */
+void band_release_all()
+{
+    std::lock_guard<std::mutex> lk(g_mu);
+    for (auto &kv : g_ws) {
+        release_workspace(kv.second->ws);
+        delete kv.second;
+    }
+    g_ws.clear();
+}
+} // namespace gb
+
 extern "C" {
 
 int gb_band_param_count(void) { return gb::MLP_PARAMS; }

@@ -327,6 +327,22 @@ void dev_args(const gb_params_t *p, const gb_dev_batch_t *b, const gb_dev_out_t 
 }
 } // namespace
 
+extern "C" int gb_release_workspaces(void)
+{
+    if (cudaDeviceSynchronize() != cudaSuccess) return GB_ERR_CUDA;
+    {
+        std::lock_guard<std::mutex> lk(g_dev_mu);
+        for (auto &kv : g_dev_ws) {
+            gb::release_workspace(kv.second->ws);
+            delete kv.second;
+        }
+        g_dev_ws.clear();
+    }
+    gb::mix_release_all();
+    gb::band_release_all();
+    return cudaGetLastError() == cudaSuccess ? GB_OK : GB_ERR_CUDA;
+}
+
 extern "C" int gb_align_dev(const gb_params_t *p, const gb_dev_batch_t *b, const gb_dev_out_t *o, void *stream)
 {
     if (!p || !b || !o || b->n < 0) return GB_ERR_ARG;

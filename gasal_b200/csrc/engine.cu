@@ -138,6 +138,32 @@ Workspace::~Workspace()
      * context is current; nothing to do at static destruction time */
 }
 
+void release_workspace(Workspace &w)
+{
+    if (w.tb) cudaFree(w.tb);
+    if (w.d_tb_off) cudaFree(w.d_tb_off);
+    if (w.h_tb_off) cudaFreeHost(w.h_tb_off);
+    if (w.scratch) cudaFree(w.scratch);
+    if (w.tb_off_free) cudaEventDestroy(w.tb_off_free);
+    if (w.order) cudaFree(w.order);
+    if (w.order2) cudaFree(w.order2);
+    if (w.wc_rows) cudaFree(w.wc_rows);
+    if (w.wc_defer) cudaFree(w.wc_defer);
+    if (w.aux) cudaStreamDestroy(w.aux);
+    if (w.queue) cudaFree(w.queue);
+    if (w.fork) cudaEventDestroy(w.fork);
+    if (w.join) cudaEventDestroy(w.join);
+    if (w.bins) cudaFree(w.bins);
+    if (w.fb) cudaFree(w.fb);
+    if (w.retry) cudaFree(w.retry);
+    if (w.feat) cudaFree(w.feat);
+    if (w.pred) cudaFree(w.pred);
+    if (w.bandw) cudaFree(w.bandw);
+    const int dev = w.device;
+    w = Workspace();
+    w.device = dev;
+}
+
 /* Every device allocation of the engine's workspaces and of the storage API's
  * regrowth goes through here.  GASAL_B200_FAIL_ALLOC_AFTER=k (read once) makes
  * the allocation after the first k fail once, as an out-of-memory would, so

@@ -87,6 +87,14 @@ struct Workspace {
     ~Workspace();
 };
 
+/* Frees every buffer, stream and event of a workspace (no work of it may be
+ * in flight) and leaves it empty, ready to grow again. */
+void release_workspace(Workspace &w);
+/* the buffers gb_align_dev_mixed keeps per (device, stream) (mixed.cu) */
+void mix_release_all();
+/* the band entry points' per-stream workspaces (band_api.cu) */
+void band_release_all();
+
 /* The decisions and allocations for one batch (plan_batch), so that
  * enqueue_batch issues stream operations only -- capturable into a graph. */
 struct Plan {

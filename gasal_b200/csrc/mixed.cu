@@ -95,6 +95,22 @@ struct MixState {
 std::mutex g_mix_mu;
 std::unordered_map<unsigned long long, MixState *> g_mix;
 
+} // namespace
+
+/* every stream's mixed-dispatch buffers and kind workspaces (gb_release_workspaces) */
+void mix_release_all()
+{
+    std::lock_guard<std::mutex> lk(g_mix_mu);
+    for (auto &kv : g_mix) {
+        MixState *m = kv.second;
+        for (auto &w : m->ws) release_workspace(w);
+        delete m;
+    }
+    g_mix.clear();
+}
+
+namespace {
+
 MixState *mix_state(cudaStream_t s)
 {
     int dev = 0;

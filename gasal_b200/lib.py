@@ -97,6 +97,7 @@ SIGNATURES = {
     "gb_align_dev_mixed": (C.c_int, [C.POINTER(GbParams), C.c_int, C.c_void_p, C.POINTER(GbDevBatch),
                                      C.POINTER(GbDevOut), C.c_void_p]),
     "gb_mixed_check": (C.c_int, [C.POINTER(GbParams), C.c_int, C.c_void_p, C.c_int32, C.c_int, C.c_void_p]),
+    "gb_release_workspaces": (C.c_int, []),
     "gb_set_reference_reverse": (C.c_int, [C.c_int]),
     "gb_set_reference_max_query_len": (C.c_int, [C.c_int]),
     "gb_set_tb_budget_mb": (C.c_int, [C.c_int64]),
@@ -422,6 +423,13 @@ def align_dev(p: Params, dev: dict, h_q_len: np.ndarray, h_t_len: np.ndarray, st
 
 
 MIXED_MAX_KINDS = 8
+
+
+def release_workspaces():
+    """gb_release_workspaces: free the per-stream buffers the device-level
+    entry points keep between calls (waits for the device first)."""
+    _check(lib().gb_release_workspaces(), "gb_release_workspaces")
+
 
 
 def _kinds_c(kinds):

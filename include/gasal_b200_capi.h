@@ -206,6 +206,14 @@ int gb_revcomp_dev(uint32_t *pq, uint32_t *pt, const uint32_t *q_off, const uint
  * nothing, as gb_align_dev does. */
 int gb_align_dev_noalloc(const gb_params_t *p, const gb_dev_batch_t *b, const gb_dev_out_t *o, void *stream);
 
+/* Frees the device and pinned buffers that gb_align_dev, gb_align_dev_mixed,
+ * gb_autotune and the band entry points keep per (device, stream) between
+ * calls (traceback tiles, row buffers, orders, streams, events), after waiting
+ * for the current device to finish its work.  The next call grows them again.
+ * Storages keep theirs until gasal_destroy_streams.  No reference
+ * counterpart: GASAL2 allocates per storage only. */
+int gb_release_workspaces(void);
+
 /* Per-pair mixed-algorithm dispatch (an extension: GASAL2 takes one algorithm
  * per launch, Parameters::algo, reference src/gasal_align.cu:249 and
  * src/gasal_align.h:89-107).  Pair i of the device batch is aligned under

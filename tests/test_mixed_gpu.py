@@ -124,3 +124,27 @@ def test_mixed_kind_without_pairs_and_empty_batch():
     empty = dict(m)
     gl.align_dev_mixed(kinds, np.zeros(0, np.uint8), empty, np.zeros(0, np.uint32), np.zeros(0, np.uint32),
                        torch.cuda.current_stream().cuda_stream)
+
+
+def test_release_workspaces_between_calls():
+    """gb_release_workspaces frees the per-stream buffers of gb_align_dev and
+    the mixed dispatch; the next calls grow them again and give the same
+    results (a traceback kind included)."""
+    torch = pytest.importorskip("torch")
+    dev = torch.device("cuda", 0)
+    parts = _parts()[:2]  # LOCAL WITH_START (second best, RC) and GLOBAL WITH_TB
+    kinds, b, kind, idx = W.concat_parts(parts, shuffle_seed=8)
+    m, keep = _device(torch, b, dev)
+    stream = torch.cuda.current_stream().cuda_stream
+    runs = []
+    for _ in range(2):
+        gl.align_dev_mixed(kinds, kind, m, b.q_len, b.t_len, stream)
+        p, pb = parts[1]
+        pm, pkeep = _device(torch, pb, dev)
+        gl.align_dev(p, pm, pb.q_len, pb.t_len, stream)
+        torch.cuda.synchronize()
+        runs.append((_host(keep), _host(pkeep)))
+        gl.release_workspaces()
+    for f in FIELDS + ("n_cigar",):
+        assert np.array_equal(runs[0][0][f], runs[1][0][f]), f
+        assert np.array_equal(runs[0][1][f], runs[1][1][f]), f
