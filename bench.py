@@ -807,6 +807,7 @@ def main():
                                           "traceback_extra": 4},
                          "peak_source": "measured live: 2-input int32 add issue rate (gb_probe_int_peak)",
                          "imnmx_tops": peak["imnmx_tops"], "dpx_tops": peak["dpx_tops"],
+                         "dpx16x2_halfword_tops": peak["dpx16x2_halfword_tops"],
                          "align_span_ms_per_step": kt["span"][0] / args.steps},
             "prep_bandwidth": dict(prep, peak_gbs=hbm, peak_source=hbm_src),
             "kernel_ms_per_step": {k: v[0] / args.steps for k, v in kt.items()},

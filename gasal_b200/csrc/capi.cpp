@@ -542,6 +542,12 @@ extern "C" int gb_kernel_timing_read(double *ms, int64_t *launches)
     return gb::timing_read(ms, launches);
 }
 
+extern "C" int gb_probe_dpx16x2_peak(double *halfword_tops)
+{
+    if (!halfword_tops) return GB_ERR_ARG;
+    return gb::probe_dpx16x2_peak(halfword_tops) == 0 ? GB_OK : GB_ERR_CUDA;
+}
+
 extern "C" int gb_probe_int_peak(double *iadd_tops, double *imnmx_tops, double *dpx_tops)
 {
     if (!iadd_tops || !imnmx_tops || !dpx_tops) return GB_ERR_ARG;

@@ -176,6 +176,7 @@ void timing_mark(int kind, bool start, cudaStream_t s);
 int timing_read(double ms[K_KINDS], int64_t launches[K_KINDS]);
 bool timing_on();
 int probe_int_peak(double *iadd, double *imnmx, double *dpx);
+int probe_dpx16x2_peak(double *halfword_tops);
 
 } // namespace gb
 

@@ -7,6 +7,8 @@
  *   imnmx   32-bit max (the ALU class that max, select, compare and the DPX
  *           max / add-max instructions share)
  *   dpx     __viaddmax_s32, the fused add-then-max the cell update uses
+ *   dpx2    __viaddmax_s16x2, its int16x2 form (two halfword results per
+ *           instruction; reported per halfword)
  * Each thread runs 8 interleaved dependency chains so the pipes stay full;
  * the grid is 8 blocks of 256 threads per SM.
  */
@@ -27,6 +29,7 @@ __global__ void __launch_bounds__(256) probe_kernel(uint32_t *out, uint32_t s0, 
             if (OP == 0) acc[k] = a + b;
             if (OP == 1) acc[k] = (uint32_t)max((int)a, (int)b);
             if (OP == 2) acc[k] = (uint32_t)__viaddmax_s32((int)a, (int)b, (int)c);
+            if (OP == 3) acc[k] = __viaddmax_s16x2(a, b, c);
         }
     }
     uint32_t r = 0;
@@ -67,6 +70,19 @@ int probe_int_peak(double *iadd, double *imnmx, double *dpx)
     *iadd = run_probe<0>(d, s);
     *imnmx = run_probe<1>(d, s);
     *dpx = run_probe<2>(d, s);
+    const cudaError_t e = cudaStreamSynchronize(s);
+    cudaStreamDestroy(s);
+    cudaFree(d);
+    return e == cudaSuccess ? 0 : -2;
+}
+
+int probe_dpx16x2_peak(double *halfword_tops)
+{
+    uint32_t *d = nullptr;
+    if (cudaMalloc(&d, 256) != cudaSuccess) return -2;
+    cudaStream_t s;
+    cudaStreamCreate(&s);
+    *halfword_tops = 2.0 * run_probe<3>(d, s);
     const cudaError_t e = cudaStreamSynchronize(s);
     cudaStreamDestroy(s);
     cudaFree(d);

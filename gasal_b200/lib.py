@@ -130,6 +130,7 @@ SIGNATURES = {
     "gb_kernel_timing": (C.c_int, [C.c_int]),
     "gb_kernel_timing_read": (C.c_int, [C.POINTER(C.c_double), C.POINTER(C.c_int64)]),
     "gb_probe_int_peak": (C.c_int, [C.POINTER(C.c_double)] * 3),
+    "gb_probe_dpx16x2_peak": (C.c_int, [C.POINTER(C.c_double)]),
 }
 
 
@@ -225,7 +226,9 @@ def kernel_timing_read() -> dict:
 def probe_int_peak() -> dict:
     a, b, c = C.c_double(), C.c_double(), C.c_double()
     _check(lib().gb_probe_int_peak(C.byref(a), C.byref(b), C.byref(c)), "gb_probe_int_peak")
-    return {"iadd_tops": a.value, "imnmx_tops": b.value, "dpx_tops": c.value}
+    d = C.c_double()
+    _check(lib().gb_probe_dpx16x2_peak(C.byref(d)), "gb_probe_dpx16x2_peak")
+    return {"iadd_tops": a.value, "imnmx_tops": b.value, "dpx_tops": c.value, "dpx16x2_halfword_tops": d.value}
 
 
 def _dev_structs(dev: dict, h_q_len: np.ndarray, h_t_len: np.ndarray):

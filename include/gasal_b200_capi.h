@@ -372,6 +372,9 @@ int gb_ksw_band_align(const gb_params_t *p, const gb_dev_batch_t *b, const gb_de
 int gb_kernel_timing(int on);
 int gb_kernel_timing_read(double *ms, int64_t *launches);
 int gb_probe_int_peak(double *iadd_tops, double *imnmx_tops, double *dpx_tops);
+/* The int16x2 form of the add-then-max (__viaddmax_s16x2) timed the same way,
+ * in halfword results per second (two per instruction), tera. */
+int gb_probe_dpx16x2_peak(double *halfword_tops);
 
 #ifdef __cplusplus
 }
