@@ -231,35 +231,10 @@ extern "C" int gb_align_dev_mixed(const gb_params_t *kinds, int n_kinds, const u
     int32_t *outs[MIX_OUTS] = {o->score, o->q_end, o->t_end, o->q_start, o->t_start,
                                o->score2, o->q_end2, o->t_end2, (int32_t *)o->n_cigar};
 
-    /* every kind's plan first: the host decisions and allocations */
-    RunCfg cfg[GB_MIXED_MAX_KINDS];
-    DevBatch db[GB_MIXED_MAX_KINDS];
-    DevOut dout[GB_MIXED_MAX_KINDS];
-    Plan plan[GB_MIXED_MAX_KINDS];
-    for (int k = 0; k < n_kinds; k++) {
-        if (!counts[k]) continue;
-        mix_cfg(kinds[k], cfg[k]);
-        const uint32_t b0 = base[k];
-        DevBatch &x = db[k];
-        x = DevBatch{};
-        x.n = (int32_t)counts[k], x.q_bytes = b->q_bytes, x.t_bytes = b->t_bytes;
-        x.q = b->q, x.t = b->t, x.pq = b->pq, x.pt = b->pt;
-        x.q_off = s_q_off + b0, x.t_off = s_t_off + b0, x.q_len = s_q_len + b0, x.t_len = s_t_len + b0;
-        x.seed = b->seed ? s_seed + b0 : nullptr;
-        x.q_op = b->q_op ? s_q_op + b0 : nullptr;
-        x.t_op = b->t_op ? s_t_op + b0 : nullptr;
-        x.h_q_len = m.h_ql.data() + b0, x.h_t_len = m.h_tl.data() + b0;
-        DevOut &y = dout[k];
-        y = DevOut{};
-        auto sh = [&](int j) { return outs[j] ? sub[j] + b0 : nullptr; };
-        y.score = sh(0), y.q_end = sh(1), y.t_end = sh(2), y.q_start = sh(3), y.t_start = sh(4);
-        y.score2 = sh(5), y.q_end2 = sh(6), y.t_end2 = sh(7);
-        y.n_cigar = o->n_cigar ? (uint32_t *)sub[8] + b0 : nullptr;
-        y.cigar = o->cigar;
-        if ((rc = plan_batch(cfg[k], x, y, m.ws[k], plan[k], m.ks[k])) != GB_OK) return rc;
-    }
-
-    /* pack once, gather, fork the kinds, join, scatter */
+    /* pack once and gather on the caller's stream, then plan and enqueue the
+     * kinds one by one: a kind's planning may wait for its own buffers from
+     * the previous call (a traceback kind's tile offsets), and the kinds
+     * already enqueued keep the GPU busy meanwhile */
 #define GB_MIX_CUDA(call)                                                                                  \
     do {                                                                                                   \
         if ((call) != cudaSuccess) return GB_ERR_CUDA;                                                     \
@@ -284,9 +259,28 @@ extern "C" int gb_align_dev_mixed(const gb_params_t *kinds, int n_kinds, const u
     GB_MIX_CUDA(cudaEventRecord(m.fork, s));
     for (int k = 0; k < n_kinds; k++) {
         if (!counts[k]) continue;
+        RunCfg cfg;
+        mix_cfg(kinds[k], cfg);
+        const uint32_t b0 = base[k];
+        DevBatch x{};
+        x.n = (int32_t)counts[k], x.q_bytes = b->q_bytes, x.t_bytes = b->t_bytes;
+        x.q = b->q, x.t = b->t, x.pq = b->pq, x.pt = b->pt;
+        x.q_off = s_q_off + b0, x.t_off = s_t_off + b0, x.q_len = s_q_len + b0, x.t_len = s_t_len + b0;
+        x.seed = b->seed ? s_seed + b0 : nullptr;
+        x.q_op = b->q_op ? s_q_op + b0 : nullptr;
+        x.t_op = b->t_op ? s_t_op + b0 : nullptr;
+        x.h_q_len = m.h_ql.data() + b0, x.h_t_len = m.h_tl.data() + b0;
+        DevOut y{};
+        auto sh = [&](int j) { return outs[j] ? sub[j] + b0 : nullptr; };
+        y.score = sh(0), y.q_end = sh(1), y.t_end = sh(2), y.q_start = sh(3), y.t_start = sh(4);
+        y.score2 = sh(5), y.q_end2 = sh(6), y.t_end2 = sh(7);
+        y.n_cigar = o->n_cigar ? (uint32_t *)sub[8] + b0 : nullptr;
+        y.cigar = o->cigar;
+        Plan plan;
+        if ((rc = plan_batch(cfg, x, y, m.ws[k], plan, m.ks[k])) != GB_OK) return rc;
         GB_MIX_CUDA(cudaStreamWaitEvent(m.ks[k], m.fork, 0));
-        if ((rc = enqueue_batch(cfg[k], db[k], dout[k], m.ws[k], plan[k], m.ks[k])) != GB_OK) return rc;
-        if (plan[k].tb) GB_MIX_CUDA(cudaEventRecord(m.ws[k].tb_off_free, m.ks[k]));
+        if ((rc = enqueue_batch(cfg, x, y, m.ws[k], plan, m.ks[k])) != GB_OK) return rc;
+        if (plan.tb) GB_MIX_CUDA(cudaEventRecord(m.ws[k].tb_off_free, m.ks[k]));
         GB_MIX_CUDA(cudaEventRecord(m.join[k], m.ks[k]));
         GB_MIX_CUDA(cudaStreamWaitEvent(s, m.join[k], 0));
     }
