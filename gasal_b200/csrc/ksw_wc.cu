@@ -132,17 +132,19 @@ __device__ __forceinline__ void ksw_tile(const TileConst &c, int pos, TileState 
         tv[k] = __viaddmax_s32(Mp[k], -c.oe, 0);
         agg = k == 0 ? tv[0] : __viaddmax_s32(agg, -c.e_del, tv[k]);
     }
-    /* F entering each lane: max-plus scan over lanes, decay e per column */
+    /* F entering each lane: max-plus scan over lanes, decay e per column.
+     * A lane below the shift gets its own value back from the shuffle, and
+     * max(x, x - eK*d) = x (e >= 0), so every lane takes the fused step. */
     const int eK = c.e_del * CPL;
     int x = agg;
 #pragma unroll
     for (int d = 1; d < 32; d <<= 1) {
         const int y = __shfl_up_sync(FULL, x, d);
-        if (lane >= d) x = max(x, y - eK * d);
+        x = __viaddmax_s32(y, -eK * d, x);
     }
     const int ex = __shfl_up_sync(FULL, x, 1);
-    int f = lane == 0 ? ts.fcarry : max(ex, ts.fcarry - eK * lane);
-    ts.fcarry = __shfl_sync(FULL, max(x, ts.fcarry - eK * (lane + 1)), 31);
+    int f = lane == 0 ? ts.fcarry : __viaddmax_s32(ts.fcarry, -eK * lane, ex);
+    ts.fcarry = __shfl_sync(FULL, __viaddmax_s32(ts.fcarry, -eK * (lane + 1), x), 31);
     /* pass 2: H, E, F, row maximum key */
     int H[CPL];
     int lkey = -1; /* FULLT: this lane's best H * 8 + k (the last column on ties) */
@@ -568,13 +570,13 @@ __device__ __forceinline__ void grp_tile(const GrpConst &c, int pos, TileState &
     const int eK = c.e_del * 8;
     int x = agg;
 #pragma unroll
-    for (int d = 1; d < G; d <<= 1) {
+    for (int d = 1; d < G; d <<= 1) { /* as in ksw_tile: lanes below the shift keep their value */
         const int y = __shfl_up_sync(c.gmask, x, d, G);
-        if (gl >= d) x = max(x, y - eK * d);
+        x = __viaddmax_s32(y, -eK * d, x);
     }
     const int ex = __shfl_up_sync(c.gmask, x, 1, G);
-    int f = gl == 0 ? ts.fcarry : max(ex, ts.fcarry - eK * gl);
-    ts.fcarry = __shfl_sync(c.gmask, max(x, ts.fcarry - eK * (gl + 1)), G - 1, G);
+    int f = gl == 0 ? ts.fcarry : __viaddmax_s32(ts.fcarry, -eK * gl, ex);
+    ts.fcarry = __shfl_sync(c.gmask, __viaddmax_s32(ts.fcarry, -eK * (gl + 1), x), G - 1, G);
     int H[8];
     int lkey = -1;
 #pragma unroll
