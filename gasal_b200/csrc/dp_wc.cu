@@ -631,6 +631,30 @@ __device__ void wc_lastcol_scan(const int *lastcol, int r0, int r1, int row0, in
     }
 }
 
+/* The first list position of this warp's groups (G <= 32: 32/G of them) or
+ * of this block's two-warp group (G = 64) for the next pass of a kernel's
+ * pair loop: taken from the launch's zeroed work counter (a.queue), so a
+ * group that finishes early takes the next pair -- the order lists the
+ * longest pairs first -- or, without one, by grid stride. */
+template <int G> __device__ __forceinline__ int wc_next(const DpArgs &a, int gpb, int iter)
+{
+    if (a.queue) {
+        if constexpr (G > 32) {
+            __shared__ int next;
+            __syncthreads(); /* both warps are done with the previous pair */
+            if (threadIdx.x == 0) next = (int)atomicAdd(a.queue, 1u);
+            __syncthreads();
+            return next;
+        } else {
+            unsigned v = 0;
+            if ((threadIdx.x & 31) == 0) v = atomicAdd(a.queue, (unsigned)(32 / G));
+            return (int)__shfl_sync(0xFFFFFFFFu, v, 0);
+        }
+    }
+    if constexpr (G > 32) __syncthreads(); /* both warps are done with the previous pair */
+    return (int)(blockIdx.x + iter * gridDim.x) * gpb + (G > 32 ? 0 : (int)(threadIdx.x >> 5) * (32 / G));
+}
+
 template <int G, bool SECOND, bool START, bool FAST>
 __global__ void __launch_bounds__(128) dp_wc_semi_kernel(DpArgs a, const uint32_t *list, int nlist, int ring_cols)
 {
@@ -647,9 +671,11 @@ __global__ void __launch_bounds__(128) dp_wc_semi_kernel(DpArgs a, const uint32_
     const bool fast_scores = a.sc.match >= -128 && a.sc.match <= 127 && a.sc.mismatch >= -127 && a.sc.mismatch <= 128;
     const bool open_nn = a.sc.o >= 0;
     const int nl = a.n_dev ? min((int)*a.n_dev, nlist) : nlist;
-    for (int item0 = blockIdx.x * gpb; item0 < nl; item0 += gridDim.x * gpb) {
-        if constexpr (G > 32) __syncthreads(); /* both warps are done with the previous pair */
-        const int item = item0 + slot;
+    const int wslot = G > 32 ? 0 : (int)((threadIdx.x & 31) / G); /* this group's place in its warp */
+    for (int iter = 0;; iter++) {
+        const int item0 = wc_next<G>(a, gpb, iter);
+        if (item0 >= nl) break; /* the same for every lane of a warp (and of a two-warp group) */
+        const int item = item0 + wslot;
         const bool listed = item < nl; /* the last warp may have groups without a pair */
         const int i = listed ? (int)list[item] : 0;
         const int qlen0 = listed ? (int)a.q_len[i] : 0, tlen0 = listed ? (int)a.t_len[i] : 0;
@@ -753,9 +779,11 @@ __global__ void __launch_bounds__(128) dp_wc_kernel(DpArgs a, const uint32_t *li
     int *bandmax = (int *)(wc_smem + (size_t)gpb * ring_cols) + (size_t)slot * a.scratch_cols;
     const bool fast_scores = a.sc.match >= -128 && a.sc.match <= 127 && a.sc.mismatch >= -127 && a.sc.mismatch <= 128;
     const int nl = a.n_dev ? min((int)*a.n_dev, nlist) : nlist;
-    for (int item0 = blockIdx.x * gpb; item0 < nl; item0 += gridDim.x * gpb) {
-        if constexpr (G > 32) __syncthreads(); /* both warps are done with the previous pair */
-        const int item = item0 + slot;
+    const int wslot = G > 32 ? 0 : (int)((threadIdx.x & 31) / G); /* this group's place in its warp */
+    for (int iter = 0;; iter++) {
+        const int item0 = wc_next<G>(a, gpb, iter);
+        if (item0 >= nl) break; /* the same for every lane of a warp (and of a two-warp group) */
+        const int item = item0 + wslot;
         const bool listed = item < nl; /* the last warp may have groups without a pair */
         const int i = listed ? (int)list[item] : 0;
         const int qlen0 = listed ? (int)a.q_len[i] : 0, tlen0 = listed ? (int)a.t_len[i] : 0;
@@ -1035,11 +1063,17 @@ size_t wc_scratch_words(int algo, const WcLaunch &l, int max_t8)
 
 cudaError_t launch_dp_wc(int algo, int start, bool second, const DpArgs &a, const uint32_t *list, int nlist,
                          int max_q8, int max_t8, const WcLaunch &l, int32_t *rows, uint32_t *defer, uint32_t *ndefer,
-                         cudaStream_t s)
+                         uint32_t *wq, cudaStream_t s)
 {
     if (nlist <= 0) return cudaSuccess;
     if (l.group == 0) return cudaErrorInvalidValue;
     DpArgs b = a;
+    /* the launches' own work counters (a.queue is the one-thread kernel's) */
+    b.queue = wq;
+    if (wq) {
+        const cudaError_t z = cudaMemsetAsync(wq, 0, 2 * sizeof(uint32_t), s);
+        if (z != cudaSuccess) return z;
+    }
     if (algo == SEMI_GLOBAL_) {
         b.scratch_cols = (uint32_t)(max_t8 + 8); /* last-column rows per group */
         b.lastcol = rows;
@@ -1066,6 +1100,7 @@ cudaError_t launch_dp_wc(int algo, int start, bool second, const DpArgs &a, cons
     if (e != cudaSuccess) return e;
     DpArgs c = b;
     c.defer = nullptr, c.ndefer = nullptr, c.n_dev = ndefer;
+    c.queue = wq ? wq + 1 : nullptr;
     int dev = 0, sms = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);

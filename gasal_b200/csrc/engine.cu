@@ -331,7 +331,7 @@ int plan_batch(const RunCfg &cfg, const DevBatch &b, const DevOut &o, Workspace 
     a.score2 = o.score2, a.q_end2 = o.q_end2, a.t_end2 = o.t_end2;
     a.max_off = cfg.algo == KSW_ ? o.max_off : nullptr;
     a.sc = cfg.sc, a.head = cfg.head, a.tail = cfg.tail, a.k_band = cfg.k_band, a.zdrop = cfg.zdrop, a.mql = cfg.mql;
-    if (!ws.queue && dev_malloc((void **)&ws.queue, 64) != cudaSuccess) {
+    if (!ws.queue && dev_malloc((void **)&ws.queue, 128) != cudaSuccess) {
         cudaGetLastError();
         return GB_ERR_ALLOC;
     }
@@ -564,13 +564,14 @@ static int launch_dp_split(int algo, int start, bool second, const Plan &p, DpAr
         GB_CUDA(cudaEventRecord(ws.fork, s));
         GB_CUDA(cudaStreamWaitEvent(ws.aux, ws.fork, 0));
         timing_mark(K_DP, true, ws.aux);
-        /* queue words 12 and 13: the two launches' counts of pairs left to compare scoring */
+        /* queue words 12 and 13: the two launches' counts of pairs left to
+         * compare scoring; 16-17 and 18-19: their work counters */
         if (nbig > 0)
             GB_CUDA(launch_dp_wc(algo, start, second, a, order, nbig, p.mq8_big, p.mt8_big, p.wc_big, ws.wc_rows,
-                                 ws.wc_defer, ws.queue + 12, ws.aux));
+                                 ws.wc_defer, ws.queue + 12, ws.queue + 16, ws.aux));
         if (nlong > nbig)
             GB_CUDA(launch_dp_wc(algo, start, second, a, order + nbig, nlong - nbig, p.mq8, p.mt8, p.wc, ws.wc_rows,
-                                 ws.wc_defer, ws.queue + 13, ws.aux));
+                                 ws.wc_defer, ws.queue + 13, ws.queue + 18, ws.aux));
         timing_mark(K_DP, false, ws.aux);
         GB_CUDA(cudaEventRecord(ws.join, ws.aux));
         DpArgs rest = a;

@@ -129,7 +129,7 @@ cudaError_t launch_start_order(const uint32_t *q_len, const int32_t *q_end, cons
  * beyond a byte) on the compare-scoring kernels after them. */
 cudaError_t launch_dp_wc(int algo, int start, bool second, const DpArgs &a, const uint32_t *list, int nlist,
                          int max_q8, int max_t8, const WcLaunch &l, int32_t *rows, uint32_t *defer, uint32_t *ndefer,
-                         cudaStream_t s);
+                         uint32_t *wq, cudaStream_t s);
 /* dynamic shared memory of one warp-cooperative block */
 size_t wc_smem_bytes(int algo, int group, int warps, int max_q8, int max_t8);
 /* launch shape for nlist pairs: the forced group, or (forced_group 0) the

@@ -24,9 +24,15 @@ static_assert((1u << ORDER_BITS) - 1 == ORDER_CAP_WORDS, "class cap of the lengt
 __device__ __forceinline__ uint32_t work_bin(uint32_t qlen, uint32_t tlen)
 {
     const uint32_t cap = (1u << ORDER_BITS) - 1;
-    const uint32_t qr = min((qlen + 7) >> 3, cap), tr = min((tlen + 7) >> 3, cap);
+    const uint32_t qw = (qlen + 7) >> 3, tw = (tlen + 7) >> 3;
+    /* queries of cap+ words form the order's prefix (bins 0..cap): sorted by
+     * the DP size qw * tw in classes of 4096 words^2, largest first, so the
+     * launches that pull them from a work counter start the longest ones
+     * first */
+    if (qw >= cap) return cap - min((uint32_t)(((uint64_t)qw * tw) >> 12), cap);
+    const uint32_t tr = min(tw, cap);
     /* descending work -> ascending bin */
-    return (uint32_t)(ORDER_BINS - 1) - ((qr << ORDER_BITS) | tr);
+    return (uint32_t)(ORDER_BINS - 1) - ((qw << ORDER_BITS) | tr);
 }
 
 /* start passes: (reverse-region query words, forward score / 2), descending */
