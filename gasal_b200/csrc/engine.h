@@ -143,7 +143,7 @@ struct Settings {
     Scores sc = {1, 4, 6, 1, 7};
     int ref_reverse = 1;
     int mql = 2048;
-    size_t tb_budget_bytes = (size_t)64 << 30; /* traceback tiles per stream (at most half the free memory) */
+    size_t tb_budget_bytes = (size_t)96 << 30; /* traceback tiles per stream (at most half the free memory) */
     int block = 32;             /* one-pair-per-thread block: 32 packs the most row buffers per SM */
     int min_order_pairs = 2048; /* batches at least this large visit pairs length-binned */
     int wc_min_qregs = 32;      /* pairs with at least this many query words go warp-cooperative */

@@ -252,7 +252,7 @@ int gb_cigar_text(const uint8_t *cigar, const uint32_t *q_off, const uint32_t *n
  *   reference's sm_100a build does; 0 reverses the real bases only.
  * reference_max_query_len: the reference build's MAX_QUERY_LEN, which bounds
  *   the semi-global last-row scan (default 2048).
- * tb_budget_mb: device memory for traceback tiles per stream (default 65536,
+ * tb_budget_mb: device memory for traceback tiles per stream (default 98304,
  *   and never more than half of the device memory free when a batch is
  *   planned); larger WITH_TB batches run in chunks. */
 int gb_set_reference_reverse(int on);

@@ -81,7 +81,7 @@ def test_graph_chunked_traceback_matches_no_graph():
             graphed = _run(st, 0, b)
             d = _delta(s0, gl.graph_stats())
     finally:
-        gl.set_tb_budget_mb(65536)
+        gl.set_tb_budget_mb(98304)
         gl.set_graphs(True)
     _same(plain, exp, "no graph")
     _same(graphed, exp, "graph")

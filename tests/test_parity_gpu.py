@@ -71,7 +71,7 @@ def test_workload2_traceback_chunked():
     try:
         _vs_oracle(Params(algo=GLOBAL, start_pos=WITH_TB), b)
     finally:
-        gl.set_tb_budget_mb(65536)
+        gl.set_tb_budget_mb(98304)
 
 
 def test_local_traceback_and_second_best():
@@ -137,7 +137,7 @@ def test_semi_global_traceback(head):
         _vs_oracle(Params(algo=SEMI_GLOBAL, start_pos=WITH_TB, head=head, tail=TARGET, second_best=1, match=2,
                           mismatch=3, gap_open=5, gap_extend=2), W.workload2(400, seed=15))
     finally:
-        gl.set_tb_budget_mb(65536)
+        gl.set_tb_budget_mb(98304)
     # other tails keep the reference's outputs (no CIGAR)
     _vs_oracle(Params(algo=SEMI_GLOBAL, start_pos=WITH_TB, head=head, tail=QUERY), b)
 

@@ -173,7 +173,7 @@ def test_long_prefix_runs_its_own_wc_launch():
         try:
             got = gl.align(p, b).as_dict(p)
         finally:
-            gl.set_tb_budget_mb(65536)
+            gl.set_tb_budget_mb(98304)
         exp = oracle_align(p, b).as_dict(p)
         for k, v in exp.items():
             assert np.array_equal(got[k], v), f"chunked {p.key()} {k}"
